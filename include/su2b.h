@@ -1,0 +1,212 @@
+/* su2b.h -- C ABI of libsu2b, the B200 (sm_100a) device path for the Monte-Carlo hot path
+ * of the su2 lattice gauge theory code.
+ *
+ * The su2 host driver (YAML input, gaugeconfig I/O, observables) keeps running on the CPU
+ * and calls these entry points instead of the OpenMP loops named beside each declaration
+ * (file:line in the su2 sources).  The gauge field lives on the device between calls; the
+ * host copy in gaugeconfig<G> is refreshed only where the driver needs it (save points,
+ * host-side observables) with su2b_download_gauge.
+ *
+ * Conventions
+ *   - Every call returns an int status (SU2B_OK == 0) and never aborts; the message of the
+ *     last error of a context is available from su2b_last_error().
+ *   - Host buffers belong to the caller and use the reference's host layout:
+ *       links   : gaugeconfig.hh:211-222, index ((((t*Lx+x)*Ly+y)*Lz+z)*ndims + mu);
+ *                 SU(2): 4 doubles {Re a, Im a, Re b, Im b} per link (su2.hh:11-70, the
+ *                 N_c member of _su2 is not part of the buffer); U(1): 1 double (angle).
+ *       adjoint : 3 doubles {a, b, c} (SU(2), adjointfield.hh:12-51) or 1 double (U(1))
+ *                 per link, same link order.
+ *       spinor  : 2 doubles {Re, Im} per site, site = ((t*Lx+x)*Ly+y)*Lz+z
+ *                 (staggered.hpp:52-69).
+ *   - A context owns its device memory and one CUDA stream; calls on one context are not
+ *     re-entrant, distinct contexts may be used from distinct host threads.
+ *   - All active extents must be even (even/odd device layout, checkerboard updates).
+ */
+#ifndef SU2B_H
+#define SU2B_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(SU2B_BUILD) && defined(__GNUC__)
+#define SU2B_API __attribute__((visibility("default")))
+#else
+#define SU2B_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------------------- */
+enum {
+  SU2B_OK = 0,
+  SU2B_ERR_INVALID = 1,         /* bad argument (NULL pointer, size, id) */
+  SU2B_ERR_CUDA = 2,            /* a CUDA runtime call or kernel launch failed */
+  SU2B_ERR_NOT_CONVERGED = 3,   /* Krylov solver hit max_iter or produced a NaN residual */
+  SU2B_ERR_UNSUPPORTED = 4,     /* valid request the reference also rejects (e.g. SU(2)
+                                   staggered fermions, staggered.hpp:343-350) */
+  SU2B_ERR_NOMEM = 5,           /* device allocation failed */
+  SU2B_ERR_TIMEOUT = 6          /* a bounded device-side wait gave up */
+};
+
+enum { SU2B_GROUP_SU2 = 0, SU2B_GROUP_U1 = 1 };
+
+/* SU2B_PREC_FP64: links, momenta, forces in FP64 (the plain path).
+ * SU2B_PREC_MIXED: SU(2) links, momenta and forces stored and computed in FP32; every
+ *   global reduction (plaquette, action, kinetic energy, Delta H), the accept/reject and
+ *   link reunitarisation in FP64.  For U(1) the links stay FP64 and MIXED selects FP32
+ *   inner iterations with FP64 reliable updates in the CG. */
+enum { SU2B_PREC_FP64 = 0, SU2B_PREC_MIXED = 1 };
+
+/* integrator ids as the reference enum (integrator.hh:15) */
+enum {
+  SU2B_LEAPFROG = 0,
+  SU2B_OMF4 = 2,
+  SU2B_EULER = 4,
+  SU2B_RUTH = 5,
+  SU2B_OMF2 = 6
+};
+
+typedef struct su2b_ctx su2b_ctx;
+
+/* ---- context ------------------------------------------------------------------------- */
+
+/* Creates a device-resident lattice.  Extents and ndims follow gaugeconfig(Lx, Ly, Lz, Lt,
+ * ndims, beta) (gaugeconfig.hh:49-63); for ndims < 4 pass Lz = 1 (and Ly = 1 for ndims = 2)
+ * as parse_input_file.cc:57-67 does.  xi != 1 selects the anisotropic action
+ * (flat-gaugemonomial.hh:196-202).  device = CUDA ordinal. */
+SU2B_API int su2b_ctx_create(int group, int Lx, int Ly, int Lz, int Lt, int ndims, double beta,
+                    double xi, int precision, int device, su2b_ctx **out);
+SU2B_API int su2b_ctx_destroy(su2b_ctx *ctx);
+SU2B_API const char *su2b_last_error(const su2b_ctx *ctx);
+/* the context's CUDA stream (a cudaStream_t), for callers that order their own work */
+SU2B_API int su2b_ctx_stream(su2b_ctx *ctx, void **stream);
+SU2B_API int su2b_set_beta(su2b_ctx *ctx, double beta);
+/* blocks until all work queued on the context's stream has finished */
+SU2B_API int su2b_synchronize(su2b_ctx *ctx);
+
+/* ---- gauge field transfer (gaugeconfig<G> <-> device) ------------------------------- */
+SU2B_API int su2b_upload_gauge(su2b_ctx *ctx, const double *U_host);
+SU2B_API int su2b_download_gauge(su2b_ctx *ctx, double *U_host);
+
+/* ---- reductions ---------------------------------------------------------------------- */
+
+/* flat_spacetime::gauge_energy(U, spatial_only) (flat-gauge_energy.hpp:109-137):
+ * sum_x sum_{mu<nu} ReTr P_{mu nu}(x). */
+SU2B_API int su2b_gauge_energy(su2b_ctx *ctx, int spatial_only, double *out);
+/* flat_spacetime::retr_sum_Wplaquettes(U, xi, anisotropic, spatial_only)
+ * (flat-gauge_energy.hpp:31-94), with the context's xi. */
+SU2B_API int su2b_retr_sum_plaquettes(su2b_ctx *ctx, int spatial_only, double *out);
+/* flat_spacetime::get_S_G_hmc (flat-gaugemonomial.hh:46-54): -beta/Nc * retr sum */
+SU2B_API int su2b_gauge_action(su2b_ctx *ctx, double *out);
+/* flat_spacetime::energy_density(U, E, Q, cloverdef, ss) (flat-energy_density.hh:57-164) */
+SU2B_API int su2b_energy_density(su2b_ctx *ctx, int cloverdef, int ss, double *E, double *Q);
+
+/* ---- gauge force and updates --------------------------------------------------------- */
+
+/* gaugemonomial::derivative(deriv, h, fac) (flat-gaugemonomial.hh:105-131) into a zeroed
+ * field: deriv(x,mu) = fac*beta/Nc * get_deriv(U(x,mu) * staples(x,mu)). */
+SU2B_API int su2b_gauge_force(su2b_ctx *ctx, double fac, double *deriv_host);
+/* gaugeconfig::restoreSU (gaugeconfig.hh:115-120) */
+SU2B_API int su2b_restore_su(su2b_ctx *ctx);
+/* update_gauge(h, dtau) (update_gauge.hh:8-16) with momenta given on the host */
+SU2B_API int su2b_update_gauge(su2b_ctx *ctx, const double *P_host, double dtau);
+
+/* ---- HMC trajectory (md_update, md_update.hh:18-81) ------------------------------------ */
+typedef struct {
+  int integrator;   /* SU2B_LEAPFROG, SU2B_OMF2, ... */
+  int n_steps;      /* md_params nsteps */
+  double tau;       /* md_params tau */
+  uint64_t seed;    /* key of the device random streams */
+  uint32_t traj;    /* trajectory index (counter of the device random streams) */
+  int revtest;      /* reversibility test (md_update.hh:62-74): fills ddH */
+  int accept_reject;/* 0: always accept (md_params acceptreject) */
+  /* optional host inputs for replaying a host random stream (all NULL/negative = device
+   * Philox streams): momenta in the adjoint host layout, and the accept uniform. */
+  const double *momenta_host;
+  double uniform_host;  /* used when >= 0 */
+  /* U(1) only: staggered det(D Ddag) monomial (detDDdag_monomial.hh).  Enabled when
+   * fermion_mass > 0. */
+  double fermion_mass;
+  double cg_tol;          /* absolute residual tolerance of the inner CG (CG.hpp:50) */
+  int cg_max_iter;
+  const double *pf_source_host; /* optional R (spinor host layout); NULL = Philox R */
+  int pf_complex;         /* 0: real R as the reference (staggered.hpp:188-191) */
+  int cg_start;           /* SU2B_CG_START_*: start vector of every inner CG */
+  long pf_seed;           /* seed of the reference's sigma=10 Gaussian CG start */
+} su2b_hmc_params;
+
+typedef struct {
+  int accepted;
+  double dH;            /* Delta H summed over the monomials */
+  double ddH;           /* reversibility violation (revtest only) */
+  double H_old[3];      /* kinetic, gauge, fermion */
+  double H_new[3];
+  double plaquette;     /* gauge_energy after the accept/reject */
+  long cg_iterations;   /* total inner CG iterations (fermions only) */
+} su2b_traj_result;
+
+SU2B_API int su2b_hmc_trajectory(su2b_ctx *ctx, const su2b_hmc_params *prm, su2b_traj_result *res);
+
+/* ---- Metropolis (flat_spacetime::sweep, flat-sweep.hh:64-164) -------------------------- */
+/* Device order: site-parity checkerboard, one pass per (mu, parity); proposal and accept
+ * rule as the reference; random numbers from Philox(seed, {link, hit, sweep}).
+ * rates[0] = accepted/(N_hit*links), rates[1] = temporal ones/(N_hit*volume). */
+SU2B_API int su2b_metropolis_sweep(su2b_ctx *ctx, double delta, int N_hit, uint64_t seed,
+                          uint32_t sweep, double *rates);
+
+/* ---- Wilson flow (flat-gradient_flow.hh) --------------------------------------------- */
+/* One Lüscher RK3 step of runge_kutta (flat-gradient_flow.hh:17-50) on the context's
+ * links (in place). */
+SU2B_API int su2b_flow_step(su2b_ctx *ctx, double eps);
+/* gradient_flow (flat-gradient_flow.hh:70-197) on a copy of the links: rows of 9 doubles
+ * {t, xi_R, P, P_ss, Ep, Ep_ss, Ec, Ec_ss, Q}, recorded at the middle of every pair of
+ * steps as the reference prints them.  *n_rows receives the number of records. */
+SU2B_API int su2b_gradient_flow(su2b_ctx *ctx, double tmax, double eps, double tstart, double *rows,
+                       int max_rows, int *n_rows);
+
+/* ---- staggered fermions, U(1) only (staggered.hpp) ------------------------------------- */
+enum { SU2B_OP_D = 0, SU2B_OP_DDAG = 1, SU2B_OP_DDDAG = 2 };
+/* apply_D / apply_Ddag / D*Ddag (staggered.hpp:290-389) */
+SU2B_API int su2b_staggered_apply(su2b_ctx *ctx, int op, double mass, const double *psi_host,
+                         double *out_host);
+
+/* start vector of the CG inside the fermion monomial: the reference's real Gaussian with
+ * sigma = 10 drawn from std::mt19937(seed) (staggered.hpp:267-268), or zero */
+enum { SU2B_CG_START_REFERENCE = 0, SU2B_CG_START_ZERO = 1 };
+
+enum { SU2B_SOLVER_CG = 0, SU2B_SOLVER_BICGSTAB = 1, SU2B_SOLVER_CG_MIXED = 2 };
+enum { SU2B_TOL_ABS = 0, SU2B_TOL_REL = 1 };
+typedef struct {
+  int solver;     /* CG on D Ddag (CG.hpp), BiCGStab on D (BiCGStab.hpp), mixed CG */
+  int op;         /* SU2B_OP_DDDAG for CG, SU2B_OP_D for BiCGStab */
+  double mass;
+  double tol;     /* residual norm bound */
+  int tol_mode;   /* SU2B_TOL_ABS (the reference, CG.hpp:50) or SU2B_TOL_REL (tol*|b|) */
+  int max_iter;
+  double delta;   /* mixed CG: reliable-update threshold (0 = default 0.1) */
+} su2b_solve_params;
+typedef struct {
+  long iterations;
+  long restarts;          /* true-residual restarts (CG.hpp:78-84) / reliable updates */
+  double residual;        /* final iterated residual norm */
+  double true_residual;   /* |b - A x| recomputed in FP64 */
+} su2b_solve_stats;
+/* LinearCG::solve / LinearBiCGStab::solve; x0_host NULL = zero start */
+SU2B_API int su2b_solve(su2b_ctx *ctx, const su2b_solve_params *prm, const double *b_host,
+               const double *x0_host, double *x_host, su2b_solve_stats *stats);
+/* detDDdag_monomial::derivative (detDDdag_monomial.hh:112-167): CG from x0 (NULL = the
+ * reference's sigma=10 Gaussian start of DDdag_matrix_lat::inv drawn with `seed`), then the
+ * per-link contraction; deriv_host receives the force (not accumulated). */
+SU2B_API int su2b_fermion_force(su2b_ctx *ctx, double mass, const double *phi_host, double tol,
+                       int max_iter, const double *x0_host, long seed, double *deriv_host,
+                       long *cg_iterations);
+/* detDDdag_monomial::accept (detDDdag_monomial.hh:93-103): Re phi^+ (D Ddag)^-1 phi */
+SU2B_API int su2b_fermion_action(su2b_ctx *ctx, double mass, const double *phi_host, double tol,
+                        int max_iter, const double *x0_host, long seed, double *out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

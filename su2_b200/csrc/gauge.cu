@@ -1,0 +1,658 @@
+// gauge.cu -- gauge-field kernels of libsu2b: layout conversion, plaquette reductions, the
+// fused staple/force/momentum kernel, link update, reunitarisation, Philox momenta, the
+// deterministic final reduction and the HMC accept/reject.
+//
+// Roofline per link (FP64 / FP32 storage), algorithmic bytes:
+//   force+momentum  read U 32/16, read+write P 48/24            = 80 / 40 B
+//   link update     read P 24/12, read+write U 64/32            = 88 / 44 B
+//   plaquette       read U once                                 = 32 / 16 B
+#include "su2b_internal.h"
+
+namespace su2b {
+
+namespace {
+
+template <class T> using LinkT = typename LinkOf<T>::type;
+
+inline int cdiv(long a, long b) { return (int)((a + b - 1) / b); }
+
+// ------------------------------------------------------------------------------------
+// layout conversion: thread i walks the reference order i = lex*nd + mu
+template <class T>
+__global__ void k_links_from_host_su2(Geom g, const double *__restrict__ aos, LinkT<T> *U) {
+  const long n = (long)g.V * g.nd;
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n;
+       i += (long)gridDim.x * blockDim.x) {
+    const int lex = (int)(i / g.nd), mu = (int)(i - (long)lex * g.nd);
+    const Site s = site_from_lex(g, lex);
+    const double *src = aos + 4 * i;
+    Su2<double> u{src[0], src[1], src[2], src[3]};
+    st_link(U + (size_t)mu * g.V + eo_of(g, lex, s.p), from64<T>(u));
+  }
+}
+template <class T>
+__global__ void k_links_to_host_su2(Geom g, const LinkT<T> *__restrict__ U, double *aos) {
+  const long n = (long)g.V * g.nd;
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n;
+       i += (long)gridDim.x * blockDim.x) {
+    const int lex = (int)(i / g.nd), mu = (int)(i - (long)lex * g.nd);
+    const Site s = site_from_lex(g, lex);
+    const Su2<double> u = to64(ld_link_rw(U + (size_t)mu * g.V + eo_of(g, lex, s.p)));
+    double *dst = aos + 4 * i;
+    dst[0] = u.ar;
+    dst[1] = u.ai;
+    dst[2] = u.br;
+    dst[3] = u.bi;
+  }
+}
+// U(1) angles and adjoint fields: na reals per link, SoA on the device
+template <class T>
+__global__ void k_adj_from_host(Geom g, const double *__restrict__ aos, T *P, int na) {
+  const long n = (long)g.V * g.nd;
+  const size_t NL = (size_t)g.V * g.nd;
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n;
+       i += (long)gridDim.x * blockDim.x) {
+    const int lex = (int)(i / g.nd), mu = (int)(i - (long)lex * g.nd);
+    const Site s = site_from_lex(g, lex);
+    const size_t l = (size_t)mu * g.V + eo_of(g, lex, s.p);
+    for (int k = 0; k < na; k++) P[k * NL + l] = (T)aos[na * i + k];
+  }
+}
+template <class T>
+__global__ void k_adj_to_host(Geom g, const T *__restrict__ P, double *aos, int na) {
+  const long n = (long)g.V * g.nd;
+  const size_t NL = (size_t)g.V * g.nd;
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n;
+       i += (long)gridDim.x * blockDim.x) {
+    const int lex = (int)(i / g.nd), mu = (int)(i - (long)lex * g.nd);
+    const Site s = site_from_lex(g, lex);
+    const size_t l = (size_t)mu * g.V + eo_of(g, lex, s.p);
+    for (int k = 0; k < na; k++) aos[na * i + k] = (double)P[k * NL + l];
+  }
+}
+__global__ void k_spinor_from_host(Geom g, const double2 *__restrict__ aos, double2 *psi) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < g.V; i += gridDim.x * blockDim.x) {
+    const Site s = site_from_lex(g, i);
+    psi[eo_of(g, i, s.p)] = aos[i];
+  }
+}
+__global__ void k_spinor_to_host(Geom g, const double2 *__restrict__ psi, double2 *aos) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < g.V; i += gridDim.x * blockDim.x) {
+    const Site s = site_from_lex(g, i);
+    aos[i] = psi[eo_of(g, i, s.p)];
+  }
+}
+
+// ------------------------------------------------------------------------------------
+// plaquettes: per site, sum over planes mu<nu of ReTr U_mu(x) U_nu(x+mu) U_mu(x+nu)^+ U_nu(x)^+
+// (flat-gauge_energy.hpp:31-94), FP64 products.  Partials {full, spatial, xi-weighted}.
+template <class T, int ND, int NT>
+__global__ void __launch_bounds__(NT)
+  k_plaq_su2(Geom g, const LinkT<T> *__restrict__ U, double xi, double *part) {
+  __shared__ double sh[NT / 32];
+  const int p = blockIdx.y;
+  const int cb = blockIdx.x * NT + threadIdx.x;
+  double full = 0., spat = 0., wsum = 0.;
+  if (cb < g.Vh) {
+    const Site s = site_from_eo(g, p, cb);
+    Su2<double> u[ND];
+#pragma unroll
+    for (int mu = 0; mu < ND; mu++) u[mu] = to64(ld_link(U + (size_t)mu * g.V + p * g.Vh + cb));
+#pragma unroll
+    for (int mu = 0; mu < ND - 1; mu++) {
+      const int lpm = s.lex + fwd(g, s, mu);
+#pragma unroll
+      for (int nu = mu + 1; nu < ND; nu++) {
+        const int lpn = s.lex + fwd(g, s, nu);
+        const Su2<double> A = to64(ld_link(U + (size_t)nu * g.V + eo_of(g, lpm, 1 - p)));
+        const Su2<double> B = to64(ld_link(U + (size_t)mu * g.V + eo_of(g, lpn, 1 - p)));
+        const double tr = retr_mul(mul(u[mu], A), dag(mul(u[nu], B)));
+        full += tr;
+        if (mu >= 1) spat += tr;
+        wsum += (((mu == 0) ^ (nu == 0)) ? 1.0 / xi : xi) * tr;
+      }
+    }
+  }
+  const int b = blockIdx.y * gridDim.x + blockIdx.x;
+  double r = block_sum<NT>(full, sh);
+  if (threadIdx.x == 0) part[3 * b] = r;
+  r = block_sum<NT>(spat, sh);
+  if (threadIdx.x == 0) part[3 * b + 1] = r;
+  r = block_sum<NT>(wsum, sh);
+  if (threadIdx.x == 0) part[3 * b + 2] = r;
+}
+
+template <int ND, int NT>
+__global__ void __launch_bounds__(NT)
+  k_plaq_u1(Geom g, const double *__restrict__ U, double xi, double *part) {
+  __shared__ double sh[NT / 32];
+  const int p = blockIdx.y;
+  const int cb = blockIdx.x * NT + threadIdx.x;
+  double full = 0., spat = 0., wsum = 0.;
+  if (cb < g.Vh) {
+    const Site s = site_from_eo(g, p, cb);
+    double u[ND];
+#pragma unroll
+    for (int mu = 0; mu < ND; mu++) u[mu] = U[(size_t)mu * g.V + p * g.Vh + cb];
+#pragma unroll
+    for (int mu = 0; mu < ND - 1; mu++) {
+      const int lpm = s.lex + fwd(g, s, mu);
+#pragma unroll
+      for (int nu = mu + 1; nu < ND; nu++) {
+        const int lpn = s.lex + fwd(g, s, nu);
+        const double A = U[(size_t)nu * g.V + eo_of(g, lpm, 1 - p)];
+        const double B = U[(size_t)mu * g.V + eo_of(g, lpn, 1 - p)];
+        const double tr = cos(((u[mu] + A) + (-B)) + (-u[nu]));
+        full += tr;
+        if (mu >= 1) spat += tr;
+        wsum += (((mu == 0) ^ (nu == 0)) ? 1.0 / xi : xi) * tr;
+      }
+    }
+  }
+  const int b = blockIdx.y * gridDim.x + blockIdx.x;
+  double r = block_sum<NT>(full, sh);
+  if (threadIdx.x == 0) part[3 * b] = r;
+  r = block_sum<NT>(spat, sh);
+  if (threadIdx.x == 0) part[3 * b + 1] = r;
+  r = block_sum<NT>(wsum, sh);
+  if (threadIdx.x == 0) part[3 * b + 2] = r;
+}
+
+template <int NT>
+__global__ void __launch_bounds__(NT)
+  k_reduce_final(const double *__restrict__ part, int n, int ncomp, double *out) {
+  __shared__ double sh[NT / 32];
+  for (int k = 0; k < ncomp; k++) {
+    double v = 0.;
+    for (int b = threadIdx.x; b < n; b += NT) v += part[(size_t)b * ncomp + k];
+    const double r = block_sum<NT>(v, sh);
+    if (threadIdx.x == 0) out[k] = r;
+  }
+}
+
+// ------------------------------------------------------------------------------------
+// staple sum K (get_staples.hh:26-80) for link (x, mu): forward staples for all nu != mu,
+// then backward ones, each optionally weighted by 1/xi (temporal plane) or xi (spatial).
+template <class T, int ND>
+__device__ __forceinline__ Su2<T> staple_su2(const Geom &g, const LinkT<T> *__restrict__ U,
+                                             const Site &s, int mu, int aniso, T wt, T ws) {
+  const int p = s.p;
+  const int lpm = s.lex + fwd(g, s, mu);
+  Su2<T> K = zero_su2<T>();
+#pragma unroll
+  for (int nu = 0; nu < ND; nu++) {
+    if (nu == mu) continue;
+    const int lpn = s.lex + fwd(g, s, nu);
+    const Su2<T> A = ld_link(U + (size_t)nu * g.V + eo_of(g, lpm, 1 - p));
+    const Su2<T> B = ld_link(U + (size_t)mu * g.V + eo_of(g, lpn, 1 - p));
+    const Su2<T> D = ld_link(U + (size_t)nu * g.V + eo_of(g, s.lex, p));
+    Su2<T> st = mul(mul(A, dag(B)), dag(D));
+    if (aniso) st = scale((nu == 0 || mu == 0) ? wt : ws, st);
+    K = add(K, st);
+  }
+#pragma unroll
+  for (int nu = 0; nu < ND; nu++) {
+    if (nu == mu) continue;
+    const int b = bwd(g, s, nu);
+    const int lmn = s.lex + b, lpmmn = lpm + b;
+    const Su2<T> A = ld_link(U + (size_t)nu * g.V + eo_of(g, lpmmn, p));
+    const Su2<T> B = ld_link(U + (size_t)mu * g.V + eo_of(g, lmn, 1 - p));
+    const Su2<T> D = ld_link(U + (size_t)nu * g.V + eo_of(g, lmn, 1 - p));
+    Su2<T> st = mul(mul(dag(A), dag(B)), D);
+    if (aniso) st = scale((nu == 0 || mu == 0) ? wt : ws, st);
+    K = add(K, st);
+  }
+  return K;
+}
+
+// fused gauge force + momentum update (flat-gaugemonomial.hh:105-131 + update_momenta.hh:10-33):
+//   d = f * get_deriv(U K) (+ extra),  P = P + scale*d   (scale = -dtau)
+template <class T, int ND, int NT>
+__global__ void __launch_bounds__(NT)
+  k_force_su2(Geom g, const LinkT<T> *__restrict__ U, T *__restrict__ P,
+              const T *__restrict__ extra, T f, T scale_, int mode, int aniso, T wt, T ws,
+              double *kin_part) {
+  __shared__ double sh[NT / 32];
+  const int mu = blockIdx.y >> 1, p = blockIdx.y & 1;
+  const int cb = blockIdx.x * NT + threadIdx.x;
+  double k2 = 0.;
+  if (cb < g.Vh) {
+    const Site s = site_from_eo(g, p, cb);
+    const Su2<T> K = staple_su2<T, ND>(g, U, s, mu, aniso, wt, ws);
+    const size_t NL = (size_t)g.V * ND;
+    const size_t l = (size_t)mu * g.V + (size_t)p * g.Vh + cb;
+    const Su2<T> u = ld_link(U + l);
+    // get_deriv(U K) = (2 Im b, 2 Re b, 2 Im a) (adjointfield.hh:53-56)
+    const T sbi = u.ar * K.bi + u.ai * K.br + (u.bi * K.ar - u.br * K.ai);
+    const T sbr = u.ar * K.br - u.ai * K.bi + (u.br * K.ar + u.bi * K.ai);
+    const T sai = u.ar * K.ai + u.ai * K.ar - (u.bi * K.br - u.br * K.bi);
+    T d0 = f * (T(2) * sbi), d1 = f * (T(2) * sbr), d2 = f * (T(2) * sai);
+    if (mode & FM_EXTRA) {
+      d0 += extra[l];
+      d1 += extra[NL + l];
+      d2 += extra[2 * NL + l];
+    }
+    T p0, p1, p2;
+    if (mode & FM_HAS_IN) {
+      p0 = P[l] + scale_ * d0;
+      p1 = P[NL + l] + scale_ * d1;
+      p2 = P[2 * NL + l] + scale_ * d2;
+    } else {
+      p0 = scale_ * d0;
+      p1 = scale_ * d1;
+      p2 = scale_ * d2;
+    }
+    P[l] = p0;
+    P[NL + l] = p1;
+    P[2 * NL + l] = p2;
+    k2 = (double)p0 * p0 + (double)p1 * p1 + (double)p2 * p2;
+  }
+  if (mode & FM_KINETIC) {
+    const double r = block_sum<NT>(k2, sh);
+    if (threadIdx.x == 0) kin_part[blockIdx.y * gridDim.x + blockIdx.x] = r;
+  }
+}
+
+template <int ND, int NT>
+__global__ void __launch_bounds__(NT)
+  k_force_u1(Geom g, const double *__restrict__ U, double *__restrict__ P,
+             const double *__restrict__ extra, double f, double scale_, int mode, int aniso,
+             double wt, double ws, double *kin_part) {
+  __shared__ double sh[NT / 32];
+  const int mu = blockIdx.y >> 1, p = blockIdx.y & 1;
+  const int cb = blockIdx.x * NT + threadIdx.x;
+  double k2 = 0.;
+  if (cb < g.Vh) {
+    const Site s = site_from_eo(g, p, cb);
+    const int lpm = s.lex + fwd(g, s, mu);
+    double Kr = 0., Ki = 0.;
+#pragma unroll
+    for (int nu = 0; nu < ND; nu++) {
+      if (nu == mu) continue;
+      const int lpn = s.lex + fwd(g, s, nu);
+      const double A = U[(size_t)nu * g.V + eo_of(g, lpm, 1 - p)];
+      const double B = U[(size_t)mu * g.V + eo_of(g, lpn, 1 - p)];
+      const double D = U[(size_t)nu * g.V + eo_of(g, s.lex, p)];
+      double sn, cs;
+      sincos((A + (-B)) + (-D), &sn, &cs);
+      const double w = aniso ? ((nu == 0 || mu == 0) ? wt : ws) : 1.0;
+      Kr += w * cs;
+      Ki += w * sn;
+    }
+#pragma unroll
+    for (int nu = 0; nu < ND; nu++) {
+      if (nu == mu) continue;
+      const int b = bwd(g, s, nu);
+      const double A = U[(size_t)nu * g.V + eo_of(g, lpm + b, p)];
+      const double B = U[(size_t)mu * g.V + eo_of(g, s.lex + b, 1 - p)];
+      const double D = U[(size_t)nu * g.V + eo_of(g, s.lex + b, 1 - p)];
+      double sn, cs;
+      sincos(((-A) + (-B)) + D, &sn, &cs);
+      const double w = aniso ? ((nu == 0 || mu == 0) ? wt : ws) : 1.0;
+      Kr += w * cs;
+      Ki += w * sn;
+    }
+    const size_t l = (size_t)mu * g.V + (size_t)p * g.Vh + cb;
+    double su, cu;
+    sincos(U[l], &su, &cu);
+    double d = f * (cu * Ki + su * Kr);  // Im(e^{i theta} K), adjointfield.hh:79-81
+    if (mode & FM_EXTRA) d += extra[l];
+    const double pn = (mode & FM_HAS_IN) ? P[l] + scale_ * d : scale_ * d;
+    P[l] = pn;
+    k2 = pn * pn;
+  }
+  if (mode & FM_KINETIC) {
+    const double r = block_sum<NT>(k2, sh);
+    if (threadIdx.x == 0) kin_part[blockIdx.y * gridDim.x + blockIdx.x] = r;
+  }
+}
+
+// ------------------------------------------------------------------------------------
+// U <- exp(dt P) U (update_gauge.hh:8-16)
+template <class T>
+__global__ void k_update_su2(size_t NL, LinkT<T> *__restrict__ U, const T *__restrict__ P,
+                             T dt) {
+  for (size_t l = blockIdx.x * (size_t)blockDim.x + threadIdx.x; l < NL;
+       l += (size_t)gridDim.x * blockDim.x) {
+    const Su2<T> e = exp_alg(dt * P[l], dt * P[NL + l], dt * P[2 * NL + l]);
+    st_link(U + l, mul(e, ld_link_rw(U + l)));
+  }
+}
+__global__ void k_update_u1(size_t NL, double *__restrict__ U, const double *__restrict__ P,
+                            double dt) {
+  for (size_t l = blockIdx.x * (size_t)blockDim.x + threadIdx.x; l < NL;
+       l += (size_t)gridDim.x * blockDim.x)
+    U[l] = dt * P[l] + U[l];
+}
+// restoreSU in FP64 (gaugeconfig.hh:115-120)
+template <class T> __global__ void k_restore(size_t NL, LinkT<T> *__restrict__ U) {
+  for (size_t l = blockIdx.x * (size_t)blockDim.x + threadIdx.x; l < NL;
+       l += (size_t)gridDim.x * blockDim.x)
+    st_link(U + l, from64<T>(restore_su(to64(ld_link_rw(U + l)))));
+}
+
+// ------------------------------------------------------------------------------------
+// momenta: standard normal per component from Philox(seed; {ref link, draw, traj, MOM})
+template <class T, int NT>
+__global__ void __launch_bounds__(NT)
+  k_momenta(Geom g, T *__restrict__ P, int na, uint64_t seed, uint32_t traj, double *kin_part) {
+  __shared__ double sh[NT / 32];
+  const int mu = blockIdx.y >> 1, p = blockIdx.y & 1;
+  const int cb = blockIdx.x * NT + threadIdx.x;
+  double k2 = 0.;
+  if (cb < g.Vh) {
+    const Site s = site_from_eo(g, p, cb);
+    const uint32_t lref = (uint32_t)s.lex * (uint32_t)g.nd + (uint32_t)mu;
+    const size_t NL = (size_t)g.V * g.nd;
+    const size_t l = (size_t)mu * g.V + (size_t)p * g.Vh + cb;
+    uint32_t r[4];
+    double n0, n1, n2, n3;
+    philox(lref, 0u, traj, TAG_MOMENTA, seed, r);
+    box_muller(u01_53(r[0], r[1]), u01_53(r[2], r[3]), n0, n1);
+    const T a = (T)n0;
+    P[l] = a;
+    k2 = (double)a * a;
+    if (na == 3) {
+      philox(lref, 1u, traj, TAG_MOMENTA, seed, r);
+      box_muller(u01_53(r[0], r[1]), u01_53(r[2], r[3]), n2, n3);
+      const T b = (T)n1, c = (T)n2;
+      P[NL + l] = b;
+      P[2 * NL + l] = c;
+      k2 += (double)b * b + (double)c * c;
+    }
+  }
+  const double rr = block_sum<NT>(k2, sh);
+  if (threadIdx.x == 0) kin_part[blockIdx.y * gridDim.x + blockIdx.x] = rr;
+}
+
+template <class T, int NT>
+__global__ void __launch_bounds__(NT)
+  k_kinetic(Geom g, const T *__restrict__ P, int na, double *part) {
+  __shared__ double sh[NT / 32];
+  const int mu = blockIdx.y >> 1, p = blockIdx.y & 1;
+  const int cb = blockIdx.x * NT + threadIdx.x;
+  double k2 = 0.;
+  if (cb < g.Vh) {
+    const size_t NL = (size_t)g.V * g.nd;
+    const size_t l = (size_t)mu * g.V + (size_t)p * g.Vh + cb;
+    for (int k = 0; k < na; k++) {
+      const double v = (double)P[k * NL + l];
+      k2 += v * v;
+    }
+  }
+  const double rr = block_sum<NT>(k2, sh);
+  if (threadIdx.x == 0) part[blockIdx.y * gridDim.x + blockIdx.x] = rr;
+}
+
+template <class T> __global__ void k_negate(size_t n, T *P) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x)
+    P[i] = -P[i];
+}
+
+// ------------------------------------------------------------------------------------
+// accept/reject (md_update.hh:45-60), one thread
+__global__ void k_accept(const double *__restrict__ red, AcceptIn in, TrajDev *out) {
+  TrajDev t;
+  t.H_old[0] = 0.5 * red[0];
+  t.H_old[1] = -in.beta * red[3] / in.Nc;
+  t.H_old[2] = red[8];
+  t.H_new[0] = 0.5 * red[4];
+  t.H_new[1] = -in.beta * red[7] / in.Nc;
+  t.H_new[2] = red[9];
+  double dH = 0.;
+  dH += t.H_new[0] - t.H_old[0];
+  dH += t.H_new[1] - t.H_old[1];
+  dH += t.H_new[2] - t.H_old[2];
+  t.dH = dH;
+  t.accepted = 1;
+  t.u = -1.0;
+  if (in.accept_reject && dH > 0) {
+    double u = in.u_host;
+    if (u < 0.0) {
+      uint32_t r[4];
+      philox(0u, 0u, in.traj, TAG_ACCEPT, in.seed, r);
+      u = u01_53(r[0], r[1]) - 0x1p-53;
+    }
+    t.u = u;
+    if (u > exp(-dH)) t.accepted = 0;
+  }
+  t.pad = 0;
+  *out = t;
+}
+
+template <class T>
+__global__ void k_cond_restore(size_t n, T *__restrict__ U, const T *__restrict__ U_old,
+                               const TrajDev *__restrict__ flag) {
+  if (flag->accepted) return;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x)
+    U[i] = U_old[i];
+}
+
+constexpr int NT_RED = 256;
+
+inline int flat_grid(size_t n, int nt) {
+  const size_t b = (n + nt - 1) / nt;
+  return (int)(b < 148u * 32u ? (b > 0 ? b : 1) : 148u * 32u);
+}
+
+}  // namespace
+
+// =====================================================================================
+// launchers
+// =====================================================================================
+
+template <class T>
+cudaError_t links_from_host(const Geom &g, const double *aos, void *U, int group,
+                            cudaStream_t s) {
+  const size_t n = (size_t)g.V * g.nd;
+  if (group == 0)
+    k_links_from_host_su2<T><<<flat_grid(n, 256), 256, 0, s>>>(g, aos, (LinkT<T> *)U);
+  else
+    k_adj_from_host<double><<<flat_grid(n, 256), 256, 0, s>>>(g, aos, (double *)U, 1);
+  return cudaGetLastError();
+}
+template <class T>
+cudaError_t links_to_host(const Geom &g, const void *U, double *aos, int group,
+                          cudaStream_t s) {
+  const size_t n = (size_t)g.V * g.nd;
+  if (group == 0)
+    k_links_to_host_su2<T><<<flat_grid(n, 256), 256, 0, s>>>(g, (const LinkT<T> *)U, aos);
+  else
+    k_adj_to_host<double><<<flat_grid(n, 256), 256, 0, s>>>(g, (const double *)U, aos, 1);
+  return cudaGetLastError();
+}
+template <class T>
+cudaError_t adj_from_host(const Geom &g, const double *aos, T *P, int group, cudaStream_t s) {
+  const size_t n = (size_t)g.V * g.nd;
+  k_adj_from_host<T><<<flat_grid(n, 256), 256, 0, s>>>(g, aos, P, group == 0 ? 3 : 1);
+  return cudaGetLastError();
+}
+template <class T>
+cudaError_t adj_to_host(const Geom &g, const T *P, double *aos, int group, cudaStream_t s) {
+  const size_t n = (size_t)g.V * g.nd;
+  k_adj_to_host<T><<<flat_grid(n, 256), 256, 0, s>>>(g, P, aos, group == 0 ? 3 : 1);
+  return cudaGetLastError();
+}
+cudaError_t spinor_from_host(const Geom &g, const double *aos, double2 *psi, cudaStream_t s) {
+  k_spinor_from_host<<<flat_grid(g.V, 256), 256, 0, s>>>(g, (const double2 *)aos, psi);
+  return cudaGetLastError();
+}
+cudaError_t spinor_to_host(const Geom &g, const double2 *psi, double *aos, cudaStream_t s) {
+  k_spinor_to_host<<<flat_grid(g.V, 256), 256, 0, s>>>(g, psi, (double2 *)aos);
+  return cudaGetLastError();
+}
+
+template <class T>
+cudaError_t plaq_partials(const Geom &g, const void *U, int group, double xi, double *part,
+                          int *nblocks, cudaStream_t s) {
+  constexpr int NT = 256;
+  const dim3 grid(cdiv(g.Vh, NT), 2);
+  *nblocks = grid.x * grid.y;
+  if (group == 0) {
+    const LinkT<T> *u = (const LinkT<T> *)U;
+    switch (g.nd) {
+      case 2: k_plaq_su2<T, 2, NT><<<grid, NT, 0, s>>>(g, u, xi, part); break;
+      case 3: k_plaq_su2<T, 3, NT><<<grid, NT, 0, s>>>(g, u, xi, part); break;
+      default: k_plaq_su2<T, 4, NT><<<grid, NT, 0, s>>>(g, u, xi, part); break;
+    }
+  } else {
+    const double *u = (const double *)U;
+    switch (g.nd) {
+      case 2: k_plaq_u1<2, NT><<<grid, NT, 0, s>>>(g, u, xi, part); break;
+      case 3: k_plaq_u1<3, NT><<<grid, NT, 0, s>>>(g, u, xi, part); break;
+      default: k_plaq_u1<4, NT><<<grid, NT, 0, s>>>(g, u, xi, part); break;
+    }
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t reduce_final(const double *part, int nblocks, int ncomp, double *out,
+                         cudaStream_t s) {
+  k_reduce_final<512><<<1, 512, 0, s>>>(part, nblocks, ncomp, out);
+  return cudaGetLastError();
+}
+
+template <class T>
+cudaError_t force_update(const Geom &g, const void *U, int group, T *P, const T *extra, double f,
+                         double scale, double xi, int mode, double *kin_part, int *nblocks,
+                         cudaStream_t s) {
+  constexpr int NT = 128;
+  const dim3 grid(cdiv(g.Vh, NT), 2 * g.nd);
+  if (nblocks) *nblocks = grid.x * grid.y;
+  const int aniso = xi != 1.0;
+  if (group == 0) {
+    const LinkT<T> *u = (const LinkT<T> *)U;
+    const T wt = (T)(1.0 / xi), ws = (T)xi;
+    switch (g.nd) {
+      case 2:
+        k_force_su2<T, 2, NT><<<grid, NT, 0, s>>>(g, u, P, extra, (T)f, (T)scale, mode, aniso,
+                                                  wt, ws, kin_part);
+        break;
+      case 3:
+        k_force_su2<T, 3, NT><<<grid, NT, 0, s>>>(g, u, P, extra, (T)f, (T)scale, mode, aniso,
+                                                  wt, ws, kin_part);
+        break;
+      default:
+        k_force_su2<T, 4, NT><<<grid, NT, 0, s>>>(g, u, P, extra, (T)f, (T)scale, mode, aniso,
+                                                  wt, ws, kin_part);
+        break;
+    }
+  } else {
+    if (sizeof(T) != 8) return cudaErrorNotSupported;
+    const double *u = (const double *)U;
+    double *PP = (double *)P;
+    const double *ex = (const double *)extra;
+    switch (g.nd) {
+      case 2:
+        k_force_u1<2, NT><<<grid, NT, 0, s>>>(g, u, PP, ex, f, scale, mode, aniso, 1.0 / xi, xi,
+                                              kin_part);
+        break;
+      case 3:
+        k_force_u1<3, NT><<<grid, NT, 0, s>>>(g, u, PP, ex, f, scale, mode, aniso, 1.0 / xi, xi,
+                                              kin_part);
+        break;
+      default:
+        k_force_u1<4, NT><<<grid, NT, 0, s>>>(g, u, PP, ex, f, scale, mode, aniso, 1.0 / xi, xi,
+                                              kin_part);
+        break;
+    }
+  }
+  return cudaGetLastError();
+}
+
+template <class T>
+cudaError_t link_update(const Geom &g, void *U, int group, const T *P, double dt,
+                        cudaStream_t s) {
+  const size_t NL = (size_t)g.V * g.nd;
+  if (group == 0)
+    k_update_su2<T><<<flat_grid(NL, 256), 256, 0, s>>>(NL, (LinkT<T> *)U, P, (T)dt);
+  else {
+    if (sizeof(T) != 8) return cudaErrorNotSupported;
+    k_update_u1<<<flat_grid(NL, 256), 256, 0, s>>>(NL, (double *)U, (const double *)P, dt);
+  }
+  return cudaGetLastError();
+}
+
+template <class T> cudaError_t restore_links(const Geom &g, void *U, int group, cudaStream_t s) {
+  if (group != 0) return cudaSuccess;  // u1.hh:178-179
+  const size_t NL = (size_t)g.V * g.nd;
+  k_restore<T><<<flat_grid(NL, 256), 256, 0, s>>>(NL, (LinkT<T> *)U);
+  return cudaGetLastError();
+}
+
+template <class T>
+cudaError_t momenta_philox(const Geom &g, T *P, int group, uint64_t seed, uint32_t traj,
+                           double *kin_part, int *nblocks, cudaStream_t s) {
+  constexpr int NT = NT_RED;
+  const dim3 grid(cdiv(g.Vh, NT), 2 * g.nd);
+  *nblocks = grid.x * grid.y;
+  k_momenta<T, NT><<<grid, NT, 0, s>>>(g, P, group == 0 ? 3 : 1, seed, traj, kin_part);
+  return cudaGetLastError();
+}
+
+template <class T>
+cudaError_t kinetic_partials(const Geom &g, const T *P, int group, double *part, int *nblocks,
+                             cudaStream_t s) {
+  constexpr int NT = NT_RED;
+  const dim3 grid(cdiv(g.Vh, NT), 2 * g.nd);
+  *nblocks = grid.x * grid.y;
+  k_kinetic<T, NT><<<grid, NT, 0, s>>>(g, P, group == 0 ? 3 : 1, part);
+  return cudaGetLastError();
+}
+
+template <class T> cudaError_t negate_adj(const Geom &g, T *P, int group, cudaStream_t s) {
+  const size_t n = (size_t)g.V * g.nd * (group == 0 ? 3 : 1);
+  k_negate<T><<<flat_grid(n, 256), 256, 0, s>>>(n, P);
+  return cudaGetLastError();
+}
+
+cudaError_t accept_step(const double *red, AcceptIn in, TrajDev *out, cudaStream_t s) {
+  k_accept<<<1, 1, 0, s>>>(red, in, out);
+  return cudaGetLastError();
+}
+
+template <class T>
+cudaError_t cond_restore(const Geom &g, void *U, const void *U_old, int group,
+                         const TrajDev *flag, cudaStream_t s) {
+  const size_t NL = (size_t)g.V * g.nd;
+  if (group == 0) {
+    // copy as 16-byte words
+    const size_t n = NL * sizeof(LinkT<T>) / sizeof(float4);
+    k_cond_restore<float4><<<flat_grid(n, 256), 256, 0, s>>>(n, (float4 *)U,
+                                                             (const float4 *)U_old, flag);
+  } else {
+    k_cond_restore<double><<<flat_grid(NL, 256), 256, 0, s>>>(NL, (double *)U,
+                                                              (const double *)U_old, flag);
+  }
+  return cudaGetLastError();
+}
+
+#define INST(T)                                                                              \
+  template cudaError_t links_from_host<T>(const Geom &, const double *, void *, int,         \
+                                          cudaStream_t);                                      \
+  template cudaError_t links_to_host<T>(const Geom &, const void *, double *, int,           \
+                                        cudaStream_t);                                        \
+  template cudaError_t adj_from_host<T>(const Geom &, const double *, T *, int, cudaStream_t); \
+  template cudaError_t adj_to_host<T>(const Geom &, const T *, double *, int, cudaStream_t);   \
+  template cudaError_t plaq_partials<T>(const Geom &, const void *, int, double, double *,   \
+                                        int *, cudaStream_t);                                 \
+  template cudaError_t force_update<T>(const Geom &, const void *, int, T *, const T *,      \
+                                       double, double, double, int, double *, int *,          \
+                                       cudaStream_t);                                         \
+  template cudaError_t link_update<T>(const Geom &, void *, int, const T *, double,          \
+                                      cudaStream_t);                                          \
+  template cudaError_t restore_links<T>(const Geom &, void *, int, cudaStream_t);            \
+  template cudaError_t momenta_philox<T>(const Geom &, T *, int, uint64_t, uint32_t,         \
+                                         double *, int *, cudaStream_t);                      \
+  template cudaError_t kinetic_partials<T>(const Geom &, const T *, int, double *, int *,    \
+                                           cudaStream_t);                                     \
+  template cudaError_t negate_adj<T>(const Geom &, T *, int, cudaStream_t);                  \
+  template cudaError_t cond_restore<T>(const Geom &, void *, const void *, int,              \
+                                       const TrajDev *, cudaStream_t);
+INST(double)
+INST(float)
+#undef INST
+
+}  // namespace su2b

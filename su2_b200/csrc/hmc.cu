@@ -1,0 +1,253 @@
+// hmc.cu -- the HMC trajectory on the device (md_update, md_update.hh:18-81).
+//
+// Sequence per trajectory, all on the context's stream:
+//   momenta (Philox, or uploaded)  + sum P^2         -> H_kin old
+//   [fermions: R, phi = D R, |R|^2]                  -> H_F old
+//   plaquette partials                               -> S_G old
+//   U_old = U
+//   integrator schedule (integrator.hh): momentum steps are the fused staple/force/momentum
+//     kernel (the last one also sums P^2), gauge steps the exp(dt P) U kernel
+//   restoreSU, plaquettes (+ fermion action)         -> H new
+//   accept/reject on the device (FP64), optional reversibility test, U = U_old on reject
+//   plaquette of the resulting field; one device->host copy of the result.
+#include <cmath>
+#include <vector>
+
+#include "su2b.h"
+#include "su2b_ctx.h"
+
+using namespace su2b;
+
+namespace {
+
+struct Op {
+  int kind;  // 0 momenta: P -= c * deriv;  1 gauge: U = exp(c P) U
+  double c;
+};
+
+// integrator.hh: the step sequence of each scheme, with the reference's coefficient
+// arithmetic (dtau = tau/nsteps, omf2 lambda = 0.1938, omf4 Omelyan constants).
+std::vector<Op> schedule(int integ, int n, double tau) {
+  std::vector<Op> o;
+  const double dtau = tau / (double)n;
+  auto M = [&](double c) { o.push_back({0, c}); };
+  auto G = [&](double c) { o.push_back({1, c}); };
+  if (integ == SU2B_OMF2) {  // integrator.hh:83-116
+    const double lambda = 0.1938;
+    const double om2l = (1. - 2. * lambda);
+    M(lambda * dtau);
+    for (int i = 0; i < n - 1; i++) {
+      G(0.5 * dtau);
+      M(om2l * dtau);
+      G(0.5 * dtau);
+      M(2 * lambda * dtau);
+    }
+    G(0.5 * dtau);
+    M(om2l * dtau);
+    G(0.5 * dtau);
+    M(lambda * dtau);
+  } else if (integ == SU2B_OMF4) {  // integrator.hh:119-156 (loop from i = 1 as there)
+    const double rho = 0.2539785108410595, theta = -0.03230286765269967,
+                 vartheta = 0.08398315262876693, lambda = 0.6822365335719091;
+    const double eps[10] = {rho * dtau,
+                            lambda * dtau,
+                            theta * dtau,
+                            0.5 * (1 - 2. * (lambda + vartheta)) * dtau,
+                            (1 - 2. * (theta + rho)) * dtau,
+                            0.5 * (1 - 2. * (lambda + vartheta)) * dtau,
+                            theta * dtau,
+                            lambda * dtau,
+                            rho * dtau,
+                            2 * vartheta * dtau};
+    M(0.5 * eps[9]);
+    for (int i = 1; i < n - 1; i++)
+      for (int j = 0; j < 5; j++) {
+        G(eps[2 * j]);
+        M(eps[2 * j + 1]);
+      }
+    for (int j = 0; j < 4; j++) {
+      G(eps[2 * j]);
+      M(eps[2 * j + 1]);
+    }
+    G(eps[8]);
+    M(0.5 * eps[9]);
+  } else if (integ == SU2B_EULER) {  // integrator.hh:201-217
+    for (int i = 0; i < n; i++) {
+      M(dtau);
+      G(dtau);
+    }
+  } else if (integ == SU2B_RUTH) {  // integrator.hh:220-241
+    for (int i = 0; i < n; i++) {
+      M(dtau);
+      G(-1. / 24. * dtau);
+      M(-2. / 3. * dtau);
+      G(3. / 4. * dtau);
+      M(2. / 3. * dtau);
+      G(7. / 24. * dtau);
+    }
+  } else {  // leapfrog, also the reference's fallback (integrator.hh:274-277)
+    M(dtau / 2.);
+    G(dtau);
+    for (int i = 0; i < n - 1; i++) {
+      M(dtau);
+      G(dtau);
+    }
+    M(dtau / 2.);
+  }
+  return o;
+}
+
+int integrate(su2b_ctx *ctx, const std::vector<Op> &ops, const su2b_hmc_params *prm,
+              int kin_slot, long *cg_iters) {
+  const bool ferm = prm->fermion_mass > 0.0;
+  int last_m = -1;
+  for (int i = 0; i < (int)ops.size(); i++)
+    if (ops[i].kind == 0) last_m = i;
+  const double f = ctx->beta / ctx->Nc();  // fac = 1 (update_momenta.hh:21)
+  for (int i = 0; i < (int)ops.size(); i++) {
+    if (ops[i].kind == 0) {
+      int mode = FM_HAS_IN | (i == last_m ? FM_KINETIC : 0);
+      const void *extra = nullptr;
+      if (ferm) {
+        long it = 0;
+        SU2B_CKS(su2b_fermion_deriv_q(ctx, prm->fermion_mass, prm->cg_tol, prm->cg_max_iter,
+                                      prm->cg_start, prm->pf_seed, &it));
+        *cg_iters += it;
+        extra = ctx->fderiv;
+        mode |= FM_EXTRA;
+      }
+      int nb = 0;
+      SU2B_CKS(su2b_q_force(ctx, ctx->U, ctx->P, extra, f, -ops[i].c, mode, ctx->part_slot(1),
+                            &nb));
+      if (mode & FM_KINETIC)
+        SU2B_CK(reduce_final(ctx->part_slot(1), nb, 1, ctx->red + kin_slot, ctx->stream));
+    } else {
+      SU2B_CKS(su2b_q_update(ctx, ctx->U, ctx->P, ops[i].c));
+    }
+  }
+  return su2b_q_restore(ctx, ctx->U);  // integrator.hh:48
+}
+
+int kinetic_now(su2b_ctx *ctx, int slot) {
+  int nb = 0;
+  if (ctx->link64)
+    SU2B_CK(kinetic_partials<double>(ctx->g, (const double *)ctx->P, ctx->group,
+                                     ctx->part_slot(1), &nb, ctx->stream));
+  else
+    SU2B_CK(kinetic_partials<float>(ctx->g, (const float *)ctx->P, ctx->group,
+                                    ctx->part_slot(1), &nb, ctx->stream));
+  SU2B_CK(reduce_final(ctx->part_slot(1), nb, 1, ctx->red + slot, ctx->stream));
+  return SU2B_OK;
+}
+
+}  // namespace
+
+extern "C" int su2b_hmc_trajectory(su2b_ctx *ctx, const su2b_hmc_params *prm,
+                                   su2b_traj_result *res) {
+  if (!ctx) return SU2B_ERR_INVALID;
+  ctx->err.clear();
+  SU2B_CK(cudaSetDevice(ctx->device));
+  SU2B_NEED(prm && res, "params or result is NULL");
+  SU2B_NEED(prm->n_steps >= 1, "n_steps must be >= 1");
+  if (prm->integrator == 1 || prm->integrator == 3)
+    return su2b_fail(ctx, SU2B_ERR_UNSUPPORTED,
+                     "decimal-rounding integrators (lp_leapfrog, lp_omf4) are not provided");
+  const bool ferm = prm->fermion_mass > 0.0;
+  if (ferm && ctx->group != SU2B_GROUP_U1)
+    return su2b_fail(ctx, SU2B_ERR_UNSUPPORTED,
+                     "staggered fermions are U(1) only (detDDdag_monomial.hh:170-192)");
+  cudaStream_t s = ctx->stream;
+  const std::vector<Op> ops = schedule(prm->integrator, prm->n_steps, prm->tau);
+  long cg_iters = 0;
+  int nb = 0;
+
+  // momenta + H_kin old -> red[0]
+  if (prm->momenta_host) {
+    SU2B_CKS(su2b_adj_upload(ctx, prm->momenta_host, ctx->P));
+    SU2B_CKS(kinetic_now(ctx, 0));
+  } else {
+    if (ctx->link64)
+      SU2B_CK(momenta_philox<double>(ctx->g, (double *)ctx->P, ctx->group, prm->seed, prm->traj,
+                                     ctx->part_slot(1), &nb, s));
+    else
+      SU2B_CK(momenta_philox<float>(ctx->g, (float *)ctx->P, ctx->group, prm->seed, prm->traj,
+                                    ctx->part_slot(1), &nb, s));
+    SU2B_CK(reduce_final(ctx->part_slot(1), nb, 1, ctx->red + 0, s));
+  }
+  SU2B_CK(cudaMemsetAsync(ctx->red + 8, 0, 2 * sizeof(double), s));
+  if (ferm)
+    SU2B_CKS(su2b_fermion_heatbath_q(ctx, prm->fermion_mass, prm->pf_source_host, prm->seed,
+                                     prm->traj, prm->pf_complex, 8));
+  // S_G old -> red[1..3]
+  SU2B_CKS(su2b_q_plaq(ctx, ctx->U, 1));
+  SU2B_CK(cudaMemcpyAsync(ctx->U_old, ctx->U, ctx->link_bytes() * ctx->NL,
+                          cudaMemcpyDeviceToDevice, s));
+  SU2B_CKS(integrate(ctx, ops, prm, 4, &cg_iters));
+  SU2B_CKS(su2b_q_plaq(ctx, ctx->U, 5));
+  if (ferm) {
+    long it = 0;
+    SU2B_CKS(su2b_fermion_action_q(ctx, prm->fermion_mass, prm->cg_tol, prm->cg_max_iter,
+                                   prm->cg_start, prm->pf_seed, 9, &it));
+    cg_iters += it;
+  }
+  AcceptIn in;
+  in.beta = ctx->beta;
+  in.Nc = ctx->Nc();
+  in.seed = prm->seed;
+  in.traj = prm->traj;
+  in.u_host = prm->uniform_host;
+  in.accept_reject = prm->accept_reject;
+  SU2B_CK(accept_step(ctx->red, in, ctx->traj, s));
+
+  if (prm->revtest) {  // md_update.hh:62-74
+    if (!ctx->U_rev) {
+      SU2B_CK(cudaMalloc(&ctx->U_rev, ctx->link_bytes() * ctx->NL));
+      ctx->allocs.push_back(ctx->U_rev);
+    }
+    SU2B_CK(cudaMemcpyAsync(ctx->U_rev, ctx->U, ctx->link_bytes() * ctx->NL,
+                            cudaMemcpyDeviceToDevice, s));
+    if (ctx->link64)
+      SU2B_CK(negate_adj<double>(ctx->g, (double *)ctx->P, ctx->group, s));
+    else
+      SU2B_CK(negate_adj<float>(ctx->g, (float *)ctx->P, ctx->group, s));
+    SU2B_CKS(integrate(ctx, ops, prm, 10, &cg_iters));
+    SU2B_CKS(su2b_q_plaq(ctx, ctx->U, 11));
+    SU2B_CK(cudaMemsetAsync(ctx->red + 14, 0, sizeof(double), s));
+    if (ferm) {
+      long it = 0;
+      SU2B_CKS(su2b_fermion_action_q(ctx, prm->fermion_mass, prm->cg_tol, prm->cg_max_iter,
+                                     prm->cg_start, prm->pf_seed, 14, &it));
+      cg_iters += it;
+    }
+    SU2B_CK(cudaMemcpyAsync(ctx->U, ctx->U_rev, ctx->link_bytes() * ctx->NL,
+                            cudaMemcpyDeviceToDevice, s));
+    ctx->phases_valid = ctx->phases32_valid = false;
+  }
+  if (ctx->link64)
+    SU2B_CK(cond_restore<double>(ctx->g, ctx->U, ctx->U_old, ctx->group, ctx->traj, s));
+  else
+    SU2B_CK(cond_restore<float>(ctx->g, ctx->U, ctx->U_old, ctx->group, ctx->traj, s));
+  ctx->phases_valid = ctx->phases32_valid = false;
+  SU2B_CKS(su2b_q_plaq(ctx, ctx->U, 16));
+  SU2B_CK(cudaMemcpyAsync(ctx->h_traj, ctx->traj, sizeof(TrajDev), cudaMemcpyDeviceToHost, s));
+  SU2B_CKS(su2b_fetch_red(ctx, 20));
+  const TrajDev &t = *ctx->h_traj;
+  const double *r = ctx->h_red;
+  res->accepted = t.accepted;
+  res->dH = t.dH;
+  for (int k = 0; k < 3; k++) {
+    res->H_old[k] = t.H_old[k];
+    res->H_new[k] = t.H_new[k];
+  }
+  res->ddH = 0.0;
+  if (prm->revtest) {
+    double d = 0.;
+    d += 0.5 * r[10] - t.H_old[0];
+    d += (-ctx->beta * r[13] / ctx->Nc()) - t.H_old[1];
+    d += r[14] - t.H_old[2];
+    res->ddH = d;
+  }
+  res->plaquette = r[16];
+  res->cg_iterations = cg_iters;
+  return SU2B_OK;
+}

@@ -1,0 +1,199 @@
+// metropolis.cu -- checkerboard Metropolis pass (flat-sweep.hh:64-164 update rule).
+//
+// One launch updates every link (x, mu) with parity(x) = p for one direction mu.  Such links
+// share no staple: the staple of U_mu(x) contains U_mu(x +- nu) (opposite parity) and links
+// of other directions only, so all of them update independently and in any order.  A sweep
+// is 2*nd launches.  Per link: staples once (get_staples.hh:26-80), then N_hit proposals
+// U -> U R with R = random_element(delta) (random_element.hh:9-34), dS = beta/Nc (ReTr(U K) -
+// ReTr(U R K)), accept with min(1, exp(-dS)), restoreSU after each accepted hit.  All
+// arithmetic is FP64 whatever the link storage.  Random numbers: one Philox4x32-10 draw per
+// hit, counter {reference link index, hit, sweep, TAG_METRO}: 32-bit uniforms for alpha, u,
+// theta and the accept test.
+#include "su2b_internal.h"
+
+namespace su2b {
+namespace {
+
+template <class T> using LinkT = typename LinkOf<T>::type;
+
+template <class T, int ND, int NT>
+__global__ void __launch_bounds__(NT)
+  k_metro_su2(Geom g, LinkT<T> *__restrict__ U, int mu, int p, double beta_nc, double delta,
+              int N_hit, uint64_t seed, uint32_t sweep, unsigned long long *counts) {
+  __shared__ unsigned int sh_acc;
+  if (threadIdx.x == 0) sh_acc = 0;
+  __syncthreads();
+  const int cb = blockIdx.x * NT + threadIdx.x;
+  unsigned int acc = 0;
+  if (cb < g.Vh) {
+    const Site s = site_from_eo(g, p, cb);
+    // staple sum in FP64
+    const int lpm = s.lex + fwd(g, s, mu);
+    Su2<double> K = zero_su2<double>();
+#pragma unroll
+    for (int nu = 0; nu < ND; nu++) {
+      if (nu == mu) continue;
+      const int lpn = s.lex + fwd(g, s, nu);
+      const Su2<double> A = to64(ld_link_rw(U + (size_t)nu * g.V + eo_of(g, lpm, 1 - p)));
+      const Su2<double> B = to64(ld_link_rw(U + (size_t)mu * g.V + eo_of(g, lpn, 1 - p)));
+      const Su2<double> D = to64(ld_link_rw(U + (size_t)nu * g.V + eo_of(g, s.lex, p)));
+      K = add(K, mul(mul(A, dag(B)), dag(D)));
+    }
+#pragma unroll
+    for (int nu = 0; nu < ND; nu++) {
+      if (nu == mu) continue;
+      const int b = bwd(g, s, nu);
+      const Su2<double> A = to64(ld_link_rw(U + (size_t)nu * g.V + eo_of(g, lpm + b, p)));
+      const Su2<double> B = to64(ld_link_rw(U + (size_t)mu * g.V + eo_of(g, s.lex + b, 1 - p)));
+      const Su2<double> D = to64(ld_link_rw(U + (size_t)nu * g.V + eo_of(g, s.lex + b, 1 - p)));
+      K = add(K, mul(mul(dag(A), dag(B)), D));
+    }
+    const size_t l = (size_t)mu * g.V + (size_t)p * g.Vh + cb;
+    Su2<double> u = to64(ld_link_rw(U + l));
+    const uint32_t lref = (uint32_t)s.lex * (uint32_t)g.nd + (uint32_t)mu;
+    for (int n = 0; n < N_hit; n++) {
+      uint32_t r[4];
+      philox(lref, (uint32_t)n, sweep, TAG_METRO, seed, r);
+      double sa, ca, st, ct;
+      sincospi(2.0 * delta * u01_32(r[0]), &sa, &ca);
+      const double uu = 2.0 * u01_32(r[1]) - 1.0;
+      sincospi(2.0 * u01_32(r[2]), &st, &ct);
+      const double rr = sqrt(1.0 - uu * uu);
+      const Su2<double> R{ca, sa * uu, sa * rr * st, sa * rr * ct};
+      const Su2<double> uR = mul(u, R);
+      const double dS = beta_nc * (retr_mul(u, K) - retr_mul(uR, K));
+      bool a = dS < 0;
+      if (!a) a = u01_32(r[3]) < exp(-dS);
+      if (a) {
+        u = restore_su(uR);
+        acc++;
+      }
+    }
+    st_link(U + l, from64<T>(u));
+  }
+  if (acc) atomicAdd(&sh_acc, acc);
+  __syncthreads();
+  if (threadIdx.x == 0 && sh_acc) {
+    atomicAdd(counts, (unsigned long long)sh_acc);
+    if (mu == 0) atomicAdd(counts + 1, (unsigned long long)sh_acc);
+  }
+}
+
+template <int ND, int NT>
+__global__ void __launch_bounds__(NT)
+  k_metro_u1(Geom g, double *__restrict__ U, int mu, int p, double beta, double delta,
+             int N_hit, uint64_t seed, uint32_t sweep, unsigned long long *counts) {
+  __shared__ unsigned int sh_acc;
+  if (threadIdx.x == 0) sh_acc = 0;
+  __syncthreads();
+  const int cb = blockIdx.x * NT + threadIdx.x;
+  unsigned int acc = 0;
+  if (cb < g.Vh) {
+    const Site s = site_from_eo(g, p, cb);
+    const int lpm = s.lex + fwd(g, s, mu);
+    double Kr = 0., Ki = 0.;
+#pragma unroll
+    for (int nu = 0; nu < ND; nu++) {
+      if (nu == mu) continue;
+      const int lpn = s.lex + fwd(g, s, nu);
+      const double A = U[(size_t)nu * g.V + eo_of(g, lpm, 1 - p)];
+      const double B = U[(size_t)mu * g.V + eo_of(g, lpn, 1 - p)];
+      const double D = U[(size_t)nu * g.V + eo_of(g, s.lex, p)];
+      double sn, cs;
+      sincos((A + (-B)) + (-D), &sn, &cs);
+      Kr += cs;
+      Ki += sn;
+    }
+#pragma unroll
+    for (int nu = 0; nu < ND; nu++) {
+      if (nu == mu) continue;
+      const int b = bwd(g, s, nu);
+      const double A = U[(size_t)nu * g.V + eo_of(g, lpm + b, p)];
+      const double B = U[(size_t)mu * g.V + eo_of(g, s.lex + b, 1 - p)];
+      const double D = U[(size_t)nu * g.V + eo_of(g, s.lex + b, 1 - p)];
+      double sn, cs;
+      sincos(((-A) + (-B)) + D, &sn, &cs);
+      Kr += cs;
+      Ki += sn;
+    }
+    const size_t l = (size_t)mu * g.V + (size_t)p * g.Vh + cb;
+    double u = U[l];
+    const uint32_t lref = (uint32_t)s.lex * (uint32_t)g.nd + (uint32_t)mu;
+    for (int n = 0; n < N_hit; n++) {
+      uint32_t r[4];
+      philox(lref, (uint32_t)n, sweep, TAG_METRO, seed, r);
+      const double th = M_PI * delta * (2.0 * u01_32(r[0]) - 1.0);
+      double s0, c0, s1, c1;
+      sincos(u, &s0, &c0);
+      sincos(u + th, &s1, &c1);
+      const double dS = beta * ((c0 * Kr - s0 * Ki) - (c1 * Kr - s1 * Ki));
+      bool a = dS < 0;
+      if (!a) a = u01_32(r[1]) < exp(-dS);
+      if (a) {
+        u = u + th;
+        acc++;
+      }
+    }
+    U[l] = u;
+  }
+  if (acc) atomicAdd(&sh_acc, acc);
+  __syncthreads();
+  if (threadIdx.x == 0 && sh_acc) {
+    atomicAdd(counts, (unsigned long long)sh_acc);
+    if (mu == 0) atomicAdd(counts + 1, (unsigned long long)sh_acc);
+  }
+}
+
+}  // namespace
+
+template <class T>
+cudaError_t metropolis_pass(const Geom &g, void *U, int group, int mu, int parity, double beta,
+                            double delta, int N_hit, uint64_t seed, uint32_t sweep,
+                            unsigned long long *counts, cudaStream_t s) {
+  constexpr int NT = 128;
+  const int grid = (g.Vh + NT - 1) / NT;
+  if (group == 0) {
+    LinkT<T> *u = (LinkT<T> *)U;
+    const double bn = beta / 2.0;
+    switch (g.nd) {
+      case 2:
+        k_metro_su2<T, 2, NT><<<grid, NT, 0, s>>>(g, u, mu, parity, bn, delta, N_hit, seed,
+                                                  sweep, counts);
+        break;
+      case 3:
+        k_metro_su2<T, 3, NT><<<grid, NT, 0, s>>>(g, u, mu, parity, bn, delta, N_hit, seed,
+                                                  sweep, counts);
+        break;
+      default:
+        k_metro_su2<T, 4, NT><<<grid, NT, 0, s>>>(g, u, mu, parity, bn, delta, N_hit, seed,
+                                                  sweep, counts);
+        break;
+    }
+  } else {
+    double *u = (double *)U;
+    switch (g.nd) {
+      case 2:
+        k_metro_u1<2, NT><<<grid, NT, 0, s>>>(g, u, mu, parity, beta, delta, N_hit, seed, sweep,
+                                              counts);
+        break;
+      case 3:
+        k_metro_u1<3, NT><<<grid, NT, 0, s>>>(g, u, mu, parity, beta, delta, N_hit, seed, sweep,
+                                              counts);
+        break;
+      default:
+        k_metro_u1<4, NT><<<grid, NT, 0, s>>>(g, u, mu, parity, beta, delta, N_hit, seed, sweep,
+                                              counts);
+        break;
+    }
+  }
+  return cudaGetLastError();
+}
+
+template cudaError_t metropolis_pass<double>(const Geom &, void *, int, int, int, double, double,
+                                             int, uint64_t, uint32_t, unsigned long long *,
+                                             cudaStream_t);
+template cudaError_t metropolis_pass<float>(const Geom &, void *, int, int, int, double, double,
+                                            int, uint64_t, uint32_t, unsigned long long *,
+                                            cudaStream_t);
+
+}  // namespace su2b

@@ -1,0 +1,600 @@
+// staggered.cu -- U(1) staggered operator, fermion force and the Krylov-solver kernels.
+//
+// Operator (staggered.hpp:305-389), eta_mu(x) = (-1)^(sum_{nu<mu} x_nu) (staggered.hpp:41-48):
+//   D psi(x)    = m psi(x) + 1/2 sum_mu eta_mu(x) [e^{i th_mu(x)} psi(x+mu)
+//                                                 - e^{-i th_mu(x-mu)} psi(x-mu)]
+//   Ddag psi(x) = m psi(x) - (the same hopping sum)
+// Spinors are complex per site in even/odd order; links enter as a phase field
+// (cos th, sin th) rebuilt whenever the angles change.  Bytes per site and application in
+// FP64: psi in 16 + out 16 + 2*nd phases 16 (plus neighbour re-reads served by L1/L2).
+//
+// Solvers: every kernel below reads a SolverState in device memory and returns at once when
+// the state says the solve has finished, so the host can queue many iterations and read
+// the state back only every few of them.  Scalars (alpha, beta, omega) are computed on the
+// device in FP64 with the reference's complex arithmetic (CG.hpp:51-64,
+// BiCGStab.hpp:49-66).
+#include "su2b_internal.h"
+#include "solver.h"
+
+namespace su2b {
+namespace {
+
+template <class R> struct C2;
+template <> struct C2<double> { typedef double2 type; };
+template <> struct C2<float> { typedef float2 type; };
+
+__device__ __forceinline__ double2 cm(double2 a, double2 b) {
+  return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ double2 cmc(double2 a, double2 b) {  // conj(a) * b
+  return make_double2(a.x * b.x + a.y * b.y, a.x * b.y - a.y * b.x);
+}
+// libgcc's complex division for ordinary magnitudes (Smith, CACM 5 (1962) 435)
+__device__ __forceinline__ double2 cdivs(double2 x, double2 y) {
+  const double a = x.x, b = x.y, c = y.x, d = y.y;
+  if (fabs(c) < fabs(d)) {
+    const double ratio = c / d, denom = (c * ratio) + d;
+    return make_double2(((a * ratio) + b) / denom, ((b * ratio) - a) / denom);
+  }
+  const double ratio = d / c, denom = (d * ratio) + c;
+  return make_double2(((b * ratio) + a) / denom, (b - (a * ratio)) / denom);
+}
+
+__device__ __forceinline__ bool finished(const SolverState *st) {
+  return st != nullptr && st->done != 0;
+}
+
+__global__ void k_phases(size_t NL, const double *__restrict__ th, double2 *ph) {
+  for (size_t l = blockIdx.x * (size_t)blockDim.x + threadIdx.x; l < NL;
+       l += (size_t)gridDim.x * blockDim.x) {
+    double s, c;
+    sincos(th[l], &s, &c);
+    ph[l] = make_double2(c, s);
+  }
+}
+__global__ void k_phases32(size_t NL, const double *__restrict__ th, float2 *ph) {
+  for (size_t l = blockIdx.x * (size_t)blockDim.x + threadIdx.x; l < NL;
+       l += (size_t)gridDim.x * blockDim.x) {
+    double s, c;
+    sincos(th[l], &s, &c);
+    ph[l] = make_float2((float)c, (float)s);
+  }
+}
+
+// out = m*in + sgn*hop(in); optional per-block partial of sum conj(a) * out (dot) and
+// sum |out|^2 (nrm).  gate: skip when the solve finished (or when gate_update says so).
+template <class R, int NT>
+__global__ void __launch_bounds__(NT)
+  k_hop(Geom g, const typename C2<R>::type *__restrict__ ph, R m, R sgn,
+        const typename C2<R>::type *__restrict__ in, typename C2<R>::type *__restrict__ out,
+        const typename C2<R>::type *__restrict__ a, double *dot_part, double *nrm_part,
+        const SolverState *st, int gate_update) {
+  typedef typename C2<R>::type cR;
+  if (finished(st) || (gate_update && !st->do_update)) return;
+  __shared__ double sh[NT / 32];
+  const int p = blockIdx.y;
+  const int cb = blockIdx.x * NT + threadIdx.x;
+  double dr = 0., di = 0., nn = 0.;
+  if (cb < g.Vh) {
+    const Site s = site_from_eo(g, p, cb);
+    R accr = 0, acci = 0;
+    int esum = 0;
+    for (int mu = 0; mu < g.nd; mu++) {
+      const R eta = (esum & 1) ? R(-0.5) : R(0.5);
+      esum += s.c[mu];
+      const int lp = s.lex + fwd(g, s, mu), lm = s.lex + bwd(g, s, mu);
+      const cR up = ph[(size_t)mu * g.V + (size_t)p * g.Vh + cb];
+      const cR um = ph[(size_t)mu * g.V + eo_of(g, lm, 1 - p)];
+      const cR fp = in[eo_of(g, lp, 1 - p)], fm = in[eo_of(g, lm, 1 - p)];
+      // e^{i th(x)} psi(x+mu) - e^{-i th(x-mu)} psi(x-mu)
+      const R tr = (up.x * fp.x - up.y * fp.y) - (um.x * fm.x + um.y * fm.y);
+      const R ti = (up.x * fp.y + up.y * fp.x) - (um.x * fm.y - um.y * fm.x);
+      accr += eta * tr;
+      acci += eta * ti;
+    }
+    const cR self = in[(size_t)p * g.Vh + cb];
+    cR o;
+    o.x = m * self.x + sgn * accr;
+    o.y = m * self.y + sgn * acci;
+    out[(size_t)p * g.Vh + cb] = o;
+    if (dot_part) {
+      const cR av = a[(size_t)p * g.Vh + cb];
+      dr = (double)av.x * o.x + (double)av.y * o.y;
+      di = (double)av.x * o.y - (double)av.y * o.x;
+    }
+    if (nrm_part) nn = (double)o.x * o.x + (double)o.y * o.y;
+  }
+  const int b = blockIdx.y * gridDim.x + blockIdx.x;
+  if (dot_part) {
+    double r = block_sum<NT>(dr, sh);
+    if (threadIdx.x == 0) dot_part[2 * b] = r;
+    r = block_sum<NT>(di, sh);
+    if (threadIdx.x == 0) dot_part[2 * b + 1] = r;
+  }
+  if (nrm_part) {
+    const double r = block_sum<NT>(nn, sh);
+    if (threadIdx.x == 0) nrm_part[b] = r;
+  }
+}
+
+// fermion force per link (detDDdag_monomial.hh:124-164)
+__global__ void k_fforce(Geom g, const double2 *__restrict__ ph, const double2 *__restrict__ chi,
+                         const double2 *__restrict__ chi1, double *deriv) {
+  const int mu = blockIdx.y >> 1, p = blockIdx.y & 1;
+  const int cb = blockIdx.x * blockDim.x + threadIdx.x;
+  if (cb >= g.Vh) return;
+  const Site s = site_from_eo(g, p, cb);
+  int esum = 0;
+  for (int nu = 0; nu < mu; nu++) esum += s.c[nu];
+  const double eta = (esum & 1) ? -1.0 : 1.0;
+  const size_t l = (size_t)mu * g.V + (size_t)p * g.Vh + cb;
+  const int sx = p * g.Vh + cb, sp = eo_of(g, s.lex + fwd(g, s, mu), 1 - p);
+  const double2 u = ph[l], ud = make_double2(u.x, -u.y);
+  // v_xp = (1/2 eta i) U chi1(x+mu);  v_x = (-1/2 eta (-i)) U^+ chi1(x)
+  const double2 v_xp = cm(cm(make_double2(0.0, 0.5 * eta), u), chi1[sp]);
+  const double2 v_x = cm(cm(make_double2(0.0, 0.5 * eta), ud), chi1[sx]);
+  const double2 d = make_double2(cmc(chi[sx], v_xp).x + cmc(chi[sp], v_x).x,
+                                 cmc(chi[sx], v_xp).y + cmc(chi[sp], v_x).y);
+  // get_deriv(-2 i d) = Im(-2 i d) = -2 Re d
+  deriv[l] = -2.0 * d.x;
+}
+
+__global__ void k_pf_source(Geom g, uint64_t seed, uint32_t traj, int cplx, double2 *R) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < g.V; i += gridDim.x * blockDim.x) {
+    const Site s = site_from_lex(g, i);
+    uint32_t r[4];
+    philox((uint32_t)i, 0u, traj, TAG_PF, seed, r);
+    double n0, n1;
+    box_muller(u01_53(r[0], r[1]), u01_53(r[2], r[3]), n0, n1);
+    const double sg = 0.7071067811865476;  // 1/sqrt(2)
+    R[eo_of(g, i, s.p)] = make_double2(sg * n0, cplx ? sg * n1 : 0.0);
+  }
+}
+
+// ---------------- solver scalar steps (one block) ----------------
+template <int NT>
+__device__ __forceinline__ double2 sum2(const double *part, int n, double *sh) {
+  double a = 0., b = 0.;
+  for (int i = threadIdx.x; i < n; i += NT) {
+    a += part[2 * i];
+    b += part[2 * i + 1];
+  }
+  const double ra = block_sum<NT>(a, sh);
+  const double rb = block_sum<NT>(b, sh);
+  return make_double2(ra, rb);
+}
+template <int NT>
+__device__ __forceinline__ double sum1(const double *part, int n, double *sh) {
+  double a = 0.;
+  for (int i = threadIdx.x; i < n; i += NT) a += part[i];
+  return block_sum<NT>(a, sh);
+}
+
+__device__ __forceinline__ void check_iter(SolverState *st) {
+  st->iters++;
+  if (st->rn != st->rn) st->done = 3;
+  else if (!(st->rn > st->tol)) st->done = 1;
+  else if (st->iters >= st->max_iter) st->done = 2;
+}
+
+// CG: alpha = rr / <p, A p>
+template <int NT> __global__ void k_cg_alpha(const double *part, int n, SolverState *st) {
+  if (finished(st)) return;
+  __shared__ double sh[NT / 32];
+  const double2 pAp = sum2<NT>(part, n, sh);
+  if (threadIdx.x == 0) st->alpha = cdivs(st->rr, pAp);
+}
+// CG: rr_new = <r, r>; beta = rr_new / rr; rr = rr_new; rn = |r|
+template <int NT> __global__ void k_cg_beta(const double *part, int n, SolverState *st) {
+  if (finished(st)) return;
+  __shared__ double sh[NT / 32];
+  const double rr = sum1<NT>(part, n, sh);
+  if (threadIdx.x == 0) {
+    const double2 rrn = make_double2(rr, 0.0);
+    st->beta = cdivs(rrn, st->rr);
+    st->rr = rrn;
+    st->rn = sqrt(rr);
+    check_iter(st);
+  }
+}
+
+// x += alpha p; r -= alpha Ap; partial |r|^2
+template <int NT>
+__global__ void __launch_bounds__(NT)
+  k_cg_xr(int n, double2 *__restrict__ x, double2 *__restrict__ r, const double2 *__restrict__ p,
+          const double2 *__restrict__ Ap, const SolverState *st, double *part) {
+  if (finished(st)) return;
+  __shared__ double sh[NT / 32];
+  const double2 al = st->alpha;
+  double nn = 0.;
+  for (int i = blockIdx.x * NT + threadIdx.x; i < n; i += gridDim.x * NT) {
+    const double2 ap = cm(al, p[i]), aq = cm(al, Ap[i]);
+    x[i] = make_double2(x[i].x + 1.0 * ap.x, x[i].y + 1.0 * ap.y);
+    const double2 rn = make_double2(r[i].x + (-1.0) * aq.x, r[i].y + (-1.0) * aq.y);
+    r[i] = rn;
+    nn += rn.x * rn.x + rn.y * rn.y;
+  }
+  const double t = block_sum<NT>(nn, sh);
+  if (threadIdx.x == 0) part[blockIdx.x] = t;
+}
+// p = r + beta p
+__global__ void k_cg_p(int n, const double2 *__restrict__ r, double2 *__restrict__ p,
+                       const SolverState *st) {
+  if (finished(st)) return;
+  const double2 be = st->beta;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const double2 bp = cm(be, p[i]);
+    p[i] = make_double2(r[i].x + 1.0 * bp.x, r[i].y + 1.0 * bp.y);
+  }
+}
+
+// ---- BiCGStab ----
+template <int NT> __global__ void k_bi_alpha(const double *part, int n, SolverState *st) {
+  if (finished(st)) return;
+  __shared__ double sh[NT / 32];
+  const double2 r0Ap = sum2<NT>(part, n, sh);
+  if (threadIdx.x == 0) st->alpha = cdivs(st->r0r, r0Ap);
+}
+__global__ void k_bi_s(int n, const double2 *__restrict__ r, const double2 *__restrict__ Ap,
+                       double2 *__restrict__ s, const SolverState *st) {
+  if (finished(st)) return;
+  const double2 al = st->alpha;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const double2 aq = cm(al, Ap[i]);
+    s[i] = make_double2(r[i].x + (-1.0) * aq.x, r[i].y + (-1.0) * aq.y);
+  }
+}
+// omega = <t, s> / <t, t>; partials: tpart = <s-side dot> written by k_hop with a = t?
+// k_hop writes sum conj(a) out with a = s, out = t  ->  <s, t>; <t, s> = conj(<s, t>)
+template <int NT>
+__global__ void k_bi_omega(const double *dpart, const double *npart, int n, SolverState *st) {
+  if (finished(st)) return;
+  __shared__ double sh[NT / 32];
+  const double2 st_ = sum2<NT>(dpart, n, sh);
+  const double tt = sum1<NT>(npart, n, sh);
+  if (threadIdx.x == 0) st->omega = cdivs(make_double2(st_.x, -st_.y), make_double2(tt, 0.0));
+}
+// r = s - omega t; x = x + omega s + alpha p; partials <r0, r>, |r|^2
+template <int NT>
+__global__ void __launch_bounds__(NT)
+  k_bi_rx(int n, double2 *__restrict__ x, double2 *__restrict__ r, const double2 *__restrict__ s,
+          const double2 *__restrict__ t, const double2 *__restrict__ p,
+          const double2 *__restrict__ r0, const SolverState *st, double *dpart, double *npart) {
+  if (finished(st)) return;
+  __shared__ double sh[NT / 32];
+  const double2 om = st->omega, al = st->alpha;
+  double dr = 0., di = 0., nn = 0.;
+  for (int i = blockIdx.x * NT + threadIdx.x; i < n; i += gridDim.x * NT) {
+    const double2 ot = cm(om, t[i]);
+    const double2 rn = make_double2(s[i].x + (-1.0) * ot.x, s[i].y + (-1.0) * ot.y);
+    r[i] = rn;
+    const double2 os = cm(om, s[i]), ap = cm(al, p[i]);
+    const double2 x1 = make_double2(x[i].x + 1.0 * os.x, x[i].y + 1.0 * os.y);
+    x[i] = make_double2(x1.x + 1.0 * ap.x, x1.y + 1.0 * ap.y);
+    const double2 d = cmc(r0[i], rn);
+    dr += d.x;
+    di += d.y;
+    nn += rn.x * rn.x + rn.y * rn.y;
+  }
+  const int b = blockIdx.x;
+  double q = block_sum<NT>(dr, sh);
+  if (threadIdx.x == 0) dpart[2 * b] = q;
+  q = block_sum<NT>(di, sh);
+  if (threadIdx.x == 0) dpart[2 * b + 1] = q;
+  q = block_sum<NT>(nn, sh);
+  if (threadIdx.x == 0) npart[b] = q;
+}
+template <int NT>
+__global__ void k_bi_beta(const double *dpart, const double *npart, int n, SolverState *st) {
+  if (finished(st)) return;
+  __shared__ double sh[NT / 32];
+  const double2 r0r = sum2<NT>(dpart, n, sh);
+  const double rr = sum1<NT>(npart, n, sh);
+  if (threadIdx.x == 0) {
+    st->beta = cm(cdivs(r0r, st->r0r), cdivs(st->alpha, st->omega));
+    st->r0r = r0r;
+    st->rn = sqrt(rr);
+    check_iter(st);
+  }
+}
+// p = r + beta p - (beta omega) Ap
+__global__ void k_bi_p(int n, const double2 *__restrict__ r, double2 *__restrict__ p,
+                       const double2 *__restrict__ Ap, const SolverState *st) {
+  if (finished(st)) return;
+  const double2 be = st->beta, bo = cm(st->beta, st->omega);
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const double2 bp = cm(be, p[i]), bq = cm(bo, Ap[i]);
+    const double2 t = make_double2(r[i].x + 1.0 * bp.x, r[i].y + 1.0 * bp.y);
+    p[i] = make_double2(t.x + (-1.0) * bq.x, t.y + (-1.0) * bq.y);
+  }
+}
+
+// ---- mixed-precision CG (FP32 iterations, FP64 reliable updates) ----
+// xs += alpha ps; rs -= alpha Aps; partial |rs|^2
+template <int NT>
+__global__ void __launch_bounds__(NT)
+  k_m_xr(int n, float2 *__restrict__ xs, float2 *__restrict__ rs, const float2 *__restrict__ ps,
+         const float2 *__restrict__ Aps, const SolverState *st, double *part) {
+  if (finished(st)) return;
+  __shared__ double sh[NT / 32];
+  const float ar = (float)st->alpha.x, ai = (float)st->alpha.y;
+  double nn = 0.;
+  for (int i = blockIdx.x * NT + threadIdx.x; i < n; i += gridDim.x * NT) {
+    const float2 pv = ps[i], qv = Aps[i];
+    float2 xv = xs[i], rv = rs[i];
+    xv.x += ar * pv.x - ai * pv.y;
+    xv.y += ar * pv.y + ai * pv.x;
+    rv.x -= ar * qv.x - ai * qv.y;
+    rv.y -= ar * qv.y + ai * qv.x;
+    xs[i] = xv;
+    rs[i] = rv;
+    nn += (double)rv.x * rv.x + (double)rv.y * rv.y;
+  }
+  const double t = block_sum<NT>(nn, sh);
+  if (threadIdx.x == 0) part[blockIdx.x] = t;
+}
+// decide on a reliable update: iterated |rs| fell below delta * (|r| at the last update) or
+// below the tolerance (then the true residual decides convergence)
+template <int NT> __global__ void k_m_check(const double *part, int n, SolverState *st) {
+  if (finished(st)) return;
+  __shared__ double sh[NT / 32];
+  const double rr = sum1<NT>(part, n, sh);
+  if (threadIdx.x == 0) {
+    st->rr_new = rr;
+    st->rn = sqrt(rr);
+    st->iters++;
+    st->do_update = (st->rn < st->delta * st->maxr || !(st->rn > st->tol)) ? 1 : 0;
+    if (st->rn != st->rn) st->done = 3;
+    else if (!st->do_update && st->iters >= st->max_iter) st->done = 2;
+  }
+}
+// x += xs; xs = 0 (only on a reliable update)
+__global__ void k_m_accum(int n, double2 *__restrict__ x, float2 *__restrict__ xs,
+                          const SolverState *st) {
+  if (finished(st) || !st->do_update) return;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const float2 v = xs[i];
+    x[i] = make_double2(x[i].x + (double)v.x, x[i].y + (double)v.y);
+    xs[i] = make_float2(0.f, 0.f);
+  }
+}
+// r = b - Ax (FP64); rs = (float) r; partial |r|^2
+template <int NT>
+__global__ void __launch_bounds__(NT)
+  k_m_resid(int n, const double2 *__restrict__ b, const double2 *__restrict__ Ax,
+            double2 *__restrict__ r, float2 *__restrict__ rs, const SolverState *st,
+            double *part) {
+  if (finished(st) || !st->do_update) return;
+  __shared__ double sh[NT / 32];
+  double nn = 0.;
+  for (int i = blockIdx.x * NT + threadIdx.x; i < n; i += gridDim.x * NT) {
+    const double2 v = make_double2(b[i].x - Ax[i].x, b[i].y - Ax[i].y);
+    r[i] = v;
+    rs[i] = make_float2((float)v.x, (float)v.y);
+    nn += v.x * v.x + v.y * v.y;
+  }
+  const double t = block_sum<NT>(nn, sh);
+  if (threadIdx.x == 0) part[blockIdx.x] = t;
+}
+template <int NT> __global__ void k_m_after(const double *part, int n, SolverState *st) {
+  if (finished(st) || !st->do_update) return;
+  __shared__ double sh[NT / 32];
+  const double rr = sum1<NT>(part, n, sh);
+  if (threadIdx.x == 0) {
+    st->rr_new = rr;
+    st->rn = sqrt(rr);
+    st->maxr = st->rn;
+    st->updates++;
+    if (!(st->rn > st->tol)) st->done = 1;
+    else if (st->iters >= st->max_iter) st->done = 2;
+  }
+}
+// beta = rr_new / rr; ps = rs + beta ps; rr = rr_new
+__global__ void k_m_p(int n, const float2 *__restrict__ rs, float2 *__restrict__ ps,
+                      SolverState *st) {
+  if (finished(st)) return;
+  const double be = st->rr_new / st->rr.x;
+  const float b = (float)be;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const float2 r = rs[i], p = ps[i];
+    ps[i] = make_float2(r.x + b * p.x, r.y + b * p.y);
+  }
+}
+// rr = rr_new, in its own launch so that no block of k_m_p can read the new value
+__global__ void k_m_commit(SolverState *st) {
+  if (finished(st)) return;
+  st->rr = make_double2(st->rr_new, 0.0);
+}
+
+// r = b + (-1)*Ax (a_plus_lambda_b, staggered.hpp:144-154); partial |r|^2
+template <int NT>
+__global__ void __launch_bounds__(NT)
+  k_resid64(int n, const double2 *__restrict__ b, const double2 *__restrict__ Ax,
+            double2 *__restrict__ r, double *part) {
+  __shared__ double sh[NT / 32];
+  double nn = 0.;
+  for (int i = blockIdx.x * NT + threadIdx.x; i < n; i += gridDim.x * NT) {
+    const double2 v = make_double2(b[i].x + (-1.0) * Ax[i].x, b[i].y + (-1.0) * Ax[i].y);
+    r[i] = v;
+    nn += v.x * v.x + v.y * v.y;
+  }
+  const double t = block_sum<NT>(nn, sh);
+  if (threadIdx.x == 0) part[blockIdx.x] = t;
+}
+__global__ void k_to32(int n, const double2 *__restrict__ a, float2 *__restrict__ b) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    b[i] = make_float2((float)a[i].x, (float)a[i].y);
+}
+// sum conj(a) b, partials
+template <int NT>
+__global__ void __launch_bounds__(NT)
+  k_dot64(int n, const double2 *__restrict__ a, const double2 *__restrict__ b, double *part) {
+  __shared__ double sh[NT / 32];
+  double dr = 0., di = 0.;
+  for (int i = blockIdx.x * NT + threadIdx.x; i < n; i += gridDim.x * NT) {
+    const double2 d = cmc(a[i], b[i]);
+    dr += d.x;
+    di += d.y;
+  }
+  double t = block_sum<NT>(dr, sh);
+  if (threadIdx.x == 0) part[2 * blockIdx.x] = t;
+  t = block_sum<NT>(di, sh);
+  if (threadIdx.x == 0) part[2 * blockIdx.x + 1] = t;
+}
+
+}  // namespace
+
+// ===================================================================================
+cudaError_t u1_phases(const Geom &g, const double *theta, double2 *ph, cudaStream_t s) {
+  const size_t NL = (size_t)g.V * g.nd;
+  k_phases<<<(int)((NL + 255) / 256), 256, 0, s>>>(NL, theta, ph);
+  return cudaGetLastError();
+}
+cudaError_t u1_phases_f32(const Geom &g, const double *theta, float2 *ph, cudaStream_t s) {
+  const size_t NL = (size_t)g.V * g.nd;
+  k_phases32<<<(int)((NL + 255) / 256), 256, 0, s>>>(NL, theta, ph);
+  return cudaGetLastError();
+}
+
+constexpr int NT_H = 128;
+static dim3 hop_grid(const Geom &g) { return dim3((g.Vh + NT_H - 1) / NT_H, 2); }
+int hop_blocks(const Geom &g) {
+  const dim3 d = hop_grid(g);
+  return d.x * d.y;
+}
+
+cudaError_t staggered_D(const Geom &g, const double2 *ph, double m, int dag, const double2 *in,
+                        double2 *out, cudaStream_t s) {
+  k_hop<double, NT_H><<<hop_grid(g), NT_H, 0, s>>>(g, ph, m, dag ? -1.0 : 1.0, in, out, nullptr,
+                                                   nullptr, nullptr, nullptr, 0);
+  return cudaGetLastError();
+}
+cudaError_t staggered_D(const Geom &g, const float2 *ph, float m, int dag, const float2 *in,
+                        float2 *out, cudaStream_t s) {
+  k_hop<float, NT_H><<<hop_grid(g), NT_H, 0, s>>>(g, ph, m, dag ? -1.f : 1.f, in, out, nullptr,
+                                                  nullptr, nullptr, nullptr, 0);
+  return cudaGetLastError();
+}
+cudaError_t hop64(const Geom &g, const double2 *ph, double m, int dag, const double2 *in,
+                  double2 *out, const double2 *a, double *dpart, double *npart,
+                  const SolverState *st, int gate_update, cudaStream_t s) {
+  k_hop<double, NT_H><<<hop_grid(g), NT_H, 0, s>>>(g, ph, m, dag ? -1.0 : 1.0, in, out, a,
+                                                   dpart, npart, st, gate_update);
+  return cudaGetLastError();
+}
+cudaError_t hop32(const Geom &g, const float2 *ph, float m, int dag, const float2 *in,
+                  float2 *out, const float2 *a, double *dpart, double *npart,
+                  const SolverState *st, cudaStream_t s) {
+  k_hop<float, NT_H><<<hop_grid(g), NT_H, 0, s>>>(g, ph, m, dag ? -1.f : 1.f, in, out, a, dpart,
+                                                  npart, st, 0);
+  return cudaGetLastError();
+}
+
+cudaError_t fermion_force(const Geom &g, const double2 *ph, const double2 *chi,
+                          const double2 *chi1, double *deriv, cudaStream_t s) {
+  const dim3 grid((g.Vh + 127) / 128, 2 * g.nd);
+  k_fforce<<<grid, 128, 0, s>>>(g, ph, chi, chi1, deriv);
+  return cudaGetLastError();
+}
+cudaError_t pf_source(const Geom &g, uint64_t seed, uint32_t traj, int complex_source,
+                      double2 *R, cudaStream_t s) {
+  k_pf_source<<<(g.V + 255) / 256, 256, 0, s>>>(g, seed, traj, complex_source, R);
+  return cudaGetLastError();
+}
+
+constexpr int NT_V = 256;
+int vec_blocks(int n) {
+  const int b = (n + NT_V - 1) / NT_V;
+  return b < 1184 ? b : 1184;  // 148 SMs x 8
+}
+
+cudaError_t cg_alpha(const double *part, int n, SolverState *st, cudaStream_t s) {
+  k_cg_alpha<512><<<1, 512, 0, s>>>(part, n, st);
+  return cudaGetLastError();
+}
+cudaError_t cg_xr(int n, double2 *x, double2 *r, const double2 *p, const double2 *Ap,
+                  const SolverState *st, double *part, cudaStream_t s) {
+  k_cg_xr<NT_V><<<vec_blocks(n), NT_V, 0, s>>>(n, x, r, p, Ap, st, part);
+  return cudaGetLastError();
+}
+cudaError_t cg_beta(const double *part, int n, SolverState *st, cudaStream_t s) {
+  k_cg_beta<512><<<1, 512, 0, s>>>(part, n, st);
+  return cudaGetLastError();
+}
+cudaError_t cg_p(int n, const double2 *r, double2 *p, const SolverState *st, cudaStream_t s) {
+  k_cg_p<<<vec_blocks(n), NT_V, 0, s>>>(n, r, p, st);
+  return cudaGetLastError();
+}
+cudaError_t bi_alpha(const double *part, int n, SolverState *st, cudaStream_t s) {
+  k_bi_alpha<512><<<1, 512, 0, s>>>(part, n, st);
+  return cudaGetLastError();
+}
+cudaError_t bi_s(int n, const double2 *r, const double2 *Ap, double2 *sv, const SolverState *st,
+                 cudaStream_t s) {
+  k_bi_s<<<vec_blocks(n), NT_V, 0, s>>>(n, r, Ap, sv, st);
+  return cudaGetLastError();
+}
+cudaError_t bi_omega(const double *dpart, const double *npart, int n, SolverState *st,
+                     cudaStream_t s) {
+  k_bi_omega<512><<<1, 512, 0, s>>>(dpart, npart, n, st);
+  return cudaGetLastError();
+}
+cudaError_t bi_rx(int n, double2 *x, double2 *r, const double2 *sv, const double2 *t,
+                  const double2 *p, const double2 *r0, const SolverState *st, double *dpart,
+                  double *npart, cudaStream_t s) {
+  k_bi_rx<NT_V><<<vec_blocks(n), NT_V, 0, s>>>(n, x, r, sv, t, p, r0, st, dpart, npart);
+  return cudaGetLastError();
+}
+cudaError_t bi_beta(const double *dpart, const double *npart, int n, SolverState *st,
+                    cudaStream_t s) {
+  k_bi_beta<512><<<1, 512, 0, s>>>(dpart, npart, n, st);
+  return cudaGetLastError();
+}
+cudaError_t bi_p(int n, const double2 *r, double2 *p, const double2 *Ap, const SolverState *st,
+                 cudaStream_t s) {
+  k_bi_p<<<vec_blocks(n), NT_V, 0, s>>>(n, r, p, Ap, st);
+  return cudaGetLastError();
+}
+cudaError_t m_xr(int n, float2 *xs, float2 *rs, const float2 *ps, const float2 *Aps,
+                 const SolverState *st, double *part, cudaStream_t s) {
+  k_m_xr<NT_V><<<vec_blocks(n), NT_V, 0, s>>>(n, xs, rs, ps, Aps, st, part);
+  return cudaGetLastError();
+}
+cudaError_t m_check(const double *part, int n, SolverState *st, cudaStream_t s) {
+  k_m_check<512><<<1, 512, 0, s>>>(part, n, st);
+  return cudaGetLastError();
+}
+cudaError_t m_accum(int n, double2 *x, float2 *xs, const SolverState *st, cudaStream_t s) {
+  k_m_accum<<<vec_blocks(n), NT_V, 0, s>>>(n, x, xs, st);
+  return cudaGetLastError();
+}
+cudaError_t m_resid(int n, const double2 *b, const double2 *Ax, double2 *r, float2 *rs,
+                    const SolverState *st, double *part, cudaStream_t s) {
+  k_m_resid<NT_V><<<vec_blocks(n), NT_V, 0, s>>>(n, b, Ax, r, rs, st, part);
+  return cudaGetLastError();
+}
+cudaError_t m_after(const double *part, int n, SolverState *st, cudaStream_t s) {
+  k_m_after<512><<<1, 512, 0, s>>>(part, n, st);
+  return cudaGetLastError();
+}
+cudaError_t m_p(int n, const float2 *rs, float2 *ps, SolverState *st, cudaStream_t s) {
+  k_m_p<<<vec_blocks(n), NT_V, 0, s>>>(n, rs, ps, st);
+  k_m_commit<<<1, 1, 0, s>>>(st);
+  return cudaGetLastError();
+}
+
+cudaError_t resid64(int n, const double2 *b, const double2 *Ax, double2 *r, double *part,
+                    cudaStream_t s) {
+  k_resid64<NT_V><<<vec_blocks(n), NT_V, 0, s>>>(n, b, Ax, r, part);
+  return cudaGetLastError();
+}
+cudaError_t to32(int n, const double2 *a, float2 *b, cudaStream_t s) {
+  k_to32<<<vec_blocks(n), NT_V, 0, s>>>(n, a, b);
+  return cudaGetLastError();
+}
+cudaError_t dot64(int n, const double2 *a, const double2 *b, double *part, cudaStream_t s) {
+  k_dot64<NT_V><<<vec_blocks(n), NT_V, 0, s>>>(n, a, b, part);
+  return cudaGetLastError();
+}
+
+}  // namespace su2b

@@ -1,0 +1,281 @@
+// su2b_common.cuh -- device-side building blocks shared by every kernel of libsu2b.
+//
+// Data layout in HBM (one lattice):
+//   site order  : even/odd.  eo(x) = parity(x)*V/2 + lex(x)/2 where
+//                 lex(x) = ((t*Lx + x)*Ly + y)*Lz + z is the reference's site order
+//                 (gaugeconfig.hh:211-222) and parity(x) = (t+x+y+z) mod 2.
+//   links       : U[mu*V + eo(x)]; SU(2) as 4 reals {Re a, Im a, Re b, Im b}
+//                 (su2.hh:11-70, U = [[a, b], [-b*, a*]]): 32 B (FP64) or 16 B (FP32);
+//                 U(1) as one angle (u1.hh:58).
+//   adjoint     : structure of arrays P_k[mu*V + eo(x)], k = 0..2 for SU(2)
+//                 (adjointsu2 {a, b, c}, adjointfield.hh:12-51), k = 0 for U(1).
+//   spinors     : complex per site in eo order (staggered, U(1) only).
+// All active extents must be even so that the pair {2k, 2k+1} of lexicographic sites has
+// opposite parities and the checkerboard is consistent across the periodic boundary.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace su2b {
+
+// ------------------------------------------------------------------------------------
+// integer division by a runtime constant, valid for numerators below 2^31:
+// q = umulhi(n, m) >> s with m = ceil(2^(31+l)/d), l = ceil(log2 d), s = l - 1.
+struct FastDiv {
+  uint32_t d, m, s;
+};
+
+inline FastDiv make_fastdiv(uint32_t d) {
+  FastDiv f{d, 0u, 0u};
+  if (d <= 1) return f;
+  uint32_t l = 0;
+  while ((1ull << l) < d) l++;
+  const unsigned __int128 num = (unsigned __int128)1 << (31 + l);
+  f.m = (uint32_t)((num + d - 1) / d);
+  f.s = l - 1;
+  return f;
+}
+
+__device__ __forceinline__ uint32_t fdiv(uint32_t n, const FastDiv &f) {
+  return f.m ? (__umulhi(n, f.m) >> f.s) : n;
+}
+
+// ------------------------------------------------------------------------------------
+struct Geom {
+  int nd;       // number of active directions (2..4)
+  int L[4];     // extents by direction: 0 = t, 1 = x, 2 = y, 3 = z (1 if inactive)
+  int st[4];    // lexicographic stride of each direction (st[3] = 1)
+  int V, Vh;    // volume, half volume
+  FastDiv dv[4];
+};
+
+// a site held in registers: coordinates, lexicographic index and parity
+struct Site {
+  int c[4];
+  int lex;
+  int p;
+};
+
+__device__ __forceinline__ Site site_from_eo(const Geom &g, int p, int cb) {
+  Site s;
+  const uint32_t lex0 = 2u * (uint32_t)cb;
+  uint32_t q = lex0;
+#pragma unroll
+  for (int k = 3; k >= 1; k--) {
+    const uint32_t qq = fdiv(q, g.dv[k]);
+    s.c[k] = (int)(q - qq * (uint32_t)g.L[k]);
+    q = qq;
+  }
+  s.c[0] = (int)q;
+  s.lex = (int)lex0;
+  if (((s.c[0] + s.c[1] + s.c[2] + s.c[3]) & 1) != p) {
+    s.c[g.nd - 1] += 1;  // fastest active direction, stride 1, even extent
+    s.lex += 1;
+  }
+  s.p = p;
+  return s;
+}
+
+__device__ __forceinline__ Site site_from_lex(const Geom &g, int lex) {
+  Site s;
+  uint32_t q = (uint32_t)lex;
+#pragma unroll
+  for (int k = 3; k >= 1; k--) {
+    const uint32_t qq = fdiv(q, g.dv[k]);
+    s.c[k] = (int)(q - qq * (uint32_t)g.L[k]);
+    q = qq;
+  }
+  s.c[0] = (int)q;
+  s.lex = lex;
+  s.p = (s.c[0] + s.c[1] + s.c[2] + s.c[3]) & 1;
+  return s;
+}
+
+// lexicographic offset of the forward / backward neighbour in direction mu (periodic)
+__device__ __forceinline__ int fwd(const Geom &g, const Site &s, int mu) {
+  return s.c[mu] == g.L[mu] - 1 ? -(g.L[mu] - 1) * g.st[mu] : g.st[mu];
+}
+__device__ __forceinline__ int bwd(const Geom &g, const Site &s, int mu) {
+  return s.c[mu] == 0 ? (g.L[mu] - 1) * g.st[mu] : -g.st[mu];
+}
+// even/odd index of the site with lexicographic index lex and parity p
+__device__ __forceinline__ int eo_of(const Geom &g, int lex, int p) {
+  return p * g.Vh + (lex >> 1);
+}
+
+// ------------------------------------------------------------------------------------
+// storage types
+struct __align__(32) Link64 {
+  double ar, ai, br, bi;
+};
+typedef float4 Link32;
+
+template <class T> struct LinkOf;
+template <> struct LinkOf<double> { typedef Link64 type; };
+template <> struct LinkOf<float> { typedef Link32 type; };
+
+template <class T> struct Su2 {
+  T ar, ai, br, bi;
+};
+
+__device__ __forceinline__ Su2<double> ld_link(const Link64 *p) {
+  Su2<double> r;
+  asm volatile("ld.global.nc.v4.f64 {%0,%1,%2,%3}, [%4];"
+               : "=d"(r.ar), "=d"(r.ai), "=d"(r.br), "=d"(r.bi)
+               : "l"(p));
+  return r;
+}
+// coherent load (for kernels that also write the links they read)
+__device__ __forceinline__ Su2<double> ld_link_rw(const Link64 *p) {
+  Su2<double> r;
+  asm volatile("ld.global.v4.f64 {%0,%1,%2,%3}, [%4];"
+               : "=d"(r.ar), "=d"(r.ai), "=d"(r.br), "=d"(r.bi)
+               : "l"(p));
+  return r;
+}
+__device__ __forceinline__ void st_link(Link64 *p, const Su2<double> &u) {
+  asm volatile("st.global.v4.f64 [%0], {%1,%2,%3,%4};" ::"l"(p), "d"(u.ar), "d"(u.ai),
+               "d"(u.br), "d"(u.bi)
+               : "memory");
+}
+__device__ __forceinline__ Su2<float> ld_link(const Link32 *p) {
+  const float4 v = __ldg(p);
+  return Su2<float>{v.x, v.y, v.z, v.w};
+}
+__device__ __forceinline__ Su2<float> ld_link_rw(const Link32 *p) {
+  const float4 v = *p;
+  return Su2<float>{v.x, v.y, v.z, v.w};
+}
+__device__ __forceinline__ void st_link(Link32 *p, const Su2<float> &u) {
+  *p = make_float4(u.ar, u.ai, u.br, u.bi);
+}
+
+template <class T> __device__ __forceinline__ Su2<double> to64(const Su2<T> &u) {
+  return Su2<double>{(double)u.ar, (double)u.ai, (double)u.br, (double)u.bi};
+}
+template <class T> __device__ __forceinline__ Su2<T> from64(const Su2<double> &u) {
+  return Su2<T>{(T)u.ar, (T)u.ai, (T)u.br, (T)u.bi};
+}
+
+// ------------------------------------------------------------------------------------
+// SU(2) algebra in the (a, b) form (su2.hh:87-113).  u*v:
+//   a = u.a v.a - u.b conj(v.b),  b = u.a v.b + u.b conj(v.a)
+template <class T> __device__ __forceinline__ Su2<T> mul(const Su2<T> &u, const Su2<T> &v) {
+  Su2<T> r;
+  r.ar = u.ar * v.ar - u.ai * v.ai - (u.br * v.br + u.bi * v.bi);
+  r.ai = u.ar * v.ai + u.ai * v.ar - (u.bi * v.br - u.br * v.bi);
+  r.br = u.ar * v.br - u.ai * v.bi + (u.br * v.ar + u.bi * v.ai);
+  r.bi = u.ar * v.bi + u.ai * v.br + (u.bi * v.ar - u.br * v.ai);
+  return r;
+}
+template <class T> __device__ __forceinline__ Su2<T> dag(const Su2<T> &u) {
+  return Su2<T>{u.ar, -u.ai, -u.br, -u.bi};
+}
+template <class T> __device__ __forceinline__ Su2<T> add(const Su2<T> &u, const Su2<T> &v) {
+  return Su2<T>{u.ar + v.ar, u.ai + v.ai, u.br + v.br, u.bi + v.bi};
+}
+template <class T> __device__ __forceinline__ Su2<T> scale(T s, const Su2<T> &u) {
+  return Su2<T>{s * u.ar, s * u.ai, s * u.br, s * u.bi};
+}
+template <class T> __device__ __forceinline__ T retr(const Su2<T> &u) { return T(2) * u.ar; }
+// ReTr(u*v) = 2 Re(u.a v.a - u.b conj(v.b))
+template <class T> __device__ __forceinline__ T retr_mul(const Su2<T> &u, const Su2<T> &v) {
+  return T(2) * (u.ar * v.ar - u.ai * v.ai - (u.br * v.br + u.bi * v.bi));
+}
+template <class T> __device__ __forceinline__ Su2<T> zero_su2() { return Su2<T>{0, 0, 0, 0}; }
+
+// restoreSU (su2.hh:62-66), always evaluated in FP64
+__device__ __forceinline__ Su2<double> restore_su(const Su2<double> &u) {
+  const double r = sqrt(u.ar * u.ar + u.ai * u.ai + u.br * u.br + u.bi * u.bi);
+  const double ir = 1.0 / r;
+  return Su2<double>{u.ar * ir, u.ai * ir, u.br * ir, u.bi * ir};
+}
+
+// exp of an algebra element (exp_gauge.cc:8-18): alpha = |x|, n = x/alpha,
+// exp = (cos alpha + i sin(alpha) n2, sin(alpha) (n1 + i n0)).  At alpha = 0 the reference
+// divides 0/0; here the limit (the identity) is returned.
+__device__ __forceinline__ Su2<double> exp_alg(double a, double b, double c) {
+  const double alpha = sqrt(a * a + b * b + c * c);
+  double s, co;
+  sincos(alpha, &s, &co);
+  const double f = alpha > 0.0 ? s / alpha : 1.0;
+  return Su2<double>{co, f * c, f * b, f * a};
+}
+__device__ __forceinline__ Su2<float> exp_alg(float a, float b, float c) {
+  const float alpha = sqrtf(a * a + b * b + c * c);
+  float s, co;
+  sincosf(alpha, &s, &co);
+  const float f = alpha > 0.0f ? s / alpha : 1.0f;
+  return Su2<float>{co, f * c, f * b, f * a};
+}
+
+// ------------------------------------------------------------------------------------
+// Philox4x32-10 (Salmon, Moraes, Dror, Shaw, SC'11); counter {index, draw, step, tag}
+enum : uint32_t {
+  TAG_MOMENTA = 0x4D4F4D31u,
+  TAG_ACCEPT = 0x41434331u,
+  TAG_METRO = 0x4D455431u,
+  TAG_PF = 0x50465331u,
+  TAG_CG0 = 0x43473031u
+};
+
+__host__ __device__ __forceinline__ void philox(uint32_t c0, uint32_t c1, uint32_t c2,
+                                                uint32_t c3, uint64_t seed, uint32_t out[4]) {
+  uint32_t k0 = (uint32_t)seed, k1 = (uint32_t)(seed >> 32);
+#pragma unroll
+  for (int r = 0; r < 10; r++) {
+#ifdef __CUDA_ARCH__
+    const uint32_t lo0 = 0xD2511F53u * c0, hi0 = __umulhi(0xD2511F53u, c0);
+    const uint32_t lo1 = 0xCD9E8D57u * c2, hi1 = __umulhi(0xCD9E8D57u, c2);
+#else
+    const uint64_t p0 = (uint64_t)0xD2511F53u * c0, p1 = (uint64_t)0xCD9E8D57u * c2;
+    const uint32_t lo0 = (uint32_t)p0, hi0 = (uint32_t)(p0 >> 32);
+    const uint32_t lo1 = (uint32_t)p1, hi1 = (uint32_t)(p1 >> 32);
+#endif
+    const uint32_t n0 = hi1 ^ c1 ^ k0, n2 = hi0 ^ c3 ^ k1;
+    c0 = n0;
+    c1 = lo1;
+    c2 = n2;
+    c3 = lo0;
+    k0 += 0x9E3779B9u;
+    k1 += 0xBB67AE85u;
+  }
+  out[0] = c0;
+  out[1] = c1;
+  out[2] = c2;
+  out[3] = c3;
+}
+// (0,1] with 53 random bits
+__device__ __forceinline__ double u01_53(uint32_t hi, uint32_t lo) {
+  const uint64_t k = ((uint64_t)hi << 21) ^ (uint64_t)(lo >> 11);
+  return ((double)k + 1.0) * 0x1p-53;
+}
+// [0,1) with 32 random bits
+__device__ __forceinline__ double u01_32(uint32_t x) { return (double)x * 0x1p-32; }
+__device__ __forceinline__ void box_muller(double u1, double u2, double &n0, double &n1) {
+  const double r = sqrt(-2.0 * log(u1));
+  double s, c;
+  sincospi(2.0 * u2, &s, &c);
+  n0 = r * c;
+  n1 = r * s;
+}
+
+// ------------------------------------------------------------------------------------
+// deterministic block reduction of doubles (fixed shape -> fixed summation order)
+template <int NT> __device__ __forceinline__ double block_sum(double v, double *sh) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  if (l == 0) sh[w] = v;
+  __syncthreads();
+  double r = 0.0;
+  if (w == 0) {
+    r = (l < NT / 32) ? sh[l] : 0.0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) r += __shfl_down_sync(0xffffffffu, r, o);
+  }
+  __syncthreads();
+  return r;  // valid in thread 0
+}
+
+}  // namespace su2b

@@ -1,0 +1,100 @@
+// su2b_ctx.h -- the context object behind the opaque su2b_ctx handle (host side only).
+#pragma once
+#include <map>
+#include <string>
+#include <vector>
+
+#include "solver.h"
+#include "su2b_internal.h"
+
+constexpr int NSLOT = 6;  // partial-sum slots: 0 plaquette, 1 kinetic, 2 clover, 3-5 solvers
+
+// device spinor buffers (U(1) staggered fermions)
+enum { SV_B, SV_X, SV_R, SV_P, SV_T, SV_AP, SV_S, SV_R0, SV_PHI, SV_CHI, SV_CHI1, SV_X0, SV_N };
+enum { SV32_XS, SV32_RS, SV32_PS, SV32_TS, SV32_APS, SV32_N };
+
+struct su2b_ctx {
+  int group = 0, prec = 0, device = 0;
+  int Lx = 0, Ly = 0, Lz = 0, Lt = 0;
+  double beta = 0., xi = 1.;
+  su2b::Geom g{};
+  size_t V = 0, NL = 0;
+  bool link64 = true;  // links/momenta in FP64 (false: SU(2) mixed precision, FP32)
+  cudaStream_t stream = nullptr;
+
+  // gauge field, backups, momenta, flow/force accumulator
+  void *U = nullptr, *U_old = nullptr, *U_aux = nullptr, *U_rev = nullptr;
+  void *P = nullptr, *Z = nullptr;
+  double *stage = nullptr;  // host-layout staging buffer on the device
+  double *part = nullptr;   // NSLOT slots of 3*part_cap partial sums
+  size_t part_cap = 0;
+  double *red = nullptr;    // 64 reduced scalars
+  su2b::TrajDev *traj = nullptr;
+  unsigned long long *counts = nullptr;
+
+  // pinned host mirrors
+  double *h_red = nullptr;
+  su2b::TrajDev *h_traj = nullptr;
+  unsigned long long *h_counts = nullptr;
+  su2b::SolverState *h_st = nullptr;
+
+  // staggered fermions
+  double2 *ph = nullptr;
+  float2 *ph32 = nullptr;
+  bool phases_valid = false, phases32_valid = false;
+  double2 *sv[SV_N] = {};
+  float2 *sv32[SV32_N] = {};
+  double *fderiv = nullptr;
+  su2b::SolverState *st = nullptr;
+  long x0_seed = -1;  // seed of the reference CG start held in sv[SV_X0]
+
+  std::map<std::string, cudaGraphExec_t> graphs;
+  std::vector<void *> allocs;
+  std::string err;
+
+  size_t link_bytes() const { return group == 0 ? (link64 ? 32 : 16) : 8; }
+  size_t adj_bytes() const { return (group == 0 ? 3 : 1) * (link64 ? 8 : 4); }
+  double Nc() const { return group == 0 ? 2.0 : 1.0; }
+  double *part_slot(int k) { return part + (size_t)k * 3 * part_cap; }
+};
+
+// helpers shared by the api*.cu files
+int su2b_fail(su2b_ctx *ctx, int code, const char *fmt, ...);
+int su2b_adj_upload(su2b_ctx *ctx, const double *host, void *dev);
+int su2b_adj_download(su2b_ctx *ctx, const void *dev, double *host);
+int su2b_q_plaq(su2b_ctx *ctx, const void *U, int red_slot);
+int su2b_q_clover(su2b_ctx *ctx, const void *U, int cloverdef, int red_slot);
+int su2b_fetch_red(su2b_ctx *ctx, int n);
+int su2b_q_force(su2b_ctx *ctx, const void *U, void *P, const void *extra, double f,
+                 double scale, int mode, double *kin_part, int *nb);
+int su2b_q_update(su2b_ctx *ctx, void *U, const void *P, double dt);
+int su2b_q_restore(su2b_ctx *ctx, void *U);
+int su2b_q_flow_step(su2b_ctx *ctx, void *U, double eps);
+int su2b_ensure_aux(su2b_ctx *ctx);
+int su2b_links_to_stage(su2b_ctx *ctx, const void *U);
+int su2b_make_geom(int Lx, int Ly, int Lz, int Lt, int nd, su2b::Geom *g, std::string *why);
+// fermions (solve.cu)
+int su2b_fermion_setup(su2b_ctx *ctx, bool need32);
+int su2b_fermion_deriv_q(su2b_ctx *ctx, double mass, double tol, int max_iter, int cg_start,
+                         long seed, long *iters);
+int su2b_fermion_action_q(su2b_ctx *ctx, double mass, double tol, int max_iter, int cg_start,
+                          long seed, int red_slot, long *iters);
+int su2b_fermion_heatbath_q(su2b_ctx *ctx, double mass, const double *R_host, uint64_t seed,
+                            uint32_t traj, int cplx, int red_slot);
+
+#define SU2B_CK(call)                                                                      \
+  do {                                                                                     \
+    cudaError_t e_ = (call);                                                               \
+    if (e_ != cudaSuccess)                                                                 \
+      return su2b_fail(ctx, SU2B_ERR_CUDA, "%s:%d %s: %s", __FILE__, __LINE__, #call,     \
+                       cudaGetErrorString(e_));                                            \
+  } while (0)
+#define SU2B_CKS(expr)                                                                     \
+  do {                                                                                     \
+    int s_ = (expr);                                                                       \
+    if (s_ != SU2B_OK) return s_;                                                          \
+  } while (0)
+#define SU2B_NEED(cond, ...)                                                               \
+  do {                                                                                     \
+    if (!(cond)) return su2b_fail(ctx, SU2B_ERR_INVALID, __VA_ARGS__);                     \
+  } while (0)

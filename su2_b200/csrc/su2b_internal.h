@@ -1,0 +1,103 @@
+// su2b_internal.h -- host-side launchers of the libsu2b kernels (not part of the C ABI).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "su2b_common.cuh"
+
+namespace su2b {
+
+// ---- layout conversion (reference host AoS <-> even/odd SoA) ----
+template <class T>
+cudaError_t links_from_host(const Geom &g, const double *aos, void *U, int group,
+                            cudaStream_t s);
+template <class T>
+cudaError_t links_to_host(const Geom &g, const void *U, double *aos, int group, cudaStream_t s);
+template <class T>
+cudaError_t adj_from_host(const Geom &g, const double *aos, T *P, int group, cudaStream_t s);
+template <class T>
+cudaError_t adj_to_host(const Geom &g, const T *P, double *aos, int group, cudaStream_t s);
+cudaError_t spinor_from_host(const Geom &g, const double *aos, double2 *psi, cudaStream_t s);
+cudaError_t spinor_to_host(const Geom &g, const double2 *psi, double *aos, cudaStream_t s);
+
+// ---- reductions ----
+// plaquette partial sums, 3 per block {full, spatial-only, xi-weighted}; returns #blocks
+template <class T>
+cudaError_t plaq_partials(const Geom &g, const void *U, int group, double xi, double *part,
+                          int *nblocks, cudaStream_t s);
+// out[k] = sum_b part[b*ncomp + k] in a fixed order, k < ncomp
+cudaError_t reduce_final(const double *part, int nblocks, int ncomp, double *out,
+                         cudaStream_t s);
+
+// ---- gauge force / momenta ----
+enum ForceMode : int {
+  FM_HAS_IN = 1,     // P_out = P_in + scale*(f*g) (else P_out = scale*(f*g))
+  FM_KINETIC = 2,    // also write per-block partials of sum P_out^2
+  FM_EXTRA = 4       // add extra[] (another monomial's derivative) to f*g before scaling
+};
+template <class T>
+cudaError_t force_update(const Geom &g, const void *U, int group, T *P, const T *extra, double f,
+                         double scale, double xi, int mode, double *kin_part, int *nblocks,
+                         cudaStream_t s);
+template <class T>
+cudaError_t link_update(const Geom &g, void *U, int group, const T *P, double dt,
+                        cudaStream_t s);
+template <class T> cudaError_t restore_links(const Geom &g, void *U, int group, cudaStream_t s);
+template <class T>
+cudaError_t momenta_philox(const Geom &g, T *P, int group, uint64_t seed, uint32_t traj,
+                           double *kin_part, int *nblocks, cudaStream_t s);
+template <class T>
+cudaError_t kinetic_partials(const Geom &g, const T *P, int group, double *part, int *nblocks,
+                             cudaStream_t s);
+template <class T>
+cudaError_t negate_adj(const Geom &g, T *P, int group, cudaStream_t s);
+
+// ---- accept / reject ----
+struct AcceptIn {
+  double beta, Nc;
+  uint64_t seed;
+  uint32_t traj;
+  double u_host;  // < 0: Philox uniform
+  int accept_reject;
+};
+// reduced values read by the accept step:
+//   red[0] sum P^2 before, red[1..3] plaquette sums before {full, spatial, xi-weighted},
+//   red[4] sum P^2 after,  red[5..7] plaquette sums after, red[8] / red[9] fermion action
+//   before / after.
+struct TrajDev {
+  double H_old[3], H_new[3];
+  double dH, u;
+  int accepted;
+  int pad;
+};
+cudaError_t accept_step(const double *red, AcceptIn in, TrajDev *out, cudaStream_t s);
+template <class T>
+cudaError_t cond_restore(const Geom &g, void *U, const void *U_old, int group,
+                         const TrajDev *flag, cudaStream_t s);
+
+// ---- Metropolis ----
+template <class T>
+cudaError_t metropolis_pass(const Geom &g, void *U, int group, int mu, int parity, double beta,
+                            double delta, int N_hit, uint64_t seed, uint32_t sweep,
+                            unsigned long long *counts, cudaStream_t s);
+
+// ---- clover energy density / charge ----
+// per-block partials {E, E_ss, Q, Q_ss}
+template <class T>
+cudaError_t clover_partials(const Geom &g, const void *U, int group, int cloverdef,
+                            double *part, int *nblocks, cudaStream_t s);
+
+// ---- staggered fermions ----
+cudaError_t u1_phases(const Geom &g, const double *theta, double2 *ph, cudaStream_t s);
+cudaError_t u1_phases_f32(const Geom &g, const double *theta, float2 *ph, cudaStream_t s);
+// out = D psi (dag=0) or Ddag psi (dag=1), staggered.hpp:305-389
+cudaError_t staggered_D(const Geom &g, const double2 *ph, double m, int dag, const double2 *in,
+                        double2 *out, cudaStream_t s);
+cudaError_t staggered_D(const Geom &g, const float2 *ph, float m, int dag, const float2 *in,
+                        float2 *out, cudaStream_t s);
+cudaError_t fermion_force(const Geom &g, const double2 *ph, const double2 *chi,
+                          const double2 *chi1, double *deriv, cudaStream_t s);
+cudaError_t pf_source(const Geom &g, uint64_t seed, uint32_t traj, int complex_source,
+                      double2 *R, cudaStream_t s);
+
+}  // namespace su2b

@@ -1,0 +1,67 @@
+"""The C ABI library loads without a GPU, exports every symbol include/su2b.h declares, and
+rejects invalid arguments before touching a device."""
+import ctypes
+import os
+import re
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_symbols():
+    text = open(os.path.join(ROOT, "include", "su2b.h")).read()
+    return sorted(set(re.findall(r"^SU2B_API [^(]*?\b(su2b_\w+)\(", text, flags=re.M)))
+
+
+def test_header_declares_the_boundary():
+    names = declared_symbols()
+    for n in ["su2b_ctx_create", "su2b_upload_gauge", "su2b_gauge_energy", "su2b_gauge_force",
+              "su2b_hmc_trajectory", "su2b_metropolis_sweep", "su2b_gradient_flow",
+              "su2b_solve", "su2b_fermion_force", "su2b_energy_density"]:
+        assert n in names
+
+
+def test_library_exports_every_declared_symbol():
+    from su2_b200 import _abi
+    lib = _abi.load()
+    for n in declared_symbols():
+        assert hasattr(lib, n), n
+    assert set(_abi.SIGNATURES) == set(declared_symbols())
+
+
+def test_invalid_geometry_rejected_without_device():
+    from su2_b200 import _abi
+    lib = _abi.load()
+    ctx = ctypes.c_void_p()
+    # odd extent, bad ndims, inactive extent != 1, bad group, bad precision, NULL out
+    assert lib.su2b_ctx_create(0, 5, 4, 4, 4, 4, 2.0, 1.0, 0, 0, ctypes.byref(ctx)) == _abi.ERR_INVALID
+    assert lib.su2b_ctx_create(0, 4, 4, 4, 4, 5, 2.0, 1.0, 0, 0, ctypes.byref(ctx)) == _abi.ERR_INVALID
+    assert lib.su2b_ctx_create(0, 4, 4, 2, 4, 3, 2.0, 1.0, 0, 0, ctypes.byref(ctx)) == _abi.ERR_INVALID
+    assert lib.su2b_ctx_create(7, 4, 4, 4, 4, 4, 2.0, 1.0, 0, 0, ctypes.byref(ctx)) == _abi.ERR_INVALID
+    assert lib.su2b_ctx_create(0, 4, 4, 4, 4, 4, 2.0, 1.0, 9, 0, ctypes.byref(ctx)) == _abi.ERR_INVALID
+    assert lib.su2b_ctx_create(0, 4, 4, 4, 4, 4, 2.0, 1.0, 0, 0, None) == _abi.ERR_INVALID
+    assert lib.su2b_ctx_destroy(None) == _abi.ERR_INVALID
+
+
+def test_null_context_is_an_error():
+    from su2_b200 import _abi
+    lib = _abi.load()
+    d = ctypes.c_double()
+    assert lib.su2b_gauge_energy(None, 0, ctypes.byref(d)) == _abi.ERR_INVALID
+    assert lib.su2b_hmc_trajectory(None, None, None) == _abi.ERR_INVALID
+    assert lib.su2b_last_error(None) == b"null context"
+
+
+def test_product_does_not_link_the_oracle():
+    """The CUDA library is self-contained: no oracle or reference symbols inside."""
+    from su2_b200 import _abi
+    data = open(_abi.LIB_PATH, "rb").read()
+    assert b"orc_" not in data and b"ref_hotstart" not in data
+
+
+@pytest.mark.parametrize("fn", ["su2b_upload_gauge", "su2b_download_gauge"])
+def test_transfer_requires_context(fn):
+    from su2_b200 import _abi
+    lib = _abi.load()
+    assert getattr(lib, fn)(None, None) == _abi.ERR_INVALID

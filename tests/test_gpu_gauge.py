@@ -1,0 +1,269 @@
+"""Parity of the gauge-field path of libsu2b (through the C ABI) against the oracle.
+
+Tolerances: FP64 results within 1e-12 relative (norm-wise for fields), FP64 sums within
+1e-12 relative; mixed precision (FP32 links and forces) within 1e-5 relative.
+"""
+import numpy as np
+import pytest
+
+from helpers import GEOM_IDS, GEOMS, group_name, rel
+
+pytestmark = pytest.mark.gpu
+
+SEED, TRAFO = 13526463, 654321
+
+
+def make(gpu, group, dims, nd, beta=2.3, xi=1.0, precision="fp64"):
+    Lx, Ly, Lz, Lt = dims
+    return gpu.gaugeconfig(Lx, Ly, Lz, Lt, nd, beta, group=group_name(group), xi=xi,
+                           precision=precision)
+
+
+def hot(orc, group, dims, nd, seed=SEED):
+    return orc.hotstart(group, dims, nd, seed, 1.0, TRAFO)
+
+
+@pytest.mark.parametrize("group,dims,nd", GEOMS, ids=GEOM_IDS)
+def test_upload_download_roundtrip(gpu, orc, group, dims, nd):
+    U = hot(orc, group, dims, nd)
+    with make(gpu, group, dims, nd) as c:
+        c.upload(U)
+        assert np.array_equal(c.download(), U)
+    if group == 0:
+        with make(gpu, group, dims, nd, precision="mixed") as c:
+            c.upload(U)
+            assert np.array_equal(c.download(), U.astype(np.float32).astype(np.float64))
+
+
+@pytest.mark.parametrize("group,dims,nd", GEOMS, ids=GEOM_IDS)
+def test_plaquette_and_action(gpu, orc, group, dims, nd):
+    U = hot(orc, group, dims, nd)
+    for xi in (1.0, 1.3):
+        with make(gpu, group, dims, nd, beta=2.3, xi=xi) as c:
+            c.upload(U)
+            e = orc.gauge_energy(group, dims, nd, U)
+            assert c.gauge_energy() == pytest.approx(e, rel=1e-12, abs=1e-12)
+            ess = orc.gauge_energy(group, dims, nd, U, spatial_only=True)
+            assert c.gauge_energy(True) == pytest.approx(ess, rel=1e-12, abs=1e-12)
+            w = orc.retr_sum_plaquettes(group, dims, nd, U, xi, xi != 1.0)
+            assert c.retr_sum_Wplaquettes() == pytest.approx(w, rel=1e-12, abs=1e-12)
+            s = orc.S_G_hmc(group, dims, nd, 2.3, U, xi, xi != 1.0)
+            assert c.get_S_G_hmc() == pytest.approx(s, rel=1e-12, abs=1e-12)
+
+
+@pytest.mark.parametrize("group,dims,nd", GEOMS, ids=GEOM_IDS)
+@pytest.mark.parametrize("xi", [1.0, 0.8])
+def test_gauge_force(gpu, orc, group, dims, nd, xi):
+    U = hot(orc, group, dims, nd)
+    ref = orc.gauge_derivative(group, dims, nd, 2.3, U, xi, 0.7)
+    with make(gpu, group, dims, nd, beta=2.3, xi=xi) as c:
+        c.upload(U)
+        assert rel(c.derivative(0.7), ref) < 1e-12
+    if group == 0:
+        with make(gpu, group, dims, nd, beta=2.3, xi=xi, precision="mixed") as c:
+            c.upload(U)
+            assert rel(c.derivative(0.7), ref) < 1e-5
+
+
+@pytest.mark.parametrize("group,dims,nd", GEOMS, ids=GEOM_IDS)
+def test_update_and_restore(gpu, orc, group, dims, nd):
+    U = hot(orc, group, dims, nd)
+    P, _ = orc.initnormal(group, dims, nd, 99)
+    want = orc.restore_su(group, dims, nd, orc.update_gauge(group, dims, nd, U, P, 0.137))
+    with make(gpu, group, dims, nd) as c:
+        c.upload(U)
+        c.update_gauge(P, 0.137)
+        c.restoreSU()
+        assert rel(c.download(), want) < 1e-13
+
+
+@pytest.mark.parametrize("group,dims,nd", GEOMS, ids=GEOM_IDS)
+def test_energy_density(gpu, orc, group, dims, nd):
+    U = hot(orc, group, dims, nd)
+    with make(gpu, group, dims, nd) as c:
+        c.upload(U)
+        for cl in (True, False):
+            for ss in (False, True):
+                E, Q = c.energy_density(cl, ss)
+                Eo, Qo = orc.energy_density(group, dims, nd, U, cl, ss)
+                assert E == pytest.approx(Eo, rel=1e-12, abs=1e-13)
+                assert Q == pytest.approx(Qo, rel=1e-11, abs=1e-13)
+
+
+def test_topological_charge_known_answer(gpu):
+    """test.cc:81-105: a hand-built U(1) 4^4 configuration has Q = 0.0126651."""
+    import math
+    U = np.zeros(4 ** 4 * 4)
+
+    def idx(t, x, y, z, mu):
+        return (((t * 4 + x) * 4 + y) * 4 + z) * 4 + mu
+
+    U[idx(1, 1, 1, 1, 0)] = 0
+    U[idx(1, 1, 1, 1, 1)] = math.pi / 2
+    U[idx(1, 1, 1, 1, 2)] = math.pi / 2
+    U[idx(1, 1, 1, 1, 3)] = 0
+    U[idx(0, 1, 1, 1, 0)] = math.pi
+    U[idx(1, 0, 1, 1, 1)] = math.pi / 2
+    U[idx(1, 1, 0, 0, 2)] = math.pi
+    U[idx(1, 1, 1, 0, 3)] = math.pi / 2
+    with gpu.gaugeconfig(4, 4, 4, 4, 4, 1.0, group="u1") as c:
+        c.upload(U)
+        _, Q = c.energy_density()
+    assert Q == pytest.approx(0.0126651, abs=5e-8)
+
+
+@pytest.mark.parametrize("group,dims,nd", GEOMS, ids=GEOM_IDS)
+def test_flow_step(gpu, orc, group, dims, nd):
+    U = hot(orc, group, dims, nd)
+    want = orc.runge_kutta(group, dims, nd, 2.3, 0.01, U)
+    with make(gpu, group, dims, nd, beta=2.3) as c:
+        c.upload(U)
+        c.runge_kutta(0.01)
+        assert rel(c.download(), want) < 1e-12
+    if group == 0:
+        with make(gpu, group, dims, nd, beta=2.3, precision="mixed") as c:
+            c.upload(U)
+            c.runge_kutta(0.01)
+            assert rel(c.download(), want) < 1e-5
+
+
+@pytest.mark.parametrize("group,dims,nd", [GEOMS[0], GEOMS[3], GEOMS[4]],
+                         ids=[GEOM_IDS[0], GEOM_IDS[3], GEOM_IDS[4]])
+def test_gradient_flow_records(gpu, orc, group, dims, nd):
+    U = hot(orc, group, dims, nd)
+    want = orc.gradient_flow_rows(group, dims, nd, 2.3, U, 0.2, 0.01)
+    with make(gpu, group, dims, nd, beta=2.3) as c:
+        c.upload(U)
+        got = c.gradient_flow(0.2, 0.01)
+        assert np.array_equal(c.download(), U)  # the flow works on a copy
+    assert got.shape == want.shape
+    fin = np.isfinite(want)
+    assert np.array_equal(fin, np.isfinite(got))
+    np.testing.assert_allclose(got[fin], want[fin], rtol=1e-11, atol=1e-13)
+
+
+@pytest.mark.parametrize("group,dims,nd", GEOMS, ids=GEOM_IDS)
+@pytest.mark.parametrize("integ", [0, 6, 2, 4, 5])
+def test_md_trajectory_injected_momenta(gpu, orc, group, dims, nd, integ):
+    U = hot(orc, group, dims, nd)
+    P, _ = orc.initnormal(group, dims, nd, 4242)
+    dH, U_want, _, H = orc.md_injected(group, dims, nd, 2.3, integ, 6, 1.0, U, P)
+    with make(gpu, group, dims, nd, beta=2.3) as c:
+        c.upload(U)
+        r = c.md_update(integ, 6, 1.0, momenta=P, accept_reject=False)
+        assert r.accepted
+        assert r.dH == pytest.approx(dH, abs=1e-9 * max(1.0, abs(H[1])))
+        assert r.H_old[0] == pytest.approx(H[0], rel=1e-13)
+        assert r.H_new[1] == pytest.approx(H[3], rel=1e-12)
+        assert rel(c.download(), U_want) < 1e-10
+
+
+def test_reference_chain_replay(gpu, orc):
+    """Replaying the reference's own random stream (std::mt19937(seed+i) momenta and accept
+    uniform), the device chain takes the same accept decisions with the same Delta H as the
+    reference's md_update (hmc.hpp:86-101) -- config: SU(2) 8^4, beta = 2.3, omf2 tau=1."""
+    group, dims, nd = 0, (8, 8, 8, 8), 4
+    U0 = hot(orc, group, dims, nd)
+    n = 6
+    U_ref, acc, dH, plaq = orc.hmc_run(group, dims, nd, 2.3, 6, 10, 1.0, 13526463, 0, n, U0)
+    with make(gpu, group, dims, nd, beta=2.3) as c:
+        c.upload(U0)
+        for i in range(n):
+            P, u = orc.initnormal(group, dims, nd, 13526463 + i)
+            r = c.md_update("omf2", 10, 1.0, momenta=P, uniform=u)
+            assert r.accepted == bool(acc[i])
+            assert r.dH == pytest.approx(dH[i], abs=1e-7)
+            assert r.plaquette == pytest.approx(plaq[i], rel=1e-11)
+        assert rel(c.download(), U_ref) < 1e-9
+
+
+@pytest.mark.parametrize("group,dims,nd", [GEOMS[0], GEOMS[2], GEOMS[4]],
+                         ids=[GEOM_IDS[0], GEOM_IDS[2], GEOM_IDS[4]])
+def test_device_momentum_stream(gpu, orc, group, dims, nd):
+    """The device's Philox momenta equal the oracle's restatement of the same stream."""
+    U = hot(orc, group, dims, nd)
+    P = orc.philox_momenta(group, dims, nd, 777, 5)
+    na = 3 if group == 0 else 1
+    assert abs(P.mean()) < 5.0 / np.sqrt(P.size) and abs(P.var() - 1) < 10.0 / np.sqrt(P.size)
+    with make(gpu, group, dims, nd) as c:
+        c.upload(U)
+        r = c.md_update("leapfrog", 1, 1e-3, seed=777, traj=5, accept_reject=False)
+    assert r.H_old[0] == pytest.approx(0.5 * float(np.sum(P * P)), rel=1e-13)
+    assert P.size == c.n_links * na
+
+
+@pytest.mark.parametrize("group,dims,nd", GEOMS, ids=GEOM_IDS)
+def test_metropolis_checkerboard(gpu, orc, group, dims, nd):
+    U = hot(orc, group, dims, nd)
+    U_want, r_want = orc.metropolis_checkerboard(group, dims, nd, 2.3, 0.3, 4, 99, 3, U)
+    with make(gpu, group, dims, nd, beta=2.3) as c:
+        c.upload(U)
+        rates = c.sweep(0.3, 4, 99, 3)
+        assert rel(c.download(), U_want) < 1e-11
+    np.testing.assert_array_equal(rates, r_want)
+
+
+@pytest.mark.parametrize("group,dims,nd", [GEOMS[0], GEOMS[4]], ids=[GEOM_IDS[0], GEOM_IDS[4]])
+def test_gauge_invariance(gpu, orc, group, dims, nd):
+    U = hot(orc, group, dims, nd)
+    V = orc.random_gauge_trafo(group, dims, nd, U, 98765)
+    with make(gpu, group, dims, nd) as c:
+        c.upload(U)
+        p0, e0 = c.gauge_energy(), c.energy_density()
+        c.upload(V)
+        p1, e1 = c.gauge_energy(), c.energy_density()
+    assert p1 == pytest.approx(p0, rel=1e-12)
+    assert e1[0] == pytest.approx(e0[0], rel=1e-12)
+
+
+def test_reversibility(gpu, orc):
+    """md_update's reversibility test (md_update.hh:62-74): ddH ~ 0 and U unchanged by it."""
+    group, dims, nd = 0, (6, 6, 6, 6), 4
+    U = hot(orc, group, dims, nd)
+    with make(gpu, group, dims, nd, beta=2.3) as c:
+        c.upload(U)
+        a = c.md_update("omf2", 8, 1.0, seed=5, traj=0, revtest=True, accept_reject=False)
+        Ua = c.download()
+        c.upload(U)
+        b = c.md_update("omf2", 8, 1.0, seed=5, traj=0, revtest=False, accept_reject=False)
+        assert np.array_equal(Ua, c.download())
+    assert a.dH == b.dH
+    assert abs(a.ddH) < 1e-8
+
+
+def test_error_paths(gpu):
+    import su2_b200
+    with pytest.raises(su2_b200.Su2bError):
+        gpu.gaugeconfig(5, 4, 4, 4, 4, 2.0)  # odd extent
+    with pytest.raises(su2_b200.Su2bError):
+        gpu.gaugeconfig(4, 4, 2, 4, 3, 2.0)  # inactive extent != 1
+    with gpu.gaugeconfig(4, 4, 4, 4, 4, 2.0) as c:
+        with pytest.raises(su2_b200.Su2bError) as e:
+            c.md_update(1, 4, 1.0)  # lp_leapfrog
+        assert e.value.code == 4
+        with pytest.raises(su2_b200.Su2bError) as e:
+            c.md_update("leapfrog", 4, 1.0, fermion_mass=0.1)  # SU(2) fermions
+        assert e.value.code == 4
+        with pytest.raises(su2_b200.Su2bError) as e:
+            c.apply_D(0.1, np.zeros(2 * 256))
+        assert e.value.code == 4
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_full_size_32_4(gpu, orc, precision):
+    """At 32^4: plaquette and force against the oracle, gauge invariance, and an omf2
+    trajectory whose reversibility violation is at rounding level."""
+    group, dims, nd = 0, (32, 32, 32, 32), 4
+    U = hot(orc, group, dims, nd, seed=4711)
+    tol = 1e-12 if precision == "fp64" else 1e-5
+    with make(gpu, group, dims, nd, beta=2.4, precision=precision) as c:
+        c.upload(U)
+        # reductions are FP64 over the stored links (FP32-rounded in mixed precision)
+        Us = U if precision == "fp64" else U.astype(np.float32).astype(np.float64)
+        assert c.gauge_energy() == pytest.approx(orc.gauge_energy(group, dims, nd, Us),
+                                                 rel=1e-12)
+        F = orc.gauge_derivative(group, dims, nd, 2.4, U)
+        assert rel(c.derivative(), F) < tol
+        r = c.md_update("omf2", 4, 0.2, seed=11, traj=1, revtest=True, accept_reject=False)
+        assert abs(r.ddH) < (1e-6 if precision == "fp64" else 5e-2)
+        assert np.isfinite(r.dH)
