@@ -1,0 +1,403 @@
+#!/usr/bin/env python
+"""Headline benchmark: SU(2) d=4 32^4 HMC at beta = 2.4, omf2 integrator, tau = 1, 16 steps.
+
+One step = one HMC trajectory (Philox momenta, 33 force evaluations, 32 link updates,
+FP64 accept/reject).  ``value`` is the trajectory rate of the mixed-precision path (FP32
+links and forces, FP64 reductions / accept / reunitarisation) over all ranks; the FP64 path
+runs the same trajectories from the same thermalised configuration for the comparison at
+equal Delta H and plaquette.
+
+    python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+
+With N > 1 (torchrun, one process per GPU) every rank runs an independent chain (replicas,
+no collective in the timed path); the slowest rank's device time sets the rate.
+``--impl reference`` times the reference's own CPU implementation (md_update from the su2
+headers, built in oracle/_ref) on the host cores for the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+L = 32
+BETA = 2.4
+NSTEPS = 16
+TAU = 1.0
+METRIC = "SU(2) 32^4 HMC traj/s mixed vs FP64 at equal ΔH/plaq; kernel HBM GB/s vs peak"
+WORKLOAD = "SU(2) d=4 32^4, beta=2.4, omf2 tau=1 n=16 HMC trajectory"
+
+
+class quiet_stdout:
+    """Silences file descriptor 1 (the reference's integrator factory prints its name)."""
+
+    def __enter__(self):
+        sys.stdout.flush()
+        self.saved = os.dup(1)
+        self.null = os.open(os.devnull, os.O_WRONLY)
+        os.dup2(self.null, 1)
+
+    def __exit__(self, *a):
+        os.dup2(self.saved, 1)
+        os.close(self.null)
+        os.close(self.saved)
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured (MEASURED_PEAKS.json hbm_gbs)"
+    return 6650.0, "fallback (6.65 TB/s)"
+
+
+def haar_links(n_links, seed):
+    """Haar-uniform SU(2) links (normalised Gaussian 4-vectors), reference host layout."""
+    rng = np.random.default_rng(seed)
+    q = rng.normal(size=(n_links, 4))
+    q /= np.linalg.norm(q, axis=1, keepdims=True)
+    return np.ascontiguousarray(q.reshape(-1))
+
+
+class Clocks:
+    """Samples SM clocks and throttle reasons with nvidia-smi during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def start(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}",
+                                       "--format=csv,noheader,nounits", "-lms", "200",
+                                       "-i", str(self.device)], stdout=self.f,
+                                      stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return None
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.p.kill()
+        self.f.flush()
+        rows = [r.split(",") for r in open(self.f.name).read().splitlines() if r.strip()]
+        os.unlink(self.f.name)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                mx = float(r[2])
+                for k, nm in enumerate(names):
+                    if "Active" in r[5 + k] and "Not" not in r[5 + k]:
+                        reasons.add(nm)
+            except (ValueError, IndexError):
+                continue
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_setup():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if ws > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    return ws, rank, local, dist
+
+
+def barrier(dist):
+    if dist is not None:
+        import torch
+        dist.barrier()
+        torch.cuda.synchronize()
+
+
+def allmax(dist, x):
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def allsum(dist, x):
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+# --------------------------------------------------------------------------------------
+def run_chain(c, K, seed, traj0, events):
+    """K timed trajectories on context c; returns (device seconds, results)."""
+    import torch
+    s = torch.cuda.ExternalStream(c.stream())
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    res = []
+    e0.record(s)
+    for k in range(K):
+        res.append(c.md_update("omf2", NSTEPS, TAU, seed=seed, traj=traj0 + k))
+    e1.record(s)
+    e1.synchronize()
+    return e0.elapsed_time(e1) / 1e3, res
+
+
+def stats(res, V):
+    dH = [r.dH for r in res]
+    return {"acceptance": sum(r.accepted for r in res) / len(res),
+            "dH_mean": float(np.mean(dH)), "dH_rms": float(np.sqrt(np.mean(np.square(dH)))),
+            "exp_minus_dH": float(np.mean(np.exp(-np.array(dH)))),
+            "plaquette": float(np.mean([r.plaquette for r in res])) / (V * 6 * 2)}
+
+
+def ours(args):
+    import torch
+
+    import su2_b200
+    ws, rank, local, dist = dist_setup()
+    torch.cuda.set_device(local)
+    K, W = args.steps, args.warmup
+    V = L ** 4
+    NL = V * 4
+    seed = 20240 + 1000 * rank
+
+    # ---- thermalised start (untimed): Haar start, Metropolis sweeps, HMC warm-up ----
+    U0 = haar_links(NL, seed)
+    mixed = su2_b200.gaugeconfig(L, L, L, L, 4, BETA, precision="mixed", device=local)
+    mixed.upload(U0)
+    for sweep in range(args.therm_sweeps):
+        mixed.sweep(0.15, 8, seed, sweep)
+    for k in range(max(W, 3)):
+        mixed.md_update("omf2", NSTEPS, TAU, seed=seed, traj=100000 + k)
+    U_th = mixed.download()
+
+    # ---- headline: mixed precision, K trajectories ----
+    clocks = Clocks(local)
+    barrier(dist)
+    n0 = mixed.kernel_launches()
+    clocks.start()
+    t_mixed, res_m = run_chain(mixed, K, seed, 0, None)
+    clk = clocks.stop()
+    launches = mixed.kernel_launches() - n0
+    t_mixed = allmax(dist, t_mixed)
+    value = ws * K / t_mixed
+
+    # ---- FP64 path, same start and seeds ----
+    fp64 = su2_b200.gaugeconfig(L, L, L, L, 4, BETA, precision="fp64", device=local)
+    fp64.upload(U_th)
+    for k in range(min(W, 2)):
+        fp64.md_update("omf2", NSTEPS, TAU, seed=seed + 7, traj=200000 + k)
+    fp64.upload(U_th)
+    barrier(dist)
+    t_fp64, res_d = run_chain(fp64, K, seed, 0, None)
+    t_fp64 = allmax(dist, t_fp64)
+
+    # ---- roofline of the dominant kernel (fused staple/force/momentum), live timers ----
+    roof = {}
+    kernels = {}
+    hbm, peak_src = peaks()
+    for name, c, bpl in (("mixed", mixed, 40), ("fp64", fp64, 80)):
+        c.upload(U_th)
+        c.profile(True)
+        for k in range(max(2, K // 2)):
+            c.md_update("omf2", NSTEPS, TAU, seed=seed, traj=300000 + k)
+        prof = c.profile_read()
+        c.profile(False)
+        n, ms = prof["force"]
+        avg = ms / 1e3 / n
+        roof[name] = {"avg_us": avg * 1e6, "GB/s": bpl * NL / avg / 1e9}
+        per = {}
+        nb = {"force": bpl, "update": 88 if name == "fp64" else 44,
+              "plaquette": 32 if name == "fp64" else 16, "restore": 64 if name == "fp64" else 32,
+              "momenta": 24 if name == "fp64" else 12}
+        for kname, (kn, kms) in prof.items():
+            if kn:
+                d = {"launches": kn, "avg_us": kms * 1e3 / kn}
+                if kname in nb:
+                    d["GB/s"] = nb[kname] * NL / (kms / 1e3 / kn) / 1e9
+                per[kname] = d
+        kernels[name] = per
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", "force_kernel_traffic.json")
+    if os.path.exists(tp):
+        traffic = json.load(open(tp)).get("mixed_bytes_per_launch")
+
+    # ---- e2e through the C ABI with host buffers (pinned), per trajectory:
+    #      upload the host gaugeconfig, one trajectory, download the gaugeconfig ----
+    Uh = torch.empty(NL * 4, dtype=torch.float64, pin_memory=True).numpy()
+    Uh[:] = U_th
+    mixed.upload(Uh)
+    barrier(dist)
+    t0 = time.perf_counter()
+    for k in range(K):
+        mixed.upload(Uh)
+        r = mixed.md_update("omf2", NSTEPS, TAU, seed=seed, traj=400000 + k)
+        Uh[:] = mixed.download()
+    t_e2e = allmax(dist, time.perf_counter() - t0)
+
+    # ---- side measurements of config 2 (Metropolis sweep, flow step) ----
+    mixed.upload(U_th)
+    s = torch.cuda.ExternalStream(mixed.stream())
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    ev[0].record(s)
+    for sweep in range(5):
+        mixed.sweep(0.15, 8, seed, 5000 + sweep)
+    ev[1].record(s)
+    fp64.upload(U_th)
+    s2 = torch.cuda.ExternalStream(fp64.stream())
+    ev[2].record(s2)
+    for _ in range(10):
+        fp64.runge_kutta(0.01)
+    ev[3].record(s2)
+    torch.cuda.synchronize()
+    metro = 5 / (ev[0].elapsed_time(ev[1]) / 1e3)
+    flow = 10 / (ev[2].elapsed_time(ev[3]) / 1e3)
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(U_th)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "traj/s", "n_gpus": ws, "steps": K,
+            "warmup": W, "ms_per_step": 1e3 * t_mixed / K, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": "fp32 links/forces + fp64 reductions/accept",
+            "data": "synthetic: seeded Haar-random start, Metropolis-thermalised on device",
+            "config": {"workload": WORKLOAD + " (mixed precision)", "lattice": [L] * 4,
+                       "beta": BETA, "integrator": "omf2", "n_steps": NSTEPS, "tau": TAU,
+                       "replicas": ws, "parallelism": f"replicas x{ws}",
+                       "l2": "working set per step (U, U_old, P) > 126 MB L2; no flush"},
+            "mixed": dict(traj_per_s=value, **stats(res_m, V)),
+            "fp64": dict(traj_per_s=ws * K / t_fp64, **stats(res_d, V)),
+            "speedup_mixed_vs_fp64": t_fp64 / t_mixed,
+            "roofline": {"bound": "hbm", "kernel": "fused staple/force/momentum (FP32)",
+                         "achieved": roof["mixed"]["GB/s"], "peak": hbm, "unit": "GB/s",
+                         "frac": roof["mixed"]["GB/s"] / hbm, "traffic": traffic,
+                         "bytes_per_launch": 40 * NL, "avg_launch_us": roof["mixed"]["avg_us"],
+                         "peak_source": peak_src,
+                         "fp64_kernel": {"achieved": roof["fp64"]["GB/s"],
+                                         "frac": roof["fp64"]["GB/s"] / hbm,
+                                         "bytes_per_launch": 80 * NL,
+                                         "avg_launch_us": roof["fp64"]["avg_us"]}},
+            "kernels": kernels,
+            "metropolis_sweeps_per_s": metro, "flow_rk3_steps_per_s_fp64": flow,
+            "e2e": {"value": ws * K / t_e2e, "unit": "traj/s",
+                    "h2d_bytes_per_step": int(NL * 4 * 8), "d2h_bytes_per_step": int(NL * 4 * 8),
+                    "note": "upload of the host gaugeconfig (reference layout, FP64, pinned) "
+                            "+ trajectory + download, wall clock"},
+            "gpu_launches": int(launches),
+            "clocks": clk,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    mixed.close()
+    fp64.close()
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+def cpu_baseline(U_th):
+    """The reference's md_update code (oracle/_ref) on the host cores: one omf2 trajectory of
+    the same 32^4 workload with injected momenta (a bounded sample)."""
+    from oracle import oracle as O
+    if not O.available("ref"):
+        return None
+    r = O.Oracle("ref")
+    threads = r._omp_threads()
+    P = np.random.default_rng(5).normal(size=L ** 4 * 4 * 3)
+    with quiet_stdout():
+        t0 = time.perf_counter()
+        r.md_injected(0, (L, L, L, L), 4, BETA, 6, NSTEPS, TAU, U_th.copy(), P)
+        dt = time.perf_counter() - t0
+    return {"value": 1.0 / dt, "unit": "traj/s", "cores": threads, "kind": "reference",
+            "sample": "1 omf2 trajectory (16 steps, 33 force evaluations) of the 32^4 workload "
+                      "through the reference's integrator/monomial code, OpenMP"}
+
+
+def reference(args):
+    """--impl reference: the reference's stock md_update (std::mt19937 momenta, accept/reject,
+    hmc.hpp:86-101) on the host cores, one trajectory per step."""
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from oracle import oracle as O
+    if not O.available("ref"):
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libsu2ref.so was not "
+                          "built (needs the reference checkout at build time)"}))
+        return
+    r = O.Oracle("ref")
+    threads = r._omp_threads()
+    U = haar_links(L ** 4 * 4, 20240)
+    with quiet_stdout():
+        for k in range(args.warmup):
+            U, *_ = r.hmc_run(0, (L, L, L, L), 4, BETA, 6, NSTEPS, TAU, 13526463, k, 1, U)
+        t0 = time.perf_counter()
+        for k in range(args.steps):
+            U, acc, dH, plaq = r.hmc_run(0, (L, L, L, L), 4, BETA, 6, NSTEPS, TAU, 13526463,
+                                         args.warmup + k, 1, U)
+        dt = time.perf_counter() - t0
+    v = args.steps / dt
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": v, "unit": "traj/s", "n_gpus": ws,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * dt / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp64",
+        "data": "synthetic: seeded Haar-random start",
+        "config": {"workload": WORKLOAD + " (reference CPU, FP64)", "lattice": [L] * 4},
+        "cpu_baseline": {"value": v, "unit": "traj/s", "cores": threads, "kind": "reference",
+                         "sample": f"{args.steps} full trajectories of the workload"},
+        "e2e": {"value": v, "unit": "traj/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--therm-sweeps", type=int, default=60)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        reference(args)
+    else:
+        ours(args)
+
+
+if __name__ == "__main__":
+    main()

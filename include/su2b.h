@@ -206,6 +206,30 @@ SU2B_API int su2b_fermion_force(su2b_ctx *ctx, double mass, const double *phi_ho
 SU2B_API int su2b_fermion_action(su2b_ctx *ctx, double mass, const double *phi_host, double tol,
                         int max_iter, const double *x0_host, long seed, double *out);
 
+/* ---- device timers -------------------------------------------------------------------- */
+/* Kernel classes.  With profiling on, every launch of a class is bracketed by CUDA events on
+ * the context's stream and its device time accumulated (the events add a few microseconds
+ * per launch; leave profiling off for headline timings). */
+enum {
+  SU2B_K_FORCE = 0,      /* fused staple / force / momentum update */
+  SU2B_K_UPDATE = 1,     /* U <- exp(dt P) U */
+  SU2B_K_PLAQUETTE = 2,  /* plaquette / action partial sums */
+  SU2B_K_MOMENTA = 3,    /* Philox momenta + kinetic partial sums */
+  SU2B_K_RESTORE = 4,    /* reunitarisation */
+  SU2B_K_METROPOLIS = 5, /* checkerboard Metropolis pass */
+  SU2B_K_CLOVER = 6,     /* clover energy density / charge */
+  SU2B_K_STAGGERED = 7,  /* staggered D / Ddag and fermion force */
+  SU2B_K_OTHER = 8,      /* reductions, solver vector updates, layout conversion */
+  SU2B_K_COUNT = 9
+};
+/* enable (1) or disable (0) the timers; enabling clears the accumulated values */
+SU2B_API int su2b_profile(su2b_ctx *ctx, int enable);
+/* launches and total device milliseconds of one class since profiling was enabled
+ * (synchronises the context's stream) */
+SU2B_API int su2b_profile_read(su2b_ctx *ctx, int kclass, long *launches, double *total_ms);
+/* number of kernels this context has launched since it was created */
+SU2B_API int su2b_kernel_launches(su2b_ctx *ctx, long *count);
+
 #ifdef __cplusplus
 }
 #endif

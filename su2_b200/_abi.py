@@ -80,7 +80,15 @@ SIGNATURES = {
     "su2b_solve": (i32, [_P, C.POINTER(SolveParams), _D, _D, _D, C.POINTER(SolveStats)]),
     "su2b_fermion_force": (i32, [_P, f64, _D, f64, i32, _D, i64, _D, C.POINTER(C.c_long)]),
     "su2b_fermion_action": (i32, [_P, f64, _D, f64, i32, _D, i64, _D]),
+    "su2b_profile": (i32, [_P, i32]),
+    "su2b_profile_read": (i32, [_P, i32, C.POINTER(C.c_long), C.POINTER(C.c_double)]),
+    "su2b_kernel_launches": (i32, [_P, C.POINTER(C.c_long)]),
 }
+
+K_FORCE, K_UPDATE, K_PLAQUETTE, K_MOMENTA, K_RESTORE, K_METROPOLIS, K_CLOVER, K_STAGGERED, \
+    K_OTHER = range(9)
+K_NAMES = ["force", "update", "plaquette", "momenta", "restore", "metropolis", "clover",
+           "staggered", "other"]
 
 _lib = None
 

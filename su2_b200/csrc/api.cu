@@ -166,6 +166,11 @@ extern "C" int su2b_ctx_destroy(su2b_ctx *ctx) {
   if (!ctx) return SU2B_ERR_INVALID;
   cudaSetDevice(ctx->device);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  for (auto &p : ctx->pend) {
+    cudaEventDestroy(p.a);
+    cudaEventDestroy(p.b);
+  }
+  for (cudaEvent_t e : ctx->ev_pool) cudaEventDestroy(e);
   for (auto &kv : ctx->graphs) cudaGraphExecDestroy(kv.second);
   for (void *p : ctx->allocs) cudaFree(p);
   if (ctx->h_red) cudaFreeHost(ctx->h_red);
@@ -197,6 +202,63 @@ extern "C" int su2b_synchronize(su2b_ctx *ctx) {
 }
 
 // ------------------------------------------------------------------------------------
+// device timers
+cudaEvent_t su2b_ev_take(su2b_ctx *ctx) {
+  if (ctx->ev_pool.empty()) {
+    cudaEvent_t e = nullptr;
+    cudaEventCreate(&e);
+    return e;
+  }
+  cudaEvent_t e = ctx->ev_pool.back();
+  ctx->ev_pool.pop_back();
+  return e;
+}
+void su2b_ev_mark(su2b_ctx *ctx, int kclass, cudaEvent_t start) {
+  cudaEvent_t b = su2b_ev_take(ctx);
+  cudaEventRecord(b, ctx->stream);
+  ctx->pend.push_back({kclass, start, b});
+}
+// resolve the recorded event pairs (synchronises the stream)
+int su2b_prof_fold(su2b_ctx *ctx) {
+  if (ctx->pend.empty()) return SU2B_OK;
+  CK(cudaStreamSynchronize(ctx->stream));
+  for (auto &p : ctx->pend) {
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, p.a, p.b) == cudaSuccess) {
+      ctx->prof_ms[p.k] += ms;
+      ctx->prof_n[p.k]++;
+    }
+    ctx->ev_pool.push_back(p.a);
+    ctx->ev_pool.push_back(p.b);
+  }
+  ctx->pend.clear();
+  return SU2B_OK;
+}
+extern "C" int su2b_profile(su2b_ctx *ctx, int enable) {
+  CKS(enter(ctx));
+  CKS(su2b_prof_fold(ctx));
+  ctx->prof = enable != 0;
+  for (int k = 0; k < 16; k++) {
+    ctx->prof_ms[k] = 0.;
+    ctx->prof_n[k] = 0;
+  }
+  return SU2B_OK;
+}
+extern "C" int su2b_profile_read(su2b_ctx *ctx, int kclass, long *launches, double *total_ms) {
+  CKS(enter(ctx));
+  NEED(kclass >= 0 && kclass < SU2B_K_COUNT, "kernel class %d", kclass);
+  CKS(su2b_prof_fold(ctx));
+  if (launches) *launches = ctx->prof_n[kclass];
+  if (total_ms) *total_ms = ctx->prof_ms[kclass];
+  return SU2B_OK;
+}
+extern "C" int su2b_kernel_launches(su2b_ctx *ctx, long *count) {
+  if (!ctx || !count) return SU2B_ERR_INVALID;
+  *count = ctx->launches;
+  return SU2B_OK;
+}
+
+// ------------------------------------------------------------------------------------
 // transfers
 extern "C" int su2b_upload_gauge(su2b_ctx *ctx, const double *U_host) {
   CKS(enter(ctx));
@@ -205,9 +267,9 @@ extern "C" int su2b_upload_gauge(su2b_ctx *ctx, const double *U_host) {
   CK(cudaMemcpyAsync(ctx->stage, U_host, n * sizeof(double), cudaMemcpyHostToDevice,
                      ctx->stream));
   if (ctx->link64)
-    CK(links_from_host<double>(ctx->g, ctx->stage, ctx->U, ctx->group, ctx->stream));
+    SU2B_LAUNCH(SU2B_K_OTHER, links_from_host<double>(ctx->g, ctx->stage, ctx->U, ctx->group, ctx->stream));
   else
-    CK(links_from_host<float>(ctx->g, ctx->stage, ctx->U, ctx->group, ctx->stream));
+    SU2B_LAUNCH(SU2B_K_OTHER, links_from_host<float>(ctx->g, ctx->stage, ctx->U, ctx->group, ctx->stream));
   CK(cudaStreamSynchronize(ctx->stream));
   ctx->phases_valid = false;
   return SU2B_OK;
@@ -215,9 +277,9 @@ extern "C" int su2b_upload_gauge(su2b_ctx *ctx, const double *U_host) {
 
 int su2b_links_to_stage(su2b_ctx *ctx, const void *U) {
   if (ctx->link64)
-    CK(links_to_host<double>(ctx->g, U, ctx->stage, ctx->group, ctx->stream));
+    SU2B_LAUNCH(SU2B_K_OTHER, links_to_host<double>(ctx->g, U, ctx->stage, ctx->group, ctx->stream));
   else
-    CK(links_to_host<float>(ctx->g, U, ctx->stage, ctx->group, ctx->stream));
+    SU2B_LAUNCH(SU2B_K_OTHER, links_to_host<float>(ctx->g, U, ctx->stage, ctx->group, ctx->stream));
   return SU2B_OK;
 }
 
@@ -238,17 +300,17 @@ int su2b_adj_upload(su2b_ctx *ctx, const double *host, void *dev) {
   CK(cudaMemcpyAsync(ctx->stage, host, n * sizeof(double), cudaMemcpyHostToDevice,
                      ctx->stream));
   if (ctx->link64)
-    CK(adj_from_host<double>(ctx->g, ctx->stage, (double *)dev, ctx->group, ctx->stream));
+    SU2B_LAUNCH(SU2B_K_OTHER, adj_from_host<double>(ctx->g, ctx->stage, (double *)dev, ctx->group, ctx->stream));
   else
-    CK(adj_from_host<float>(ctx->g, ctx->stage, (float *)dev, ctx->group, ctx->stream));
+    SU2B_LAUNCH(SU2B_K_OTHER, adj_from_host<float>(ctx->g, ctx->stage, (float *)dev, ctx->group, ctx->stream));
   return SU2B_OK;
 }
 int su2b_adj_download(su2b_ctx *ctx, const void *dev, double *host) {
   const size_t n = ctx->NL * (ctx->group == 0 ? 3 : 1);
   if (ctx->link64)
-    CK(adj_to_host<double>(ctx->g, (const double *)dev, ctx->stage, ctx->group, ctx->stream));
+    SU2B_LAUNCH(SU2B_K_OTHER, adj_to_host<double>(ctx->g, (const double *)dev, ctx->stage, ctx->group, ctx->stream));
   else
-    CK(adj_to_host<float>(ctx->g, (const float *)dev, ctx->stage, ctx->group, ctx->stream));
+    SU2B_LAUNCH(SU2B_K_OTHER, adj_to_host<float>(ctx->g, (const float *)dev, ctx->stage, ctx->group, ctx->stream));
   CK(cudaMemcpyAsync(host, ctx->stage, n * sizeof(double), cudaMemcpyDeviceToHost,
                      ctx->stream));
   CK(cudaStreamSynchronize(ctx->stream));
@@ -261,20 +323,20 @@ int su2b_q_plaq(su2b_ctx *ctx, const void *U, int red_slot) {
   int nb = 0;
   double *part = ctx->part_slot(0);
   if (ctx->link64)
-    CK(plaq_partials<double>(ctx->g, U, ctx->group, ctx->xi, part, &nb, ctx->stream));
+    SU2B_LAUNCH(SU2B_K_PLAQUETTE, plaq_partials<double>(ctx->g, U, ctx->group, ctx->xi, part, &nb, ctx->stream));
   else
-    CK(plaq_partials<float>(ctx->g, U, ctx->group, ctx->xi, part, &nb, ctx->stream));
-  CK(reduce_final(part, nb, 3, ctx->red + red_slot, ctx->stream));
+    SU2B_LAUNCH(SU2B_K_PLAQUETTE, plaq_partials<float>(ctx->g, U, ctx->group, ctx->xi, part, &nb, ctx->stream));
+  SU2B_LAUNCH(SU2B_K_OTHER, reduce_final(part, nb, 3, ctx->red + red_slot, ctx->stream));
   return SU2B_OK;
 }
 int su2b_q_clover(su2b_ctx *ctx, const void *U, int cloverdef, int red_slot) {
   int nb = 0;
   double *part = ctx->part_slot(2);
   if (ctx->link64)
-    CK(clover_partials<double>(ctx->g, U, ctx->group, cloverdef, part, &nb, ctx->stream));
+    SU2B_LAUNCH(SU2B_K_CLOVER, clover_partials<double>(ctx->g, U, ctx->group, cloverdef, part, &nb, ctx->stream));
   else
-    CK(clover_partials<float>(ctx->g, U, ctx->group, cloverdef, part, &nb, ctx->stream));
-  CK(reduce_final(part, nb, 3, ctx->red + red_slot, ctx->stream));
+    SU2B_LAUNCH(SU2B_K_CLOVER, clover_partials<float>(ctx->g, U, ctx->group, cloverdef, part, &nb, ctx->stream));
+  SU2B_LAUNCH(SU2B_K_OTHER, reduce_final(part, nb, 3, ctx->red + red_slot, ctx->stream));
   return SU2B_OK;
 }
 int su2b_fetch_red(su2b_ctx *ctx, int n) {
@@ -338,7 +400,7 @@ extern "C" int su2b_energy_density(su2b_ctx *ctx, int cloverdef, int ss, double 
 template <class T>
 static int q_force(su2b_ctx *ctx, const void *U, T *P, const T *extra, double f, double scale,
                    int mode, double *kin_part, int *nb) {
-  CK(force_update<T>(ctx->g, U, ctx->group, P, extra, f, scale, ctx->xi, mode, kin_part, nb,
+  SU2B_LAUNCH(SU2B_K_FORCE, force_update<T>(ctx->g, U, ctx->group, P, extra, f, scale, ctx->xi, mode, kin_part, nb,
                      ctx->stream));
   return SU2B_OK;
 }
@@ -351,17 +413,17 @@ int su2b_q_force(su2b_ctx *ctx, const void *U, void *P, const void *extra, doubl
 }
 int su2b_q_update(su2b_ctx *ctx, void *U, const void *P, double dt) {
   if (ctx->link64)
-    CK(link_update<double>(ctx->g, U, ctx->group, (const double *)P, dt, ctx->stream));
+    SU2B_LAUNCH(SU2B_K_UPDATE, link_update<double>(ctx->g, U, ctx->group, (const double *)P, dt, ctx->stream));
   else
-    CK(link_update<float>(ctx->g, U, ctx->group, (const float *)P, dt, ctx->stream));
+    SU2B_LAUNCH(SU2B_K_UPDATE, link_update<float>(ctx->g, U, ctx->group, (const float *)P, dt, ctx->stream));
   ctx->phases_valid = false;
   return SU2B_OK;
 }
 int su2b_q_restore(su2b_ctx *ctx, void *U) {
   if (ctx->link64)
-    CK(restore_links<double>(ctx->g, U, ctx->group, ctx->stream));
+    SU2B_LAUNCH(SU2B_K_RESTORE, restore_links<double>(ctx->g, U, ctx->group, ctx->stream));
   else
-    CK(restore_links<float>(ctx->g, U, ctx->group, ctx->stream));
+    SU2B_LAUNCH(SU2B_K_RESTORE, restore_links<float>(ctx->g, U, ctx->group, ctx->stream));
   return SU2B_OK;
 }
 
@@ -398,16 +460,17 @@ extern "C" int su2b_metropolis_sweep(su2b_ctx *ctx, double delta, int N_hit, uin
   for (int mu = 0; mu < ctx->g.nd; mu++)
     for (int p = 0; p < 2; p++) {
       if (ctx->link64)
-        CK(metropolis_pass<double>(ctx->g, ctx->U, ctx->group, mu, p, ctx->beta, delta, N_hit,
+        SU2B_LAUNCH(SU2B_K_METROPOLIS, metropolis_pass<double>(ctx->g, ctx->U, ctx->group, mu, p, ctx->beta, delta, N_hit,
                                    seed, sweep, ctx->counts, ctx->stream));
       else
-        CK(metropolis_pass<float>(ctx->g, ctx->U, ctx->group, mu, p, ctx->beta, delta, N_hit,
+        SU2B_LAUNCH(SU2B_K_METROPOLIS, metropolis_pass<float>(ctx->g, ctx->U, ctx->group, mu, p, ctx->beta, delta, N_hit,
                                   seed, sweep, ctx->counts, ctx->stream));
     }
   CK(cudaMemcpyAsync(ctx->h_counts, ctx->counts, 2 * sizeof(unsigned long long),
                      cudaMemcpyDeviceToHost, ctx->stream));
   CK(cudaStreamSynchronize(ctx->stream));
   ctx->phases_valid = false;
+  if (ctx->pend.size() > 4096) CKS(su2b_prof_fold(ctx));
   const double nh = (double)(N_hit > 0 ? N_hit : 1);
   rates[0] = (double)ctx->h_counts[0] / nh / (double)ctx->NL;
   rates[1] = (double)ctx->h_counts[1] / nh / (double)ctx->V;

@@ -28,8 +28,8 @@ template <class T, int ND, int NT>
 __global__ void __launch_bounds__(NT)
   k_clover_su2(Geom g, const LinkT<T> *__restrict__ U, int cloverdef, double *part) {
   __shared__ double sh[NT / 32];
-  const int p = blockIdx.y;
-  const int cb = blockIdx.x * NT + threadIdx.x;
+  const int p = blockIdx.x & 1;
+  const int cb = (blockIdx.x >> 1) * NT + threadIdx.x;
   double e_all = 0., e_ss = 0., q = 0.;
   if (cb < g.Vh) {
     const Site s = site_from_eo(g, p, cb);
@@ -73,7 +73,7 @@ __global__ void __launch_bounds__(NT)
       q += retr_mul(G[2][3], G[0][1]);
     }
   }
-  const int b = blockIdx.y * gridDim.x + blockIdx.x;
+  const int b = blockIdx.x;
   double r = block_sum<NT>(e_all, sh);
   if (threadIdx.x == 0) part[3 * b] = r;
   r = block_sum<NT>(e_ss, sh);
@@ -86,8 +86,8 @@ template <int ND, int NT>
 __global__ void __launch_bounds__(NT)
   k_clover_u1(Geom g, const double *__restrict__ U, int cloverdef, double *part) {
   __shared__ double sh[NT / 32];
-  const int p = blockIdx.y;
-  const int cb = blockIdx.x * NT + threadIdx.x;
+  const int p = blockIdx.x & 1;
+  const int cb = (blockIdx.x >> 1) * NT + threadIdx.x;
   double e_all = 0., e_ss = 0., q = 0.;
   if (cb < g.Vh) {
     const Site s = site_from_eo(g, p, cb);
@@ -125,7 +125,7 @@ __global__ void __launch_bounds__(NT)
     }
     if (ND == 2) q += -G[0][1];
   }
-  const int b = blockIdx.y * gridDim.x + blockIdx.x;
+  const int b = blockIdx.x;
   double r = block_sum<NT>(e_all, sh);
   if (threadIdx.x == 0) part[3 * b] = r;
   r = block_sum<NT>(e_ss, sh);
@@ -140,8 +140,8 @@ template <class T>
 cudaError_t clover_partials(const Geom &g, const void *U, int group, int cloverdef,
                             double *part, int *nblocks, cudaStream_t s) {
   constexpr int NT = 128;
-  const dim3 grid((g.Vh + NT - 1) / NT, 2);
-  *nblocks = grid.x * grid.y;
+  const dim3 grid(2 * ((g.Vh + NT - 1) / NT));
+  *nblocks = grid.x;
   if (group == 0) {
     const LinkT<T> *u = (const LinkT<T> *)U;
     switch (g.nd) {

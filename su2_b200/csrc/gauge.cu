@@ -90,8 +90,8 @@ template <class T, int ND, int NT>
 __global__ void __launch_bounds__(NT)
   k_plaq_su2(Geom g, const LinkT<T> *__restrict__ U, double xi, double *part) {
   __shared__ double sh[NT / 32];
-  const int p = blockIdx.y;
-  const int cb = blockIdx.x * NT + threadIdx.x;
+  const int p = blockIdx.x & 1;
+  const int cb = (blockIdx.x >> 1) * NT + threadIdx.x;
   double full = 0., spat = 0., wsum = 0.;
   if (cb < g.Vh) {
     const Site s = site_from_eo(g, p, cb);
@@ -113,7 +113,7 @@ __global__ void __launch_bounds__(NT)
       }
     }
   }
-  const int b = blockIdx.y * gridDim.x + blockIdx.x;
+  const int b = blockIdx.x;
   double r = block_sum<NT>(full, sh);
   if (threadIdx.x == 0) part[3 * b] = r;
   r = block_sum<NT>(spat, sh);
@@ -126,8 +126,8 @@ template <int ND, int NT>
 __global__ void __launch_bounds__(NT)
   k_plaq_u1(Geom g, const double *__restrict__ U, double xi, double *part) {
   __shared__ double sh[NT / 32];
-  const int p = blockIdx.y;
-  const int cb = blockIdx.x * NT + threadIdx.x;
+  const int p = blockIdx.x & 1;
+  const int cb = (blockIdx.x >> 1) * NT + threadIdx.x;
   double full = 0., spat = 0., wsum = 0.;
   if (cb < g.Vh) {
     const Site s = site_from_eo(g, p, cb);
@@ -149,7 +149,7 @@ __global__ void __launch_bounds__(NT)
       }
     }
   }
-  const int b = blockIdx.y * gridDim.x + blockIdx.x;
+  const int b = blockIdx.x;
   double r = block_sum<NT>(full, sh);
   if (threadIdx.x == 0) part[3 * b] = r;
   r = block_sum<NT>(spat, sh);
@@ -170,86 +170,107 @@ __global__ void __launch_bounds__(NT)
   }
 }
 
-// ------------------------------------------------------------------------------------
-// staple sum K (get_staples.hh:26-80) for link (x, mu): forward staples for all nu != mu,
-// then backward ones, each optionally weighted by 1/xi (temporal plane) or xi (spatial).
-template <class T, int ND>
-__device__ __forceinline__ Su2<T> staple_su2(const Geom &g, const LinkT<T> *__restrict__ U,
-                                             const Site &s, int mu, int aniso, T wt, T ws) {
-  const int p = s.p;
-  const int lpm = s.lex + fwd(g, s, mu);
-  Su2<T> K = zero_su2<T>();
-#pragma unroll
-  for (int nu = 0; nu < ND; nu++) {
-    if (nu == mu) continue;
-    const int lpn = s.lex + fwd(g, s, nu);
-    const Su2<T> A = ld_link(U + (size_t)nu * g.V + eo_of(g, lpm, 1 - p));
-    const Su2<T> B = ld_link(U + (size_t)mu * g.V + eo_of(g, lpn, 1 - p));
-    const Su2<T> D = ld_link(U + (size_t)nu * g.V + eo_of(g, s.lex, p));
-    Su2<T> st = mul(mul(A, dag(B)), dag(D));
-    if (aniso) st = scale((nu == 0 || mu == 0) ? wt : ws, st);
-    K = add(K, st);
-  }
-#pragma unroll
-  for (int nu = 0; nu < ND; nu++) {
-    if (nu == mu) continue;
-    const int b = bwd(g, s, nu);
-    const int lmn = s.lex + b, lpmmn = lpm + b;
-    const Su2<T> A = ld_link(U + (size_t)nu * g.V + eo_of(g, lpmmn, p));
-    const Su2<T> B = ld_link(U + (size_t)mu * g.V + eo_of(g, lmn, 1 - p));
-    const Su2<T> D = ld_link(U + (size_t)nu * g.V + eo_of(g, lmn, 1 - p));
-    Su2<T> st = mul(mul(dag(A), dag(B)), D);
-    if (aniso) st = scale((nu == 0 || mu == 0) ? wt : ws, st);
-    K = add(K, st);
-  }
-  return K;
-}
-
-// fused gauge force + momentum update (flat-gaugemonomial.hh:105-131 + update_momenta.hh:10-33):
-//   d = f * get_deriv(U K) (+ extra),  P = P + scale*d   (scale = -dtau)
+// Fused gauge force + momentum update for all ND links of a site
+// (flat-gaugemonomial.hh:105-131 + update_momenta.hh:10-33):
+//   K_mu = sum_{nu != mu} U_nu(x+mu) U_mu(x+nu)^+ U_nu(x)^+ + U_nu(x+mu-nu)^+ U_mu(x-nu)^+ U_nu(x-nu)
+//   d_mu = f * get_deriv(U_mu(x) K_mu) (+ extra),  P_mu = P_mu + scale * d_mu  (scale = -dtau)
+// One thread per site.  The two forward staples of a plane share the product
+// A = U_nu(x+mu) U_mu(x+nu)^+:  forward(mu; nu) = A U_nu(x)^+,  forward(nu; mu) = A^+ U_mu(x)^+.
+// Per site 4 + ND(ND-1) + ND^2 + ND(ND-1) = 44 (d = 4) distinct link loads.  Blocks alternate
+// between the parities (block b -> parity b & 1), so the blocks resident at any time cover
+// one narrow band of sites in every direction and parity and the links stream from HBM about
+// once per launch.
 template <class T, int ND, int NT>
 __global__ void __launch_bounds__(NT)
   k_force_su2(Geom g, const LinkT<T> *__restrict__ U, T *__restrict__ P,
               const T *__restrict__ extra, T f, T scale_, int mode, int aniso, T wt, T ws,
               double *kin_part) {
   __shared__ double sh[NT / 32];
-  const int mu = blockIdx.y >> 1, p = blockIdx.y & 1;
-  const int cb = blockIdx.x * NT + threadIdx.x;
+  const int p = blockIdx.x & 1, q = 1 - p;
+  const int cb = (blockIdx.x >> 1) * NT + threadIdx.x;
   double k2 = 0.;
   if (cb < g.Vh) {
     const Site s = site_from_eo(g, p, cb);
-    const Su2<T> K = staple_su2<T, ND>(g, U, s, mu, aniso, wt, ws);
-    const size_t NL = (size_t)g.V * ND;
-    const size_t l = (size_t)mu * g.V + (size_t)p * g.Vh + cb;
-    const Su2<T> u = ld_link(U + l);
-    // get_deriv(U K) = (2 Im b, 2 Re b, 2 Im a) (adjointfield.hh:53-56)
-    const T sbi = u.ar * K.bi + u.ai * K.br + (u.bi * K.ar - u.br * K.ai);
-    const T sbr = u.ar * K.br - u.ai * K.bi + (u.br * K.ar + u.bi * K.ai);
-    const T sai = u.ar * K.ai + u.ai * K.ar - (u.bi * K.br - u.br * K.bi);
-    T d0 = f * (T(2) * sbi), d1 = f * (T(2) * sbr), d2 = f * (T(2) * sai);
-    if (mode & FM_EXTRA) {
-      d0 += extra[l];
-      d1 += extra[NL + l];
-      d2 += extra[2 * NL + l];
+    const size_t V = (size_t)g.V, NL = V * ND;
+    const size_t self = (size_t)p * g.Vh + cb;
+    int lf[ND], lb[ND];
+#pragma unroll
+    for (int mu = 0; mu < ND; mu++) {
+      lf[mu] = s.lex + fwd(g, s, mu);
+      lb[mu] = bwd(g, s, mu);
     }
-    T p0, p1, p2;
-    if (mode & FM_HAS_IN) {
-      p0 = P[l] + scale_ * d0;
-      p1 = P[NL + l] + scale_ * d1;
-      p2 = P[2 * NL + l] + scale_ * d2;
-    } else {
-      p0 = scale_ * d0;
-      p1 = scale_ * d1;
-      p2 = scale_ * d2;
+    Su2<T> ux[ND], K[ND];
+#pragma unroll
+    for (int mu = 0; mu < ND; mu++) {
+      ux[mu] = ld_link(U + mu * V + self);
+      K[mu] = zero_su2<T>();
     }
-    P[l] = p0;
-    P[NL + l] = p1;
-    P[2 * NL + l] = p2;
-    k2 = (double)p0 * p0 + (double)p1 * p1 + (double)p2 * p2;
+    // forward staples, one plane (mu < nu) at a time
+#pragma unroll
+    for (int mu = 0; mu < ND - 1; mu++)
+#pragma unroll
+      for (int nu = mu + 1; nu < ND; nu++) {
+        const Su2<T> a = ld_link(U + nu * V + eo_of(g, lf[mu], q));  // U_nu(x+mu)
+        const Su2<T> b = ld_link(U + mu * V + eo_of(g, lf[nu], q));  // U_mu(x+nu)
+        const Su2<T> A = mul(a, dag(b));
+        Su2<T> fmn = mul(A, dag(ux[nu]));
+        Su2<T> fnm = mul(dag(A), dag(ux[mu]));
+        if (aniso) {
+          const T w = (mu == 0) ? wt : ws;
+          fmn = scale(w, fmn);
+          fnm = scale(w, fnm);
+        }
+        K[mu] = add(K[mu], fmn);
+        K[nu] = add(K[nu], fnm);
+      }
+    // backward staples U_nu(x+mu-nu)^+ U_mu(x-nu)^+ U_nu(x-nu)
+#pragma unroll
+    for (int nu = 0; nu < ND; nu++) {
+      const int lmn = s.lex + lb[nu];
+      const Su2<T> c = ld_link(U + nu * V + eo_of(g, lmn, q));  // U_nu(x-nu)
+#pragma unroll
+      for (int mu = 0; mu < ND; mu++) {
+        if (mu == nu) continue;
+        const Su2<T> h = ld_link(U + mu * V + eo_of(g, lmn, q));          // U_mu(x-nu)
+        const Su2<T> e = ld_link(U + nu * V + eo_of(g, lf[mu] + lb[nu], p));  // U_nu(x+mu-nu)
+        Su2<T> st = mul(mul(dag(e), dag(h)), c);
+        if (aniso) st = scale((nu == 0 || mu == 0) ? wt : ws, st);
+        K[mu] = add(K[mu], st);
+      }
+    }
+#pragma unroll
+    for (int mu = 0; mu < ND; mu++) {
+      const Su2<T> &u = ux[mu];
+      const Su2<T> &k = K[mu];
+      const size_t l = mu * V + self;
+      // get_deriv(U K) = (2 Im b, 2 Re b, 2 Im a) (adjointfield.hh:53-56)
+      const T sbi = u.ar * k.bi + u.ai * k.br + (u.bi * k.ar - u.br * k.ai);
+      const T sbr = u.ar * k.br - u.ai * k.bi + (u.br * k.ar + u.bi * k.ai);
+      const T sai = u.ar * k.ai + u.ai * k.ar - (u.bi * k.br - u.br * k.bi);
+      T d0 = f * (T(2) * sbi), d1 = f * (T(2) * sbr), d2 = f * (T(2) * sai);
+      if (mode & FM_EXTRA) {
+        d0 += extra[l];
+        d1 += extra[NL + l];
+        d2 += extra[2 * NL + l];
+      }
+      T p0 = 0, p1 = 0, p2 = 0;
+      if (mode & FM_HAS_IN) {
+        p0 = P[l];
+        p1 = P[NL + l];
+        p2 = P[2 * NL + l];
+      }
+      p0 = p0 + scale_ * d0;
+      p1 = p1 + scale_ * d1;
+      p2 = p2 + scale_ * d2;
+      P[l] = p0;
+      P[NL + l] = p1;
+      P[2 * NL + l] = p2;
+      k2 += (double)p0 * p0 + (double)p1 * p1 + (double)p2 * p2;
+    }
   }
   if (mode & FM_KINETIC) {
     const double r = block_sum<NT>(k2, sh);
-    if (threadIdx.x == 0) kin_part[blockIdx.y * gridDim.x + blockIdx.x] = r;
+    if (threadIdx.x == 0) kin_part[blockIdx.x] = r;
   }
 }
 
@@ -488,8 +509,8 @@ template <class T>
 cudaError_t plaq_partials(const Geom &g, const void *U, int group, double xi, double *part,
                           int *nblocks, cudaStream_t s) {
   constexpr int NT = 256;
-  const dim3 grid(cdiv(g.Vh, NT), 2);
-  *nblocks = grid.x * grid.y;
+  const dim3 grid(2 * cdiv(g.Vh, NT));
+  *nblocks = grid.x;
   if (group == 0) {
     const LinkT<T> *u = (const LinkT<T> *)U;
     switch (g.nd) {
@@ -519,10 +540,10 @@ cudaError_t force_update(const Geom &g, const void *U, int group, T *P, const T 
                          double scale, double xi, int mode, double *kin_part, int *nblocks,
                          cudaStream_t s) {
   constexpr int NT = 128;
-  const dim3 grid(cdiv(g.Vh, NT), 2 * g.nd);
-  if (nblocks) *nblocks = grid.x * grid.y;
   const int aniso = xi != 1.0;
   if (group == 0) {
+    const dim3 grid(2 * cdiv(g.Vh, NT));
+    if (nblocks) *nblocks = grid.x;
     const LinkT<T> *u = (const LinkT<T> *)U;
     const T wt = (T)(1.0 / xi), ws = (T)xi;
     switch (g.nd) {
@@ -541,6 +562,8 @@ cudaError_t force_update(const Geom &g, const void *U, int group, T *P, const T 
     }
   } else {
     if (sizeof(T) != 8) return cudaErrorNotSupported;
+    const dim3 grid(cdiv(g.Vh, NT), 2 * g.nd);
+    if (nblocks) *nblocks = grid.x * grid.y;
     const double *u = (const double *)U;
     double *PP = (double *)P;
     const double *ex = (const double *)extra;

@@ -120,7 +120,7 @@ int integrate(su2b_ctx *ctx, const std::vector<Op> &ops, const su2b_hmc_params *
       SU2B_CKS(su2b_q_force(ctx, ctx->U, ctx->P, extra, f, -ops[i].c, mode, ctx->part_slot(1),
                             &nb));
       if (mode & FM_KINETIC)
-        SU2B_CK(reduce_final(ctx->part_slot(1), nb, 1, ctx->red + kin_slot, ctx->stream));
+        SU2B_LAUNCH(SU2B_K_OTHER, reduce_final(ctx->part_slot(1), nb, 1, ctx->red + kin_slot, ctx->stream));
     } else {
       SU2B_CKS(su2b_q_update(ctx, ctx->U, ctx->P, ops[i].c));
     }
@@ -131,12 +131,12 @@ int integrate(su2b_ctx *ctx, const std::vector<Op> &ops, const su2b_hmc_params *
 int kinetic_now(su2b_ctx *ctx, int slot) {
   int nb = 0;
   if (ctx->link64)
-    SU2B_CK(kinetic_partials<double>(ctx->g, (const double *)ctx->P, ctx->group,
+    SU2B_LAUNCH(SU2B_K_OTHER, kinetic_partials<double>(ctx->g, (const double *)ctx->P, ctx->group,
                                      ctx->part_slot(1), &nb, ctx->stream));
   else
-    SU2B_CK(kinetic_partials<float>(ctx->g, (const float *)ctx->P, ctx->group,
+    SU2B_LAUNCH(SU2B_K_OTHER, kinetic_partials<float>(ctx->g, (const float *)ctx->P, ctx->group,
                                     ctx->part_slot(1), &nb, ctx->stream));
-  SU2B_CK(reduce_final(ctx->part_slot(1), nb, 1, ctx->red + slot, ctx->stream));
+  SU2B_LAUNCH(SU2B_K_OTHER, reduce_final(ctx->part_slot(1), nb, 1, ctx->red + slot, ctx->stream));
   return SU2B_OK;
 }
 
@@ -167,12 +167,12 @@ extern "C" int su2b_hmc_trajectory(su2b_ctx *ctx, const su2b_hmc_params *prm,
     SU2B_CKS(kinetic_now(ctx, 0));
   } else {
     if (ctx->link64)
-      SU2B_CK(momenta_philox<double>(ctx->g, (double *)ctx->P, ctx->group, prm->seed, prm->traj,
+      SU2B_LAUNCH(SU2B_K_MOMENTA, momenta_philox<double>(ctx->g, (double *)ctx->P, ctx->group, prm->seed, prm->traj,
                                      ctx->part_slot(1), &nb, s));
     else
-      SU2B_CK(momenta_philox<float>(ctx->g, (float *)ctx->P, ctx->group, prm->seed, prm->traj,
+      SU2B_LAUNCH(SU2B_K_MOMENTA, momenta_philox<float>(ctx->g, (float *)ctx->P, ctx->group, prm->seed, prm->traj,
                                     ctx->part_slot(1), &nb, s));
-    SU2B_CK(reduce_final(ctx->part_slot(1), nb, 1, ctx->red + 0, s));
+    SU2B_LAUNCH(SU2B_K_OTHER, reduce_final(ctx->part_slot(1), nb, 1, ctx->red + 0, s));
   }
   SU2B_CK(cudaMemsetAsync(ctx->red + 8, 0, 2 * sizeof(double), s));
   if (ferm)
@@ -197,7 +197,7 @@ extern "C" int su2b_hmc_trajectory(su2b_ctx *ctx, const su2b_hmc_params *prm,
   in.traj = prm->traj;
   in.u_host = prm->uniform_host;
   in.accept_reject = prm->accept_reject;
-  SU2B_CK(accept_step(ctx->red, in, ctx->traj, s));
+  SU2B_LAUNCH(SU2B_K_OTHER, accept_step(ctx->red, in, ctx->traj, s));
 
   if (prm->revtest) {  // md_update.hh:62-74
     if (!ctx->U_rev) {
@@ -207,9 +207,9 @@ extern "C" int su2b_hmc_trajectory(su2b_ctx *ctx, const su2b_hmc_params *prm,
     SU2B_CK(cudaMemcpyAsync(ctx->U_rev, ctx->U, ctx->link_bytes() * ctx->NL,
                             cudaMemcpyDeviceToDevice, s));
     if (ctx->link64)
-      SU2B_CK(negate_adj<double>(ctx->g, (double *)ctx->P, ctx->group, s));
+      SU2B_LAUNCH(SU2B_K_OTHER, negate_adj<double>(ctx->g, (double *)ctx->P, ctx->group, s));
     else
-      SU2B_CK(negate_adj<float>(ctx->g, (float *)ctx->P, ctx->group, s));
+      SU2B_LAUNCH(SU2B_K_OTHER, negate_adj<float>(ctx->g, (float *)ctx->P, ctx->group, s));
     SU2B_CKS(integrate(ctx, ops, prm, 10, &cg_iters));
     SU2B_CKS(su2b_q_plaq(ctx, ctx->U, 11));
     SU2B_CK(cudaMemsetAsync(ctx->red + 14, 0, sizeof(double), s));
@@ -224,9 +224,9 @@ extern "C" int su2b_hmc_trajectory(su2b_ctx *ctx, const su2b_hmc_params *prm,
     ctx->phases_valid = ctx->phases32_valid = false;
   }
   if (ctx->link64)
-    SU2B_CK(cond_restore<double>(ctx->g, ctx->U, ctx->U_old, ctx->group, ctx->traj, s));
+    SU2B_LAUNCH(SU2B_K_OTHER, cond_restore<double>(ctx->g, ctx->U, ctx->U_old, ctx->group, ctx->traj, s));
   else
-    SU2B_CK(cond_restore<float>(ctx->g, ctx->U, ctx->U_old, ctx->group, ctx->traj, s));
+    SU2B_LAUNCH(SU2B_K_OTHER, cond_restore<float>(ctx->g, ctx->U, ctx->U_old, ctx->group, ctx->traj, s));
   ctx->phases_valid = ctx->phases32_valid = false;
   SU2B_CKS(su2b_q_plaq(ctx, ctx->U, 16));
   SU2B_CK(cudaMemcpyAsync(ctx->h_traj, ctx->traj, sizeof(TrajDev), cudaMemcpyDeviceToHost, s));
@@ -249,5 +249,6 @@ extern "C" int su2b_hmc_trajectory(su2b_ctx *ctx, const su2b_hmc_params *prm,
   }
   res->plaquette = r[16];
   res->cg_iterations = cg_iters;
+  if (ctx->pend.size() > 4096) SU2B_CKS(su2b_prof_fold(ctx));
   return SU2B_OK;
 }

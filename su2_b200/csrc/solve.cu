@@ -32,11 +32,11 @@ int dalloc2(su2b_ctx *ctx, void **p, size_t bytes) {
 int put_spinor(su2b_ctx *ctx, const double *host, double2 *dev) {
   SU2B_CK(cudaMemcpyAsync(ctx->stage, host, 2 * ctx->V * sizeof(double), cudaMemcpyHostToDevice,
                           ctx->stream));
-  SU2B_CK(spinor_from_host(ctx->g, ctx->stage, dev, ctx->stream));
+  SU2B_LAUNCH(SU2B_K_OTHER, spinor_from_host(ctx->g, ctx->stage, dev, ctx->stream));
   return SU2B_OK;
 }
 int get_spinor(su2b_ctx *ctx, const double2 *dev, double *host) {
-  SU2B_CK(spinor_to_host(ctx->g, dev, ctx->stage, ctx->stream));
+  SU2B_LAUNCH(SU2B_K_OTHER, spinor_to_host(ctx->g, dev, ctx->stage, ctx->stream));
   SU2B_CK(cudaMemcpyAsync(host, ctx->stage, 2 * ctx->V * sizeof(double), cudaMemcpyDeviceToHost,
                           ctx->stream));
   SU2B_CK(cudaStreamSynchronize(ctx->stream));
@@ -58,12 +58,12 @@ int fetch_state(su2b_ctx *ctx) {
 
 int ensure_phases(su2b_ctx *ctx, bool need32) {
   if (!ctx->phases_valid) {
-    SU2B_CK(u1_phases(ctx->g, (const double *)ctx->U, ctx->ph, ctx->stream));
+    SU2B_LAUNCH(SU2B_K_OTHER, u1_phases(ctx->g, (const double *)ctx->U, ctx->ph, ctx->stream));
     ctx->phases_valid = true;
     ctx->phases32_valid = false;
   }
   if (need32 && !ctx->phases32_valid) {
-    SU2B_CK(u1_phases_f32(ctx->g, (const double *)ctx->U, ctx->ph32, ctx->stream));
+    SU2B_LAUNCH(SU2B_K_OTHER, u1_phases_f32(ctx->g, (const double *)ctx->U, ctx->ph32, ctx->stream));
     ctx->phases32_valid = true;
   }
   return SU2B_OK;
@@ -71,9 +71,9 @@ int ensure_phases(su2b_ctx *ctx, bool need32) {
 
 // out = D Ddag in (uses SV_T as scratch)
 int apply_ddag64(su2b_ctx *ctx, double m, const double2 *in, double2 *out) {
-  SU2B_CK(hop64(ctx->g, ctx->ph, m, 1, in, ctx->sv[SV_T], nullptr, nullptr, nullptr, nullptr, 0,
+  SU2B_LAUNCH(SU2B_K_STAGGERED, hop64(ctx->g, ctx->ph, m, 1, in, ctx->sv[SV_T], nullptr, nullptr, nullptr, nullptr, 0,
                 ctx->stream));
-  SU2B_CK(hop64(ctx->g, ctx->ph, m, 0, ctx->sv[SV_T], out, nullptr, nullptr, nullptr, nullptr, 0,
+  SU2B_LAUNCH(SU2B_K_STAGGERED, hop64(ctx->g, ctx->ph, m, 0, ctx->sv[SV_T], out, nullptr, nullptr, nullptr, nullptr, 0,
                 ctx->stream));
   return SU2B_OK;
 }
@@ -85,10 +85,10 @@ int true_residual(su2b_ctx *ctx, double m, bool ddag, const double2 *b, const do
   if (ddag)
     SU2B_CKS(apply_ddag64(ctx, m, x, ctx->sv[SV_AP]));
   else
-    SU2B_CK(hop64(ctx->g, ctx->ph, m, 0, x, ctx->sv[SV_AP], nullptr, nullptr, nullptr, nullptr,
+    SU2B_LAUNCH(SU2B_K_STAGGERED, hop64(ctx->g, ctx->ph, m, 0, x, ctx->sv[SV_AP], nullptr, nullptr, nullptr, nullptr,
                   0, ctx->stream));
-  SU2B_CK(resid64(n, b, ctx->sv[SV_AP], r, ctx->part_slot(4), ctx->stream));
-  SU2B_CK(reduce_final(ctx->part_slot(4), vec_blocks(n), 1, ctx->red + slot, ctx->stream));
+  SU2B_LAUNCH(SU2B_K_OTHER, resid64(n, b, ctx->sv[SV_AP], r, ctx->part_slot(4), ctx->stream));
+  SU2B_LAUNCH(SU2B_K_OTHER, reduce_final(ctx->part_slot(4), vec_blocks(n), 1, ctx->red + slot, ctx->stream));
   return SU2B_OK;
 }
 
@@ -123,12 +123,12 @@ int cg64(su2b_ctx *ctx, double m, double tol, int max_iter, su2b_solve_stats *st
     int done = h.done;
     while (!done) {
       for (int k = 0; k < CHUNK; k++) {
-        SU2B_CK(hop64(g, ctx->ph, m, 1, p, t, nullptr, nullptr, nullptr, ctx->st, 0, s));
-        SU2B_CK(hop64(g, ctx->ph, m, 0, t, Ap, p, dp, nullptr, ctx->st, 0, s));
-        SU2B_CK(cg_alpha(dp, hop_blocks(g), ctx->st, s));
-        SU2B_CK(cg_xr(n, x, r, p, Ap, ctx->st, np, s));
-        SU2B_CK(cg_beta(np, vec_blocks(n), ctx->st, s));
-        SU2B_CK(cg_p(n, r, p, ctx->st, s));
+        SU2B_LAUNCH(SU2B_K_STAGGERED, hop64(g, ctx->ph, m, 1, p, t, nullptr, nullptr, nullptr, ctx->st, 0, s));
+        SU2B_LAUNCH(SU2B_K_STAGGERED, hop64(g, ctx->ph, m, 0, t, Ap, p, dp, nullptr, ctx->st, 0, s));
+        SU2B_LAUNCH(SU2B_K_OTHER, cg_alpha(dp, hop_blocks(g), ctx->st, s));
+        SU2B_LAUNCH(SU2B_K_OTHER, cg_xr(n, x, r, p, Ap, ctx->st, np, s));
+        SU2B_LAUNCH(SU2B_K_OTHER, cg_beta(np, vec_blocks(n), ctx->st, s));
+        SU2B_LAUNCH(SU2B_K_OTHER, cg_p(n, r, p, ctx->st, s));
       }
       SU2B_CKS(fetch_state(ctx));
       done = ctx->h_st->done;
@@ -182,14 +182,14 @@ int bicgstab64(su2b_ctx *ctx, double m, double tol, int max_iter, su2b_solve_sta
     int done = h.done;
     while (!done) {
       for (int k = 0; k < CHUNK; k++) {
-        SU2B_CK(hop64(g, ctx->ph, m, 0, p, Ap, r0, dp, nullptr, ctx->st, 0, s));
-        SU2B_CK(bi_alpha(dp, hop_blocks(g), ctx->st, s));
-        SU2B_CK(bi_s(n, r, Ap, sv, ctx->st, s));
-        SU2B_CK(hop64(g, ctx->ph, m, 0, sv, t, sv, dp, np, ctx->st, 0, s));
-        SU2B_CK(bi_omega(dp, np, hop_blocks(g), ctx->st, s));
-        SU2B_CK(bi_rx(n, x, r, sv, t, p, r0, ctx->st, dp2, np2, s));
-        SU2B_CK(bi_beta(dp2, np2, vec_blocks(n), ctx->st, s));
-        SU2B_CK(bi_p(n, r, p, Ap, ctx->st, s));
+        SU2B_LAUNCH(SU2B_K_STAGGERED, hop64(g, ctx->ph, m, 0, p, Ap, r0, dp, nullptr, ctx->st, 0, s));
+        SU2B_LAUNCH(SU2B_K_OTHER, bi_alpha(dp, hop_blocks(g), ctx->st, s));
+        SU2B_LAUNCH(SU2B_K_OTHER, bi_s(n, r, Ap, sv, ctx->st, s));
+        SU2B_LAUNCH(SU2B_K_STAGGERED, hop64(g, ctx->ph, m, 0, sv, t, sv, dp, np, ctx->st, 0, s));
+        SU2B_LAUNCH(SU2B_K_OTHER, bi_omega(dp, np, hop_blocks(g), ctx->st, s));
+        SU2B_LAUNCH(SU2B_K_OTHER, bi_rx(n, x, r, sv, t, p, r0, ctx->st, dp2, np2, s));
+        SU2B_LAUNCH(SU2B_K_OTHER, bi_beta(dp2, np2, vec_blocks(n), ctx->st, s));
+        SU2B_LAUNCH(SU2B_K_OTHER, bi_p(n, r, p, Ap, ctx->st, s));
       }
       SU2B_CKS(fetch_state(ctx));
       done = ctx->h_st->done;
@@ -232,7 +232,7 @@ int cg_mixed(su2b_ctx *ctx, double m, double tol, int max_iter, double delta,
   const float m32 = (float)m;
   double *dp = ctx->part_slot(3), *np = ctx->part_slot(4), *np2 = ctx->part_slot(5);
   SU2B_CKS(true_residual(ctx, m, true, b, x, r, 20));
-  SU2B_CK(to32(n, r, rs, s));
+  SU2B_LAUNCH(SU2B_K_OTHER, to32(n, r, rs, s));
   SU2B_CK(cudaMemsetAsync(xs, 0, n * sizeof(float2), s));
   SU2B_CK(cudaMemcpyAsync(ps, rs, n * sizeof(float2), cudaMemcpyDeviceToDevice, s));
   SU2B_CKS(su2b_fetch_red(ctx, 21));
@@ -248,17 +248,17 @@ int cg_mixed(su2b_ctx *ctx, double m, double tol, int max_iter, double delta,
   int done = h.done;
   while (!done) {
     for (int k = 0; k < CHUNK; k++) {
-      SU2B_CK(hop32(g, ctx->ph32, m32, 1, ps, ts, nullptr, nullptr, nullptr, ctx->st, s));
-      SU2B_CK(hop32(g, ctx->ph32, m32, 0, ts, Aps, ps, dp, nullptr, ctx->st, s));
-      SU2B_CK(cg_alpha(dp, hop_blocks(g), ctx->st, s));
-      SU2B_CK(m_xr(n, xs, rs, ps, Aps, ctx->st, np, s));
-      SU2B_CK(m_check(np, vec_blocks(n), ctx->st, s));
-      SU2B_CK(m_accum(n, x, xs, ctx->st, s));
-      SU2B_CK(hop64(g, ctx->ph, m, 1, x, t, nullptr, nullptr, nullptr, ctx->st, 1, s));
-      SU2B_CK(hop64(g, ctx->ph, m, 0, t, Ap, nullptr, nullptr, nullptr, ctx->st, 1, s));
-      SU2B_CK(m_resid(n, b, Ap, r, rs, ctx->st, np2, s));
-      SU2B_CK(m_after(np2, vec_blocks(n), ctx->st, s));
-      SU2B_CK(m_p(n, rs, ps, ctx->st, s));
+      SU2B_LAUNCH(SU2B_K_STAGGERED, hop32(g, ctx->ph32, m32, 1, ps, ts, nullptr, nullptr, nullptr, ctx->st, s));
+      SU2B_LAUNCH(SU2B_K_STAGGERED, hop32(g, ctx->ph32, m32, 0, ts, Aps, ps, dp, nullptr, ctx->st, s));
+      SU2B_LAUNCH(SU2B_K_OTHER, cg_alpha(dp, hop_blocks(g), ctx->st, s));
+      SU2B_LAUNCH(SU2B_K_OTHER, m_xr(n, xs, rs, ps, Aps, ctx->st, np, s));
+      SU2B_LAUNCH(SU2B_K_OTHER, m_check(np, vec_blocks(n), ctx->st, s));
+      SU2B_LAUNCH(SU2B_K_OTHER, m_accum(n, x, xs, ctx->st, s));
+      SU2B_LAUNCH(SU2B_K_STAGGERED, hop64(g, ctx->ph, m, 1, x, t, nullptr, nullptr, nullptr, ctx->st, 1, s));
+      SU2B_LAUNCH(SU2B_K_STAGGERED, hop64(g, ctx->ph, m, 0, t, Ap, nullptr, nullptr, nullptr, ctx->st, 1, s));
+      SU2B_LAUNCH(SU2B_K_OTHER, m_resid(n, b, Ap, r, rs, ctx->st, np2, s));
+      SU2B_LAUNCH(SU2B_K_OTHER, m_after(np2, vec_blocks(n), ctx->st, s));
+      SU2B_LAUNCH(SU2B_K_OTHER, m_p(n, rs, ps, ctx->st, s));
     }
     SU2B_CKS(fetch_state(ctx));
     done = ctx->h_st->done;
@@ -269,7 +269,7 @@ int cg_mixed(su2b_ctx *ctx, double m, double tol, int max_iter, double delta,
     h.do_update = 1;
     h.done = 0;
     SU2B_CKS(upload_state(ctx, h));
-    SU2B_CK(m_accum(n, x, xs, ctx->st, s));
+    SU2B_LAUNCH(SU2B_K_OTHER, m_accum(n, x, xs, ctx->st, s));
   }
   if (stats) {
     stats->iterations = h.iters;
@@ -354,9 +354,9 @@ int su2b_fermion_deriv_q(su2b_ctx *ctx, double mass, double tol, int max_iter, i
   SU2B_CKS(su2b_fermion_setup(ctx, ctx->prec == SU2B_PREC_MIXED));
   SU2B_CKS(set_start(ctx, cg_start, seed));
   SU2B_CKS(solve_phi(ctx, mass, tol, max_iter, iters));
-  SU2B_CK(hop64(ctx->g, ctx->ph, mass, 1, ctx->sv[SV_X], ctx->sv[SV_CHI1], nullptr, nullptr,
+  SU2B_LAUNCH(SU2B_K_STAGGERED, hop64(ctx->g, ctx->ph, mass, 1, ctx->sv[SV_X], ctx->sv[SV_CHI1], nullptr, nullptr,
                 nullptr, nullptr, 0, ctx->stream));
-  SU2B_CK(fermion_force(ctx->g, ctx->ph, ctx->sv[SV_X], ctx->sv[SV_CHI1], ctx->fderiv,
+  SU2B_LAUNCH(SU2B_K_STAGGERED, fermion_force(ctx->g, ctx->ph, ctx->sv[SV_X], ctx->sv[SV_CHI1], ctx->fderiv,
                         ctx->stream));
   return SU2B_OK;
 }
@@ -368,8 +368,8 @@ int su2b_fermion_action_q(su2b_ctx *ctx, double mass, double tol, int max_iter, 
   SU2B_CKS(set_start(ctx, cg_start, seed));
   SU2B_CKS(solve_phi(ctx, mass, tol, max_iter, iters));
   const int n = (int)ctx->V;
-  SU2B_CK(dot64(n, ctx->sv[SV_PHI], ctx->sv[SV_X], ctx->part_slot(4), ctx->stream));
-  SU2B_CK(reduce_final(ctx->part_slot(4), vec_blocks(n), 2, ctx->red + 30, ctx->stream));
+  SU2B_LAUNCH(SU2B_K_OTHER, dot64(n, ctx->sv[SV_PHI], ctx->sv[SV_X], ctx->part_slot(4), ctx->stream));
+  SU2B_LAUNCH(SU2B_K_OTHER, reduce_final(ctx->part_slot(4), vec_blocks(n), 2, ctx->red + 30, ctx->stream));
   SU2B_CK(cudaMemcpyAsync(ctx->red + red_slot, ctx->red + 30, sizeof(double),
                           cudaMemcpyDeviceToDevice, ctx->stream));
   return SU2B_OK;
@@ -383,12 +383,12 @@ int su2b_fermion_heatbath_q(su2b_ctx *ctx, double mass, const double *R_host, ui
   if (R_host)
     SU2B_CKS(put_spinor(ctx, R_host, R));
   else
-    SU2B_CK(pf_source(ctx->g, seed, traj, cplx, R, ctx->stream));
-  SU2B_CK(hop64(ctx->g, ctx->ph, mass, 0, R, ctx->sv[SV_PHI], nullptr, nullptr, nullptr, nullptr,
+    SU2B_LAUNCH(SU2B_K_OTHER, pf_source(ctx->g, seed, traj, cplx, R, ctx->stream));
+  SU2B_LAUNCH(SU2B_K_STAGGERED, hop64(ctx->g, ctx->ph, mass, 0, R, ctx->sv[SV_PHI], nullptr, nullptr, nullptr, nullptr,
                 0, ctx->stream));
   const int n = (int)ctx->V;
-  SU2B_CK(dot64(n, R, R, ctx->part_slot(4), ctx->stream));
-  SU2B_CK(reduce_final(ctx->part_slot(4), vec_blocks(n), 2, ctx->red + 30, ctx->stream));
+  SU2B_LAUNCH(SU2B_K_OTHER, dot64(n, R, R, ctx->part_slot(4), ctx->stream));
+  SU2B_LAUNCH(SU2B_K_OTHER, reduce_final(ctx->part_slot(4), vec_blocks(n), 2, ctx->red + 30, ctx->stream));
   SU2B_CK(cudaMemcpyAsync(ctx->red + red_slot, ctx->red + 30, sizeof(double),
                           cudaMemcpyDeviceToDevice, ctx->stream));
   return SU2B_OK;
@@ -406,7 +406,7 @@ extern "C" int su2b_staggered_apply(su2b_ctx *ctx, int op, double mass, const do
   if (op == SU2B_OP_DDDAG)
     SU2B_CKS(apply_ddag64(ctx, mass, ctx->sv[SV_B], ctx->sv[SV_X]));
   else
-    SU2B_CK(hop64(ctx->g, ctx->ph, mass, op == SU2B_OP_DDAG, ctx->sv[SV_B], ctx->sv[SV_X],
+    SU2B_LAUNCH(SU2B_K_STAGGERED, hop64(ctx->g, ctx->ph, mass, op == SU2B_OP_DDAG, ctx->sv[SV_B], ctx->sv[SV_X],
                   nullptr, nullptr, nullptr, nullptr, 0, ctx->stream));
   return get_spinor(ctx, ctx->sv[SV_X], out_host);
 }
@@ -434,8 +434,8 @@ extern "C" int su2b_solve(su2b_ctx *ctx, const su2b_solve_params *prm, const dou
   double tol = prm->tol;
   if (prm->tol_mode == SU2B_TOL_REL) {
     const int n = (int)ctx->V;
-    SU2B_CK(dot64(n, ctx->sv[SV_B], ctx->sv[SV_B], ctx->part_slot(4), ctx->stream));
-    SU2B_CK(reduce_final(ctx->part_slot(4), vec_blocks(n), 2, ctx->red + 30, ctx->stream));
+    SU2B_LAUNCH(SU2B_K_OTHER, dot64(n, ctx->sv[SV_B], ctx->sv[SV_B], ctx->part_slot(4), ctx->stream));
+    SU2B_LAUNCH(SU2B_K_OTHER, reduce_final(ctx->part_slot(4), vec_blocks(n), 2, ctx->red + 30, ctx->stream));
     SU2B_CKS(su2b_fetch_red(ctx, 32));
     tol = prm->tol * sqrt(ctx->h_red[30]);
   }
@@ -475,9 +475,9 @@ extern "C" int su2b_fermion_force(su2b_ctx *ctx, double mass, const double *phi_
   SU2B_NEED(deriv_host, "deriv_host is NULL");
   long it = 0;
   SU2B_CKS(fermion_common(ctx, mass, phi_host, tol, max_iter, x0_host, seed, &it));
-  SU2B_CK(hop64(ctx->g, ctx->ph, mass, 1, ctx->sv[SV_X], ctx->sv[SV_CHI1], nullptr, nullptr,
+  SU2B_LAUNCH(SU2B_K_STAGGERED, hop64(ctx->g, ctx->ph, mass, 1, ctx->sv[SV_X], ctx->sv[SV_CHI1], nullptr, nullptr,
                 nullptr, nullptr, 0, ctx->stream));
-  SU2B_CK(fermion_force(ctx->g, ctx->ph, ctx->sv[SV_X], ctx->sv[SV_CHI1], ctx->fderiv,
+  SU2B_LAUNCH(SU2B_K_STAGGERED, fermion_force(ctx->g, ctx->ph, ctx->sv[SV_X], ctx->sv[SV_CHI1], ctx->fderiv,
                         ctx->stream));
   if (cg_iterations) *cg_iterations = it;
   return su2b_adj_download(ctx, ctx->fderiv, deriv_host);
@@ -493,8 +493,8 @@ extern "C" int su2b_fermion_action(su2b_ctx *ctx, double mass, const double *phi
   long it = 0;
   SU2B_CKS(fermion_common(ctx, mass, phi_host, tol, max_iter, x0_host, seed, &it));
   const int n = (int)ctx->V;
-  SU2B_CK(dot64(n, ctx->sv[SV_PHI], ctx->sv[SV_X], ctx->part_slot(4), ctx->stream));
-  SU2B_CK(reduce_final(ctx->part_slot(4), vec_blocks(n), 2, ctx->red + 30, ctx->stream));
+  SU2B_LAUNCH(SU2B_K_OTHER, dot64(n, ctx->sv[SV_PHI], ctx->sv[SV_X], ctx->part_slot(4), ctx->stream));
+  SU2B_LAUNCH(SU2B_K_OTHER, reduce_final(ctx->part_slot(4), vec_blocks(n), 2, ctx->red + 30, ctx->stream));
   SU2B_CKS(su2b_fetch_red(ctx, 32));
   *out = ctx->h_red[30];
   return SU2B_OK;

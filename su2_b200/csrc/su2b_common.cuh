@@ -118,9 +118,11 @@ template <class T> struct Su2 {
   T ar, ai, br, bi;
 };
 
+// The loads carry no side effect, so they are not volatile: the compiler may hoist and
+// overlap them.
 __device__ __forceinline__ Su2<double> ld_link(const Link64 *p) {
   Su2<double> r;
-  asm volatile("ld.global.nc.v4.f64 {%0,%1,%2,%3}, [%4];"
+  asm("ld.global.nc.v4.f64 {%0,%1,%2,%3}, [%4];"
                : "=d"(r.ar), "=d"(r.ai), "=d"(r.br), "=d"(r.bi)
                : "l"(p));
   return r;
@@ -130,7 +132,8 @@ __device__ __forceinline__ Su2<double> ld_link_rw(const Link64 *p) {
   Su2<double> r;
   asm volatile("ld.global.v4.f64 {%0,%1,%2,%3}, [%4];"
                : "=d"(r.ar), "=d"(r.ai), "=d"(r.br), "=d"(r.bi)
-               : "l"(p));
+               : "l"(p)
+               : "memory");
   return r;
 }
 __device__ __forceinline__ void st_link(Link64 *p, const Su2<double> &u) {

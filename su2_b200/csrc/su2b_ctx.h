@@ -48,6 +48,18 @@ struct su2b_ctx {
   su2b::SolverState *st = nullptr;
   long x0_seed = -1;  // seed of the reference CG start held in sv[SV_X0]
 
+  // kernel launch counter and the per-class device timers (su2b_profile)
+  long launches = 0;
+  bool prof = false;
+  struct Pending {
+    int k;
+    cudaEvent_t a, b;
+  };
+  std::vector<Pending> pend;
+  std::vector<cudaEvent_t> ev_pool;
+  double prof_ms[16] = {};
+  long prof_n[16] = {};
+
   std::map<std::string, cudaGraphExec_t> graphs;
   std::vector<void *> allocs;
   std::string err;
@@ -81,6 +93,23 @@ int su2b_fermion_action_q(su2b_ctx *ctx, double mass, double tol, int max_iter, 
                           long seed, int red_slot, long *iters);
 int su2b_fermion_heatbath_q(su2b_ctx *ctx, double mass, const double *R_host, uint64_t seed,
                             uint32_t traj, int cplx, int red_slot);
+
+cudaEvent_t su2b_ev_take(su2b_ctx *ctx);
+void su2b_ev_mark(su2b_ctx *ctx, int kclass, cudaEvent_t start);
+int su2b_prof_fold(su2b_ctx *ctx);
+
+// launch a kernel through its launcher: counts it and, with profiling on, times it
+#define SU2B_LAUNCH(kclass, call)                                                          \
+  do {                                                                                     \
+    cudaEvent_t a_ = nullptr;                                                              \
+    if (ctx->prof) {                                                                       \
+      a_ = su2b_ev_take(ctx);                                                              \
+      cudaEventRecord(a_, ctx->stream);                                                    \
+    }                                                                                      \
+    SU2B_CK(call);                                                                         \
+    ctx->launches++;                                                                       \
+    if (ctx->prof) su2b_ev_mark(ctx, kclass, a_);                                          \
+  } while (0)
 
 #define SU2B_CK(call)                                                                      \
   do {                                                                                     \

@@ -108,6 +108,23 @@ class gaugeconfig:
         self._c(self.lib.su2b_ctx_stream(self.ctx, C.byref(s)))
         return s.value or 0
 
+    def profile(self, enable=True):
+        """Per-kernel-class device timers (CUDA events on the context's stream)."""
+        self._c(self.lib.su2b_profile(self.ctx, int(enable)))
+
+    def profile_read(self) -> dict:
+        out = {}
+        for k, name in enumerate(_abi.K_NAMES):
+            n, ms = C.c_long(), C.c_double()
+            self._c(self.lib.su2b_profile_read(self.ctx, k, C.byref(n), C.byref(ms)))
+            out[name] = (n.value, ms.value)
+        return out
+
+    def kernel_launches(self) -> int:
+        n = C.c_long()
+        self._c(self.lib.su2b_kernel_launches(self.ctx, C.byref(n)))
+        return n.value
+
     def setBeta(self, beta):
         self.beta = beta
         self._c(self.lib.su2b_set_beta(self.ctx, beta))
