@@ -206,6 +206,22 @@ SU2B_API int su2b_fermion_force(su2b_ctx *ctx, double mass, const double *phi_ho
 SU2B_API int su2b_fermion_action(su2b_ctx *ctx, double mass, const double *phi_host, double tol,
                         int max_iter, const double *x0_host, long seed, double *out);
 
+/* ---- plaquette sums without allocation ------------------------------------------------ */
+/* No counterpart in the reference.  For callers that cannot allocate device memory (a host
+ * framework that owns the GPU's memory through its own pool and forbids cudaMalloc in
+ * plug-ins, or code running during CUDA graph capture): gauge_energy(U) and
+ * gauge_energy(U, spatial_only) of a field the caller already holds on the device in the
+ * reference host layout (FP64, see "links" above), written to out_dev[0] and out_dev[1] (a
+ * device buffer of the caller) on `stream` (a cudaStream_t, NULL = default stream).  No
+ * context is created and nothing is allocated: the only scratch is a fixed array of
+ * 16384 partial-sum pairs inside the library, so the lattice may have at most 4,194,304
+ * sites (larger sizes return SU2B_ERR_INVALID).  All calls share that array: calls that
+ * overlap on the GPU race and must be ordered by the caller.  The first call on a device
+ * looks up the array's device address and should come before any stream capture.  Returns
+ * without waiting for the kernels; errors are reported only through the status code. */
+SU2B_API int su2b_gauge_energy_noalloc(int group, int Lx, int Ly, int Lz, int Lt, int ndims,
+                                       const double *U_dev, double *out_dev, void *stream);
+
 /* ---- device timers -------------------------------------------------------------------- */
 /* Kernel classes.  With profiling on, every launch of a class is bracketed by CUDA events on
  * the context's stream and its device time accumulated (the events add a few microseconds

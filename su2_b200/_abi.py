@@ -83,6 +83,7 @@ SIGNATURES = {
     "su2b_profile": (i32, [_P, i32]),
     "su2b_profile_read": (i32, [_P, i32, C.POINTER(C.c_long), C.POINTER(C.c_double)]),
     "su2b_kernel_launches": (i32, [_P, C.POINTER(C.c_long)]),
+    "su2b_gauge_energy_noalloc": (i32, [i32, i32, i32, i32, i32, i32, _P, _P, _P]),
 }
 
 K_FORCE, K_UPDATE, K_PLAQUETTE, K_MOMENTA, K_RESTORE, K_METROPOLIS, K_CLOVER, K_STAGGERED, \
