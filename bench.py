@@ -203,6 +203,7 @@ def ours(args):
     for k in range(max(W, 3)):
         mixed.md_update("omf2", NSTEPS, TAU, seed=seed, traj=100000 + k)
     U_th = mixed.download()
+    tune_m = mixed.autotune()  # launch shape of the force kernel, timed on this field
 
     # ---- headline: mixed precision, K trajectories ----
     clocks = Clocks(local)
@@ -218,6 +219,8 @@ def ours(args):
     # ---- FP64 path, same start and seeds ----
     fp64 = su2_b200.gaugeconfig(L, L, L, L, 4, BETA, precision="fp64", device=local)
     fp64.upload(U_th)
+    tune_d = fp64.autotune()
+    fp64.upload(U_th)
     for k in range(min(W, 2)):
         fp64.md_update("omf2", NSTEPS, TAU, seed=seed + 7, traj=200000 + k)
     fp64.upload(U_th)
@@ -229,7 +232,10 @@ def ours(args):
     roof = {}
     kernels = {}
     hbm, peak_src = peaks()
-    for name, c, bpl in (("mixed", mixed, 40), ("fp64", fp64, 80)):
+    # every force launch of the fused trajectory reads U and P, writes P and writes the next
+    # link buffer (exp(dt P) U, or restoreSU(U) after the last step): 56 B/link in FP32
+    # storage, 112 B/link in FP64
+    for name, c, bpl in (("mixed", mixed, 56), ("fp64", fp64, 112)):
         c.upload(U_th)
         c.profile(True)
         for k in range(max(2, K // 2)):
@@ -240,8 +246,7 @@ def ours(args):
         avg = ms / 1e3 / n
         roof[name] = {"avg_us": avg * 1e6, "GB/s": bpl * NL / avg / 1e9}
         per = {}
-        nb = {"force": bpl, "update": 88 if name == "fp64" else 44,
-              "plaquette": 32 if name == "fp64" else 16, "restore": 64 if name == "fp64" else 32,
+        nb = {"force": bpl, "plaquette": 32 if name == "fp64" else 16,
               "momenta": 24 if name == "fp64" else 12}
         for kname, (kn, kms) in prof.items():
             if kn:
@@ -304,16 +309,24 @@ def ours(args):
             "mixed": dict(traj_per_s=value, **stats(res_m, V)),
             "fp64": dict(traj_per_s=ws * K / t_fp64, **stats(res_d, V)),
             "speedup_mixed_vs_fp64": t_fp64 / t_mixed,
-            "roofline": {"bound": "hbm", "kernel": "fused staple/force/momentum (FP32)",
+            "roofline": {"bound": "hbm",
+                         "kernel": "k_force_su2<float,4>: staples, force, momentum step and the "
+                                   "following link update, fused (FP32 storage)",
                          "achieved": roof["mixed"]["GB/s"], "peak": hbm, "unit": "GB/s",
                          "frac": roof["mixed"]["GB/s"] / hbm, "traffic": traffic,
-                         "bytes_per_launch": 40 * NL, "avg_launch_us": roof["mixed"]["avg_us"],
+                         "bytes_per_launch": 56 * NL, "avg_launch_us": roof["mixed"]["avg_us"],
                          "peak_source": peak_src,
                          "fp64_kernel": {"achieved": roof["fp64"]["GB/s"],
                                          "frac": roof["fp64"]["GB/s"] / hbm,
-                                         "bytes_per_launch": 80 * NL,
+                                         "bytes_per_launch": 112 * NL,
                                          "avg_launch_us": roof["fp64"]["avg_us"]}},
             "kernels": kernels,
+            "autotune_force_us": {"mixed": {str(su2_b200._abi.FORCE_SHAPES[k]): v
+                                            for k, v in tune_m.items()},
+                                  "fp64": {str(su2_b200._abi.FORCE_SHAPES[k]): v
+                                           for k, v in tune_d.items()},
+                                  "chosen": {"mixed": su2_b200._abi.FORCE_SHAPES[mixed.force_variant],
+                                             "fp64": su2_b200._abi.FORCE_SHAPES[fp64.force_variant]}},
             "metropolis_sweeps_per_s": metro, "flow_rk3_steps_per_s_fp64": flow,
             "e2e": {"value": ws * K / t_e2e, "unit": "traj/s",
                     "h2d_bytes_per_step": int(NL * 4 * 8), "d2h_bytes_per_step": int(NL * 4 * 8),

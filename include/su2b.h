@@ -206,6 +206,19 @@ SU2B_API int su2b_fermion_force(su2b_ctx *ctx, double mass, const double *phi_ho
 SU2B_API int su2b_fermion_action(su2b_ctx *ctx, double mass, const double *phi_host, double tol,
                         int max_iter, const double *x0_host, long seed, double *out);
 
+/* ---- launch-shape autotuning ------------------------------------------------------------ */
+/* The SU(2) force kernel has SU2B_FORCE_VARIANTS launch shapes (threads per block x register
+ * cap).  su2b_autotune times them all on the context's field (CUDA events, the same memory
+ * traffic as a trajectory step, into scratch buffers) and keeps the fastest for this context;
+ * with cache_path it first looks the choice up in that text file (unless retune) and writes
+ * new measurements to it.  times_us (optional, SU2B_FORCE_VARIANTS entries) receives the
+ * average launch time of each shape (-1 when not measured). */
+#define SU2B_FORCE_VARIANTS 8
+enum { SU2B_TUNE_FORCE = 0 };
+SU2B_API int su2b_autotune(su2b_ctx *ctx, const char *cache_path, int retune, double *times_us);
+SU2B_API int su2b_tune_get(su2b_ctx *ctx, int kernel, int *variant);
+SU2B_API int su2b_tune_set(su2b_ctx *ctx, int kernel, int variant);
+
 /* ---- plaquette sums without allocation ------------------------------------------------ */
 /* No counterpart in the reference.  For callers that cannot allocate device memory (a host
  * framework that owns the GPU's memory through its own pool and forbids cudaMalloc in

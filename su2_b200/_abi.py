@@ -84,7 +84,13 @@ SIGNATURES = {
     "su2b_profile_read": (i32, [_P, i32, C.POINTER(C.c_long), C.POINTER(C.c_double)]),
     "su2b_kernel_launches": (i32, [_P, C.POINTER(C.c_long)]),
     "su2b_gauge_energy_noalloc": (i32, [i32, i32, i32, i32, i32, i32, _P, _P, _P]),
+    "su2b_autotune": (i32, [_P, C.c_char_p, i32, _D]),
+    "su2b_tune_get": (i32, [_P, i32, C.POINTER(C.c_int)]),
+    "su2b_tune_set": (i32, [_P, i32, i32]),
 }
+FORCE_VARIANTS = 8
+FORCE_SHAPES = [(64, 8), (128, 1), (128, 4), (128, 6), (256, 2), (256, 3), ("async", 64),
+                ("async", 128)]
 
 K_FORCE, K_UPDATE, K_PLAQUETTE, K_MOMENTA, K_RESTORE, K_METROPOLIS, K_CLOVER, K_STAGGERED, \
     K_OTHER = range(9)

@@ -145,6 +145,8 @@ extern "C" int su2b_ctx_create(int group, int Lx, int Ly, int Lz, int Lt, int nd
   const size_t ab = ctx->adj_bytes();
   ctx->part_cap = (size_t)2 * ndims * ((g.Vh + 63) / 64) + 2048;
   if ((st = dalloc(ctx, &ctx->U, lb * NL)) || (st = dalloc(ctx, &ctx->U_old, lb * NL)) ||
+      (st = dalloc(ctx, &ctx->U2, lb * NL)) ||
+      (st = dalloc(ctx, &ctx->tparams, sizeof(TrajParams))) ||
       (st = dalloc(ctx, &ctx->P, ab * NL)) || (st = dalloc(ctx, &ctx->Z, ab * NL)) ||
       (st = dalloc(ctx, &ctx->stage, sizeof(double) * NL * (group == 0 ? 4 : 1))) ||
       (st = dalloc(ctx, &ctx->part, sizeof(double) * 3 * ctx->part_cap * NSLOT)) ||
@@ -155,8 +157,10 @@ extern "C" int su2b_ctx_create(int group, int Lx, int Ly, int Lz, int Lt, int nd
   if (cudaMallocHost((void **)&ctx->h_red, sizeof(double) * 64) != cudaSuccess ||
       cudaMallocHost((void **)&ctx->h_traj, sizeof(TrajDev)) != cudaSuccess ||
       cudaMallocHost((void **)&ctx->h_counts, sizeof(unsigned long long) * 4) != cudaSuccess ||
-      cudaMallocHost((void **)&ctx->h_st, sizeof(SolverState)) != cudaSuccess)
+      cudaMallocHost((void **)&ctx->h_st, sizeof(SolverState)) != cudaSuccess ||
+      cudaMallocHost((void **)&ctx->h_tparams, sizeof(TrajParams)) != cudaSuccess)
     return fin(SU2B_ERR_NOMEM);
+  if (force_prepare() != cudaSuccess) return fin(SU2B_ERR_CUDA);
   if (cudaMemsetAsync(ctx->U, 0, lb * NL, ctx->stream) != cudaSuccess) return fin(SU2B_ERR_CUDA);
   if (cudaStreamSynchronize(ctx->stream) != cudaSuccess) return fin(SU2B_ERR_CUDA);
   return fin(SU2B_OK);
@@ -171,12 +175,13 @@ extern "C" int su2b_ctx_destroy(su2b_ctx *ctx) {
     cudaEventDestroy(p.b);
   }
   for (cudaEvent_t e : ctx->ev_pool) cudaEventDestroy(e);
-  for (auto &kv : ctx->graphs) cudaGraphExecDestroy(kv.second);
+  for (auto &kv : ctx->graphs) cudaGraphExecDestroy(kv.second.exec);
   for (void *p : ctx->allocs) cudaFree(p);
   if (ctx->h_red) cudaFreeHost(ctx->h_red);
   if (ctx->h_traj) cudaFreeHost(ctx->h_traj);
   if (ctx->h_counts) cudaFreeHost(ctx->h_counts);
   if (ctx->h_st) cudaFreeHost(ctx->h_st);
+  if (ctx->h_tparams) cudaFreeHost(ctx->h_tparams);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
   return SU2B_OK;
@@ -400,8 +405,9 @@ extern "C" int su2b_energy_density(su2b_ctx *ctx, int cloverdef, int ss, double 
 template <class T>
 static int q_force(su2b_ctx *ctx, const void *U, T *P, const T *extra, double f, double scale,
                    int mode, double *kin_part, int *nb) {
-  SU2B_LAUNCH(SU2B_K_FORCE, force_update<T>(ctx->g, U, ctx->group, P, extra, f, scale, ctx->xi, mode, kin_part, nb,
-                     ctx->stream));
+  SU2B_LAUNCH(SU2B_K_FORCE, force_update<T>(ctx->g, U, ctx->group, P, extra, f, scale, ctx->xi,
+                                            mode, kin_part, nb, nullptr, 0.0, ctx->stream,
+                                            ctx->tune_force));
   return SU2B_OK;
 }
 int su2b_q_force(su2b_ctx *ctx, const void *U, void *P, const void *extra, double f,

@@ -1,0 +1,143 @@
+// autotune.cu -- launch-shape autotuner for the SU(2) force kernel.
+//
+// The fused staple/force/momentum kernel is bound by the latency of its neighbour loads, so
+// its speed depends on the balance between resident warps and loads in flight per thread,
+// i.e. on the block size and the register cap (minimum resident blocks per SM).  The tuner
+// times every shape on the context's own field with CUDA events -- the same reads and writes
+// as a trajectory step, into scratch buffers -- and keeps the fastest.  Choices persist in a
+// plain-text cache, one "key variant microseconds" line per GPU model, precision and
+// geometry, so later processes skip the measurement.
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <sstream>
+#include <string>
+#include <vector>
+
+#include "su2b.h"
+#include "su2b_ctx.h"
+
+using namespace su2b;
+
+namespace {
+
+std::string tune_key(su2b_ctx *ctx) {
+  cudaDeviceProp prop;
+  std::string gpu = "gpu";
+  if (cudaGetDeviceProperties(&prop, ctx->device) == cudaSuccess) gpu = prop.name;
+  for (char &c : gpu)
+    if (c == ' ') c = '_';
+  char buf[256];
+  snprintf(buf, sizeof buf, "%s/force/%s/%dx%dx%dx%d/d%d", gpu.c_str(),
+           ctx->link64 ? "fp64" : "fp32", ctx->Lx, ctx->Ly, ctx->Lz, ctx->Lt, ctx->g.nd);
+  return buf;
+}
+
+bool cache_lookup(const char *path, const std::string &key, int *variant) {
+  std::ifstream in(path);
+  std::string line;
+  while (std::getline(in, line)) {
+    std::istringstream ss(line);
+    std::string k;
+    int v;
+    if (ss >> k >> v && k == key && v >= 0 && v < FORCE_VARIANTS) {
+      *variant = v;
+      return true;
+    }
+  }
+  return false;
+}
+
+void cache_store(const char *path, const std::string &key, int variant, double us) {
+  std::vector<std::string> keep;
+  {
+    std::ifstream in(path);
+    std::string line;
+    while (std::getline(in, line)) {
+      std::istringstream ss(line);
+      std::string k;
+      if (ss >> k && k != key) keep.push_back(line);
+    }
+  }
+  std::ofstream out(path, std::ios::trunc);
+  for (const auto &l : keep) out << l << "\n";
+  out << key << " " << variant << " " << us << "\n";
+}
+
+}  // namespace
+
+extern "C" int su2b_autotune(su2b_ctx *ctx, const char *cache_path, int retune,
+                             double *times_us) {
+  if (!ctx) return SU2B_ERR_INVALID;
+  ctx->err.clear();
+  SU2B_CK(cudaSetDevice(ctx->device));
+  if (times_us)
+    for (int v = 0; v < FORCE_VARIANTS; v++) times_us[v] = -1.0;
+  if (ctx->group != SU2B_GROUP_SU2) return SU2B_OK;  // only the SU(2) force kernel has shapes
+  const std::string key = tune_key(ctx);
+  int v = 0;
+  if (cache_path && !retune && cache_lookup(cache_path, key, &v)) {
+    ctx->tune_force = v;
+    return SU2B_OK;
+  }
+  cudaStream_t s = ctx->stream;
+  const size_t nadj = ctx->NL * 3;
+  SU2B_CK(cudaMemsetAsync(ctx->Z, 0, ctx->adj_bytes() * ctx->NL, s));
+  cudaEvent_t e0, e1;
+  SU2B_CK(cudaEventCreate(&e0));
+  SU2B_CK(cudaEventCreate(&e1));
+  const double f = ctx->beta / ctx->Nc();
+  const int mode = FM_HAS_IN | FM_UPDATE;
+  int best = 1;
+  double best_us = 1e300;
+  int rc = SU2B_OK;
+  for (int var = 0; var < FORCE_VARIANTS && rc == SU2B_OK; var++) {
+    auto launch = [&]() -> cudaError_t {
+      if (ctx->link64)
+        return force_update<double>(ctx->g, ctx->U, 0, (double *)ctx->Z, nullptr, f, -1e-3,
+                                    ctx->xi, mode, nullptr, nullptr, ctx->U2, 0.0, s, var);
+      return force_update<float>(ctx->g, ctx->U, 0, (float *)ctx->Z, nullptr, f, -1e-3, ctx->xi,
+                                 mode, nullptr, nullptr, ctx->U2, 0.0, s, var);
+    };
+    cudaError_t e = cudaSuccess;
+    for (int k = 0; k < 2 && e == cudaSuccess; k++) e = launch();
+    float ms = 0.f;
+    const int reps = 5;
+    if (e == cudaSuccess) e = cudaEventRecord(e0, s);
+    for (int k = 0; k < reps && e == cudaSuccess; k++) e = launch();
+    if (e == cudaSuccess) e = cudaEventRecord(e1, s);
+    if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+    if (e != cudaSuccess) {
+      rc = su2b_fail(ctx, SU2B_ERR_CUDA, "autotune variant %d: %s", var, cudaGetErrorString(e));
+      break;
+    }
+    ctx->launches += 2 + reps;
+    const double us = 1e3 * ms / reps;
+    if (times_us) times_us[var] = us;
+    if (us < best_us) {
+      best_us = us;
+      best = var;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  (void)nadj;
+  if (rc != SU2B_OK) return rc;
+  ctx->tune_force = best;
+  if (cache_path) cache_store(cache_path, key, best, best_us);
+  return SU2B_OK;
+}
+
+extern "C" int su2b_tune_get(su2b_ctx *ctx, int kernel, int *variant) {
+  if (!ctx || !variant || kernel != SU2B_TUNE_FORCE) return SU2B_ERR_INVALID;
+  *variant = ctx->tune_force;
+  return SU2B_OK;
+}
+
+extern "C" int su2b_tune_set(su2b_ctx *ctx, int kernel, int variant) {
+  if (!ctx || kernel != SU2B_TUNE_FORCE || variant < 0 || variant >= FORCE_VARIANTS)
+    return SU2B_ERR_INVALID;
+  ctx->tune_force = variant;
+  return SU2B_OK;
+}

@@ -90,8 +90,8 @@ template <class T, int ND, int NT>
 __global__ void __launch_bounds__(NT)
   k_plaq_su2(Geom g, const LinkT<T> *__restrict__ U, double xi, double *part) {
   __shared__ double sh[NT / 32];
-  const int p = blockIdx.x & 1;
-  const int cb = (blockIdx.x >> 1) * NT + threadIdx.x;
+  const int w = threadIdx.x >> 5, p = w & 1;
+  const int cb = blockIdx.x * (NT / 2) + (w >> 1) * 32 + (threadIdx.x & 31);
   double full = 0., spat = 0., wsum = 0.;
   if (cb < g.Vh) {
     const Site s = site_from_eo(g, p, cb);
@@ -126,8 +126,8 @@ template <int ND, int NT>
 __global__ void __launch_bounds__(NT)
   k_plaq_u1(Geom g, const double *__restrict__ U, double xi, double *part) {
   __shared__ double sh[NT / 32];
-  const int p = blockIdx.x & 1;
-  const int cb = (blockIdx.x >> 1) * NT + threadIdx.x;
+  const int w = threadIdx.x >> 5, p = w & 1;
+  const int cb = blockIdx.x * (NT / 2) + (w >> 1) * 32 + (threadIdx.x & 31);
   double full = 0., spat = 0., wsum = 0.;
   if (cb < g.Vh) {
     const Site s = site_from_eo(g, p, cb);
@@ -180,14 +180,17 @@ __global__ void __launch_bounds__(NT)
 // between the parities (block b -> parity b & 1), so the blocks resident at any time cover
 // one narrow band of sites in every direction and parity and the links stream from HBM about
 // once per launch.
-template <class T, int ND, int NT>
-__global__ void __launch_bounds__(NT)
+template <class T, int ND, int NT, int MINB>
+__global__ void __launch_bounds__(NT, MINB)
   k_force_su2(Geom g, const LinkT<T> *__restrict__ U, T *__restrict__ P,
               const T *__restrict__ extra, T f, T scale_, int mode, int aniso, T wt, T ws,
-              double *kin_part) {
+              double *kin_part, LinkT<T> *__restrict__ Uout, T dt_upd) {
   __shared__ double sh[NT / 32];
-  const int p = blockIdx.x & 1, q = 1 - p;
-  const int cb = (blockIdx.x >> 1) * NT + threadIdx.x;
+  // warps alternate between the parities of one band of NT/2 sites per parity, so the
+  // +-z / +-y neighbours of a site are mostly the own links of another warp of the block
+  const int w = threadIdx.x >> 5;
+  const int p = w & 1, q = 1 - p;
+  const int cb = blockIdx.x * (NT / 2) + (w >> 1) * 32 + (threadIdx.x & 31);
   double k2 = 0.;
   if (cb < g.Vh) {
     const Site s = site_from_eo(g, p, cb);
@@ -266,12 +269,176 @@ __global__ void __launch_bounds__(NT)
       P[NL + l] = p1;
       P[2 * NL + l] = p2;
       k2 += (double)p0 * p0 + (double)p1 * p1 + (double)p2 * p2;
+      // the following gauge step U <- exp(dt P) U (update_gauge.hh:8-16) into the other buffer
+      if (mode & FM_UPDATE)
+        st_link(Uout + l, mul(exp_alg(dt_upd * p0, dt_upd * p1, dt_upd * p2), u));
+      else if (mode & FM_RESTORE)
+        st_link(Uout + l, from64<T>(restore_su(to64(u))));
     }
   }
   if (mode & FM_KINETIC) {
     const double r = block_sum<NT>(k2, sh);
     if (threadIdx.x == 0) kin_part[blockIdx.x] = r;
   }
+}
+
+// The same fused force step with all 4 + 2 ND(ND-1) + ND^2 neighbour links of a site first
+// copied into shared memory by cp.async (44 copies of 16 B per thread in d = 4, FP64 links as
+// two copies), so every load of a thread is in flight at once without holding registers;
+// the arithmetic then reads shared memory.  Slots are private to a thread (slot-major,
+// conflict-free), so only the thread's own copies are awaited.
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+
+template <class T, int ND> struct AsyncSlots {
+  static constexpr int N = ND + 2 * ND * (ND - 1) + ND * ND;
+  static constexpr int W = (int)(sizeof(LinkT<T>) / 16);
+};
+
+template <class T, int ND, int NT>
+__global__ void __launch_bounds__(NT)
+  k_force_su2_async(Geom g, const LinkT<T> *__restrict__ U, T *__restrict__ P,
+                    const T *__restrict__ extra, T f, T scale_, int mode, int aniso, T wt, T ws,
+                    double *kin_part, LinkT<T> *__restrict__ Uout, T dt_upd) {
+  extern __shared__ float4 smem[];
+  __shared__ double sh[NT / 32];
+  constexpr int W = AsyncSlots<T, ND>::W;
+  const int tid = threadIdx.x;
+  const int w = tid >> 5;
+  const int p = w & 1, q = 1 - p;
+  const int cb = blockIdx.x * (NT / 2) + (w >> 1) * 32 + (tid & 31);
+  double k2 = 0.;
+  auto slot_ptr = [&](int slot, int part) { return smem + ((size_t)(slot * W + part) * NT + tid); };
+  auto ld_slot = [&](int slot) -> Su2<T> {
+    if constexpr (W == 1) {
+      const float4 v = *slot_ptr(slot, 0);
+      return Su2<T>{(T)v.x, (T)v.y, (T)v.z, (T)v.w};
+    } else {
+      const double2 a = *reinterpret_cast<const double2 *>(slot_ptr(slot, 0));
+      const double2 b = *reinterpret_cast<const double2 *>(slot_ptr(slot, 1));
+      return Su2<T>{(T)a.x, (T)a.y, (T)b.x, (T)b.y};
+    }
+  };
+  if (cb < g.Vh) {
+    const Site s = site_from_eo(g, p, cb);
+    const size_t V = (size_t)g.V, NL = V * ND;
+    const size_t self = (size_t)p * g.Vh + cb;
+    int lf[ND], lb[ND];
+#pragma unroll
+    for (int mu = 0; mu < ND; mu++) {
+      lf[mu] = s.lex + fwd(g, s, mu);
+      lb[mu] = bwd(g, s, mu);
+    }
+    int slot = 0;
+    auto issue = [&](const LinkT<T> *gp) {
+#pragma unroll
+      for (int k = 0; k < W; k++)
+        cp_async16(slot_ptr(slot, k), reinterpret_cast<const float4 *>(gp) + k);
+      slot++;
+    };
+#pragma unroll
+    for (int mu = 0; mu < ND; mu++) issue(U + mu * V + self);
+#pragma unroll
+    for (int mu = 0; mu < ND - 1; mu++)
+#pragma unroll
+      for (int nu = mu + 1; nu < ND; nu++) {
+        issue(U + nu * V + eo_of(g, lf[mu], q));
+        issue(U + mu * V + eo_of(g, lf[nu], q));
+      }
+#pragma unroll
+    for (int nu = 0; nu < ND; nu++) {
+      const int lmn = s.lex + lb[nu];
+      issue(U + nu * V + eo_of(g, lmn, q));
+#pragma unroll
+      for (int mu = 0; mu < ND; mu++) {
+        if (mu == nu) continue;
+        issue(U + mu * V + eo_of(g, lmn, q));
+        issue(U + nu * V + eo_of(g, lf[mu] + lb[nu], p));
+      }
+    }
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+    // arithmetic, reading the slots in the order they were filled
+    slot = 0;
+    Su2<T> ux[ND], K[ND];
+#pragma unroll
+    for (int mu = 0; mu < ND; mu++) {
+      ux[mu] = ld_slot(slot++);
+      K[mu] = zero_su2<T>();
+    }
+#pragma unroll
+    for (int mu = 0; mu < ND - 1; mu++)
+#pragma unroll
+      for (int nu = mu + 1; nu < ND; nu++) {
+        const Su2<T> a = ld_slot(slot++);
+        const Su2<T> b = ld_slot(slot++);
+        const Su2<T> A = mul(a, dag(b));
+        Su2<T> fmn = mul(A, dag(ux[nu]));
+        Su2<T> fnm = mul(dag(A), dag(ux[mu]));
+        if (aniso) {
+          const T wgt = (mu == 0) ? wt : ws;
+          fmn = scale(wgt, fmn);
+          fnm = scale(wgt, fnm);
+        }
+        K[mu] = add(K[mu], fmn);
+        K[nu] = add(K[nu], fnm);
+      }
+#pragma unroll
+    for (int nu = 0; nu < ND; nu++) {
+      const Su2<T> c = ld_slot(slot++);
+#pragma unroll
+      for (int mu = 0; mu < ND; mu++) {
+        if (mu == nu) continue;
+        const Su2<T> h = ld_slot(slot++);
+        const Su2<T> e = ld_slot(slot++);
+        Su2<T> st = mul(mul(dag(e), dag(h)), c);
+        if (aniso) st = scale((nu == 0 || mu == 0) ? wt : ws, st);
+        K[mu] = add(K[mu], st);
+      }
+    }
+#pragma unroll
+    for (int mu = 0; mu < ND; mu++) {
+      const Su2<T> &u = ux[mu];
+      const Su2<T> &k = K[mu];
+      const size_t l = mu * V + self;
+      const T sbi = u.ar * k.bi + u.ai * k.br + (u.bi * k.ar - u.br * k.ai);
+      const T sbr = u.ar * k.br - u.ai * k.bi + (u.br * k.ar + u.bi * k.ai);
+      const T sai = u.ar * k.ai + u.ai * k.ar - (u.bi * k.br - u.br * k.bi);
+      T d0 = f * (T(2) * sbi), d1 = f * (T(2) * sbr), d2 = f * (T(2) * sai);
+      if (mode & FM_EXTRA) {
+        d0 += extra[l];
+        d1 += extra[NL + l];
+        d2 += extra[2 * NL + l];
+      }
+      T p0 = 0, p1 = 0, p2 = 0;
+      if (mode & FM_HAS_IN) {
+        p0 = P[l];
+        p1 = P[NL + l];
+        p2 = P[2 * NL + l];
+      }
+      p0 = p0 + scale_ * d0;
+      p1 = p1 + scale_ * d1;
+      p2 = p2 + scale_ * d2;
+      P[l] = p0;
+      P[NL + l] = p1;
+      P[2 * NL + l] = p2;
+      k2 += (double)p0 * p0 + (double)p1 * p1 + (double)p2 * p2;
+      if (mode & FM_UPDATE)
+        st_link(Uout + l, mul(exp_alg(dt_upd * p0, dt_upd * p1, dt_upd * p2), u));
+      else if (mode & FM_RESTORE)
+        st_link(Uout + l, from64<T>(restore_su(to64(u))));
+    }
+  }
+  if (mode & FM_KINETIC) {
+    const double r = block_sum<NT>(k2, sh);
+    if (threadIdx.x == 0) kin_part[blockIdx.x] = r;
+  }
+}
+
+template <class T, int ND, int NT> constexpr size_t async_smem() {
+  return (size_t)AsyncSlots<T, ND>::N * AsyncSlots<T, ND>::W * NT * 16;
 }
 
 template <int ND, int NT>
@@ -353,11 +520,33 @@ template <class T> __global__ void k_restore(size_t NL, LinkT<T> *__restrict__ U
 }
 
 // ------------------------------------------------------------------------------------
+// Box-Muller pair from one Philox draw: FP64 from two 53-bit uniforms; the FP32 (mixed
+// precision) path uses 24-bit uniforms of the same words and FP32 transcendentals.
+template <class T> __device__ __forceinline__ void gauss_pair(const uint32_t r[4], T &a, T &b);
+template <>
+__device__ __forceinline__ void gauss_pair<double>(const uint32_t r[4], double &a, double &b) {
+  box_muller(u01_53(r[0], r[1]), u01_53(r[2], r[3]), a, b);
+}
+template <>
+__device__ __forceinline__ void gauss_pair<float>(const uint32_t r[4], float &a, float &b) {
+  const float u1 = ((float)(r[0] >> 8) + 1.0f) * 0x1p-24f;  // (0, 1]
+  const float u2 = (float)(r[2] >> 8) * 0x1p-24f;           // [0, 1)
+  const float rad = sqrtf(-2.0f * logf(u1));
+  float sn, cs;
+  sincospif(2.0f * u2, &sn, &cs);
+  a = rad * cs;
+  b = rad * sn;
+}
+
+// ------------------------------------------------------------------------------------
 // momenta: standard normal per component from Philox(seed; {ref link, draw, traj, MOM})
 template <class T, int NT>
 __global__ void __launch_bounds__(NT)
-  k_momenta(Geom g, T *__restrict__ P, int na, uint64_t seed, uint32_t traj, double *kin_part) {
+  k_momenta(Geom g, T *__restrict__ P, int na, const TrajParams *__restrict__ tp,
+            double *kin_part) {
   __shared__ double sh[NT / 32];
+  const uint64_t seed = tp->seed;
+  const uint32_t traj = tp->traj;
   const int mu = blockIdx.y >> 1, p = blockIdx.y & 1;
   const int cb = blockIdx.x * NT + threadIdx.x;
   double k2 = 0.;
@@ -367,19 +556,17 @@ __global__ void __launch_bounds__(NT)
     const size_t NL = (size_t)g.V * g.nd;
     const size_t l = (size_t)mu * g.V + (size_t)p * g.Vh + cb;
     uint32_t r[4];
-    double n0, n1, n2, n3;
+    T n0, n1, n2, n3;
     philox(lref, 0u, traj, TAG_MOMENTA, seed, r);
-    box_muller(u01_53(r[0], r[1]), u01_53(r[2], r[3]), n0, n1);
-    const T a = (T)n0;
-    P[l] = a;
-    k2 = (double)a * a;
+    gauss_pair<T>(r, n0, n1);
+    P[l] = n0;
+    k2 = (double)n0 * n0;
     if (na == 3) {
       philox(lref, 1u, traj, TAG_MOMENTA, seed, r);
-      box_muller(u01_53(r[0], r[1]), u01_53(r[2], r[3]), n2, n3);
-      const T b = (T)n1, c = (T)n2;
-      P[NL + l] = b;
-      P[2 * NL + l] = c;
-      k2 += (double)b * b + (double)c * c;
+      gauss_pair<T>(r, n2, n3);
+      P[NL + l] = n1;
+      P[2 * NL + l] = n2;
+      k2 += (double)n1 * n1 + (double)n2 * n2;
     }
   }
   const double rr = block_sum<NT>(k2, sh);
@@ -413,7 +600,9 @@ template <class T> __global__ void k_negate(size_t n, T *P) {
 
 // ------------------------------------------------------------------------------------
 // accept/reject (md_update.hh:45-60), one thread
-__global__ void k_accept(const double *__restrict__ red, AcceptIn in, TrajDev *out) {
+__global__ void k_accept(const double *__restrict__ red, const TrajParams *__restrict__ tp,
+                         TrajDev *out) {
+  const TrajParams in = *tp;
   TrajDev t;
   t.H_old[0] = 0.5 * red[0];
   t.H_old[1] = -in.beta * red[3] / in.Nc;
@@ -509,7 +698,7 @@ template <class T>
 cudaError_t plaq_partials(const Geom &g, const void *U, int group, double xi, double *part,
                           int *nblocks, cudaStream_t s) {
   constexpr int NT = 256;
-  const dim3 grid(2 * cdiv(g.Vh, NT));
+  const dim3 grid(cdiv(g.Vh, NT / 2));
   *nblocks = grid.x;
   if (group == 0) {
     const LinkT<T> *u = (const LinkT<T> *)U;
@@ -538,28 +727,69 @@ cudaError_t reduce_final(const double *part, int nblocks, int ncomp, double *out
 template <class T>
 cudaError_t force_update(const Geom &g, const void *U, int group, T *P, const T *extra, double f,
                          double scale, double xi, int mode, double *kin_part, int *nblocks,
-                         cudaStream_t s) {
+                         void *Uout, double dt_upd, cudaStream_t s, int variant) {
   constexpr int NT = 128;
   const int aniso = xi != 1.0;
   if (group == 0) {
-    const dim3 grid(2 * cdiv(g.Vh, NT));
-    if (nblocks) *nblocks = grid.x;
     const LinkT<T> *u = (const LinkT<T> *)U;
     const T wt = (T)(1.0 / xi), ws = (T)xi;
-    switch (g.nd) {
-      case 2:
-        k_force_su2<T, 2, NT><<<grid, NT, 0, s>>>(g, u, P, extra, (T)f, (T)scale, mode, aniso,
-                                                  wt, ws, kin_part);
-        break;
-      case 3:
-        k_force_su2<T, 3, NT><<<grid, NT, 0, s>>>(g, u, P, extra, (T)f, (T)scale, mode, aniso,
-                                                  wt, ws, kin_part);
-        break;
-      default:
-        k_force_su2<T, 4, NT><<<grid, NT, 0, s>>>(g, u, P, extra, (T)f, (T)scale, mode, aniso,
-                                                  wt, ws, kin_part);
-        break;
+    LinkT<T> *uo = (LinkT<T> *)Uout;
+    int nb = 0;
+    const int v = (variant >= 0 && variant < FORCE_VARIANTS) ? variant : 1;
+#define SU2B_FORCE_LAUNCH(NTV, MB)                                                           \
+  do {                                                                                     \
+    const dim3 grid(cdiv(g.Vh, NTV / 2));                                                  \
+    nb = grid.x;                                                                           \
+    switch (g.nd) {                                                                        \
+      case 2:                                                                              \
+        k_force_su2<T, 2, NTV, MB><<<grid, NTV, 0, s>>>(g, u, P, extra, (T)f, (T)scale, mode, \
+                                                        aniso, wt, ws, kin_part, uo,          \
+                                                        (T)dt_upd);                           \
+        break;                                                                             \
+      case 3:                                                                              \
+        k_force_su2<T, 3, NTV, MB><<<grid, NTV, 0, s>>>(g, u, P, extra, (T)f, (T)scale, mode, \
+                                                        aniso, wt, ws, kin_part, uo,          \
+                                                        (T)dt_upd);                           \
+        break;                                                                             \
+      default:                                                                             \
+        k_force_su2<T, 4, NTV, MB><<<grid, NTV, 0, s>>>(g, u, P, extra, (T)f, (T)scale, mode, \
+                                                        aniso, wt, ws, kin_part, uo,          \
+                                                        (T)dt_upd);                           \
+        break;                                                                             \
+    }                                                                                      \
+  } while (0)
+#define SU2B_FORCE_ASYNC(NTV)                                                                \
+  do {                                                                                     \
+    const dim3 grid(cdiv(g.Vh, NTV / 2));                                                  \
+    nb = grid.x;                                                                           \
+    switch (g.nd) {                                                                        \
+      case 2:                                                                              \
+        k_force_su2_async<T, 2, NTV><<<grid, NTV, async_smem<T, 2, NTV>(), s>>>(            \
+          g, u, P, extra, (T)f, (T)scale, mode, aniso, wt, ws, kin_part, uo, (T)dt_upd);   \
+        break;                                                                             \
+      case 3:                                                                              \
+        k_force_su2_async<T, 3, NTV><<<grid, NTV, async_smem<T, 3, NTV>(), s>>>(            \
+          g, u, P, extra, (T)f, (T)scale, mode, aniso, wt, ws, kin_part, uo, (T)dt_upd);   \
+        break;                                                                             \
+      default:                                                                             \
+        k_force_su2_async<T, 4, NTV><<<grid, NTV, async_smem<T, 4, NTV>(), s>>>(            \
+          g, u, P, extra, (T)f, (T)scale, mode, aniso, wt, ws, kin_part, uo, (T)dt_upd);   \
+        break;                                                                             \
+    }                                                                                      \
+  } while (0)
+    switch (v) {
+      case 0: SU2B_FORCE_LAUNCH(64, 8); break;
+      case 1: SU2B_FORCE_LAUNCH(128, 1); break;
+      case 2: SU2B_FORCE_LAUNCH(128, 4); break;
+      case 3: SU2B_FORCE_LAUNCH(128, 6); break;
+      case 4: SU2B_FORCE_LAUNCH(256, 2); break;
+      case 5: SU2B_FORCE_LAUNCH(256, 3); break;
+      case 6: SU2B_FORCE_ASYNC(64); break;
+      default: SU2B_FORCE_ASYNC(128); break;
     }
+#undef SU2B_FORCE_LAUNCH
+#undef SU2B_FORCE_ASYNC
+    if (nblocks) *nblocks = nb;
   } else {
     if (sizeof(T) != 8) return cudaErrorNotSupported;
     const dim3 grid(cdiv(g.Vh, NT), 2 * g.nd);
@@ -606,12 +836,12 @@ template <class T> cudaError_t restore_links(const Geom &g, void *U, int group, 
 }
 
 template <class T>
-cudaError_t momenta_philox(const Geom &g, T *P, int group, uint64_t seed, uint32_t traj,
+cudaError_t momenta_philox(const Geom &g, T *P, int group, const TrajParams *tp,
                            double *kin_part, int *nblocks, cudaStream_t s) {
   constexpr int NT = NT_RED;
   const dim3 grid(cdiv(g.Vh, NT), 2 * g.nd);
   *nblocks = grid.x * grid.y;
-  k_momenta<T, NT><<<grid, NT, 0, s>>>(g, P, group == 0 ? 3 : 1, seed, traj, kin_part);
+  k_momenta<T, NT><<<grid, NT, 0, s>>>(g, P, group == 0 ? 3 : 1, tp, kin_part);
   return cudaGetLastError();
 }
 
@@ -631,8 +861,8 @@ template <class T> cudaError_t negate_adj(const Geom &g, T *P, int group, cudaSt
   return cudaGetLastError();
 }
 
-cudaError_t accept_step(const double *red, AcceptIn in, TrajDev *out, cudaStream_t s) {
-  k_accept<<<1, 1, 0, s>>>(red, in, out);
+cudaError_t accept_step(const double *red, const TrajParams *tp, TrajDev *out, cudaStream_t s) {
+  k_accept<<<1, 1, 0, s>>>(red, tp, out);
   return cudaGetLastError();
 }
 
@@ -652,6 +882,25 @@ cudaError_t cond_restore(const Geom &g, void *U, const void *U_old, int group,
   return cudaGetLastError();
 }
 
+// raise the dynamic shared-memory limit of the cp.async force kernels (once per process)
+template <class T> cudaError_t force_prepare_t() {
+  cudaError_t e = cudaSuccess;
+#define SU2B_ATTR(ND, NTV)                                                                   \
+  if (e == cudaSuccess)                                                                    \
+    e = cudaFuncSetAttribute(k_force_su2_async<T, ND, NTV>,                                \
+                             cudaFuncAttributeMaxDynamicSharedMemorySize,                  \
+                             (int)async_smem<T, ND, NTV>());
+  SU2B_ATTR(2, 64) SU2B_ATTR(3, 64) SU2B_ATTR(4, 64)
+  SU2B_ATTR(2, 128) SU2B_ATTR(3, 128) SU2B_ATTR(4, 128)
+#undef SU2B_ATTR
+  return e;
+}
+cudaError_t force_prepare() {
+  cudaError_t e = force_prepare_t<float>();
+  if (e == cudaSuccess) e = force_prepare_t<double>();
+  return e;
+}
+
 #define INST(T)                                                                              \
   template cudaError_t links_from_host<T>(const Geom &, const double *, void *, int,         \
                                           cudaStream_t);                                      \
@@ -662,12 +911,12 @@ cudaError_t cond_restore(const Geom &g, void *U, const void *U_old, int group,
   template cudaError_t plaq_partials<T>(const Geom &, const void *, int, double, double *,   \
                                         int *, cudaStream_t);                                 \
   template cudaError_t force_update<T>(const Geom &, const void *, int, T *, const T *,      \
-                                       double, double, double, int, double *, int *,          \
-                                       cudaStream_t);                                         \
+                                       double, double, double, int, double *, int *, void *,  \
+                                       double, cudaStream_t, int);                            \
   template cudaError_t link_update<T>(const Geom &, void *, int, const T *, double,          \
                                       cudaStream_t);                                          \
   template cudaError_t restore_links<T>(const Geom &, void *, int, cudaStream_t);            \
-  template cudaError_t momenta_philox<T>(const Geom &, T *, int, uint64_t, uint32_t,         \
+  template cudaError_t momenta_philox<T>(const Geom &, T *, int, const TrajParams *,         \
                                          double *, int *, cudaStream_t);                      \
   template cudaError_t kinetic_partials<T>(const Geom &, const T *, int, double *, int *,    \
                                            cudaStream_t);                                     \

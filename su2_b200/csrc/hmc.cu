@@ -140,6 +140,167 @@ int kinetic_now(su2b_ctx *ctx, int slot) {
   return SU2B_OK;
 }
 
+// ------------------------------------------------------------------------------------
+// fused SU(2) trajectory: a momentum step and the gauge step after it are one kernel that
+// reads links from one buffer and writes the updated links to another.  The start field S
+// is never written, so a rejected trajectory needs no copy; the two other buffers X, Y
+// alternate.  The closing restoreSU writes the final field and sums its plaquettes.
+struct FOp {
+  int kind;  // 0 momentum step, 1 momentum + gauge step, 2 gauge step alone
+  double cm, cg;
+  bool kinetic;
+};
+
+std::vector<FOp> fuse(const std::vector<Op> &ops) {
+  int last_m = -1;
+  for (int i = 0; i < (int)ops.size(); i++)
+    if (ops[i].kind == 0) last_m = i;
+  std::vector<FOp> f;
+  for (int i = 0; i < (int)ops.size(); i++) {
+    if (ops[i].kind == 0 && i + 1 < (int)ops.size() && ops[i + 1].kind == 1) {
+      f.push_back({1, ops[i].c, ops[i + 1].c, i == last_m});
+      i++;
+    } else if (ops[i].kind == 0) {
+      f.push_back({0, ops[i].c, 0.0, i == last_m});
+    } else {
+      f.push_back({2, 0.0, ops[i].c, false});
+    }
+  }
+  return f;
+}
+
+// queues the trajectory; returns the buffer that holds the final field in *fin
+int enqueue_fused(su2b_ctx *ctx, const std::vector<FOp> &fops, bool host_momenta, void *S,
+                  void *X, void *Y, void **fin) {
+  cudaStream_t s = ctx->stream;
+  int nb = 0;
+  if (!host_momenta) {
+    if (ctx->link64)
+      SU2B_LAUNCH(SU2B_K_MOMENTA, momenta_philox<double>(ctx->g, (double *)ctx->P, 0,
+                                                         ctx->tparams, ctx->part_slot(1), &nb, s));
+    else
+      SU2B_LAUNCH(SU2B_K_MOMENTA, momenta_philox<float>(ctx->g, (float *)ctx->P, 0, ctx->tparams,
+                                                        ctx->part_slot(1), &nb, s));
+    SU2B_LAUNCH(SU2B_K_OTHER, reduce_final(ctx->part_slot(1), nb, 1, ctx->red + 0, s));
+  }
+  SU2B_CK(cudaMemsetAsync(ctx->red + 8, 0, 2 * sizeof(double), s));
+  SU2B_CKS(su2b_q_plaq(ctx, S, 1));
+  const double f = ctx->beta / ctx->Nc();
+  void *cur = S;
+  auto next = [&](void *c) { return c == X ? Y : X; };
+  void *F = nullptr;
+  for (size_t i = 0; i < fops.size(); i++) {
+    const FOp &o = fops[i];
+    const bool last = i + 1 == fops.size();
+    if (o.kind == 2) {  // a gauge step that no momentum step precedes
+      void *out = next(cur);
+      SU2B_CK(cudaMemcpyAsync(out, cur, ctx->link_bytes() * ctx->NL, cudaMemcpyDeviceToDevice,
+                              s));
+      SU2B_CKS(su2b_q_update(ctx, out, ctx->P, o.cg));
+      cur = out;
+      continue;
+    }
+    int mode = FM_HAS_IN | (o.kinetic ? FM_KINETIC : 0);
+    void *out = nullptr;
+    if (o.kind == 1) {
+      mode |= FM_UPDATE;
+      out = next(cur);
+    } else if (last) {
+      // the closing restoreSU (integrator.hh:48) written by the last momentum step
+      mode |= FM_RESTORE;
+      out = F = (cur == S) ? X : next(cur);
+    }
+    if (ctx->link64)
+      SU2B_LAUNCH(SU2B_K_FORCE,
+                  force_update<double>(ctx->g, cur, 0, (double *)ctx->P, nullptr, f, -o.cm,
+                                       ctx->xi, mode, ctx->part_slot(1), &nb, out, o.cg, s,
+                                       ctx->tune_force));
+    else
+      SU2B_LAUNCH(SU2B_K_FORCE,
+                  force_update<float>(ctx->g, cur, 0, (float *)ctx->P, nullptr, f, -o.cm,
+                                      ctx->xi, mode, ctx->part_slot(1), &nb, out, o.cg, s,
+                                       ctx->tune_force));
+    if (o.kinetic) SU2B_LAUNCH(SU2B_K_OTHER, reduce_final(ctx->part_slot(1), nb, 1, ctx->red + 4, s));
+    if (o.kind == 1) cur = out;
+  }
+  if (!F) {  // the schedule ended with a gauge step: restore in place in a scratch buffer
+    if (cur == S) {
+      SU2B_CK(cudaMemcpyAsync(X, S, ctx->link_bytes() * ctx->NL, cudaMemcpyDeviceToDevice, s));
+      cur = X;
+    }
+    SU2B_CKS(su2b_q_restore(ctx, cur));
+    F = cur;
+  }
+  SU2B_CKS(su2b_q_plaq(ctx, F, 5));
+  SU2B_LAUNCH(SU2B_K_OTHER, accept_step(ctx->red, ctx->tparams, ctx->traj, s));
+  SU2B_CK(cudaMemcpyAsync(ctx->h_traj, ctx->traj, sizeof(TrajDev), cudaMemcpyDeviceToHost, s));
+  SU2B_CK(cudaMemcpyAsync(ctx->h_red, ctx->red, 20 * sizeof(double), cudaMemcpyDeviceToHost, s));
+  *fin = F;
+  return SU2B_OK;
+}
+
+int traj_fused(su2b_ctx *ctx, const su2b_hmc_params *prm, su2b_traj_result *res) {
+  cudaStream_t s = ctx->stream;
+  const std::vector<FOp> fops = fuse(schedule(prm->integrator, prm->n_steps, prm->tau));
+  void *S = ctx->U, *X = ctx->U_old, *Y = ctx->U2, *F = nullptr;
+  const bool host_momenta = prm->momenta_host != nullptr;
+  if (host_momenta) {
+    SU2B_CKS(su2b_adj_upload(ctx, prm->momenta_host, ctx->P));
+    SU2B_CKS(kinetic_now(ctx, 0));
+  }
+  if (ctx->prof || host_momenta) {
+    SU2B_CKS(enqueue_fused(ctx, fops, host_momenta, S, X, Y, &F));
+  } else {
+    // one CUDA graph per schedule, coupling and buffer assignment; seed, trajectory index
+    // and accept uniform come from ctx->tparams, so the graph replays for every trajectory
+    char key[256];
+    snprintf(key, sizeof key, "%d/%d/%.17g/%.17g/%p/%p/%p/%d", prm->integrator, prm->n_steps,
+             prm->tau, ctx->beta, S, X, Y, ctx->tune_force);
+    auto it = ctx->graphs.find(key);
+    if (it == ctx->graphs.end()) {
+      const long n0 = ctx->launches;
+      cudaGraph_t graph = nullptr;
+      SU2B_CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+      const int rc = enqueue_fused(ctx, fops, false, S, X, Y, &F);
+      const cudaError_t ec = cudaStreamEndCapture(s, &graph);
+      if (rc != SU2B_OK) {
+        if (graph) cudaGraphDestroy(graph);
+        return rc;
+      }
+      SU2B_CK(ec);
+      su2b_ctx::GraphEntry e{nullptr, ctx->launches - n0};
+      ctx->launches = n0;
+      const cudaError_t ei = cudaGraphInstantiate(&e.exec, graph, 0);
+      cudaGraphDestroy(graph);
+      SU2B_CK(ei);
+      it = ctx->graphs.emplace(key, e).first;
+      ctx->graph_final[key] = F;
+    }
+    F = ctx->graph_final[key];
+    SU2B_CK(cudaGraphLaunch(it->second.exec, s));
+    ctx->launches += it->second.kernels;
+  }
+  SU2B_CK(cudaStreamSynchronize(s));
+  const TrajDev &t = *ctx->h_traj;
+  const double *r = ctx->h_red;
+  if (t.accepted) {  // the final field becomes current; S and the spare become scratch
+    ctx->U = F;
+    ctx->U_old = S;
+    ctx->U2 = (F == X) ? Y : X;
+  }
+  res->accepted = t.accepted;
+  res->dH = t.dH;
+  for (int k = 0; k < 3; k++) {
+    res->H_old[k] = t.H_old[k];
+    res->H_new[k] = t.H_new[k];
+  }
+  res->ddH = 0.0;
+  res->plaquette = t.accepted ? r[5] : r[1];
+  res->cg_iterations = 0;
+  if (ctx->pend.size() > 4096) SU2B_CKS(su2b_prof_fold(ctx));
+  return SU2B_OK;
+}
+
 }  // namespace
 
 extern "C" int su2b_hmc_trajectory(su2b_ctx *ctx, const su2b_hmc_params *prm,
@@ -157,21 +318,34 @@ extern "C" int su2b_hmc_trajectory(su2b_ctx *ctx, const su2b_hmc_params *prm,
     return su2b_fail(ctx, SU2B_ERR_UNSUPPORTED,
                      "staggered fermions are U(1) only (detDDdag_monomial.hh:170-192)");
   cudaStream_t s = ctx->stream;
+  TrajParams tp;
+  tp.beta = ctx->beta;
+  tp.Nc = ctx->Nc();
+  tp.u_host = prm->uniform_host;
+  tp.seed = prm->seed;
+  tp.traj = prm->traj;
+  tp.accept_reject = prm->accept_reject;
+  *ctx->h_tparams = tp;
+  SU2B_CK(cudaMemcpyAsync(ctx->tparams, ctx->h_tparams, sizeof(TrajParams),
+                          cudaMemcpyHostToDevice, s));
+  if (ctx->group == SU2B_GROUP_SU2 && !ferm && !prm->revtest)
+    return traj_fused(ctx, prm, res);
+
+  // generic path: U(1), fermions, reversibility test
   const std::vector<Op> ops = schedule(prm->integrator, prm->n_steps, prm->tau);
   long cg_iters = 0;
   int nb = 0;
-
   // momenta + H_kin old -> red[0]
   if (prm->momenta_host) {
     SU2B_CKS(su2b_adj_upload(ctx, prm->momenta_host, ctx->P));
     SU2B_CKS(kinetic_now(ctx, 0));
   } else {
     if (ctx->link64)
-      SU2B_LAUNCH(SU2B_K_MOMENTA, momenta_philox<double>(ctx->g, (double *)ctx->P, ctx->group, prm->seed, prm->traj,
-                                     ctx->part_slot(1), &nb, s));
+      SU2B_LAUNCH(SU2B_K_MOMENTA, momenta_philox<double>(ctx->g, (double *)ctx->P, ctx->group,
+                                                         ctx->tparams, ctx->part_slot(1), &nb, s));
     else
-      SU2B_LAUNCH(SU2B_K_MOMENTA, momenta_philox<float>(ctx->g, (float *)ctx->P, ctx->group, prm->seed, prm->traj,
-                                    ctx->part_slot(1), &nb, s));
+      SU2B_LAUNCH(SU2B_K_MOMENTA, momenta_philox<float>(ctx->g, (float *)ctx->P, ctx->group,
+                                                        ctx->tparams, ctx->part_slot(1), &nb, s));
     SU2B_LAUNCH(SU2B_K_OTHER, reduce_final(ctx->part_slot(1), nb, 1, ctx->red + 0, s));
   }
   SU2B_CK(cudaMemsetAsync(ctx->red + 8, 0, 2 * sizeof(double), s));
@@ -190,14 +364,7 @@ extern "C" int su2b_hmc_trajectory(su2b_ctx *ctx, const su2b_hmc_params *prm,
                                    prm->cg_start, prm->pf_seed, 9, &it));
     cg_iters += it;
   }
-  AcceptIn in;
-  in.beta = ctx->beta;
-  in.Nc = ctx->Nc();
-  in.seed = prm->seed;
-  in.traj = prm->traj;
-  in.u_host = prm->uniform_host;
-  in.accept_reject = prm->accept_reject;
-  SU2B_LAUNCH(SU2B_K_OTHER, accept_step(ctx->red, in, ctx->traj, s));
+  SU2B_LAUNCH(SU2B_K_OTHER, accept_step(ctx->red, ctx->tparams, ctx->traj, s));
 
   if (prm->revtest) {  // md_update.hh:62-74
     if (!ctx->U_rev) {
@@ -224,11 +391,12 @@ extern "C" int su2b_hmc_trajectory(su2b_ctx *ctx, const su2b_hmc_params *prm,
     ctx->phases_valid = ctx->phases32_valid = false;
   }
   if (ctx->link64)
-    SU2B_LAUNCH(SU2B_K_OTHER, cond_restore<double>(ctx->g, ctx->U, ctx->U_old, ctx->group, ctx->traj, s));
+    SU2B_LAUNCH(SU2B_K_OTHER,
+                cond_restore<double>(ctx->g, ctx->U, ctx->U_old, ctx->group, ctx->traj, s));
   else
-    SU2B_LAUNCH(SU2B_K_OTHER, cond_restore<float>(ctx->g, ctx->U, ctx->U_old, ctx->group, ctx->traj, s));
+    SU2B_LAUNCH(SU2B_K_OTHER,
+                cond_restore<float>(ctx->g, ctx->U, ctx->U_old, ctx->group, ctx->traj, s));
   ctx->phases_valid = ctx->phases32_valid = false;
-  SU2B_CKS(su2b_q_plaq(ctx, ctx->U, 16));
   SU2B_CK(cudaMemcpyAsync(ctx->h_traj, ctx->traj, sizeof(TrajDev), cudaMemcpyDeviceToHost, s));
   SU2B_CKS(su2b_fetch_red(ctx, 20));
   const TrajDev &t = *ctx->h_traj;
@@ -247,7 +415,7 @@ extern "C" int su2b_hmc_trajectory(su2b_ctx *ctx, const su2b_hmc_params *prm,
     d += r[14] - t.H_old[2];
     res->ddH = d;
   }
-  res->plaquette = r[16];
+  res->plaquette = t.accepted ? r[5] : r[1];
   res->cg_iterations = cg_iters;
   if (ctx->pend.size() > 4096) SU2B_CKS(su2b_prof_fold(ctx));
   return SU2B_OK;

@@ -23,13 +23,16 @@ struct su2b_ctx {
   cudaStream_t stream = nullptr;
 
   // gauge field, backups, momenta, flow/force accumulator
-  void *U = nullptr, *U_old = nullptr, *U_aux = nullptr, *U_rev = nullptr;
+  // U is the current field; U_old and U2 are the other two link buffers of the fused
+  // trajectory (the start configuration stays untouched in one of them until accept/reject)
+  void *U = nullptr, *U_old = nullptr, *U2 = nullptr, *U_aux = nullptr, *U_rev = nullptr;
   void *P = nullptr, *Z = nullptr;
   double *stage = nullptr;  // host-layout staging buffer on the device
   double *part = nullptr;   // NSLOT slots of 3*part_cap partial sums
   size_t part_cap = 0;
   double *red = nullptr;    // 64 reduced scalars
   su2b::TrajDev *traj = nullptr;
+  su2b::TrajParams *tparams = nullptr, *h_tparams = nullptr;
   unsigned long long *counts = nullptr;
 
   // pinned host mirrors
@@ -48,6 +51,9 @@ struct su2b_ctx {
   su2b::SolverState *st = nullptr;
   long x0_seed = -1;  // seed of the reference CG start held in sv[SV_X0]
 
+  // launch shape of the SU(2) force kernel (su2b_autotune)
+  int tune_force = 1;
+
   // kernel launch counter and the per-class device timers (su2b_profile)
   long launches = 0;
   bool prof = false;
@@ -60,7 +66,12 @@ struct su2b_ctx {
   double prof_ms[16] = {};
   long prof_n[16] = {};
 
-  std::map<std::string, cudaGraphExec_t> graphs;
+  struct GraphEntry {
+    cudaGraphExec_t exec;
+    long kernels;
+  };
+  std::map<std::string, GraphEntry> graphs;
+  std::map<std::string, void *> graph_final;  // buffer holding the result of each graph
   std::vector<void *> allocs;
   std::string err;
 
@@ -84,6 +95,7 @@ int su2b_q_restore(su2b_ctx *ctx, void *U);
 int su2b_q_flow_step(su2b_ctx *ctx, void *U, double eps);
 int su2b_ensure_aux(su2b_ctx *ctx);
 int su2b_links_to_stage(su2b_ctx *ctx, const void *U);
+int su2b_prof_fold(su2b_ctx *ctx);
 int su2b_make_geom(int Lx, int Ly, int Lz, int Lt, int nd, su2b::Geom *g, std::string *why);
 // fermions (solve.cu)
 int su2b_fermion_setup(su2b_ctx *ctx, bool need32);

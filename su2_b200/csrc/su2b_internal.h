@@ -33,18 +33,35 @@ cudaError_t reduce_final(const double *part, int nblocks, int ncomp, double *out
 enum ForceMode : int {
   FM_HAS_IN = 1,     // P_out = P_in + scale*(f*g) (else P_out = scale*(f*g))
   FM_KINETIC = 2,    // also write per-block partials of sum P_out^2
-  FM_EXTRA = 4       // add extra[] (another monomial's derivative) to f*g before scaling
+  FM_EXTRA = 4,      // add extra[] (another monomial's derivative) to f*g before scaling
+  FM_UPDATE = 8,     // SU(2): also write Uout = exp(dt_upd * P_out) U (the next gauge step)
+  FM_RESTORE = 16    // SU(2): also write Uout = restoreSU(U) (the end of the trajectory)
 };
+// launch shapes of the SU(2) force kernel (threads per block, minimum resident blocks per
+// SM, which caps registers): 0 (64,8) 1 (128,1) 2 (128,4) 3 (128,6) 4 (256,2) 5 (256,3);
+// 6, 7: neighbour links staged in shared memory by cp.async, 64 / 128 threads per block
+constexpr int FORCE_VARIANTS = 8;
+cudaError_t force_prepare();  // once per device before the first launch
 template <class T>
 cudaError_t force_update(const Geom &g, const void *U, int group, T *P, const T *extra, double f,
                          double scale, double xi, int mode, double *kin_part, int *nblocks,
-                         cudaStream_t s);
+                         void *Uout, double dt_upd, cudaStream_t s, int variant = 1);
+
 template <class T>
 cudaError_t link_update(const Geom &g, void *U, int group, const T *P, double dt,
                         cudaStream_t s);
 template <class T> cudaError_t restore_links(const Geom &g, void *U, int group, cudaStream_t s);
+// per-trajectory parameters read by the kernels from device memory, so that a captured
+// trajectory graph can be replayed with a new seed and trajectory index
+struct TrajParams {
+  double beta, Nc;
+  double u_host;  // < 0: Philox uniform
+  uint64_t seed;
+  uint32_t traj;
+  int accept_reject;
+};
 template <class T>
-cudaError_t momenta_philox(const Geom &g, T *P, int group, uint64_t seed, uint32_t traj,
+cudaError_t momenta_philox(const Geom &g, T *P, int group, const TrajParams *tp,
                            double *kin_part, int *nblocks, cudaStream_t s);
 template <class T>
 cudaError_t kinetic_partials(const Geom &g, const T *P, int group, double *part, int *nblocks,
@@ -53,13 +70,6 @@ template <class T>
 cudaError_t negate_adj(const Geom &g, T *P, int group, cudaStream_t s);
 
 // ---- accept / reject ----
-struct AcceptIn {
-  double beta, Nc;
-  uint64_t seed;
-  uint32_t traj;
-  double u_host;  // < 0: Philox uniform
-  int accept_reject;
-};
 // reduced values read by the accept step:
 //   red[0] sum P^2 before, red[1..3] plaquette sums before {full, spatial, xi-weighted},
 //   red[4] sum P^2 after,  red[5..7] plaquette sums after, red[8] / red[9] fermion action
@@ -70,7 +80,7 @@ struct TrajDev {
   int accepted;
   int pad;
 };
-cudaError_t accept_step(const double *red, AcceptIn in, TrajDev *out, cudaStream_t s);
+cudaError_t accept_step(const double *red, const TrajParams *tp, TrajDev *out, cudaStream_t s);
 template <class T>
 cudaError_t cond_restore(const Geom &g, void *U, const void *U_old, int group,
                          const TrajDev *flag, cudaStream_t s);

@@ -120,6 +120,24 @@ class gaugeconfig:
             out[name] = (n.value, ms.value)
         return out
 
+    def autotune(self, cache_path=None, retune=False):
+        """Time the launch shapes of the force kernel on this field and keep the fastest;
+        returns {variant: microseconds}."""
+        t = np.zeros(_abi.FORCE_VARIANTS)
+        cp = cache_path.encode() if cache_path else None
+        self._c(self.lib.su2b_autotune(self.ctx, cp, int(retune), _dp(t)))
+        return {v: float(t[v]) for v in range(_abi.FORCE_VARIANTS)}
+
+    @property
+    def force_variant(self) -> int:
+        v = C.c_int()
+        self._c(self.lib.su2b_tune_get(self.ctx, 0, C.byref(v)))
+        return v.value
+
+    @force_variant.setter
+    def force_variant(self, v):
+        self._c(self.lib.su2b_tune_set(self.ctx, 0, int(v)))
+
     def kernel_launches(self) -> int:
         n = C.c_long()
         self._c(self.lib.su2b_kernel_launches(self.ctx, C.byref(n)))
