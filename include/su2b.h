@@ -206,6 +206,26 @@ SU2B_API int su2b_fermion_force(su2b_ctx *ctx, double mass, const double *phi_ho
 SU2B_API int su2b_fermion_action(su2b_ctx *ctx, double mass, const double *phi_host, double tol,
                         int max_iter, const double *x0_host, long seed, double *out);
 
+/* ---- derivatives (SU(2)) ------------------------------------------------------------------ */
+/* Left Lie-algebra derivatives, the convention of gaugemonomial::derivative
+ * (flat-gaugemonomial.hh:105-131): grad(x,mu)_k = d/dw O(exp(w e_k) U_mu(x)) at w = 0 with
+ * exp of exp_gauge.cc:8-18.  Results use the adjoint host layout. */
+/* Wilson action S = get_S_G_hmc (flat-gaugemonomial.hh:46-54) into *S (may be NULL) and
+ * grad_out * dS/dU into dS_host (may be NULL); dS/dU is the gauge force with fac = 1. */
+SU2B_API int su2b_action_backward(su2b_ctx *ctx, double grad_out, double *S, double *dS_host);
+/* Vector-Jacobian product of the force field g(U)(x,mu) = get_deriv(U_mu(x) K_mu(x)):
+ * out = (dg/dU)^T mu, i.e. the left derivative of sum mu.g (a Hessian-vector product of the
+ * Wilson action up to beta/Nc). */
+SU2B_API int su2b_force_vjp(su2b_ctx *ctx, const double *mu_host, double *out_host);
+/* O = t^2 E_p(t) after n_steps Wilson-flow RK3 steps (runge_kutta, flat-gradient_flow.hh:
+ * 17-50) of size eps from the context's links, t = n_steps*eps, E_p = d(d-1)/2 - P/(V Nc)
+ * the plaquette energy of gradient_flow (flat-gradient_flow.hh:151); *objective receives O
+ * and grad_host (NULL: objective only) its derivative with respect to the starting links,
+ * by the adjoint of the RK3 steps with checkpoints every checkpoint_every steps
+ * (0 = sqrt(n_steps)).  The links are not modified. */
+SU2B_API int su2b_flow_adjoint(su2b_ctx *ctx, double eps, int n_steps, int checkpoint_every,
+                               double *objective, double *grad_host);
+
 /* ---- launch-shape autotuning ------------------------------------------------------------ */
 /* The SU(2) force kernel has SU2B_FORCE_VARIANTS launch shapes (threads per block x register
  * cap).  su2b_autotune times them all on the context's field (CUDA events, the same memory

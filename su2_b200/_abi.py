@@ -85,6 +85,9 @@ SIGNATURES = {
     "su2b_kernel_launches": (i32, [_P, C.POINTER(C.c_long)]),
     "su2b_gauge_energy_noalloc": (i32, [i32, i32, i32, i32, i32, i32, _P, _P, _P]),
     "su2b_autotune": (i32, [_P, C.c_char_p, i32, _D]),
+    "su2b_action_backward": (i32, [_P, f64, _D, _D]),
+    "su2b_force_vjp": (i32, [_P, _D, _D]),
+    "su2b_flow_adjoint": (i32, [_P, f64, i32, i32, _D, _D]),
     "su2b_tune_get": (i32, [_P, i32, C.POINTER(C.c_int)]),
     "su2b_tune_set": (i32, [_P, i32, i32]),
 }

@@ -193,6 +193,28 @@ class gaugeconfig:
         P = _f64(P)
         self._c(self.lib.su2b_update_gauge(self.ctx, _dp(P), dtau))
 
+    # ---- derivatives (SU(2)) ----
+    def action_backward(self, grad_out=1.0):
+        """(S, grad_out * dS/dU): the Wilson action and its left derivative."""
+        S = C.c_double()
+        out = np.empty(self.n_links * 3)
+        self._c(self.lib.su2b_action_backward(self.ctx, grad_out, C.byref(S), _dp(out)))
+        return S.value, out
+
+    def force_vjp(self, mu):
+        mu = _f64(mu)
+        out = np.empty(self.n_links * 3)
+        self._c(self.lib.su2b_force_vjp(self.ctx, _dp(mu), _dp(out)))
+        return out
+
+    def flow_objective(self, eps, n_steps, grad=True, checkpoint_every=0):
+        """t^2 E_p(t) after n_steps flow steps and (if grad) its derivative w.r.t. the links."""
+        O = C.c_double()
+        g = np.empty(self.n_links * 3) if grad else None
+        self._c(self.lib.su2b_flow_adjoint(self.ctx, eps, n_steps, checkpoint_every, C.byref(O),
+                                           _dp(g) if grad else None))
+        return (O.value, g) if grad else O.value
+
     # ---- HMC ----
     def md_update(self, integrator="leapfrog", n_steps=10, tau=1.0, seed=0, traj=0,
                   momenta=None, uniform=None, revtest=False, accept_reject=True,
