@@ -206,6 +206,29 @@ SU2B_API int su2b_fermion_force(su2b_ctx *ctx, double mass, const double *phi_ho
 SU2B_API int su2b_fermion_action(su2b_ctx *ctx, double mass, const double *phi_host, double tol,
                         int max_iter, const double *x0_host, long seed, double *out);
 
+/* ---- batched ensembles of independent SU(2) chains ------------------------------------------ */
+/* Chains of different geometry (d = 3 or 4, even extents), coupling and seed advanced together:
+ * every stage of a trajectory is one persistent launch over all chains, a trajectory is one
+ * CUDA graph, and each chain keeps its own accept/reject (md_update.hh:18-81).  A chain's
+ * trajectory equals the one of a single-lattice context with the same seed and traj. */
+typedef struct {
+  int Lx, Ly, Lz, Lt, ndims;
+  double beta;
+  uint64_t seed;
+} su2b_chain_desc;
+typedef struct su2b_batch su2b_batch;
+SU2B_API int su2b_batch_create(int n_chains, const su2b_chain_desc *chains, int precision,
+                               int device, su2b_batch **out);
+SU2B_API int su2b_batch_destroy(su2b_batch *b);
+SU2B_API const char *su2b_batch_last_error(const su2b_batch *b);
+SU2B_API int su2b_batch_stream(su2b_batch *b, void **stream);
+SU2B_API int su2b_batch_kernel_launches(su2b_batch *b, long *count);
+SU2B_API int su2b_batch_upload(su2b_batch *b, int chain, const double *U_host);
+SU2B_API int su2b_batch_download(su2b_batch *b, int chain, double *U_host);
+/* one trajectory (SU2B_LEAPFROG or SU2B_OMF2) of every chain; results[n_chains] */
+SU2B_API int su2b_batch_hmc(su2b_batch *b, int integrator, int n_steps, double tau, uint32_t traj,
+                            su2b_traj_result *results);
+
 /* ---- derivatives (SU(2)) ------------------------------------------------------------------ */
 /* Left Lie-algebra derivatives, the convention of gaugemonomial::derivative
  * (flat-gaugemonomial.hh:105-131): grad(x,mu)_k = d/dw O(exp(w e_k) U_mu(x)) at w = 0 with

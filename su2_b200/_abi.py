@@ -42,6 +42,11 @@ class TrajResult(C.Structure):
                 ("plaquette", C.c_double), ("cg_iterations", C.c_long)]
 
 
+class ChainDesc(C.Structure):
+    _fields_ = [("Lx", C.c_int), ("Ly", C.c_int), ("Lz", C.c_int), ("Lt", C.c_int),
+                ("ndims", C.c_int), ("beta", C.c_double), ("seed", C.c_uint64)]
+
+
 class SolveParams(C.Structure):
     _fields_ = [("solver", C.c_int), ("op", C.c_int), ("mass", C.c_double), ("tol", C.c_double),
                 ("tol_mode", C.c_int), ("max_iter", C.c_int), ("delta", C.c_double)]
@@ -85,6 +90,14 @@ SIGNATURES = {
     "su2b_kernel_launches": (i32, [_P, C.POINTER(C.c_long)]),
     "su2b_gauge_energy_noalloc": (i32, [i32, i32, i32, i32, i32, i32, _P, _P, _P]),
     "su2b_autotune": (i32, [_P, C.c_char_p, i32, _D]),
+    "su2b_batch_create": (i32, [i32, C.POINTER(ChainDesc), i32, i32, C.POINTER(_P)]),
+    "su2b_batch_destroy": (i32, [_P]),
+    "su2b_batch_last_error": (C.c_char_p, [_P]),
+    "su2b_batch_stream": (i32, [_P, C.POINTER(_P)]),
+    "su2b_batch_kernel_launches": (i32, [_P, C.POINTER(C.c_long)]),
+    "su2b_batch_upload": (i32, [_P, i32, _D]),
+    "su2b_batch_download": (i32, [_P, i32, _D]),
+    "su2b_batch_hmc": (i32, [_P, i32, i32, f64, u32, C.POINTER(TrajResult)]),
     "su2b_action_backward": (i32, [_P, f64, _D, _D]),
     "su2b_force_vjp": (i32, [_P, _D, _D]),
     "su2b_flow_adjoint": (i32, [_P, f64, i32, i32, _D, _D]),

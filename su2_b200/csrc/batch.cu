@@ -1,0 +1,548 @@
+// batch.cu -- an ensemble of independent SU(2) chains (different geometries, dimensions and
+// couplings) advanced together: every stage of an HMC trajectory is ONE persistent launch
+// over a tile list that spans all chains, and the whole trajectory is one CUDA graph.
+//
+// Storage: the links of all chains are concatenated in each of three link buffers, the
+// momenta in one adjoint buffer (per chain the single-lattice layout, see su2b_common.cuh).
+// Each chain's triple-buffer rotation (which buffer holds its current field) lives in device
+// memory and is advanced by the per-chain accept kernel, so replaying the graph needs no host
+// decision.  A tile is NT/2 sites of each parity of one chain; block b finds its chain in the
+// tile prefix table.  The per-site arithmetic is force_site / plaq_site, shared with the
+// single-lattice kernels, so a chain gives the same trajectory alone or in a batch.
+#include <algorithm>
+#include <cstdarg>
+#include <cstdio>
+#include <string>
+#include <vector>
+
+#include "site_ops.cuh"
+#include "su2b.h"
+
+using namespace su2b;
+
+namespace {
+
+struct ChainDev {
+  Geom g;
+  double beta;
+  uint64_t seed;
+  size_t off_link;  // offset of the chain in the link buffers (in links)
+  size_t off_adj;   // offset of the chain's momenta (3 * NL reals)
+  int tile0, ntiles;
+};
+
+constexpr int RS = 16;  // reduced scalars per chain
+
+__device__ __forceinline__ int chain_of(const ChainDev *__restrict__ ch, int n, int tile) {
+  int c = 0;
+  while (c + 1 < n && __ldg(&ch[c + 1].tile0) <= tile) c++;
+  return c;
+}
+
+template <class T> struct Bufs {
+  LinkT<T> *b[3];
+};
+
+template <class T, int NT>
+__global__ void __launch_bounds__(NT)
+  k_batch_force(const ChainDev *__restrict__ ch, int nchains, int ntiles, Bufs<T> bufs,
+                T *__restrict__ Pall, const int *__restrict__ cur, int rel_in, int rel_out,
+                double cm, double cg, int mode, double *kin_part) {
+  __shared__ double sh[NT / 32];
+  const int w = threadIdx.x >> 5, p = w & 1;
+  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const int c = chain_of(ch, nchains, tile);
+    const ChainDev &d = ch[c];
+    const int cb = (tile - d.tile0) * (NT / 2) + (w >> 1) * 32 + (threadIdx.x & 31);
+    const int S = cur[c];
+    const LinkT<T> *U = bufs.b[(S + rel_in) % 3] + d.off_link;
+    LinkT<T> *Uo = rel_out >= 0 ? bufs.b[(S + rel_out) % 3] + d.off_link : nullptr;
+    T *P = Pall + d.off_adj;
+    const T f = (T)(d.beta / 2.0);
+    double k2 = 0.;
+    if (cb < d.g.Vh) {
+      if (d.g.nd == 4)
+        k2 = force_site<T, 4>(d.g, U, P, nullptr, f, (T)(-cm), mode, 0, T(1), T(1), Uo, (T)cg, p,
+                              cb);
+      else
+        k2 = force_site<T, 3>(d.g, U, P, nullptr, f, (T)(-cm), mode, 0, T(1), T(1), Uo, (T)cg, p,
+                              cb);
+    }
+    if (mode & FM_KINETIC) {
+      const double r = block_sum<NT>(k2, sh);
+      if (threadIdx.x == 0) kin_part[tile] = r;
+    }
+  }
+}
+
+// momenta of the batch: the single-lattice Philox stream of each chain (its own seed)
+template <class T, int NT>
+__global__ void __launch_bounds__(NT)
+  k_batch_momenta(const ChainDev *__restrict__ ch, int nchains, int ntiles, T *__restrict__ Pall,
+                  const uint32_t *__restrict__ traj, double *kin_part) {
+  __shared__ double sh[NT / 32];
+  const int w = threadIdx.x >> 5, p = w & 1;
+  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const int c = chain_of(ch, nchains, tile);
+    const ChainDev &d = ch[c];
+    const int cb = (tile - d.tile0) * (NT / 2) + (w >> 1) * 32 + (threadIdx.x & 31);
+    double k2 = 0.;
+    if (cb < d.g.Vh) {
+      const Site s = site_from_eo(d.g, p, cb);
+      const size_t NL = (size_t)d.g.V * d.g.nd;
+      T *P = Pall + d.off_adj;
+      for (int mu = 0; mu < d.g.nd; mu++) {
+        const uint32_t lref = (uint32_t)s.lex * (uint32_t)d.g.nd + (uint32_t)mu;
+        const size_t l = (size_t)mu * d.g.V + (size_t)p * d.g.Vh + cb;
+        uint32_t r[4];
+        T n[4];
+        philox(lref, 0u, *traj, TAG_MOMENTA, d.seed, r);
+        gauss_pair<T>(r, n[0], n[1]);
+        philox(lref, 1u, *traj, TAG_MOMENTA, d.seed, r);
+        gauss_pair<T>(r, n[2], n[3]);
+        const T a = n[0], b = n[1], cc = n[2];
+        P[l] = a;
+        P[NL + l] = b;
+        P[2 * NL + l] = cc;
+        k2 += (double)a * a + (double)b * b + (double)cc * cc;
+      }
+    }
+    const double rr = block_sum<NT>(k2, sh);
+    if (threadIdx.x == 0) kin_part[tile] = rr;
+  }
+}
+
+template <class T, int NT>
+__global__ void __launch_bounds__(NT)
+  k_batch_plaq(const ChainDev *__restrict__ ch, int nchains, int ntiles, Bufs<T> bufs,
+               const int *__restrict__ cur, int rel, double *part) {
+  __shared__ double sh[NT / 32];
+  const int w = threadIdx.x >> 5, p = w & 1;
+  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const int c = chain_of(ch, nchains, tile);
+    const ChainDev &d = ch[c];
+    const int cb = (tile - d.tile0) * (NT / 2) + (w >> 1) * 32 + (threadIdx.x & 31);
+    const LinkT<T> *U = bufs.b[(cur[c] + rel) % 3] + d.off_link;
+    double full = 0., spat = 0., wsum = 0.;
+    if (cb < d.g.Vh) {
+      if (d.g.nd == 4)
+        plaq_site<T, 4>(d.g, U, p, cb, 1.0, full, spat, wsum);
+      else
+        plaq_site<T, 3>(d.g, U, p, cb, 1.0, full, spat, wsum);
+    }
+    double r = block_sum<NT>(full, sh);
+    if (threadIdx.x == 0) part[3 * tile] = r;
+    r = block_sum<NT>(spat, sh);
+    if (threadIdx.x == 0) part[3 * tile + 1] = r;
+  }
+}
+
+// per chain: red[c*RS + slot + k] = sum of part[tile*ncomp + k] over the chain's tiles
+__global__ void __launch_bounds__(256)
+  k_batch_reduce(const ChainDev *__restrict__ ch, const double *__restrict__ part, int ncomp,
+                 double *red, int slot) {
+  __shared__ double sh[8];
+  const ChainDev &d = ch[blockIdx.x];
+  for (int k = 0; k < ncomp; k++) {
+    double v = 0.;
+    for (int t = threadIdx.x; t < d.ntiles; t += 256) v += part[(size_t)(d.tile0 + t) * ncomp + k];
+    const double r = block_sum<256>(v, sh);
+    if (threadIdx.x == 0) red[blockIdx.x * RS + slot + k] = r;
+  }
+}
+
+// per chain accept/reject (md_update.hh:45-60) and advance of the buffer rotation
+__global__ void k_batch_accept(const ChainDev *__restrict__ ch, int nchains,
+                               const double *__restrict__ red, const uint32_t *__restrict__ traj,
+                               int rel_final, int *cur, TrajDev *out) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= nchains) return;
+  const ChainDev &d = ch[c];
+  const double *r = red + c * RS;
+  TrajDev t;
+  t.H_old[0] = 0.5 * r[0];
+  t.H_old[1] = -d.beta * r[1] / 2.0;
+  t.H_old[2] = 0.0;
+  t.H_new[0] = 0.5 * r[4];
+  t.H_new[1] = -d.beta * r[5] / 2.0;
+  t.H_new[2] = 0.0;
+  double dH = 0.;
+  dH += t.H_new[0] - t.H_old[0];
+  dH += t.H_new[1] - t.H_old[1];
+  t.dH = dH;
+  t.accepted = 1;
+  t.u = -1.0;
+  if (dH > 0) {
+    uint32_t rr[4];
+    philox(0u, 0u, *traj, TAG_ACCEPT, d.seed, rr);
+    t.u = u01_53(rr[0], rr[1]) - 0x1p-53;
+    if (t.u > exp(-dH)) t.accepted = 0;
+  }
+  t.pad = 0;
+  out[c] = t;
+  if (t.accepted) cur[c] = (cur[c] + rel_final) % 3;
+}
+
+}  // namespace
+
+// =====================================================================================
+struct su2b_batch {
+  int n = 0, prec = 0, device = 0;
+  bool link64 = true;
+  cudaStream_t stream = nullptr;
+  std::vector<su2b_chain_desc> desc;
+  std::vector<ChainDev> hch;
+  ChainDev *ch = nullptr;
+  int ntiles = 0, nt = 128;
+  size_t total_links = 0;
+  void *buf[3] = {};
+  void *P = nullptr;
+  double *part = nullptr, *red = nullptr, *stage = nullptr;
+  int *cur = nullptr;
+  uint32_t *traj = nullptr, *h_traj = nullptr;
+  TrajDev *res = nullptr, *h_res = nullptr;
+  double *h_red = nullptr;
+  int *h_cur = nullptr;
+  struct Graph {
+    std::string key;
+    cudaGraphExec_t exec;
+    long kernels;
+  };
+  std::vector<Graph> graphs;
+  std::vector<void *> allocs;
+  std::string err;
+  long launches = 0;
+};
+
+static int bfail(su2b_batch *b, int code, const char *fmt, ...) {
+  if (b) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    b->err = buf;
+  }
+  return code;
+}
+#define BCK(call)                                                                          \
+  do {                                                                                     \
+    cudaError_t e_ = (call);                                                               \
+    if (e_ != cudaSuccess)                                                                 \
+      return bfail(b, SU2B_ERR_CUDA, "%s:%d %s: %s", __FILE__, __LINE__, #call,            \
+                   cudaGetErrorString(e_));                                                \
+  } while (0)
+
+int su2b_make_geom(int Lx, int Ly, int Lz, int Lt, int nd, Geom *g, std::string *why);
+
+extern "C" int su2b_batch_create(int n_chains, const su2b_chain_desc *chains, int precision,
+                                 int device, su2b_batch **out) {
+  if (!out || !chains || n_chains < 1) return SU2B_ERR_INVALID;
+  *out = nullptr;
+  if (precision != SU2B_PREC_FP64 && precision != SU2B_PREC_MIXED) return SU2B_ERR_INVALID;
+  su2b_batch *b = new su2b_batch();
+  b->n = n_chains;
+  b->prec = precision;
+  b->device = device;
+  b->link64 = precision == SU2B_PREC_FP64;
+  b->desc.assign(chains, chains + n_chains);
+  auto fin = [&](int s) -> int {
+    if (s != SU2B_OK) {
+      su2b_batch_destroy(b);
+      return s;
+    }
+    *out = b;
+    return SU2B_OK;
+  };
+  size_t off_l = 0, off_a = 0;
+  int tile = 0;
+  const int half = b->nt / 2;
+  for (int c = 0; c < n_chains; c++) {
+    const su2b_chain_desc &d = chains[c];
+    ChainDev cd{};
+    std::string why;
+    if (d.ndims < 3 || !su2b_make_geom(d.Lx, d.Ly, d.Lz, d.Lt, d.ndims, &cd.g, &why))
+      return fin(bfail(b, SU2B_ERR_INVALID, "chain %d: %s", c,
+                       d.ndims < 3 ? "batches hold d = 3 or 4 chains" : why.c_str()));
+    cd.beta = d.beta;
+    cd.seed = d.seed;
+    cd.off_link = off_l;
+    cd.off_adj = off_a;
+    cd.tile0 = tile;
+    cd.ntiles = (cd.g.Vh + half - 1) / half;
+    const size_t NL = (size_t)cd.g.V * d.ndims;
+    off_l += NL;
+    off_a += 3 * NL;
+    tile += cd.ntiles;
+    b->hch.push_back(cd);
+  }
+  b->ntiles = tile;
+  b->total_links = off_l;
+  if (cudaSetDevice(device) != cudaSuccess) return fin(SU2B_ERR_CUDA);
+  if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess)
+    return fin(SU2B_ERR_CUDA);
+  const size_t lb = b->link64 ? 32 : 16, ab = b->link64 ? 8 : 4;
+  auto dal = [&](void **p, size_t bytes) -> bool {
+    if (cudaMalloc(p, bytes) != cudaSuccess) return false;
+    b->allocs.push_back(*p);
+    return true;
+  };
+  size_t maxNL = 0;
+  for (auto &c : b->hch) maxNL = std::max(maxNL, (size_t)c.g.V * c.g.nd);
+  bool ok = dal(&b->buf[0], lb * off_l) && dal(&b->buf[1], lb * off_l) &&
+            dal(&b->buf[2], lb * off_l) && dal(&b->P, ab * off_a) &&
+            dal((void **)&b->part, sizeof(double) * 3 * (size_t)tile) &&
+            dal((void **)&b->red, sizeof(double) * RS * n_chains) &&
+            dal((void **)&b->stage, sizeof(double) * 4 * maxNL) &&
+            dal((void **)&b->cur, sizeof(int) * n_chains) &&
+            dal((void **)&b->traj, sizeof(uint32_t)) &&
+            dal((void **)&b->res, sizeof(TrajDev) * n_chains) &&
+            dal((void **)&b->ch, sizeof(ChainDev) * n_chains);
+  if (!ok) return fin(bfail(b, SU2B_ERR_NOMEM, "device allocation failed"));
+  if (cudaMallocHost((void **)&b->h_traj, sizeof(uint32_t)) != cudaSuccess ||
+      cudaMallocHost((void **)&b->h_res, sizeof(TrajDev) * n_chains) != cudaSuccess ||
+      cudaMallocHost((void **)&b->h_red, sizeof(double) * RS * n_chains) != cudaSuccess ||
+      cudaMallocHost((void **)&b->h_cur, sizeof(int) * n_chains) != cudaSuccess)
+    return fin(SU2B_ERR_NOMEM);
+  if (cudaMemcpy(b->ch, b->hch.data(), sizeof(ChainDev) * n_chains, cudaMemcpyHostToDevice) !=
+        cudaSuccess ||
+      cudaMemset(b->cur, 0, sizeof(int) * n_chains) != cudaSuccess ||
+      cudaMemset(b->buf[0], 0, lb * off_l) != cudaSuccess)
+    return fin(SU2B_ERR_CUDA);
+  return fin(SU2B_OK);
+}
+
+extern "C" int su2b_batch_destroy(su2b_batch *b) {
+  if (!b) return SU2B_ERR_INVALID;
+  cudaSetDevice(b->device);
+  if (b->stream) cudaStreamSynchronize(b->stream);
+  for (auto &g : b->graphs) cudaGraphExecDestroy(g.exec);
+  for (void *p : b->allocs) cudaFree(p);
+  if (b->h_traj) cudaFreeHost(b->h_traj);
+  if (b->h_res) cudaFreeHost(b->h_res);
+  if (b->h_red) cudaFreeHost(b->h_red);
+  if (b->h_cur) cudaFreeHost(b->h_cur);
+  if (b->stream) cudaStreamDestroy(b->stream);
+  delete b;
+  return SU2B_OK;
+}
+
+extern "C" const char *su2b_batch_last_error(const su2b_batch *b) {
+  return b ? b->err.c_str() : "null batch";
+}
+extern "C" int su2b_batch_stream(su2b_batch *b, void **stream) {
+  if (!b || !stream) return SU2B_ERR_INVALID;
+  *stream = (void *)b->stream;
+  return SU2B_OK;
+}
+extern "C" int su2b_batch_kernel_launches(su2b_batch *b, long *count) {
+  if (!b || !count) return SU2B_ERR_INVALID;
+  *count = b->launches;
+  return SU2B_OK;
+}
+
+static int chain_transfer(su2b_batch *b, int chain, double *host, bool up) {
+  if (chain < 0 || chain >= b->n || !host) return bfail(b, SU2B_ERR_INVALID, "bad chain/buffer");
+  BCK(cudaSetDevice(b->device));
+  const ChainDev &c = b->hch[chain];
+  const size_t NL = (size_t)c.g.V * c.g.nd;
+  BCK(cudaMemcpy(b->h_cur, b->cur, sizeof(int) * b->n, cudaMemcpyDeviceToHost));
+  const size_t lb = b->link64 ? 32 : 16;
+  char *U = (char *)b->buf[b->h_cur[chain]] + lb * c.off_link;
+  if (up) {
+    BCK(cudaMemcpyAsync(b->stage, host, 4 * NL * sizeof(double), cudaMemcpyHostToDevice,
+                        b->stream));
+    if (b->link64)
+      BCK(links_from_host<double>(c.g, b->stage, U, 0, b->stream));
+    else
+      BCK(links_from_host<float>(c.g, b->stage, U, 0, b->stream));
+  } else {
+    if (b->link64)
+      BCK(links_to_host<double>(c.g, U, b->stage, 0, b->stream));
+    else
+      BCK(links_to_host<float>(c.g, U, b->stage, 0, b->stream));
+    BCK(cudaMemcpyAsync(host, b->stage, 4 * NL * sizeof(double), cudaMemcpyDeviceToHost,
+                        b->stream));
+  }
+  b->launches++;
+  BCK(cudaStreamSynchronize(b->stream));
+  return SU2B_OK;
+}
+
+extern "C" int su2b_batch_upload(su2b_batch *b, int chain, const double *U_host) {
+  return b ? chain_transfer(b, chain, const_cast<double *>(U_host), true) : SU2B_ERR_INVALID;
+}
+extern "C" int su2b_batch_download(su2b_batch *b, int chain, double *U_host) {
+  return b ? chain_transfer(b, chain, U_host, false) : SU2B_ERR_INVALID;
+}
+
+namespace {
+
+struct BOp {
+  int kind;  // 0 momentum step, 1 momentum + gauge step
+  double cm, cg;
+  bool kinetic;
+};
+
+std::vector<BOp> batch_schedule(int integ, int n, double tau, bool *ok) {
+  // the reference's leapfrog and omf2 (integrator.hh:26-50, 83-116), fused as in hmc.cu
+  std::vector<std::pair<int, double>> ops;
+  const double dtau = tau / (double)n;
+  *ok = true;
+  if (integ == SU2B_OMF2) {
+    const double lambda = 0.1938, om2l = (1. - 2. * lambda);
+    ops.push_back({0, lambda * dtau});
+    for (int i = 0; i < n - 1; i++) {
+      ops.push_back({1, 0.5 * dtau});
+      ops.push_back({0, om2l * dtau});
+      ops.push_back({1, 0.5 * dtau});
+      ops.push_back({0, 2 * lambda * dtau});
+    }
+    ops.push_back({1, 0.5 * dtau});
+    ops.push_back({0, om2l * dtau});
+    ops.push_back({1, 0.5 * dtau});
+    ops.push_back({0, lambda * dtau});
+  } else if (integ == SU2B_LEAPFROG) {
+    ops.push_back({0, dtau / 2.});
+    ops.push_back({1, dtau});
+    for (int i = 0; i < n - 1; i++) {
+      ops.push_back({0, dtau});
+      ops.push_back({1, dtau});
+    }
+    ops.push_back({0, dtau / 2.});
+  } else {
+    *ok = false;
+    return {};
+  }
+  std::vector<BOp> f;
+  for (size_t i = 0; i < ops.size(); i++) {
+    if (ops[i].first == 0 && i + 1 < ops.size() && ops[i + 1].first == 1) {
+      f.push_back({1, ops[i].second, ops[i + 1].second, false});
+      i++;
+    } else {
+      f.push_back({0, ops[i].second, 0.0, false});
+    }
+  }
+  if (!f.empty()) f.back().kinetic = true;
+  return f;
+}
+
+template <class T, int NT> int grid_for(const void *kernel, int ntiles) {
+  int per_sm = 1;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, NT, 0);
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  return std::max(1, std::min(ntiles, std::max(1, per_sm) * sms));
+}
+
+template <class T>
+int enqueue_batch(su2b_batch *b, const std::vector<BOp> &ops, int *rel_final) {
+  constexpr int NT = 128;
+  cudaStream_t s = b->stream;
+  Bufs<T> bufs{{(LinkT<T> *)b->buf[0], (LinkT<T> *)b->buf[1], (LinkT<T> *)b->buf[2]}};
+  T *P = (T *)b->P;
+  const int gF = grid_for<T, NT>((const void *)k_batch_force<T, NT>, b->ntiles);
+  const int gM = grid_for<T, NT>((const void *)k_batch_momenta<T, NT>, b->ntiles);
+  const int gP = grid_for<T, NT>((const void *)k_batch_plaq<T, NT>, b->ntiles);
+  long nl = 0;
+  k_batch_momenta<T, NT><<<gM, NT, 0, s>>>(b->ch, b->n, b->ntiles, P, b->traj, b->part);
+  k_batch_reduce<<<b->n, 256, 0, s>>>(b->ch, b->part, 1, b->red, 0);
+  k_batch_plaq<T, NT><<<gP, NT, 0, s>>>(b->ch, b->n, b->ntiles, bufs, b->cur, 0, b->part);
+  k_batch_reduce<<<b->n, 256, 0, s>>>(b->ch, b->part, 3, b->red, 1);
+  nl += 4;
+  int cur = 0;
+  auto next = [](int c) { return c == 1 ? 2 : 1; };
+  int fin = -1;
+  for (size_t i = 0; i < ops.size(); i++) {
+    const BOp &o = ops[i];
+    int mode = FM_HAS_IN | (o.kinetic ? FM_KINETIC : 0);
+    int out = -1;
+    if (o.kind == 1) {
+      mode |= FM_UPDATE;
+      out = next(cur);
+    } else if (i + 1 == ops.size()) {
+      mode |= FM_RESTORE;
+      out = fin = (cur == 0) ? 1 : next(cur);
+    }
+    k_batch_force<T, NT><<<gF, NT, 0, s>>>(b->ch, b->n, b->ntiles, bufs, P, b->cur, cur, out,
+                                           o.cm, o.cg, mode, b->part);
+    nl++;
+    if (o.kinetic) {
+      k_batch_reduce<<<b->n, 256, 0, s>>>(b->ch, b->part, 1, b->red, 4);
+      nl++;
+    }
+    if (o.kind == 1) cur = out;
+  }
+  if (fin < 0) return bfail(b, SU2B_ERR_UNSUPPORTED, "schedule must end with a momentum step");
+  k_batch_plaq<T, NT><<<gP, NT, 0, s>>>(b->ch, b->n, b->ntiles, bufs, b->cur, fin, b->part);
+  k_batch_reduce<<<b->n, 256, 0, s>>>(b->ch, b->part, 3, b->red, 5);
+  k_batch_accept<<<(b->n + 63) / 64, 64, 0, s>>>(b->ch, b->n, b->red, b->traj, fin, b->cur,
+                                                 b->res);
+  nl += 3;
+  BCK(cudaGetLastError());
+  BCK(cudaMemcpyAsync(b->h_res, b->res, sizeof(TrajDev) * b->n, cudaMemcpyDeviceToHost, s));
+  BCK(cudaMemcpyAsync(b->h_red, b->red, sizeof(double) * RS * b->n, cudaMemcpyDeviceToHost, s));
+  *rel_final = fin;
+  return (int)nl;
+}
+
+}  // namespace
+
+extern "C" int su2b_batch_hmc(su2b_batch *b, int integrator, int n_steps, double tau,
+                              uint32_t traj, su2b_traj_result *results) {
+  if (!b) return SU2B_ERR_INVALID;
+  b->err.clear();
+  BCK(cudaSetDevice(b->device));
+  if (!results || n_steps < 1) return bfail(b, SU2B_ERR_INVALID, "bad arguments");
+  bool ok = true;
+  const std::vector<BOp> ops = batch_schedule(integrator, n_steps, tau, &ok);
+  if (!ok)
+    return bfail(b, SU2B_ERR_UNSUPPORTED, "batched trajectories support leapfrog and omf2");
+  *b->h_traj = traj;
+  BCK(cudaMemcpyAsync(b->traj, b->h_traj, sizeof(uint32_t), cudaMemcpyHostToDevice, b->stream));
+  char key[128];
+  snprintf(key, sizeof key, "%d/%d/%.17g", integrator, n_steps, tau);
+  cudaGraphExec_t exec = nullptr;
+  long kernels = 0;
+  for (auto &g : b->graphs)
+    if (g.key == key) {
+      exec = g.exec;
+      kernels = g.kernels;
+    }
+  if (!exec) {
+    cudaGraph_t graph = nullptr;
+    BCK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+    int rel = 0;
+    const int nl =
+      b->link64 ? enqueue_batch<double>(b, ops, &rel) : enqueue_batch<float>(b, ops, &rel);
+    const cudaError_t ec = cudaStreamEndCapture(b->stream, &graph);
+    if (nl < 0) {
+      if (graph) cudaGraphDestroy(graph);
+      return nl;
+    }
+    BCK(ec);
+    const cudaError_t ei = cudaGraphInstantiate(&exec, graph, 0);
+    cudaGraphDestroy(graph);
+    BCK(ei);
+    kernels = nl;
+    b->graphs.push_back({key, exec, kernels});
+  }
+  BCK(cudaGraphLaunch(exec, b->stream));
+  BCK(cudaStreamSynchronize(b->stream));
+  b->launches += kernels;
+  for (int c = 0; c < b->n; c++) {
+    const TrajDev &t = b->h_res[c];
+    su2b_traj_result &r = results[c];
+    r.accepted = t.accepted;
+    r.dH = t.dH;
+    for (int k = 0; k < 3; k++) {
+      r.H_old[k] = t.H_old[k];
+      r.H_new[k] = t.H_new[k];
+    }
+    r.ddH = 0.0;
+    r.plaquette = t.accepted ? b->h_red[c * RS + 5] : b->h_red[c * RS + 1];
+    r.cg_iterations = 0;
+  }
+  return SU2B_OK;
+}

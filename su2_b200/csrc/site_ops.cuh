@@ -1,0 +1,158 @@
+// site_ops.cuh -- per-site bodies of the gauge kernels, shared by the single-lattice
+// kernels (gauge.cu) and the batched multi-chain kernels (batch.cu), so both paths perform
+// identical arithmetic.
+#pragma once
+#include "su2b_internal.h"
+
+namespace su2b {
+
+template <class T> using LinkT = typename LinkOf<T>::type;
+
+// Fused gauge force + momentum update for all ND links of a site
+// (flat-gaugemonomial.hh:105-131 + update_momenta.hh:10-33):
+//   K_mu = sum_{nu != mu} U_nu(x+mu) U_mu(x+nu)^+ U_nu(x)^+ + U_nu(x+mu-nu)^+ U_mu(x-nu)^+ U_nu(x-nu)
+//   d_mu = f * get_deriv(U_mu(x) K_mu) (+ extra),  P_mu = P_mu + scale * d_mu  (scale = -dtau)
+// One thread per site.  The two forward staples of a plane share the product
+// A = U_nu(x+mu) U_mu(x+nu)^+:  forward(mu; nu) = A U_nu(x)^+,  forward(nu; mu) = A^+ U_mu(x)^+.
+// Per site 4 + ND(ND-1) + ND^2 + ND(ND-1) = 44 (d = 4) distinct link loads.  The kernels
+// that call this give each block one band of sites of both parities (warps alternate), so
+// the blocks resident at any time cover one narrow band of the lattice and the links stream
+// from HBM about once per launch.  Returns the sum of the updated P^2 of the site.
+template <class T, int ND>
+__device__ __forceinline__ double force_site(const Geom &g, const LinkT<T> *__restrict__ U,
+                                             T *__restrict__ P, const T *__restrict__ extra, T f,
+                                             T scale_, int mode, int aniso, T wt, T ws,
+                                             LinkT<T> *__restrict__ Uout, T dt_upd, int p,
+                                             int cb) {
+  const int q = 1 - p;
+  double k2 = 0.;
+  const Site s = site_from_eo(g, p, cb);
+  const size_t V = (size_t)g.V, NL = V * ND;
+  const size_t self = (size_t)p * g.Vh + cb;
+  int lf[ND], lb[ND];
+#pragma unroll
+  for (int mu = 0; mu < ND; mu++) {
+    lf[mu] = s.lex + fwd(g, s, mu);
+    lb[mu] = bwd(g, s, mu);
+  }
+  Su2<T> ux[ND], K[ND];
+#pragma unroll
+  for (int mu = 0; mu < ND; mu++) {
+    ux[mu] = ld_link(U + mu * V + self);
+    K[mu] = zero_su2<T>();
+  }
+  // forward staples, one plane (mu < nu) at a time
+#pragma unroll
+  for (int mu = 0; mu < ND - 1; mu++)
+#pragma unroll
+    for (int nu = mu + 1; nu < ND; nu++) {
+      const Su2<T> a = ld_link(U + nu * V + eo_of(g, lf[mu], q));  // U_nu(x+mu)
+      const Su2<T> b = ld_link(U + mu * V + eo_of(g, lf[nu], q));  // U_mu(x+nu)
+      const Su2<T> A = mul(a, dag(b));
+      Su2<T> fmn = mul(A, dag(ux[nu]));
+      Su2<T> fnm = mul(dag(A), dag(ux[mu]));
+      if (aniso) {
+        const T w = (mu == 0) ? wt : ws;
+        fmn = scale(w, fmn);
+        fnm = scale(w, fnm);
+      }
+      K[mu] = add(K[mu], fmn);
+      K[nu] = add(K[nu], fnm);
+    }
+  // backward staples U_nu(x+mu-nu)^+ U_mu(x-nu)^+ U_nu(x-nu)
+#pragma unroll
+  for (int nu = 0; nu < ND; nu++) {
+    const int lmn = s.lex + lb[nu];
+    const Su2<T> c = ld_link(U + nu * V + eo_of(g, lmn, q));  // U_nu(x-nu)
+#pragma unroll
+    for (int mu = 0; mu < ND; mu++) {
+      if (mu == nu) continue;
+      const Su2<T> h = ld_link(U + mu * V + eo_of(g, lmn, q));          // U_mu(x-nu)
+      const Su2<T> e = ld_link(U + nu * V + eo_of(g, lf[mu] + lb[nu], p));  // U_nu(x+mu-nu)
+      Su2<T> st = mul(mul(dag(e), dag(h)), c);
+      if (aniso) st = scale((nu == 0 || mu == 0) ? wt : ws, st);
+      K[mu] = add(K[mu], st);
+    }
+  }
+#pragma unroll
+  for (int mu = 0; mu < ND; mu++) {
+    const Su2<T> &u = ux[mu];
+    const Su2<T> &k = K[mu];
+    const size_t l = mu * V + self;
+    // get_deriv(U K) = (2 Im b, 2 Re b, 2 Im a) (adjointfield.hh:53-56)
+    const T sbi = u.ar * k.bi + u.ai * k.br + (u.bi * k.ar - u.br * k.ai);
+    const T sbr = u.ar * k.br - u.ai * k.bi + (u.br * k.ar + u.bi * k.ai);
+    const T sai = u.ar * k.ai + u.ai * k.ar - (u.bi * k.br - u.br * k.bi);
+    T d0 = f * (T(2) * sbi), d1 = f * (T(2) * sbr), d2 = f * (T(2) * sai);
+    if (mode & FM_EXTRA) {
+      d0 += extra[l];
+      d1 += extra[NL + l];
+      d2 += extra[2 * NL + l];
+    }
+    T p0 = 0, p1 = 0, p2 = 0;
+    if (mode & FM_HAS_IN) {
+      p0 = P[l];
+      p1 = P[NL + l];
+      p2 = P[2 * NL + l];
+    }
+    p0 = p0 + scale_ * d0;
+    p1 = p1 + scale_ * d1;
+    p2 = p2 + scale_ * d2;
+    P[l] = p0;
+    P[NL + l] = p1;
+    P[2 * NL + l] = p2;
+    k2 += (double)p0 * p0 + (double)p1 * p1 + (double)p2 * p2;
+    // the following gauge step U <- exp(dt P) U (update_gauge.hh:8-16) into the other buffer
+    if (mode & FM_UPDATE)
+      st_link(Uout + l, mul(exp_alg(dt_upd * p0, dt_upd * p1, dt_upd * p2), u));
+    else if (mode & FM_RESTORE)
+      st_link(Uout + l, from64<T>(restore_su(to64(u))));
+  }
+  return k2;
+}
+
+// plaquettes of one site: sums over planes mu<nu of ReTr U_mu(x) U_nu(x+mu) U_mu(x+nu)^+
+// U_nu(x)^+ (flat-gauge_energy.hpp:31-94), FP64 products; {full, spatial (mu >= 1), xi-weighted}
+template <class T, int ND>
+__device__ __forceinline__ void plaq_site(const Geom &g, const LinkT<T> *__restrict__ U, int p,
+                                          int cb, double xi, double &full, double &spat,
+                                          double &wsum) {
+  const Site s = site_from_eo(g, p, cb);
+  Su2<double> u[ND];
+#pragma unroll
+  for (int mu = 0; mu < ND; mu++) u[mu] = to64(ld_link(U + (size_t)mu * g.V + p * g.Vh + cb));
+#pragma unroll
+  for (int mu = 0; mu < ND - 1; mu++) {
+    const int lpm = s.lex + fwd(g, s, mu);
+#pragma unroll
+    for (int nu = mu + 1; nu < ND; nu++) {
+      const int lpn = s.lex + fwd(g, s, nu);
+      const Su2<double> A = to64(ld_link(U + (size_t)nu * g.V + eo_of(g, lpm, 1 - p)));
+      const Su2<double> B = to64(ld_link(U + (size_t)mu * g.V + eo_of(g, lpn, 1 - p)));
+      const double tr = retr_mul(mul(u[mu], A), dag(mul(u[nu], B)));
+      full += tr;
+      if (mu >= 1) spat += tr;
+      wsum += (((mu == 0) ^ (nu == 0)) ? 1.0 / xi : xi) * tr;
+    }
+  }
+}
+
+// Box-Muller pair from one Philox draw: FP64 from two 53-bit uniforms; the FP32 (mixed
+// precision) path uses 24-bit uniforms of the same words and FP32 transcendentals.
+template <class T> __device__ __forceinline__ void gauss_pair(const uint32_t r[4], T &a, T &b);
+template <>
+__device__ __forceinline__ void gauss_pair<double>(const uint32_t r[4], double &a, double &b) {
+  box_muller(u01_53(r[0], r[1]), u01_53(r[2], r[3]), a, b);
+}
+template <>
+__device__ __forceinline__ void gauss_pair<float>(const uint32_t r[4], float &a, float &b) {
+  const float u1 = ((float)(r[0] >> 8) + 1.0f) * 0x1p-24f;  // (0, 1]
+  const float u2 = (float)(r[2] >> 8) * 0x1p-24f;           // [0, 1)
+  const float rad = sqrtf(-2.0f * logf(u1));
+  float sn, cs;
+  sincospif(2.0f * u2, &sn, &cs);
+  a = rad * cs;
+  b = rad * sn;
+}
+
+}  // namespace su2b
