@@ -21,9 +21,7 @@ import json
 import math
 import os
 import statistics
-import subprocess
 import sys
-import tempfile
 import threading
 import time
 
@@ -38,6 +36,7 @@ NSTEPS = 16
 TAU = 1.0
 METRIC = "SU(2) 32^4 HMC traj/s mixed vs FP64 at equal ΔH/plaq; kernel HBM GB/s vs peak"
 WORKLOAD = "SU(2) d=4 32^4, beta=2.4, omf2 tau=1 n=16 HMC trajectory"
+THERM_TRAJ = 20  # untimed HMC trajectories after the Metropolis thermalisation
 
 
 class quiet_stdout:
@@ -72,52 +71,71 @@ def haar_links(n_links, seed):
 
 
 class Clocks:
-    """Samples SM clocks and throttle reasons with nvidia-smi during the timed region."""
+    """Samples the SM clock and the clock-event (throttle) reasons during the timed region.
 
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    An NVML polling thread reads them every 2 ms, so that even a timed region of a few tens
+    of milliseconds carries a clock record; the sampler only reads, it changes no setting.
+    """
+
+    # NVML clocks-event reason bits
+    REASONS = {0x4: "sw_power_cap", 0x8: "hw_slowdown", 0x20: "sw_thermal_slowdown",
+               0x40: "hw_thermal_slowdown", 0x80: "hw_power_brake_slowdown"}
 
     def __init__(self, device):
         self.device = device
-        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
-        self.p = None
+        self.h = None
+        self.samples = []
+        self.reasons = 0
+        self.max_mhz = None
+        self.stop_flag = threading.Event()
+        self.t = None
+        try:
+            import pynvml as N
+            import torch
+            N.nvmlInit()
+            self.N = N
+            pr = torch.cuda.get_device_properties(device)
+            try:
+                bus = f"{pr.pci_domain_id:08x}:{pr.pci_bus_id:02x}:{pr.pci_device_id:02x}.0"
+                self.h = N.nvmlDeviceGetHandleByPciBusId(bus)
+            except Exception:
+                self.h = N.nvmlDeviceGetHandleByIndex(device)
+            self.max_mhz = float(N.nvmlDeviceGetMaxClockInfo(self.h, N.NVML_CLOCK_SM))
+        except Exception:
+            self.h = None
+
+    def _poll(self):
+        N = self.N
+        get_r = getattr(N, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+            N.nvmlDeviceGetCurrentClocksThrottleReasons
+        while True:
+            try:
+                self.samples.append(float(N.nvmlDeviceGetClockInfo(self.h, N.NVML_CLOCK_SM)))
+                self.reasons |= int(get_r(self.h))
+            except Exception:
+                pass
+            if self.stop_flag.wait(0.002):
+                break
 
     def start(self):
-        try:
-            self.p = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}",
-                                       "--format=csv,noheader,nounits", "-lms", "200",
-                                       "-i", str(self.device)], stdout=self.f,
-                                      stderr=subprocess.DEVNULL)
-        except OSError:
-            self.p = None
+        if self.h is None:
+            return
+        self.samples, self.reasons = [], 0
+        self.stop_flag.clear()
+        self.t = threading.Thread(target=self._poll, daemon=True)
+        self.t.start()
 
     def stop(self):
-        if self.p is None:
+        if self.t is None:
             return None
-        self.p.terminate()
-        try:
-            self.p.wait(timeout=5)
-        except subprocess.TimeoutExpired:
-            self.p.kill()
-        self.f.flush()
-        rows = [r.split(",") for r in open(self.f.name).read().splitlines() if r.strip()]
-        os.unlink(self.f.name)
-        sm, mx, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for r in rows:
-            try:
-                sm.append(float(r[1]))
-                mx = float(r[2])
-                for k, nm in enumerate(names):
-                    if "Active" in r[5 + k] and "Not" not in r[5 + k]:
-                        reasons.add(nm)
-            except (ValueError, IndexError):
-                continue
-        if not sm:
+        self.stop_flag.set()
+        self.t.join()
+        self.t = None
+        if not self.samples:
             return None
-        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
-                "samples": len(sm)}
+        return {"sm_mhz": statistics.median(self.samples), "sm_max_mhz": self.max_mhz,
+                "reasons": sorted(v for b, v in self.REASONS.items() if self.reasons & b),
+                "samples": len(self.samples), "source": "NVML, 2 ms polling"}
 
 
 def dist_setup():
@@ -200,7 +218,7 @@ def ours(args):
     mixed.upload(U0)
     for sweep in range(args.therm_sweeps):
         mixed.sweep(0.15, 8, seed, sweep)
-    for k in range(max(W, 3)):
+    for k in range(THERM_TRAJ + max(W, 3)):
         mixed.md_update("omf2", NSTEPS, TAU, seed=seed, traj=100000 + k)
     U_th = mixed.download()
     tune_m = mixed.autotune()  # launch shape of the force kernel, timed on this field
@@ -397,16 +415,54 @@ def reference(args):
     }), flush=True)
 
 
+def profile_run(args):
+    """--profile-run: the bare timed loop of the headline workload, for ncu.
+
+    A Haar-random 32^4 start (untimed work does not change what a kernel reads or writes),
+    the force kernel's launch shape fixed by --force-variant instead of the tuner, W warm-up
+    and K trajectories of one precision.  Prints one JSON line with the number of kernel
+    launches made before the K trajectories (the ncu ``-s`` to skip to them) and per
+    trajectory.
+    """
+    import torch
+
+    import su2_b200
+    V = L ** 4
+    c = su2_b200.gaugeconfig(L, L, L, L, 4, BETA, precision=args.precision)
+    c.upload(haar_links(V * 4, 20240))
+    c.force_variant = args.force_variant
+    for k in range(args.warmup):
+        c.md_update("omf2", NSTEPS, TAU, seed=20240, traj=k)
+    c.synchronize()
+    n0 = c.kernel_launches()
+    for k in range(args.steps):
+        c.md_update("omf2", NSTEPS, TAU, seed=20240, traj=args.warmup + k)
+    c.synchronize()
+    n1 = c.kernel_launches()
+    print(json.dumps({"profile_run": WORKLOAD, "precision": args.precision,
+                      "force_variant": su2_b200._abi.FORCE_SHAPES[args.force_variant],
+                      "setup_launches": n0, "launches_per_traj": (n1 - n0) / max(1, args.steps),
+                      "steps": args.steps, "warmup": args.warmup}), flush=True)
+    c.close()
+    torch.cuda.synchronize()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--therm-sweeps", type=int, default=60)
+    ap.add_argument("--therm-sweeps", type=int, default=300)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile-run", action="store_true",
+                    help="only the timed loop of one precision, for ncu (no bench line)")
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
+    ap.add_argument("--force-variant", type=int, default=3)
     args = ap.parse_args()
-    if args.impl == "reference":
+    if args.profile_run:
+        profile_run(args)
+    elif args.impl == "reference":
         reference(args)
     else:
         ours(args)

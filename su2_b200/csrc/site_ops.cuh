@@ -18,12 +18,13 @@ template <class T> using LinkT = typename LinkOf<T>::type;
 // that call this give each block one band of sites of both parities (warps alternate), so
 // the blocks resident at any time cover one narrow band of the lattice and the links stream
 // from HBM about once per launch.  Returns the sum of the updated P^2 of the site.
-template <class T, int ND>
-__device__ __forceinline__ double force_site(const Geom &g, const LinkT<T> *__restrict__ U,
-                                             T *__restrict__ P, const T *__restrict__ extra, T f,
-                                             T scale_, int mode, int aniso, T wt, T ws,
-                                             LinkT<T> *__restrict__ Uout, T dt_upd, int p,
-                                             int cb) {
+template <class T, int ND, bool ANISO>
+__device__ __forceinline__ double force_site_impl(const Geom &g, const LinkT<T> *__restrict__ U,
+                                                  T *__restrict__ P,
+                                                  const T *__restrict__ extra, T f, T scale_,
+                                                  int mode, T wt, T ws,
+                                                  LinkT<T> *__restrict__ Uout, T dt_upd, int p,
+                                                  int cb) {
   const int q = 1 - p;
   double k2 = 0.;
   const Site s = site_from_eo(g, p, cb);
@@ -41,23 +42,18 @@ __device__ __forceinline__ double force_site(const Geom &g, const LinkT<T> *__re
     ux[mu] = ld_link(U + mu * V + self);
     K[mu] = zero_su2<T>();
   }
-  // forward staples, one plane (mu < nu) at a time
+  // forward staples, one plane (mu < nu) at a time; the plane weight of the anisotropic
+  // action multiplies the shared product A
 #pragma unroll
   for (int mu = 0; mu < ND - 1; mu++)
 #pragma unroll
     for (int nu = mu + 1; nu < ND; nu++) {
       const Su2<T> a = ld_link(U + nu * V + eo_of(g, lf[mu], q));  // U_nu(x+mu)
       const Su2<T> b = ld_link(U + mu * V + eo_of(g, lf[nu], q));  // U_mu(x+nu)
-      const Su2<T> A = mul(a, dag(b));
-      Su2<T> fmn = mul(A, dag(ux[nu]));
-      Su2<T> fnm = mul(dag(A), dag(ux[mu]));
-      if (aniso) {
-        const T w = (mu == 0) ? wt : ws;
-        fmn = scale(w, fmn);
-        fnm = scale(w, fnm);
-      }
-      K[mu] = add(K[mu], fmn);
-      K[nu] = add(K[nu], fnm);
+      Su2<T> A = mul(a, dag(b));
+      if (ANISO) A = scale(mu == 0 ? wt : ws, A);
+      K[mu] = mul_acc(K[mu], A, dag(ux[nu]));
+      K[nu] = mul_acc(K[nu], dag(A), dag(ux[mu]));
     }
   // backward staples U_nu(x+mu-nu)^+ U_mu(x-nu)^+ U_nu(x-nu)
 #pragma unroll
@@ -69,9 +65,9 @@ __device__ __forceinline__ double force_site(const Geom &g, const LinkT<T> *__re
       if (mu == nu) continue;
       const Su2<T> h = ld_link(U + mu * V + eo_of(g, lmn, q));          // U_mu(x-nu)
       const Su2<T> e = ld_link(U + nu * V + eo_of(g, lf[mu] + lb[nu], p));  // U_nu(x+mu-nu)
-      Su2<T> st = mul(mul(dag(e), dag(h)), c);
-      if (aniso) st = scale((nu == 0 || mu == 0) ? wt : ws, st);
-      K[mu] = add(K[mu], st);
+      Su2<T> eh = mul(dag(e), dag(h));
+      if (ANISO) eh = scale((nu == 0 || mu == 0) ? wt : ws, eh);
+      K[mu] = mul_acc(K[mu], eh, c);
     }
   }
 #pragma unroll
@@ -80,10 +76,11 @@ __device__ __forceinline__ double force_site(const Geom &g, const LinkT<T> *__re
     const Su2<T> &k = K[mu];
     const size_t l = mu * V + self;
     // get_deriv(U K) = (2 Im b, 2 Re b, 2 Im a) (adjointfield.hh:53-56)
-    const T sbi = u.ar * k.bi + u.ai * k.br + (u.bi * k.ar - u.br * k.ai);
-    const T sbr = u.ar * k.br - u.ai * k.bi + (u.br * k.ar + u.bi * k.ai);
-    const T sai = u.ar * k.ai + u.ai * k.ar - (u.bi * k.br - u.br * k.bi);
-    T d0 = f * (T(2) * sbi), d1 = f * (T(2) * sbr), d2 = f * (T(2) * sai);
+    const T sbi = fm(u.ar, k.bi, fm(u.ai, k.br, fm(u.bi, k.ar, -u.br * k.ai)));
+    const T sbr = fm(u.ar, k.br, fm(-u.ai, k.bi, fm(u.br, k.ar, u.bi * k.ai)));
+    const T sai = fm(u.ar, k.ai, fm(u.ai, k.ar, fm(-u.bi, k.br, u.br * k.bi)));
+    const T f2 = T(2) * f;
+    T d0 = f2 * sbi, d1 = f2 * sbr, d2 = f2 * sai;
     if (mode & FM_EXTRA) {
       d0 += extra[l];
       d1 += extra[NL + l];
@@ -109,6 +106,19 @@ __device__ __forceinline__ double force_site(const Geom &g, const LinkT<T> *__re
       st_link(Uout + l, from64<T>(restore_su(to64(u))));
   }
   return k2;
+}
+
+template <class T, int ND>
+__device__ __forceinline__ double force_site(const Geom &g, const LinkT<T> *__restrict__ U,
+                                             T *__restrict__ P, const T *__restrict__ extra, T f,
+                                             T scale_, int mode, int aniso, T wt, T ws,
+                                             LinkT<T> *__restrict__ Uout, T dt_upd, int p,
+                                             int cb) {
+  if (aniso)
+    return force_site_impl<T, ND, true>(g, U, P, extra, f, scale_, mode, wt, ws, Uout, dt_upd,
+                                        p, cb);
+  return force_site_impl<T, ND, false>(g, U, P, extra, f, scale_, mode, wt, ws, Uout, dt_upd, p,
+                                       cb);
 }
 
 // plaquettes of one site: sums over planes mu<nu of ReTr U_mu(x) U_nu(x+mu) U_mu(x+nu)^+

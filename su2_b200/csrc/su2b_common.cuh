@@ -163,12 +163,27 @@ template <class T> __device__ __forceinline__ Su2<T> from64(const Su2<double> &u
 // ------------------------------------------------------------------------------------
 // SU(2) algebra in the (a, b) form (su2.hh:87-113).  u*v:
 //   a = u.a v.a - u.b conj(v.b),  b = u.a v.b + u.b conj(v.a)
+// written as chains of fused multiply-adds (one multiply and three FMAs per component; the
+// sign flips of dag() fold into the FMA operands).
+__device__ __forceinline__ float fm(float a, float b, float c) { return fmaf(a, b, c); }
+__device__ __forceinline__ double fm(double a, double b, double c) { return fma(a, b, c); }
+
 template <class T> __device__ __forceinline__ Su2<T> mul(const Su2<T> &u, const Su2<T> &v) {
   Su2<T> r;
-  r.ar = u.ar * v.ar - u.ai * v.ai - (u.br * v.br + u.bi * v.bi);
-  r.ai = u.ar * v.ai + u.ai * v.ar - (u.bi * v.br - u.br * v.bi);
-  r.br = u.ar * v.br - u.ai * v.bi + (u.br * v.ar + u.bi * v.ai);
-  r.bi = u.ar * v.bi + u.ai * v.br + (u.bi * v.ar - u.br * v.ai);
+  r.ar = fm(u.ar, v.ar, fm(-u.ai, v.ai, fm(-u.br, v.br, -u.bi * v.bi)));
+  r.ai = fm(u.ar, v.ai, fm(u.ai, v.ar, fm(-u.bi, v.br, u.br * v.bi)));
+  r.br = fm(u.ar, v.br, fm(-u.ai, v.bi, fm(u.br, v.ar, u.bi * v.ai)));
+  r.bi = fm(u.ar, v.bi, fm(u.ai, v.br, fm(u.bi, v.ar, -u.br * v.ai)));
+  return r;
+}
+// k + u*v, sixteen FMAs
+template <class T>
+__device__ __forceinline__ Su2<T> mul_acc(const Su2<T> &k, const Su2<T> &u, const Su2<T> &v) {
+  Su2<T> r;
+  r.ar = fm(u.ar, v.ar, fm(-u.ai, v.ai, fm(-u.br, v.br, fm(-u.bi, v.bi, k.ar))));
+  r.ai = fm(u.ar, v.ai, fm(u.ai, v.ar, fm(-u.bi, v.br, fm(u.br, v.bi, k.ai))));
+  r.br = fm(u.ar, v.br, fm(-u.ai, v.bi, fm(u.br, v.ar, fm(u.bi, v.ai, k.br))));
+  r.bi = fm(u.ar, v.bi, fm(u.ai, v.br, fm(u.bi, v.ar, fm(-u.br, v.ai, k.bi))));
   return r;
 }
 template <class T> __device__ __forceinline__ Su2<T> dag(const Su2<T> &u) {
@@ -195,20 +210,63 @@ __device__ __forceinline__ Su2<double> restore_su(const Su2<double> &u) {
 }
 
 // exp of an algebra element (exp_gauge.cc:8-18): alpha = |x|, n = x/alpha,
-// exp = (cos alpha + i sin(alpha) n2, sin(alpha) (n1 + i n0)).  At alpha = 0 the reference
-// divides 0/0; here the limit (the identity) is returned.
+// exp = (cos alpha + i sin(alpha) n2, sin(alpha) (n1 + i n0)).  Both cos(alpha) and
+// sin(alpha)/alpha are even functions of alpha, so for alpha^2 <= 1/4 (every molecular-dynamics
+// and flow step in practice) they are summed directly as their Taylor series in alpha^2,
+// Horner form, with no square root, division or argument reduction:
+//   cos a = sum_k (-1)^k a^2k/(2k)!,   sin(a)/a = sum_k (-1)^k a^2k/(2k+1)!.
+// FP64 keeps k <= 7 (first omitted terms below 1e-18), FP32 k <= 4 (below 3e-10).  Larger
+// arguments take the square root and sincos.  At alpha = 0 the reference divides 0/0; here
+// the limit (the identity) is returned.
+namespace detail {
+// n! is exact in double for n <= 18, so (+-1)/n! below is the correctly rounded coefficient
+__host__ __device__ constexpr double fact(int n) { return n <= 1 ? 1.0 : n * fact(n - 1); }
+template <int k> struct Coef {
+  static constexpr double c = ((k & 1) ? -1.0 : 1.0) / fact(2 * k);      // cos
+  static constexpr double s = ((k & 1) ? -1.0 : 1.0) / fact(2 * k + 1);  // sin(x)/x
+};
+template <class T, int k> struct Horner {
+  static __device__ __forceinline__ void run(T t2, T &c, T &s) {
+    c = fm(c, t2, T(Coef<k>::c));
+    s = fm(s, t2, T(Coef<k>::s));
+    Horner<T, k - 1>::run(t2, c, s);
+  }
+};
+template <class T> struct Horner<T, -1> {
+  static __device__ __forceinline__ void run(T, T &, T &) {}
+};
+template <class T, int K>
+__device__ __forceinline__ void cos_sinc_series(T t2, T &co, T &sc) {
+  co = T(Coef<K>::c);
+  sc = T(Coef<K>::s);
+  Horner<T, K - 1>::run(t2, co, sc);
+}
+}  // namespace detail
+
 __device__ __forceinline__ Su2<double> exp_alg(double a, double b, double c) {
-  const double alpha = sqrt(a * a + b * b + c * c);
-  double s, co;
-  sincos(alpha, &s, &co);
-  const double f = alpha > 0.0 ? s / alpha : 1.0;
+  const double t2 = fma(a, a, fma(b, b, c * c));
+  double co, f;
+  if (t2 <= 0.25) {
+    detail::cos_sinc_series<double, 7>(t2, co, f);
+  } else {
+    const double alpha = sqrt(t2);
+    double s;
+    sincos(alpha, &s, &co);
+    f = s / alpha;
+  }
   return Su2<double>{co, f * c, f * b, f * a};
 }
 __device__ __forceinline__ Su2<float> exp_alg(float a, float b, float c) {
-  const float alpha = sqrtf(a * a + b * b + c * c);
-  float s, co;
-  sincosf(alpha, &s, &co);
-  const float f = alpha > 0.0f ? s / alpha : 1.0f;
+  const float t2 = fmaf(a, a, fmaf(b, b, c * c));
+  float co, f;
+  if (t2 <= 0.25f) {
+    detail::cos_sinc_series<float, 4>(t2, co, f);
+  } else {
+    const float alpha = sqrtf(t2);
+    float s;
+    sincosf(alpha, &s, &co);
+    f = s / alpha;
+  }
   return Su2<float>{co, f * c, f * b, f * a};
 }
 

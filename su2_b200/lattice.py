@@ -108,6 +108,10 @@ class gaugeconfig:
         self._c(self.lib.su2b_ctx_stream(self.ctx, C.byref(s)))
         return s.value or 0
 
+    def synchronize(self):
+        """Waits for all work queued on the context's stream."""
+        self._c(self.lib.su2b_synchronize(self.ctx))
+
     def profile(self, enable=True):
         """Per-kernel-class device timers (CUDA events on the context's stream)."""
         self._c(self.lib.su2b_profile(self.ctx, int(enable)))
