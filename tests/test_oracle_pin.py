@@ -209,18 +209,43 @@ def test_metropolis_statistics_match_reference(orc, ref):
 
 # ---------------------------------------------------------------- golden fixtures
 def test_golden_fixtures(orc):
+    """The restatement against vectors the reference itself produced (make_golden.py)."""
     path = os.path.join(GOLDEN, "golden.npz")
     if not os.path.exists(path):
         pytest.skip("golden fixtures not generated")
     g = np.load(path)
     U = g["su2_U"]
-    dims, nd = tuple(g["su2_dims"]), 4
+    dims, nd = tuple(int(v) for v in g["su2_dims"]), 4
     assert np.array_equal(orc.hotstart(0, dims, nd, 13526463, 1.0, 654321), U)
     assert orc.gauge_energy(0, dims, nd, U) == pytest.approx(float(g["su2_plaq"]), rel=1e-13)
+    assert orc.gauge_energy(0, dims, nd, U, spatial_only=True) == \
+        pytest.approx(float(g["su2_plaq_ss"]), rel=1e-13)
     assert np.array_equal(orc.gauge_derivative(0, dims, nd, 2.4, U), g["su2_force"])
     assert np.array_equal(orc.runge_kutta(0, dims, nd, 2.4, 0.01, U), g["su2_flow"])
     E, Q = orc.energy_density(0, dims, nd, U)
     assert (E, Q) == (float(g["su2_E"]), float(g["su2_Q"]))
+    rows = orc.gradient_flow_rows(0, dims, nd, 2.4, U, 0.05, 0.01)
+    want = g["su2_flow_rows"]  # written as text by the reference: compare at print precision
+    assert rows.shape == want.shape
+    np.testing.assert_allclose(rows, want, rtol=1e-5, atol=1e-7)
+    for name, integ, n in (("leapfrog", 0, 10), ("omf2", 6, 4)):
+        dH, Ut, _, _ = orc.md_injected(0, dims, nd, 2.4, integ, n, 1.0, U, g["su2_P"])
+        assert dH == pytest.approx(float(g[f"su2_md_{name}_dH"]), abs=1e-10)
+        assert np.array_equal(Ut, g[f"su2_md_{name}_U"])
+    d3 = tuple(int(v) for v in g["su2d3_dims"])
+    U3 = g["su2d3_U"]
+    assert np.array_equal(orc.hotstart(0, d3, 3, 4711, 1.0, 99), U3)
+    assert orc.gauge_energy(0, d3, 3, U3) == pytest.approx(float(g["su2d3_plaq"]), rel=1e-13)
+    assert np.array_equal(orc.gauge_derivative(0, d3, 3, 2.0, U3), g["su2d3_force"])
     Uu = g["u1_U"]
-    du = tuple(g["u1_dims"])
+    du = tuple(int(v) for v in g["u1_dims"])
+    assert np.array_equal(orc.hotstart(1, du, 2, 13526463, 1.0, 654321), Uu)
+    assert orc.gauge_energy(1, du, 2, Uu) == pytest.approx(float(g["u1_plaq"]), rel=1e-13)
+    assert np.array_equal(orc.gauge_derivative(1, du, 2, 4.0, Uu), g["u1_force"])
     assert np.array_equal(orc.staggered_apply(du, 2, Uu, 0.05, 2, g["u1_psi"]), g["u1_DDdag_psi"])
+    x, it = orc.cg_ddag(du, 2, Uu, 0.05, g["u1_psi"], g["u1_x0"], 1e-10)
+    assert np.array_equal(x, g["u1_cg_x"])
+    assert int(g["u1_cg_iter"]) == it + orc._last_solve_calls() - 1
+    x, it = orc.bicgstab_d(du, 2, Uu, 0.05, g["u1_psi"], g["u1_x0"], 1e-10)
+    assert np.array_equal(x, g["u1_bicgstab_x"])
+    assert int(g["u1_bicgstab_iter"]) == it + orc._last_solve_calls() - 1
