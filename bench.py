@@ -161,21 +161,8 @@ def barrier(dist):
 
 
 def allmax(dist, x):
-    if dist is None:
-        return x
-    import torch
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
-
-
-def allsum(dist, x):
-    if dist is None:
-        return x
-    import torch
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.SUM)
-    return float(t.item())
+    from su2_b200 import replicas
+    return replicas.max_over_ranks(x) if dist is not None else x
 
 
 # --------------------------------------------------------------------------------------
@@ -210,7 +197,8 @@ def ours(args):
     K, W = args.steps, args.warmup
     V = L ** 4
     NL = V * 4
-    seed = 20240 + 1000 * rank
+    from su2_b200 import replicas
+    seed = replicas.replica_seed(20240, rank)
 
     # ---- thermalised start (untimed): Haar start, Metropolis sweeps, HMC warm-up ----
     U0 = haar_links(NL, seed)
@@ -447,6 +435,343 @@ def profile_run(args):
     torch.cuda.synchronize()
 
 
+# --------------------------------------------------------------------------------------
+# The other workloads of the su2 hot path (``--config N``).  Each prints one JSON line of
+# its own; the default run (config 2) is the headline above.
+
+def _line(metric, value, unit, args, ws, ms_per_step, config, **extra):
+    d = {"metric": metric, "value": value, "unit": unit, "n_gpus": ws, "steps": args.steps,
+         "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
+         "scaling": "weak", "vs_baseline": None, "data": "synthetic (seeded)",
+         "config": config}
+    d.update(extra)
+    print(json.dumps(d), flush=True)
+
+
+def _events(stream):
+    import torch
+    s = torch.cuda.ExternalStream(stream)
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    return s, a, b
+
+
+def config1(args):
+    """SU(2) d=4 8^4, beta 2.3, leapfrog tau 1 n 10, FP64, plaquette every trajectory: the
+    reference's own CPU run and the plain method.  K trajectories (default 200) after W."""
+    import torch
+
+    import su2_b200
+    ws, rank, local, dist = dist_setup()
+    torch.cuda.set_device(local)
+    from su2_b200 import replicas
+    seed = replicas.replica_seed(13526463, rank)
+    K, W = args.steps, args.warmup
+    c = su2_b200.gaugeconfig(8, 8, 8, 8, 4, 2.3, precision="fp64", device=local)
+    c.upload(haar_links(8 ** 4 * 4, seed))
+    for k in range(W):
+        c.md_update("leapfrog", 10, 1.0, seed=seed, traj=k)
+    s, e0, e1 = _events(c.stream())
+    barrier(dist)
+    n0 = c.kernel_launches()
+    e0.record(s)
+    res = [c.md_update("leapfrog", 10, 1.0, seed=seed, traj=W + k) for k in range(K)]
+    e1.record(s)
+    e1.synchronize()
+    t = allmax(dist, e0.elapsed_time(e1) / 1e3)
+    plaq = [r.plaquette / (8 ** 4 * 6 * 2) for r in res]
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        from oracle import oracle as O
+        if O.available("ref"):
+            r = O.Oracle("ref")
+            U = haar_links(8 ** 4 * 4, seed)
+            n = 200
+            with quiet_stdout():
+                t0 = time.perf_counter()
+                r.hmc_run(0, (8, 8, 8, 8), 4, 2.3, 0, 10, 1.0, 13526463, 0, n, U)
+                dt = time.perf_counter() - t0
+            cpu = {"value": n / dt, "unit": "traj/s", "cores": r._omp_threads(),
+                   "kind": "reference", "sample": f"{n} leapfrog trajectories of the 8^4 "
+                                                  "workload, md_update + accept/reject"}
+    if rank == 0:
+        _line("SU(2) 8^4 leapfrog HMC traj/s (FP64)", ws * K / t, "traj/s", args, ws,
+              1e3 * t / K, {"workload": "SU(2) d=4 8^4 beta=2.3 leapfrog tau=1 n=10, FP64, "
+                                        "Haar start", "replicas": ws},
+              dtype="fp64", acceptance=sum(r.accepted for r in res) / K,
+              plaquette_mean=float(np.mean(plaq)), plaquette_last=plaq[-1],
+              gpu_launches=c.kernel_launches() - n0, cpu_baseline=cpu)
+    c.close()
+
+
+def config3(args):
+    """U(1) d=2 256^2, beta 4.0, staggered m 0.05: CG on D D^+ to relative 1e-10 in FP64 and
+    FP32-inner / FP64-reliable-update, BiCGStab on D with the same right-hand side, and the
+    HMC trajectory with the det(D D^+) monomial (omf2 tau 1, n 10)."""
+    import torch
+
+    import su2_b200
+    ws, rank, local, dist = dist_setup()
+    torch.cuda.set_device(local)
+    L, m, beta = 256, 0.05, 4.0
+    V = L * L
+    rng = np.random.default_rng(4242 + rank)
+    U = rng.uniform(-np.pi, np.pi, size=V * 2)
+    b = rng.normal(size=2 * V)
+    out = {}
+    solves = {}
+    for name, prec, solver in (("cg_fp64", "fp64", "CG"), ("cg_mixed", "mixed", "CG_mixed"),
+                               ("bicgstab_fp64", "fp64", "BiCGStab")):
+        c = su2_b200.gaugeconfig(L, 1, 1, L, 2, beta, group="u1", precision=prec, device=local)
+        c.upload(U)
+        for _ in range(max(1, args.warmup)):
+            c.solve(b, m, tol=1e-10, solver=solver, tol_mode="rel")
+        s, e0, e1 = _events(c.stream())
+        barrier(dist)
+        e0.record(s)
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            r = c.solve(b, m, tol=1e-10, solver=solver, tol_mode="rel")
+        e1.record(s)
+        e1.synchronize()
+        wall = time.perf_counter() - t0
+        t = allmax(dist, e0.elapsed_time(e1) / 1e3)
+        solves[name] = {"ms_per_solve": 1e3 * t / args.steps, "iterations": r.iterations,
+                        "restarts": r.restarts,
+                        "true_residual_rel": r.true_residual / float(np.linalg.norm(b)),
+                        "wall_ms_per_solve": 1e3 * wall / args.steps}
+        if name == "cg_fp64":
+            x64 = r.x
+        elif name == "cg_mixed":
+            solves[name]["x_rel_diff_vs_cg_fp64"] = float(np.linalg.norm(r.x - x64) /
+                                                          np.linalg.norm(x64))
+        if name == "cg_fp64":
+            # pseudofermion HMC trajectory (det D D^+ monomial), FP64
+            c.md_update("omf2", 10, 1.0, seed=7, traj=0, fermion_mass=m, cg_tol=1e-10)
+            acc = []
+            e0.record(s)
+            nt = max(2, args.steps // 2)
+            for k in range(nt):
+                acc.append(c.md_update("omf2", 10, 1.0, seed=7, traj=1 + k, fermion_mass=m,
+                                       cg_tol=1e-10))
+            e1.record(s)
+            e1.synchronize()
+            out["hmc"] = {"traj_per_s": nt / (e0.elapsed_time(e1) / 1e3),
+                          "acceptance": sum(a.accepted for a in acc) / nt,
+                          "cg_iterations_per_traj": float(np.mean([a.cg_iterations
+                                                                   for a in acc]))}
+        c.close()
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        from oracle import oracle as O
+        if O.available("ref"):
+            r = O.Oracle("ref")
+            tol_abs = 1e-10 * float(np.linalg.norm(b))  # CG.hpp stops on |r| < tol
+            t0 = time.perf_counter()
+            xr, it = r.cg_ddag((L, 1, 1, L), 2, U, m, b, np.zeros_like(b), tol_abs)
+            dt = time.perf_counter() - t0
+            cpu = {"value": 1.0 / dt, "unit": "solves/s", "cores": r._omp_threads(),
+                   "kind": "reference", "sample": f"1 LinearCG solve on D D^+ to |r| < 1e-10 |b| "
+                                                  f"({it} iterations incl. restarts)",
+                   "x_rel_diff_vs_cg_fp64": float(np.linalg.norm(xr - x64) /
+                                                  np.linalg.norm(xr))}
+    if rank == 0:
+        v = ws * 1e3 / solves["cg_fp64"]["ms_per_solve"]
+        _line("U(1) 256^2 staggered CG on DD^+ to rel 1e-10: solves/s", v, "solves/s", args,
+              ws, solves["cg_fp64"]["ms_per_solve"],
+              {"workload": "U(1) d=2 256x256 beta=4.0 staggered m=0.05, hot start",
+               "replicas": ws}, dtype="fp64 (and fp32-inner mixed CG)", solvers=solves,
+              fermion_hmc=out.get("hmc"), cpu_baseline=cpu)
+
+
+def ensemble_chains(n=64, seed=20250):
+    """Seeded ensemble: SU(2) d=4 with L in {8..24} and d=3 with L in {16..48} (even extents,
+    as the even/odd layout and the checkerboard require), beta uniform in [2.0, 2.6]."""
+    rng = np.random.default_rng(seed)
+    chains = []
+    for i in range(n):
+        if i % 2 == 0:
+            L = int(rng.integers(4, 13)) * 2
+            chains.append(dict(dims=(L, L, L, L), ndims=4, beta=float(rng.uniform(2.0, 2.6)),
+                               seed=7000 + i))
+        else:
+            L = int(rng.integers(8, 25)) * 2
+            chains.append(dict(dims=(L, L, 1, L), ndims=3, beta=float(rng.uniform(2.0, 2.6)),
+                               seed=7000 + i))
+    return chains
+
+
+def config4(args):
+    """64 independent SU(2) chains of uneven sizes, leapfrog tau 1 n 10, FP32 links with FP64
+    sums: one batched graph per trajectory (persistent kernels over all chains' tiles) against
+    the same chains run one by one (one context and graph per chain).  Site-updates = sites x
+    trajectories.  With N ranks the chains are partitioned by replicas.partition_chains."""
+    import torch
+
+    import su2_b200
+    from su2_b200 import replicas
+    from su2_b200.batch import chain_batch
+    ws, rank, local, dist = dist_setup()
+    torch.cuda.set_device(local)
+    chains = ensemble_chains()
+    mine = [chains[i] for i in replicas.partition_chains(chains, ws, rank)]
+    sites = sum(replicas.chain_cost(c) for c in mine)
+    starts = [haar_links(replicas.chain_cost(c) * c["ndims"], c["seed"]) for c in mine]
+    K, W = args.steps, args.warmup
+    with chain_batch(mine, precision="mixed", device=local) as b:
+        for i, U in enumerate(starts):
+            b.upload(i, U)
+        for k in range(W):
+            b.md_update("leapfrog", 10, 1.0, traj=k)
+        s, e0, e1 = _events(b.stream())
+        barrier(dist)
+        n0 = b.kernel_launches()
+        e0.record(s)
+        res = [b.md_update("leapfrog", 10, 1.0, traj=W + k) for k in range(K)]
+        e1.record(s)
+        e1.synchronize()
+        t_b = allmax(dist, e0.elapsed_time(e1) / 1e3)
+        launches = b.kernel_launches() - n0
+    total_sites = replicas.sum_over_ranks(sites) if dist is not None else sites
+    # one by one: every chain its own context and trajectory graph, run back to back
+    ctxs = []
+    for c, U in zip(mine, starts):
+        Lx, Ly, Lz, Lt = c["dims"]
+        g = su2_b200.gaugeconfig(Lx, Ly, Lz, Lt, c["ndims"], c["beta"], precision="mixed",
+                                 device=local)
+        g.upload(U)
+        for k in range(W):
+            g.md_update("leapfrog", 10, 1.0, seed=c["seed"], traj=k)
+        ctxs.append(g)
+    torch.cuda.synchronize()
+    barrier(dist)
+    t0 = time.perf_counter()
+    for k in range(K):
+        for c, g in zip(mine, ctxs):
+            g.md_update("leapfrog", 10, 1.0, seed=c["seed"], traj=W + k)
+    torch.cuda.synchronize()
+    t_1 = allmax(dist, time.perf_counter() - t0)
+    for g in ctxs:
+        g.close()
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        from oracle import oracle as O
+        if O.available("ref"):
+            r = O.Oracle("ref")
+            c = max(chains, key=replicas.chain_cost)
+            Lx, Ly, Lz, Lt = c["dims"]
+            U = haar_links(replicas.chain_cost(c) * c["ndims"], 1)
+            with quiet_stdout():
+                t0 = time.perf_counter()
+                r.hmc_run(0, c["dims"], c["ndims"], c["beta"], 0, 10, 1.0, 1, 0, 1, U)
+                dt = time.perf_counter() - t0
+            cpu = {"value": replicas.chain_cost(c) / dt, "unit": "site-updates/s",
+                   "cores": r._omp_threads(), "kind": "reference",
+                   "sample": f"1 leapfrog trajectory of the largest chain {c['dims']} "
+                             f"d={c['ndims']}"}
+    if rank == 0:
+        _line("64-chain SU(2) ensemble leapfrog HMC site-updates/s (batched)",
+              total_sites * K / t_b, "site-updates/s", args, ws, 1e3 * t_b / K,
+              {"workload": "64 SU(2) chains, d=4 L in 8..24 and d=3 L in 16..48 (even), beta "
+                           "U[2.0,2.6], leapfrog tau=1 n=10, FP32 links + FP64 sums",
+               "chains": len(chains), "sites_total": int(total_sites),
+               "parallelism": f"chains partitioned over {ws} rank(s)"},
+              dtype="fp32 links + fp64 sums", one_by_one_site_updates_per_s=total_sites * K / t_1,
+              batched_over_one_by_one=t_1 / t_b,
+              acceptance=float(np.mean([r.accepted for rr in res for r in rr])),
+              gpu_launches=int(launches), cpu_baseline=cpu)
+
+
+def config5(args):
+    """SU(2) d=4 24^4 beta 2.4 from a GPU-thermalised field: the Wilson action's backward
+    against central finite differences (eps 1e-6, FP64) on 1000 random links and against the
+    gauge force, and the gradient of t^2 E(t = 2) (eps 0.01, 200 RK3 steps, checkpoints every
+    14 steps) in FP64 and FP32 with the FP32 error against FP64."""
+    import torch
+
+    import su2_b200
+    ws, rank, local, dist = dist_setup()
+    torch.cuda.set_device(local)
+    L = 24
+    NL = L ** 4 * 4
+    c = su2_b200.gaugeconfig(L, L, L, L, 4, 2.4, precision="fp64", device=local)
+    c.upload(haar_links(NL, 99 + rank))
+    for sweep in range(100):
+        c.sweep(0.15, 8, 99, sweep)
+    for k in range(10):
+        c.md_update("omf2", 16, 1.0, seed=99, traj=k)
+    U = c.download()
+    S, dS = c.action_backward()
+    F = c.derivative()
+    force_rel = float(np.linalg.norm(dS - F) / np.linalg.norm(F))
+    rng = np.random.default_rng(5)
+    links = rng.choice(NL, size=1000, replace=False)
+    comps = rng.integers(0, 3, size=1000)
+    eps = 1e-6
+    fd_err = []
+    V_ = U.copy()
+    t0 = time.perf_counter()
+    for l, k in zip(links, comps):
+        vals = []
+        for sgn in (1.0, -1.0):
+            x = np.zeros(3)
+            x[k] = sgn * eps
+            q = U[4 * l:4 * l + 4]
+            # exp(x) (exp_gauge.cc:8-18) times the link, in the (a, b) form of su2.hh
+            al = np.linalg.norm(x)
+            e = np.array([np.cos(al), np.sin(al) * x[2] / al, np.sin(al) * x[1] / al,
+                          np.sin(al) * x[0] / al])
+            a = complex(e[0], e[1]) * complex(q[0], q[1]) - complex(e[2], e[3]) * \
+                complex(q[2], -q[3])
+            bb = complex(e[0], e[1]) * complex(q[2], q[3]) + complex(e[2], e[3]) * \
+                complex(q[0], -q[1])
+            V_[4 * l:4 * l + 4] = [a.real, a.imag, bb.real, bb.imag]
+            c.upload(V_)
+            vals.append(c.get_S_G_hmc())
+            V_[4 * l:4 * l + 4] = q
+        fd = (vals[0] - vals[1]) / (2 * eps)
+        fd_err.append(abs(fd - dS[3 * l + k]) / max(1.0, abs(dS[3 * l + k])))
+    t_fd = time.perf_counter() - t0
+    c.upload(U)
+    out = {}
+    grads = {}
+    for prec in ("fp64", "mixed"):
+        g = c if prec == "fp64" else su2_b200.gaugeconfig(L, L, L, L, 4, 2.4, precision=prec,
+                                                           device=local)
+        g.upload(U)
+        g.flow_objective(0.01, 200, grad=True, checkpoint_every=14)  # warm-up
+        s, e0, e1 = _events(g.stream())
+        barrier(dist)
+        e0.record(s)
+        for _ in range(args.steps):
+            O, grad = g.flow_objective(0.01, 200, grad=True, checkpoint_every=14)
+        e1.record(s)
+        e1.synchronize()
+        t = allmax(dist, e0.elapsed_time(e1) / 1e3) / args.steps
+        out[prec] = {"ms_per_gradient": 1e3 * t, "objective": O}
+        grads[prec] = grad
+        if g is not c:
+            g.close()
+    out["mixed"]["grad_rel_err_vs_fp64"] = float(np.linalg.norm(grads["mixed"] - grads["fp64"]) /
+                                                 np.linalg.norm(grads["fp64"]))
+    out["mixed"]["objective_rel_err_vs_fp64"] = abs(out["mixed"]["objective"] -
+                                                    out["fp64"]["objective"]) / \
+        abs(out["fp64"]["objective"])
+    c.close()
+    if rank == 0:
+        t = out["fp64"]["ms_per_gradient"] / 1e3
+        _line("SU(2) 24^4 gradient of t^2 E(t=2) w.r.t. the initial links: gradients/s (FP64)",
+              ws / t, "gradients/s", args, ws, 1e3 * t,
+              {"workload": "SU(2) d=4 24^4 beta=2.4, GPU-thermalised (100 Metropolis sweeps + "
+                           "10 omf2 trajectories); flow eps=0.01 to t=2, checkpoints every 14",
+               "replicas": ws},
+              dtype="fp64 (and fp32)", flow_gradient=out,
+              action_backward={"S": S, "rel_diff_vs_gauge_force": force_rel,
+                               "fd_links": 1000, "fd_eps": eps,
+                               "fd_max_rel_err": float(np.max(fd_err)),
+                               "fd_median_rel_err": float(np.median(fd_err)),
+                               "fd_seconds": t_fd})
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -459,9 +784,13 @@ def main():
                     help="only the timed loop of one precision, for ncu (no bench line)")
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--force-variant", type=int, default=3)
+    ap.add_argument("--config", type=int, default=2, choices=[1, 2, 3, 4, 5],
+                    help="2: the headline 32^4 HMC; 1, 3, 4, 5: the other workloads")
     args = ap.parse_args()
     if args.profile_run:
         profile_run(args)
+    elif args.impl == "ours" and args.config != 2:
+        {1: config1, 3: config3, 4: config4, 5: config5}[args.config](args)
     elif args.impl == "reference":
         reference(args)
     else:

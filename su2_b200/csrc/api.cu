@@ -496,6 +496,11 @@ int su2b_q_flow_step(su2b_ctx *ctx, void *U, double eps) {
                      nullptr));
     CKS(su2b_q_update(ctx, U, ctx->Z, -eps * expfac[f]));
   }
+  // FP32 links: every exp(.)U product rounds |U| by about one ulp in a direction that does not
+  // average out over hundreds of steps, and the flowed plaquette (close to 1) amplifies that
+  // drift in E = d(d-1)/2 - P/(V Nc).  Reunitarise in FP64 after each step, as the trajectory
+  // does at its end; FP64 links keep the reference's step unchanged.
+  if (!ctx->link64 && ctx->group == SU2B_GROUP_SU2) CKS(su2b_q_restore(ctx, U));
   return SU2B_OK;
 }
 
