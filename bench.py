@@ -22,6 +22,7 @@ import math
 import os
 import statistics
 import sys
+import tempfile
 import threading
 import time
 
@@ -620,6 +621,7 @@ def config4(args):
     with chain_batch(mine, precision="mixed", device=local) as b:
         for i, U in enumerate(starts):
             b.upload(i, U)
+        tune = b.autotune()  # launch shape of the batched kernels, timed on this ensemble
         for k in range(W):
             b.md_update("leapfrog", 10, 1.0, traj=k)
         s, e0, e1 = _events(b.stream())
@@ -639,6 +641,7 @@ def config4(args):
         g = su2_b200.gaugeconfig(Lx, Ly, Lz, Lt, c["ndims"], c["beta"], precision="mixed",
                                  device=local)
         g.upload(U)
+        g.autotune(os.path.join(tempfile.gettempdir(), "su2b_tune_cache.txt"))
         for k in range(W):
             g.md_update("leapfrog", 10, 1.0, seed=c["seed"], traj=k)
         ctxs.append(g)
@@ -676,6 +679,8 @@ def config4(args):
                "chains": len(chains), "sites_total": int(total_sites),
                "parallelism": f"chains partitioned over {ws} rank(s)"},
               dtype="fp32 links + fp64 sums", one_by_one_site_updates_per_s=total_sites * K / t_1,
+              batch_autotune_force_us={str(su2_b200._abi.BATCH_SHAPES[v]): us
+                                       for v, us in tune.items()},
               batched_over_one_by_one=t_1 / t_b,
               acceptance=float(np.mean([r.accepted for rr in res for r in rr])),
               gpu_launches=int(launches), cpu_baseline=cpu)

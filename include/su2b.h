@@ -228,6 +228,15 @@ SU2B_API int su2b_batch_download(su2b_batch *b, int chain, double *U_host);
 /* one trajectory (SU2B_LEAPFROG or SU2B_OMF2) of every chain; results[n_chains] */
 SU2B_API int su2b_batch_hmc(su2b_batch *b, int integrator, int n_steps, double tau, uint32_t traj,
                             su2b_traj_result *results);
+/* Launch shapes of the batched kernels (threads per block 64/128/128/256, the tile of a block
+ * being half that many sites of each parity of one chain; force-kernel register caps from
+ * 8/4/6/3 resident blocks per SM).  su2b_batch_autotune times the batched force step of each
+ * shape on the ensemble's current fields (without changing them), keeps the fastest and
+ * writes the microseconds per launch to times_us (SU2B_BATCH_VARIANTS entries, may be NULL). */
+#define SU2B_BATCH_VARIANTS 4
+SU2B_API int su2b_batch_autotune(su2b_batch *b, double *times_us);
+SU2B_API int su2b_batch_tune_get(su2b_batch *b, int *variant);
+SU2B_API int su2b_batch_tune_set(su2b_batch *b, int variant);
 
 /* ---- derivatives (SU(2)) ------------------------------------------------------------------ */
 /* Left Lie-algebra derivatives, the convention of gaugemonomial::derivative

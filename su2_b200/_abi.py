@@ -98,6 +98,9 @@ SIGNATURES = {
     "su2b_batch_upload": (i32, [_P, i32, _D]),
     "su2b_batch_download": (i32, [_P, i32, _D]),
     "su2b_batch_hmc": (i32, [_P, i32, i32, f64, u32, C.POINTER(TrajResult)]),
+    "su2b_batch_autotune": (i32, [_P, _D]),
+    "su2b_batch_tune_get": (i32, [_P, C.POINTER(i32)]),
+    "su2b_batch_tune_set": (i32, [_P, i32]),
     "su2b_action_backward": (i32, [_P, f64, _D, _D]),
     "su2b_force_vjp": (i32, [_P, _D, _D]),
     "su2b_flow_adjoint": (i32, [_P, f64, i32, i32, _D, _D]),
@@ -105,8 +108,13 @@ SIGNATURES = {
     "su2b_tune_set": (i32, [_P, i32, i32]),
 }
 FORCE_VARIANTS = 8
-FORCE_SHAPES = [(64, 8), (128, 1), (128, 4), (128, 6), (256, 2), (256, 3), ("async", 64),
-                ("async", 128)]
+BATCH_VARIANTS = 4
+# (threads per block, min blocks per SM) of the batched force kernel
+BATCH_SHAPES = [(64, 8), (128, 4), (128, 6), (256, 3)]
+# (threads per block, min blocks per SM) of the gather kernel; ("brick", BX, BY, BZ) of the
+# shared-memory 2.5D kernel (d = 4 with extents divisible by the brick; else gather (128, 6))
+FORCE_SHAPES = [(64, 8), (128, 1), (128, 4), (128, 6), (256, 2), (256, 3), ("brick", 4, 4, 8),
+                ("brick", 2, 4, 16)]
 
 K_FORCE, K_UPDATE, K_PLAQUETTE, K_MOMENTA, K_RESTORE, K_METROPOLIS, K_CLOVER, K_STAGGERED, \
     K_OTHER = range(9)

@@ -72,6 +72,23 @@ class chain_batch:
         self._c(self.lib.su2b_batch_kernel_launches(self.h, C.byref(n)))
         return n.value
 
+    def autotune(self):
+        """Times the batched force step of every launch shape on the current fields (which it
+        leaves unchanged), keeps the fastest; returns {variant: microseconds per launch}."""
+        t = np.zeros(_abi.BATCH_VARIANTS)
+        self._c(self.lib.su2b_batch_autotune(self.h, _dp(t)))
+        return {v: float(t[v]) for v in range(_abi.BATCH_VARIANTS)}
+
+    @property
+    def variant(self) -> int:
+        v = C.c_int()
+        self._c(self.lib.su2b_batch_tune_get(self.h, C.byref(v)))
+        return v.value
+
+    @variant.setter
+    def variant(self, v):
+        self._c(self.lib.su2b_batch_tune_set(self.h, int(v)))
+
     def md_update(self, integrator="leapfrog", n_steps=10, tau=1.0, traj=0):
         res = (_abi.TrajResult * len(self.chains))()
         integ = INTEGRATORS[integrator] if isinstance(integrator, str) else integrator

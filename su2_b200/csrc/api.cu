@@ -128,6 +128,7 @@ extern "C" int su2b_ctx_create(int group, int Lx, int Ly, int Lz, int Lt, int nd
   ctx->V = (size_t)g.V;
   ctx->NL = (size_t)g.V * ndims;
   ctx->link64 = !(group == SU2B_GROUP_SU2 && precision == SU2B_PREC_MIXED);
+  ctx->tune_force = ctx->link64 ? 2 : 3;  // launch shape before any tuning: (128,4) / (128,6)
   int st = SU2B_OK;
   auto fin = [&](int s) -> int {
     if (s != SU2B_OK) {

@@ -33,18 +33,30 @@ struct ChainDev {
 
 constexpr int RS = 16;  // reduced scalars per chain
 
+// the chain that owns a tile: the last chain whose first tile is <= tile (binary search)
 __device__ __forceinline__ int chain_of(const ChainDev *__restrict__ ch, int n, int tile) {
-  int c = 0;
-  while (c + 1 < n && __ldg(&ch[c + 1].tile0) <= tile) c++;
-  return c;
+  int lo = 0, hi = n - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (__ldg(&ch[mid].tile0) <= tile)
+      lo = mid;
+    else
+      hi = mid - 1;
+  }
+  return lo;
 }
+
+// launch shapes of the batched kernels: threads per block (a tile is NT/2 sites of each
+// parity of one chain) and, for the force kernel, the minimum resident blocks per SM
+constexpr int BATCH_NT[SU2B_BATCH_VARIANTS] = {64, 128, 128, 256};
+constexpr int BATCH_MINB[SU2B_BATCH_VARIANTS] = {8, 4, 6, 3};
 
 template <class T> struct Bufs {
   LinkT<T> *b[3];
 };
 
-template <class T, int NT>
-__global__ void __launch_bounds__(NT)
+template <class T, int NT, int MINB>
+__global__ void __launch_bounds__(NT, MINB)
   k_batch_force(const ChainDev *__restrict__ ch, int nchains, int ntiles, Bufs<T> bufs,
                 T *__restrict__ Pall, const int *__restrict__ cur, int rel_in, int rel_out,
                 double cm, double cg, int mode, double *kin_part) {
@@ -191,9 +203,10 @@ struct su2b_batch {
   bool link64 = true;
   cudaStream_t stream = nullptr;
   std::vector<su2b_chain_desc> desc;
-  std::vector<ChainDev> hch;
-  ChainDev *ch = nullptr;
-  int ntiles = 0, nt = 128;
+  std::vector<ChainDev> hch[SU2B_BATCH_VARIANTS];  // tile tables per launch shape
+  ChainDev *ch[SU2B_BATCH_VARIANTS] = {};
+  int ntiles[SU2B_BATCH_VARIANTS] = {};
+  int variant = 2;
   size_t total_links = 0;
   void *buf[3] = {};
   void *P = nullptr;
@@ -254,30 +267,37 @@ extern "C" int su2b_batch_create(int n_chains, const su2b_chain_desc *chains, in
     *out = b;
     return SU2B_OK;
   };
+  b->variant = b->link64 ? 1 : 2;
   size_t off_l = 0, off_a = 0;
-  int tile = 0;
-  const int half = b->nt / 2;
-  for (int c = 0; c < n_chains; c++) {
-    const su2b_chain_desc &d = chains[c];
-    ChainDev cd{};
-    std::string why;
-    if (d.ndims < 3 || !su2b_make_geom(d.Lx, d.Ly, d.Lz, d.Lt, d.ndims, &cd.g, &why))
-      return fin(bfail(b, SU2B_ERR_INVALID, "chain %d: %s", c,
-                       d.ndims < 3 ? "batches hold d = 3 or 4 chains" : why.c_str()));
-    cd.beta = d.beta;
-    cd.seed = d.seed;
-    cd.off_link = off_l;
-    cd.off_adj = off_a;
-    cd.tile0 = tile;
-    cd.ntiles = (cd.g.Vh + half - 1) / half;
-    const size_t NL = (size_t)cd.g.V * d.ndims;
-    off_l += NL;
-    off_a += 3 * NL;
-    tile += cd.ntiles;
-    b->hch.push_back(cd);
+  int maxtiles = 0;
+  for (int v = 0; v < SU2B_BATCH_VARIANTS; v++) {
+    const int half = BATCH_NT[v] / 2;
+    off_l = off_a = 0;
+    int tile = 0;
+    for (int c = 0; c < n_chains; c++) {
+      const su2b_chain_desc &d = chains[c];
+      ChainDev cd{};
+      std::string why;
+      if (d.ndims < 3 || !su2b_make_geom(d.Lx, d.Ly, d.Lz, d.Lt, d.ndims, &cd.g, &why))
+        return fin(bfail(b, SU2B_ERR_INVALID, "chain %d: %s", c,
+                         d.ndims < 3 ? "batches hold d = 3 or 4 chains" : why.c_str()));
+      cd.beta = d.beta;
+      cd.seed = d.seed;
+      cd.off_link = off_l;
+      cd.off_adj = off_a;
+      cd.tile0 = tile;
+      cd.ntiles = (cd.g.Vh + half - 1) / half;
+      const size_t NL = (size_t)cd.g.V * d.ndims;
+      off_l += NL;
+      off_a += 3 * NL;
+      tile += cd.ntiles;
+      b->hch[v].push_back(cd);
+    }
+    b->ntiles[v] = tile;
+    maxtiles = std::max(maxtiles, tile);
   }
-  b->ntiles = tile;
   b->total_links = off_l;
+  const int tile = maxtiles;
   if (cudaSetDevice(device) != cudaSuccess) return fin(SU2B_ERR_CUDA);
   if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess)
     return fin(SU2B_ERR_CUDA);
@@ -288,7 +308,7 @@ extern "C" int su2b_batch_create(int n_chains, const su2b_chain_desc *chains, in
     return true;
   };
   size_t maxNL = 0;
-  for (auto &c : b->hch) maxNL = std::max(maxNL, (size_t)c.g.V * c.g.nd);
+  for (auto &c : b->hch[0]) maxNL = std::max(maxNL, (size_t)c.g.V * c.g.nd);
   bool ok = dal(&b->buf[0], lb * off_l) && dal(&b->buf[1], lb * off_l) &&
             dal(&b->buf[2], lb * off_l) && dal(&b->P, ab * off_a) &&
             dal((void **)&b->part, sizeof(double) * 3 * (size_t)tile) &&
@@ -296,18 +316,22 @@ extern "C" int su2b_batch_create(int n_chains, const su2b_chain_desc *chains, in
             dal((void **)&b->stage, sizeof(double) * 4 * maxNL) &&
             dal((void **)&b->cur, sizeof(int) * n_chains) &&
             dal((void **)&b->traj, sizeof(uint32_t)) &&
-            dal((void **)&b->res, sizeof(TrajDev) * n_chains) &&
-            dal((void **)&b->ch, sizeof(ChainDev) * n_chains);
+            dal((void **)&b->res, sizeof(TrajDev) * n_chains);
+  for (int v = 0; v < SU2B_BATCH_VARIANTS && ok; v++)
+    ok = dal((void **)&b->ch[v], sizeof(ChainDev) * n_chains);
   if (!ok) return fin(bfail(b, SU2B_ERR_NOMEM, "device allocation failed"));
   if (cudaMallocHost((void **)&b->h_traj, sizeof(uint32_t)) != cudaSuccess ||
       cudaMallocHost((void **)&b->h_res, sizeof(TrajDev) * n_chains) != cudaSuccess ||
       cudaMallocHost((void **)&b->h_red, sizeof(double) * RS * n_chains) != cudaSuccess ||
       cudaMallocHost((void **)&b->h_cur, sizeof(int) * n_chains) != cudaSuccess)
     return fin(SU2B_ERR_NOMEM);
-  if (cudaMemcpy(b->ch, b->hch.data(), sizeof(ChainDev) * n_chains, cudaMemcpyHostToDevice) !=
-        cudaSuccess ||
-      cudaMemset(b->cur, 0, sizeof(int) * n_chains) != cudaSuccess ||
-      cudaMemset(b->buf[0], 0, lb * off_l) != cudaSuccess)
+  for (int v = 0; v < SU2B_BATCH_VARIANTS; v++)
+    if (cudaMemcpy(b->ch[v], b->hch[v].data(), sizeof(ChainDev) * n_chains,
+                   cudaMemcpyHostToDevice) != cudaSuccess)
+      return fin(SU2B_ERR_CUDA);
+  if (cudaMemset(b->cur, 0, sizeof(int) * n_chains) != cudaSuccess ||
+      cudaMemset(b->buf[0], 0, lb * off_l) != cudaSuccess ||
+      cudaMemset(b->P, 0, ab * off_a) != cudaSuccess)
     return fin(SU2B_ERR_CUDA);
   return fin(SU2B_OK);
 }
@@ -344,7 +368,7 @@ extern "C" int su2b_batch_kernel_launches(su2b_batch *b, long *count) {
 static int chain_transfer(su2b_batch *b, int chain, double *host, bool up) {
   if (chain < 0 || chain >= b->n || !host) return bfail(b, SU2B_ERR_INVALID, "bad chain/buffer");
   BCK(cudaSetDevice(b->device));
-  const ChainDev &c = b->hch[chain];
+  const ChainDev &c = b->hch[0][chain];
   const size_t NL = (size_t)c.g.V * c.g.nd;
   BCK(cudaMemcpy(b->h_cur, b->cur, sizeof(int) * b->n, cudaMemcpyDeviceToHost));
   const size_t lb = b->link64 ? 32 : 16;
@@ -427,7 +451,7 @@ std::vector<BOp> batch_schedule(int integ, int n, double tau, bool *ok) {
   return f;
 }
 
-template <class T, int NT> int grid_for(const void *kernel, int ntiles) {
+template <int NT> int grid_for(const void *kernel, int ntiles) {
   int per_sm = 1;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, NT, 0);
   int dev = 0, sms = 148;
@@ -436,20 +460,22 @@ template <class T, int NT> int grid_for(const void *kernel, int ntiles) {
   return std::max(1, std::min(ntiles, std::max(1, per_sm) * sms));
 }
 
-template <class T>
-int enqueue_batch(su2b_batch *b, const std::vector<BOp> &ops, int *rel_final) {
-  constexpr int NT = 128;
+template <class T, int NT, int MINB>
+int enqueue_batch_v(su2b_batch *b, const std::vector<BOp> &ops, int *rel_final) {
   cudaStream_t s = b->stream;
+  const int v = b->variant;
+  const ChainDev *ch = b->ch[v];
+  const int ntiles = b->ntiles[v];
   Bufs<T> bufs{{(LinkT<T> *)b->buf[0], (LinkT<T> *)b->buf[1], (LinkT<T> *)b->buf[2]}};
   T *P = (T *)b->P;
-  const int gF = grid_for<T, NT>((const void *)k_batch_force<T, NT>, b->ntiles);
-  const int gM = grid_for<T, NT>((const void *)k_batch_momenta<T, NT>, b->ntiles);
-  const int gP = grid_for<T, NT>((const void *)k_batch_plaq<T, NT>, b->ntiles);
+  const int gF = grid_for<NT>((const void *)k_batch_force<T, NT, MINB>, ntiles);
+  const int gM = grid_for<NT>((const void *)k_batch_momenta<T, NT>, ntiles);
+  const int gP = grid_for<NT>((const void *)k_batch_plaq<T, NT>, ntiles);
   long nl = 0;
-  k_batch_momenta<T, NT><<<gM, NT, 0, s>>>(b->ch, b->n, b->ntiles, P, b->traj, b->part);
-  k_batch_reduce<<<b->n, 256, 0, s>>>(b->ch, b->part, 1, b->red, 0);
-  k_batch_plaq<T, NT><<<gP, NT, 0, s>>>(b->ch, b->n, b->ntiles, bufs, b->cur, 0, b->part);
-  k_batch_reduce<<<b->n, 256, 0, s>>>(b->ch, b->part, 3, b->red, 1);
+  k_batch_momenta<T, NT><<<gM, NT, 0, s>>>(ch, b->n, ntiles, P, b->traj, b->part);
+  k_batch_reduce<<<b->n, 256, 0, s>>>(ch, b->part, 1, b->red, 0);
+  k_batch_plaq<T, NT><<<gP, NT, 0, s>>>(ch, b->n, ntiles, bufs, b->cur, 0, b->part);
+  k_batch_reduce<<<b->n, 256, 0, s>>>(ch, b->part, 3, b->red, 1);
   nl += 4;
   int cur = 0;
   auto next = [](int c) { return c == 1 ? 2 : 1; };
@@ -465,19 +491,19 @@ int enqueue_batch(su2b_batch *b, const std::vector<BOp> &ops, int *rel_final) {
       mode |= FM_RESTORE;
       out = fin = (cur == 0) ? 1 : next(cur);
     }
-    k_batch_force<T, NT><<<gF, NT, 0, s>>>(b->ch, b->n, b->ntiles, bufs, P, b->cur, cur, out,
-                                           o.cm, o.cg, mode, b->part);
+    k_batch_force<T, NT, MINB><<<gF, NT, 0, s>>>(ch, b->n, ntiles, bufs, P, b->cur, cur, out,
+                                                 o.cm, o.cg, mode, b->part);
     nl++;
     if (o.kinetic) {
-      k_batch_reduce<<<b->n, 256, 0, s>>>(b->ch, b->part, 1, b->red, 4);
+      k_batch_reduce<<<b->n, 256, 0, s>>>(ch, b->part, 1, b->red, 4);
       nl++;
     }
     if (o.kind == 1) cur = out;
   }
   if (fin < 0) return bfail(b, SU2B_ERR_UNSUPPORTED, "schedule must end with a momentum step");
-  k_batch_plaq<T, NT><<<gP, NT, 0, s>>>(b->ch, b->n, b->ntiles, bufs, b->cur, fin, b->part);
-  k_batch_reduce<<<b->n, 256, 0, s>>>(b->ch, b->part, 3, b->red, 5);
-  k_batch_accept<<<(b->n + 63) / 64, 64, 0, s>>>(b->ch, b->n, b->red, b->traj, fin, b->cur,
+  k_batch_plaq<T, NT><<<gP, NT, 0, s>>>(ch, b->n, ntiles, bufs, b->cur, fin, b->part);
+  k_batch_reduce<<<b->n, 256, 0, s>>>(ch, b->part, 3, b->red, 5);
+  k_batch_accept<<<(b->n + 63) / 64, 64, 0, s>>>(ch, b->n, b->red, b->traj, fin, b->cur,
                                                  b->res);
   nl += 3;
   BCK(cudaGetLastError());
@@ -485,6 +511,63 @@ int enqueue_batch(su2b_batch *b, const std::vector<BOp> &ops, int *rel_final) {
   BCK(cudaMemcpyAsync(b->h_red, b->red, sizeof(double) * RS * b->n, cudaMemcpyDeviceToHost, s));
   *rel_final = fin;
   return (int)nl;
+}
+
+template <class T>
+int enqueue_batch(su2b_batch *b, const std::vector<BOp> &ops, int *rel_final) {
+  switch (b->variant) {
+    case 0: return enqueue_batch_v<T, 64, 8>(b, ops, rel_final);
+    case 1: return enqueue_batch_v<T, 128, 4>(b, ops, rel_final);
+    case 2: return enqueue_batch_v<T, 128, 6>(b, ops, rel_final);
+    default: return enqueue_batch_v<T, 256, 3>(b, ops, rel_final);
+  }
+}
+
+// Times the batched force step (momentum step + link update of every chain, one persistent
+// launch) of one launch shape: fresh momenta from the Philox stream, then `reps` launches
+// that read each chain's current field and write the update into a buffer the chain does
+// not use, so the chains' states are untouched.  Returns microseconds per launch.
+template <class T, int NT, int MINB> int time_force_v(su2b_batch *b, int v, double *us) {
+  cudaStream_t s = b->stream;
+  const ChainDev *ch = b->ch[v];
+  const int ntiles = b->ntiles[v];
+  Bufs<T> bufs{{(LinkT<T> *)b->buf[0], (LinkT<T> *)b->buf[1], (LinkT<T> *)b->buf[2]}};
+  T *P = (T *)b->P;
+  const int gF = grid_for<NT>((const void *)k_batch_force<T, NT, MINB>, ntiles);
+  const int gM = grid_for<NT>((const void *)k_batch_momenta<T, NT>, ntiles);
+  k_batch_momenta<T, NT><<<gM, NT, 0, s>>>(ch, b->n, ntiles, P, b->traj, b->part);
+  const int mode = FM_HAS_IN | FM_UPDATE;
+  auto launch = [&]() {
+    k_batch_force<T, NT, MINB><<<gF, NT, 0, s>>>(ch, b->n, ntiles, bufs, P, b->cur, 0, 1, 0.01,
+                                                 0.01, mode, b->part);
+  };
+  launch();  // warm-up
+  cudaEvent_t e0, e1;
+  BCK(cudaEventCreate(&e0));
+  BCK(cudaEventCreate(&e1));
+  const int reps = 5;
+  cudaEventRecord(e0, s);
+  for (int r = 0; r < reps; r++) launch();
+  cudaEventRecord(e1, s);
+  const cudaError_t e = cudaEventSynchronize(e1);
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  BCK(e);
+  BCK(cudaGetLastError());
+  b->launches += reps + 2;
+  *us = 1e3 * (double)ms / reps;
+  return SU2B_OK;
+}
+
+template <class T> int time_force(su2b_batch *b, int v, double *us) {
+  switch (v) {
+    case 0: return time_force_v<T, 64, 8>(b, v, us);
+    case 1: return time_force_v<T, 128, 4>(b, v, us);
+    case 2: return time_force_v<T, 128, 6>(b, v, us);
+    default: return time_force_v<T, 256, 3>(b, v, us);
+  }
 }
 
 }  // namespace
@@ -502,7 +585,7 @@ extern "C" int su2b_batch_hmc(su2b_batch *b, int integrator, int n_steps, double
   *b->h_traj = traj;
   BCK(cudaMemcpyAsync(b->traj, b->h_traj, sizeof(uint32_t), cudaMemcpyHostToDevice, b->stream));
   char key[128];
-  snprintf(key, sizeof key, "%d/%d/%.17g", integrator, n_steps, tau);
+  snprintf(key, sizeof key, "%d/%d/%.17g/v%d", integrator, n_steps, tau, b->variant);
   cudaGraphExec_t exec = nullptr;
   long kernels = 0;
   for (auto &g : b->graphs)
@@ -544,5 +627,39 @@ extern "C" int su2b_batch_hmc(su2b_batch *b, int integrator, int n_steps, double
     r.plaquette = t.accepted ? b->h_red[c * RS + 5] : b->h_red[c * RS + 1];
     r.cg_iterations = 0;
   }
+  return SU2B_OK;
+}
+
+extern "C" int su2b_batch_autotune(su2b_batch *b, double *times_us) {
+  if (!b) return SU2B_ERR_INVALID;
+  b->err.clear();
+  BCK(cudaSetDevice(b->device));
+  double best = 0.;
+  int bv = b->variant;
+  for (int v = 0; v < SU2B_BATCH_VARIANTS; v++) {
+    double us = 0.;
+    const int rc = b->link64 ? time_force<double>(b, v, &us) : time_force<float>(b, v, &us);
+    if (rc != SU2B_OK) return rc;
+    if (times_us) times_us[v] = us;
+    if (v == 0 || us < best) {
+      best = us;
+      bv = v;
+    }
+  }
+  b->variant = bv;
+  return SU2B_OK;
+}
+
+extern "C" int su2b_batch_tune_get(su2b_batch *b, int *variant) {
+  if (!b || !variant) return SU2B_ERR_INVALID;
+  *variant = b->variant;
+  return SU2B_OK;
+}
+
+extern "C" int su2b_batch_tune_set(su2b_batch *b, int variant) {
+  if (!b) return SU2B_ERR_INVALID;
+  if (variant < 0 || variant >= SU2B_BATCH_VARIANTS)
+    return bfail(b, SU2B_ERR_INVALID, "batch launch shape %d out of range", variant);
+  b->variant = variant;
   return SU2B_OK;
 }

@@ -18,6 +18,45 @@ template <class T> using LinkT = typename LinkOf<T>::type;
 // that call this give each block one band of sites of both parities (warps alternate), so
 // the blocks resident at any time cover one narrow band of the lattice and the links stream
 // from HBM about once per launch.  Returns the sum of the updated P^2 of the site.
+// The per-link tail of the fused force step for link l with staple sum k:
+//   d = f get_deriv(U K) (+ extra),  P = P + scale d,  then (FM_UPDATE) the following gauge
+//   step U' = exp(dt P) U (update_gauge.hh:8-16) or (FM_RESTORE) U' = restoreSU(U) into Uout.
+// Returns the link's |P|^2 in FP64.
+template <class T>
+__device__ __forceinline__ double finish_link(const Su2<T> &u, const Su2<T> &k, size_t l,
+                                              size_t NL, T *__restrict__ P,
+                                              const T *__restrict__ extra, T f, T scale_,
+                                              int mode, LinkT<T> *__restrict__ Uout, T dt_upd) {
+  // get_deriv(U K) = (2 Im b, 2 Re b, 2 Im a) (adjointfield.hh:53-56)
+  const T sbi = fm(u.ar, k.bi, fm(u.ai, k.br, fm(u.bi, k.ar, -u.br * k.ai)));
+  const T sbr = fm(u.ar, k.br, fm(-u.ai, k.bi, fm(u.br, k.ar, u.bi * k.ai)));
+  const T sai = fm(u.ar, k.ai, fm(u.ai, k.ar, fm(-u.bi, k.br, u.br * k.bi)));
+  const T f2 = T(2) * f;
+  T d0 = f2 * sbi, d1 = f2 * sbr, d2 = f2 * sai;
+  if (mode & FM_EXTRA) {
+    d0 += extra[l];
+    d1 += extra[NL + l];
+    d2 += extra[2 * NL + l];
+  }
+  T p0 = 0, p1 = 0, p2 = 0;
+  if (mode & FM_HAS_IN) {
+    p0 = P[l];
+    p1 = P[NL + l];
+    p2 = P[2 * NL + l];
+  }
+  p0 = p0 + scale_ * d0;
+  p1 = p1 + scale_ * d1;
+  p2 = p2 + scale_ * d2;
+  P[l] = p0;
+  P[NL + l] = p1;
+  P[2 * NL + l] = p2;
+  if (mode & FM_UPDATE)
+    st_link(Uout + l, mul(exp_alg(dt_upd * p0, dt_upd * p1, dt_upd * p2), u));
+  else if (mode & FM_RESTORE)
+    st_link(Uout + l, from64<T>(restore_su(to64(u))));
+  return (double)p0 * p0 + (double)p1 * p1 + (double)p2 * p2;
+}
+
 template <class T, int ND, bool ANISO>
 __device__ __forceinline__ double force_site_impl(const Geom &g, const LinkT<T> *__restrict__ U,
                                                   T *__restrict__ P,
@@ -71,40 +110,9 @@ __device__ __forceinline__ double force_site_impl(const Geom &g, const LinkT<T> 
     }
   }
 #pragma unroll
-  for (int mu = 0; mu < ND; mu++) {
-    const Su2<T> &u = ux[mu];
-    const Su2<T> &k = K[mu];
-    const size_t l = mu * V + self;
-    // get_deriv(U K) = (2 Im b, 2 Re b, 2 Im a) (adjointfield.hh:53-56)
-    const T sbi = fm(u.ar, k.bi, fm(u.ai, k.br, fm(u.bi, k.ar, -u.br * k.ai)));
-    const T sbr = fm(u.ar, k.br, fm(-u.ai, k.bi, fm(u.br, k.ar, u.bi * k.ai)));
-    const T sai = fm(u.ar, k.ai, fm(u.ai, k.ar, fm(-u.bi, k.br, u.br * k.bi)));
-    const T f2 = T(2) * f;
-    T d0 = f2 * sbi, d1 = f2 * sbr, d2 = f2 * sai;
-    if (mode & FM_EXTRA) {
-      d0 += extra[l];
-      d1 += extra[NL + l];
-      d2 += extra[2 * NL + l];
-    }
-    T p0 = 0, p1 = 0, p2 = 0;
-    if (mode & FM_HAS_IN) {
-      p0 = P[l];
-      p1 = P[NL + l];
-      p2 = P[2 * NL + l];
-    }
-    p0 = p0 + scale_ * d0;
-    p1 = p1 + scale_ * d1;
-    p2 = p2 + scale_ * d2;
-    P[l] = p0;
-    P[NL + l] = p1;
-    P[2 * NL + l] = p2;
-    k2 += (double)p0 * p0 + (double)p1 * p1 + (double)p2 * p2;
-    // the following gauge step U <- exp(dt P) U (update_gauge.hh:8-16) into the other buffer
-    if (mode & FM_UPDATE)
-      st_link(Uout + l, mul(exp_alg(dt_upd * p0, dt_upd * p1, dt_upd * p2), u));
-    else if (mode & FM_RESTORE)
-      st_link(Uout + l, from64<T>(restore_su(to64(u))));
-  }
+  for (int mu = 0; mu < ND; mu++)
+    k2 += finish_link<T>(ux[mu], K[mu], mu * V + self, NL, P, extra, f, scale_, mode, Uout,
+                         dt_upd);
   return k2;
 }
 

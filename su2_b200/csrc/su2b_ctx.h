@@ -52,7 +52,7 @@ struct su2b_ctx {
   long x0_seed = -1;  // seed of the reference CG start held in sv[SV_X0]
 
   // launch shape of the SU(2) force kernel (su2b_autotune)
-  int tune_force = 1;
+  int tune_force = 3;  // (128 threads, 6 blocks/SM) until tuned; FP64 contexts start at 2
 
   // kernel launch counter and the per-class device timers (su2b_profile)
   long launches = 0;

@@ -50,3 +50,36 @@ def test_batch_rejects_bad_chains(gpu):
     with chain_batch([dict(dims=(4, 4, 4, 4), ndims=4, beta=2.0, seed=1)]) as b:
         with pytest.raises(su2_b200.Su2bError):
             b.md_update("omf4", 4, 1.0)
+
+
+def test_batch_autotune_leaves_fields_and_every_shape_agrees(gpu, orc):
+    """The batch tuner times every launch shape without touching the chains' fields, keeps
+    the fastest, and every shape advances the ensemble identically up to the rounding of the
+    per-tile partial sums (different tile sizes group the sums differently)."""
+    from su2_b200.batch import chain_batch
+    chains = [dict(dims=(4, 4, 4, 6), ndims=4, beta=2.3, seed=11),
+              dict(dims=(8, 6, 1, 4), ndims=3, beta=2.1, seed=12)]
+    starts = [orc.hotstart(0, c["dims"], c["ndims"], 100 + i, 1.0, 654321)
+              for i, c in enumerate(chains)]
+    runs = []
+    for v in range(gpu._abi.BATCH_VARIANTS):
+        with chain_batch(chains, precision="mixed") as b:
+            for i, U in enumerate(starts):
+                b.upload(i, U)
+            if v == 0:
+                t = b.autotune()
+                assert all(x > 0 for x in t.values())
+                assert b.variant == min(t, key=t.get)
+                for i, U in enumerate(starts):
+                    assert np.array_equal(b.download(i), U.astype(np.float32).astype(np.float64))
+            b.variant = v
+            res = [b.md_update("leapfrog", 5, 1.0, traj=k) for k in range(3)]
+            runs.append((res, [b.download(i) for i in range(len(chains))]))
+    ref_res, ref_U = runs[0]
+    for res, Us in runs[1:]:
+        for ra, rb in zip(ref_res, res):
+            for a, b_ in zip(ra, rb):
+                assert a.accepted == b_.accepted
+                assert a.dH == pytest.approx(b_.dH, abs=1e-8)
+        for a, b_ in zip(ref_U, Us):
+            assert np.array_equal(a, b_)

@@ -311,8 +311,13 @@ def test_rejected_trajectory_keeps_start_field(gpu, orc):
 
 
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
-def test_every_force_launch_shape_is_exact(gpu, orc, precision):
-    group, dims, nd = 0, (8, 6, 4, 8), 4
+@pytest.mark.parametrize("dims", [(8, 6, 4, 8), (4, 4, 8, 4), (8, 8, 16, 6)],
+                         ids=["8x6x4x8", "4x4x8x4", "8x8x16x6"])
+def test_every_force_launch_shape_is_exact(gpu, orc, precision, dims):
+    """Every launch shape, including the shared-memory brick kernels (which need extents
+    divisible by the brick: 4x4x8 takes the second and third lattice, 2x4x16 the third; the
+    others fall back to the gather kernel), gives the oracle's force and a finite trajectory."""
+    group, nd = 0, 4
     U = hot(orc, group, dims, nd)
     F = orc.gauge_derivative(group, dims, nd, 2.3, U)
     tol = 1e-12 if precision == "fp64" else 1e-5
