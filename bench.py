@@ -277,7 +277,7 @@ def ours(args):
     for k in range(K):
         mixed.upload(Uh)
         r = mixed.md_update("omf2", NSTEPS, TAU, seed=seed, traj=400000 + k)
-        Uh[:] = mixed.download()
+        mixed.download(out=Uh)
     t_e2e = allmax(dist, time.perf_counter() - t0)
 
     # ---- side measurements of config 2 (Metropolis sweep, flow step) ----

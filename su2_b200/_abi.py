@@ -111,10 +111,10 @@ FORCE_VARIANTS = 8
 BATCH_VARIANTS = 4
 # (threads per block, min blocks per SM) of the batched force kernel
 BATCH_SHAPES = [(64, 8), (128, 4), (128, 6), (256, 3)]
-# (threads per block, min blocks per SM) of the gather kernel; ("brick", BX, BY, BZ) of the
-# shared-memory 2.5D kernel (d = 4 with extents divisible by the brick; else gather (128, 6))
-FORCE_SHAPES = [(64, 8), (128, 1), (128, 4), (128, 6), (256, 2), (256, 3), ("brick", 4, 4, 8),
-                ("brick", 2, 4, 16)]
+# (threads per block, min resident blocks per SM) of the force kernel's launch shapes; the
+# "split" shapes run two threads per site (d = 4; other d use (128, 8))
+FORCE_SHAPES = [(256, 4), (128, 8), (128, 4), (128, 6), (256, 2), (256, 3), ("split", 128, 8),
+                ("split", 256, 4)]
 
 K_FORCE, K_UPDATE, K_PLAQUETTE, K_MOMENTA, K_RESTORE, K_METROPOLIS, K_CLOVER, K_STAGGERED, \
     K_OTHER = range(9)

@@ -161,7 +161,6 @@ extern "C" int su2b_ctx_create(int group, int Lx, int Ly, int Lz, int Lt, int nd
       cudaMallocHost((void **)&ctx->h_st, sizeof(SolverState)) != cudaSuccess ||
       cudaMallocHost((void **)&ctx->h_tparams, sizeof(TrajParams)) != cudaSuccess)
     return fin(SU2B_ERR_NOMEM);
-  if (force_prepare() != cudaSuccess) return fin(SU2B_ERR_CUDA);
   if (cudaMemsetAsync(ctx->U, 0, lb * NL, ctx->stream) != cudaSuccess) return fin(SU2B_ERR_CUDA);
   if (cudaStreamSynchronize(ctx->stream) != cudaSuccess) return fin(SU2B_ERR_CUDA);
   return fin(SU2B_OK);

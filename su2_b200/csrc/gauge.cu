@@ -170,220 +170,6 @@ __global__ void __launch_bounds__(NT, MINB)
   }
 }
 
-// The same fused force step (d = 4) with the links staged in shared memory, 2.5D-blocked.
-// A block owns a BX x BY x BZ brick of (x, y, z) and marches along t over a contiguous range
-// of (brick, t) units; the units of the whole lattice are split evenly over the resident
-// blocks, so the grid is one wave.  Three time slices (t-1, t, t+1) of the brick with a
-// one-site halo in x, y and z are held in shared memory as a ring; moving to t+1 loads one
-// new slice (cp.async, periodic wrap) into the slot of t-2.  Every staple of the site is then
-// read from shared memory: each link crosses L2 -> SM about (BX+2)(BY+2)(BZ+2)/(BX BY BZ)
-// times per launch instead of the 11 times of the gather kernel.
-// Two threads share a site: half h updates the links mu = 2h, 2h+1.  The forward product A
-// of a plane inside the half is shared by its two links; the four planes that cross the halves
-// compute A in both (64 FMAs more per site), which halves the registers per thread and gives
-// twice the warps for the same brick.
-namespace tile {
-__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
-  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void cp_async_wait_all() {
-  asm volatile("cp.async.wait_all;\n" ::: "memory");
-}
-__device__ __forceinline__ int wrap(int c, int L) { return c < 0 ? c + L : (c >= L ? c - L : c); }
-}  // namespace tile
-
-template <int BX, int BY, int BZ> struct Brick {
-  static constexpr int NS = BX * BY * BZ;  // sites per slice
-  static constexpr int NT = 2 * NS;        // threads
-  static constexpr int HY = BY + 2, HZ = BZ + 2, H = (BX + 2) * HY * HZ;
-};
-
-template <class T, int BX, int BY, int BZ> constexpr size_t tile_smem() {
-  return (size_t)4 * 4 * Brick<BX, BY, BZ>::H * sizeof(LinkT<T>) +
-         (size_t)Brick<BX, BY, BZ>::H * sizeof(int);
-}
-
-template <class T, int BX, int BY, int BZ, int HALF, bool ANISO>
-__device__ __forceinline__ double tile_site(const Geom &g, const float4 *sm, const int slot[4],
-                                            int hc, size_t self, T *__restrict__ P,
-                                            const T *__restrict__ extra, T f, T scale_,
-                                            int mode, T wt, T ws,
-                                            LinkT<T> *__restrict__ Uout, T dt_upd) {
-  using B = Brick<BX, BY, BZ>;
-  constexpr int W = (int)(sizeof(LinkT<T>) / 16);
-  // link U_mu at offset (dt, dx, dy, dz) from the site, dt in {-1, 0, 1}
-  auto L = [&](int mu, int dt, int dx, int dy, int dz) -> Su2<T> {
-    const float4 *q = sm + ((size_t)(slot[dt + 1] * 4 + mu) * B::H + hc + (dx * B::HY + dy) * B::HZ + dz) * W;
-    if constexpr (W == 1) {
-      const float4 v = *q;
-      return Su2<T>{(T)v.x, (T)v.y, (T)v.z, (T)v.w};
-    } else {
-      const double2 a = *reinterpret_cast<const double2 *>(q);
-      const double2 b = *reinterpret_cast<const double2 *>(q + 1);
-      return Su2<T>{(T)a.x, (T)a.y, (T)b.x, (T)b.y};
-    }
-  };
-  // unit offset of direction d (0 = t, 1 = x, 2 = y, 3 = z)
-  auto E = [](int d, int k) { return d == k ? 1 : 0; };
-  constexpr int m0 = 2 * HALF, m1 = 2 * HALF + 1;
-  Su2<T> K[2] = {zero_su2<T>(), zero_su2<T>()};
-  // forward staples: U_nu(x+mu) U_mu(x+nu)^+ U_nu(x)^+
-#pragma unroll
-  for (int j = 0; j < 2; j++) {
-    const int mu = m0 + j;
-#pragma unroll
-    for (int nu = 0; nu < 4; nu++) {
-      if (nu == mu) continue;
-      const bool both = (nu == m0 || nu == m1);
-      if (both && nu < mu) continue;  // the plane was done from the other link
-      const Su2<T> a = L(nu, E(mu, 0), E(mu, 1), E(mu, 2), E(mu, 3));  // U_nu(x+mu)
-      const Su2<T> b = L(mu, E(nu, 0), E(nu, 1), E(nu, 2), E(nu, 3));  // U_mu(x+nu)
-      Su2<T> A = mul(a, dag(b));
-      if (ANISO) A = scale((mu == 0 || nu == 0) ? wt : ws, A);
-      K[j] = mul_acc(K[j], A, dag(L(nu, 0, 0, 0, 0)));
-      if (both) K[nu - m0] = mul_acc(K[nu - m0], dag(A), dag(L(mu, 0, 0, 0, 0)));
-    }
-  }
-  // backward staples U_nu(x+mu-nu)^+ U_mu(x-nu)^+ U_nu(x-nu)
-#pragma unroll
-  for (int j = 0; j < 2; j++) {
-    const int mu = m0 + j;
-#pragma unroll
-    for (int nu = 0; nu < 4; nu++) {
-      if (nu == mu) continue;
-      const Su2<T> e = L(nu, E(mu, 0) - E(nu, 0), E(mu, 1) - E(nu, 1), E(mu, 2) - E(nu, 2),
-                         E(mu, 3) - E(nu, 3));
-      const Su2<T> h = L(mu, -E(nu, 0), -E(nu, 1), -E(nu, 2), -E(nu, 3));
-      const Su2<T> c = L(nu, -E(nu, 0), -E(nu, 1), -E(nu, 2), -E(nu, 3));
-      Su2<T> eh = mul(dag(e), dag(h));
-      if (ANISO) eh = scale((mu == 0 || nu == 0) ? wt : ws, eh);
-      K[j] = mul_acc(K[j], eh, c);
-    }
-  }
-  const size_t V = (size_t)g.V, NL = 4 * V;
-  double k2 = 0.;
-#pragma unroll
-  for (int j = 0; j < 2; j++)
-    k2 += finish_link<T>(L(m0 + j, 0, 0, 0, 0), K[j], (m0 + j) * V + self, NL, P, extra, f,
-                         scale_, mode, Uout, dt_upd);
-  return k2;
-}
-
-template <class T, int BX, int BY, int BZ, int MINB>
-__global__ void __launch_bounds__(Brick<BX, BY, BZ>::NT, MINB)
-  k_force_su2_tile(Geom g, const LinkT<T> *__restrict__ U, T *__restrict__ P,
-                   const T *__restrict__ extra, T f, T scale_, int mode, int aniso, T wt, T ws,
-                   double *kin_part, LinkT<T> *__restrict__ Uout, T dt_upd) {
-  using B = Brick<BX, BY, BZ>;
-  constexpr int W = (int)(sizeof(LinkT<T>) / 16);
-  extern __shared__ float4 sm[];
-  __shared__ double sh[B::NT / 32];
-  // spatial part of every halo site of the brick: lexicographic offset within a time slice,
-  // parity of x+y+z in bit 31
-  int *soff = reinterpret_cast<int *>(sm + (size_t)4 * 4 * B::H * W);
-  const int tid = threadIdx.x;
-  const int half = tid / B::NS, sidx = tid % B::NS;
-  const int sx = sidx / (BY * BZ), sy = (sidx / BZ) % BY, sz = sidx % BZ;
-  const int hc = ((sx + 1) * B::HY + (sy + 1)) * B::HZ + (sz + 1);
-  const int LT = g.L[0], LX = g.L[1], LY = g.L[2], LZ = g.L[3];
-  const int V3 = LX * LY * LZ;
-  const int nbx = LX / BX, nby = LY / BY, nbz = LZ / BZ;
-  const long units = (long)nbx * nby * nbz * LT;
-  const long u0 = units * blockIdx.x / gridDim.x, u1 = units * (blockIdx.x + 1) / gridDim.x;
-  // copy time slice t of the brick (halo included) into ring slot sl
-  auto load = [&](int sl, int t) {
-    const int tb = t * V3;
-#pragma unroll 2
-    for (int i = tid; i < 4 * B::H * W; i += B::NT) {
-      const int part = i % W, hm = i / W;
-      const int mu = hm / B::H, h = hm % B::H;
-      const int so = soff[h];
-      const int lex = tb + (so & 0x7fffffff);
-      const int eo = ((t + (int)((unsigned)so >> 31)) & 1) * g.Vh + (lex >> 1);
-      tile::cp_async16(sm + ((size_t)(sl * 4 + mu) * B::H + h) * W + part,
-                       reinterpret_cast<const float4 *>(U + (size_t)mu * g.V + eo) + part);
-    }
-    asm volatile("cp.async.commit_group;\n" ::: "memory");
-  };
-  // ring: slot[0..2] hold t-1, t, t+1; slot[3] receives t+2 while t is computed
-  int slot[4] = {0, 1, 2, 3};
-  long cur_brick = -1;
-  double k2 = 0.;
-  for (long u = u0; u < u1; u++) {
-    const long brick = u / LT;
-    const int t = (int)(u % LT);
-    const int bz = (int)(brick % nbz), by = (int)((brick / nbz) % nby),
-              bx = (int)(brick / (nbz * nby));
-    const int x0 = bx * BX, y0 = by * BY, z0 = bz * BZ;
-    if (brick != cur_brick) {
-      tile::cp_async_wait_all();
-      __syncthreads();  // nothing in flight or being read before the table and ring restart
-      for (int h = tid; h < B::H; h += B::NT) {
-        const int hz = h % B::HZ, hy = (h / B::HZ) % B::HY, hx = h / (B::HZ * B::HY);
-        const int x = tile::wrap(x0 - 1 + hx, LX), y = tile::wrap(y0 - 1 + hy, LY),
-                  z = tile::wrap(z0 - 1 + hz, LZ);
-        soff[h] = ((x * LY + y) * LZ + z) | (int)((unsigned)((x + y + z) & 1) << 31);
-      }
-      __syncthreads();
-      slot[0] = 0;
-      slot[1] = 1;
-      slot[2] = 2;
-      slot[3] = 3;
-      load(slot[0], tile::wrap(t - 1, LT));
-      load(slot[1], t);
-      load(slot[2], tile::wrap(t + 1, LT));
-      cur_brick = brick;
-    }
-    load(slot[3], tile::wrap(t + 2, LT));            // prefetch, overlaps the compute of t
-    asm volatile("cp.async.wait_group 1;\n" ::: "memory");  // all but the prefetch landed
-    __syncthreads();
-    const int x = x0 + sx, y = y0 + sy, z = z0 + sz;
-    const int lex = t * V3 + (x * LY + y) * LZ + z;
-    const size_t self = (size_t)((t + x + y + z) & 1) * g.Vh + (lex >> 1);
-    if (half == 0)
-      k2 += aniso ? tile_site<T, BX, BY, BZ, 0, true>(g, sm, slot, hc, self, P, extra, f, scale_,
-                                                      mode, wt, ws, Uout, dt_upd)
-                  : tile_site<T, BX, BY, BZ, 0, false>(g, sm, slot, hc, self, P, extra, f,
-                                                       scale_, mode, wt, ws, Uout, dt_upd);
-    else
-      k2 += aniso ? tile_site<T, BX, BY, BZ, 1, true>(g, sm, slot, hc, self, P, extra, f, scale_,
-                                                      mode, wt, ws, Uout, dt_upd)
-                  : tile_site<T, BX, BY, BZ, 1, false>(g, sm, slot, hc, self, P, extra, f,
-                                                       scale_, mode, wt, ws, Uout, dt_upd);
-    __syncthreads();  // the slot of t-1 is free: it takes the prefetch of the next step
-    const int fr = slot[0];
-    slot[0] = slot[1];
-    slot[1] = slot[2];
-    slot[2] = slot[3];
-    slot[3] = fr;
-  }
-  tile::cp_async_wait_all();
-  if (mode & FM_KINETIC) {
-    const double r = block_sum<B::NT>(k2, sh);
-    if (threadIdx.x == 0) kin_part[blockIdx.x] = r;
-  }
-}
-
-template <class T, int BX, int BY, int BZ>
-bool tile_fits(const Geom &g) {
-  return g.nd == 4 && g.L[1] % BX == 0 && g.L[2] % BY == 0 && g.L[3] % BZ == 0;
-}
-
-// resident blocks of a tile kernel on this device (one wave), cached per instantiation
-template <class T, int BX, int BY, int BZ, int MINB> int tile_grid() {
-  static int grid = 0;
-  if (!grid) {
-    int per_sm = 0, dev = 0, sms = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_force_su2_tile<T, BX, BY, BZ, MINB>,
-                                                  Brick<BX, BY, BZ>::NT,
-                                                  tile_smem<T, BX, BY, BZ>());
-    grid = std::max(1, per_sm) * std::max(1, sms);
-  }
-  return grid;
-}
 
 template <int ND, int NT>
 __global__ void __launch_bounds__(NT)
@@ -650,6 +436,26 @@ cudaError_t reduce_final(const double *part, int nblocks, int ncomp, double *out
   return cudaGetLastError();
 }
 
+// the force step with two threads per site (d = 4): warps (4k, 4k+1) are the two halves of 32
+// sites of one parity, warps (4k+2, 4k+3) of the 32 sites of the other parity beside them
+template <class T, int NT, int MINB>
+__global__ void __launch_bounds__(NT, MINB)
+  k_force_su2_split(Geom g, const LinkT<T> *__restrict__ U, T *__restrict__ P,
+                    const T *__restrict__ extra, T f, T scale_, int mode, int aniso, T wt, T ws,
+                    double *kin_part, LinkT<T> *__restrict__ Uout, T dt_upd) {
+  __shared__ double sh[NT / 32];
+  const int w = threadIdx.x >> 5;
+  const int half = w & 1, p = (w >> 1) & 1;
+  const int cb = blockIdx.x * (NT / 4) + (w >> 2) * 32 + (threadIdx.x & 31);
+  double k2 = 0.;
+  if (cb < g.Vh)
+    k2 = force_half<T>(g, U, P, extra, f, scale_, mode, aniso, wt, ws, Uout, dt_upd, half, p, cb);
+  if (mode & FM_KINETIC) {
+    const double r = block_sum<NT>(k2, sh);
+    if (threadIdx.x == 0) kin_part[blockIdx.x] = r;
+  }
+}
+
 template <class T>
 cudaError_t force_update(const Geom &g, const void *U, int group, T *P, const T *extra, double f,
                          double scale, double xi, int mode, double *kin_part, int *nblocks,
@@ -684,17 +490,17 @@ cudaError_t force_update(const Geom &g, const void *U, int group, T *P, const T 
         break;                                                                             \
     }                                                                                      \
   } while (0)
-#define SU2B_FORCE_TILE(BX, BY, BZ, MB)                                                     \
+#define SU2B_FORCE_SPLIT(NTV, MB)                                                            \
   do {                                                                                     \
-    if (!tile_fits<T, BX, BY, BZ>(g)) {                                                    \
-      SU2B_FORCE_LAUNCH(128, 6);                                                           \
+    if (g.nd != 4) {                                                                       \
+      SU2B_FORCE_LAUNCH(128, 8);                                                           \
       break;                                                                               \
     }                                                                                      \
-    const int grid = tile_grid<T, BX, BY, BZ, MB>();                                       \
-    nb = grid;                                                                             \
-    k_force_su2_tile<T, BX, BY, BZ, MB>                                                    \
-      <<<grid, Brick<BX, BY, BZ>::NT, tile_smem<T, BX, BY, BZ>(), s>>>(                    \
-        g, u, P, extra, (T)f, (T)scale, mode, aniso, wt, ws, kin_part, uo, (T)dt_upd);     \
+    const dim3 grid(cdiv(g.Vh, NTV / 4));                                                  \
+    nb = grid.x;                                                                           \
+    k_force_su2_split<T, NTV, MB><<<grid, NTV, 0, s>>>(g, u, P, extra, (T)f, (T)scale, mode, \
+                                                       aniso, wt, ws, kin_part, uo,          \
+                                                       (T)dt_upd);                           \
   } while (0)
     switch (v) {
       case 0: SU2B_FORCE_LAUNCH(256, 4); break;
@@ -703,11 +509,11 @@ cudaError_t force_update(const Geom &g, const void *U, int group, T *P, const T 
       case 3: SU2B_FORCE_LAUNCH(128, 6); break;
       case 4: SU2B_FORCE_LAUNCH(256, 2); break;
       case 5: SU2B_FORCE_LAUNCH(256, 3); break;
-      case 6: SU2B_FORCE_TILE(4, 4, 8, (sizeof(T) == 4 ? 2 : 1)); break;
-      default: SU2B_FORCE_TILE(2, 4, 16, (sizeof(T) == 4 ? 2 : 1)); break;
+      case 6: SU2B_FORCE_SPLIT(128, 8); break;
+      default: SU2B_FORCE_SPLIT(256, 4); break;
     }
+#undef SU2B_FORCE_SPLIT
 #undef SU2B_FORCE_LAUNCH
-#undef SU2B_FORCE_TILE
     if (nblocks) *nblocks = nb;
   } else {
     if (sizeof(T) != 8) return cudaErrorNotSupported;
@@ -799,23 +605,6 @@ cudaError_t cond_restore(const Geom &g, void *U, const void *U_old, int group,
                                                               (const double *)U_old, flag);
   }
   return cudaGetLastError();
-}
-
-// raise the dynamic shared-memory limit of the tiled force kernels (once per process)
-template <class T> cudaError_t force_prepare_t() {
-  cudaError_t e = cudaFuncSetAttribute(k_force_su2_tile<T, 4, 4, 8, (sizeof(T) == 4 ? 2 : 1)>,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)tile_smem<T, 4, 4, 8>());
-  if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(k_force_su2_tile<T, 2, 4, 16, (sizeof(T) == 4 ? 2 : 1)>,
-                             cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)tile_smem<T, 2, 4, 16>());
-  return e;
-}
-cudaError_t force_prepare() {
-  cudaError_t e = force_prepare_t<float>();
-  if (e == cudaSuccess) e = force_prepare_t<double>();
-  return e;
 }
 
 #define INST(T)                                                                              \

@@ -116,6 +116,97 @@ __device__ __forceinline__ double force_site_impl(const Geom &g, const LinkT<T> 
   return k2;
 }
 
+// The same fused force step for half of a d = 4 site: links mu = 2 HALF and 2 HALF + 1.  Two
+// threads share a site, so each holds two staple sums instead of four and needs about half
+// the registers; the forward product A of the plane inside the half serves both of its links,
+// the four planes that cross the halves compute A in both threads (64 FMAs more per site).
+template <class T, int HALF, bool ANISO>
+__device__ __forceinline__ double force_half_impl(const Geom &g, const LinkT<T> *__restrict__ U,
+                                                  T *__restrict__ P,
+                                                  const T *__restrict__ extra, T f, T scale_,
+                                                  int mode, T wt, T ws,
+                                                  LinkT<T> *__restrict__ Uout, T dt_upd, int p,
+                                                  int cb) {
+  const Site s = site_from_eo(g, p, cb);
+  const size_t V = (size_t)g.V, NL = 4 * V;
+  int fo[4], bo[4];
+#pragma unroll
+  for (int d = 0; d < 4; d++) {
+    fo[d] = fwd(g, s, d);
+    bo[d] = bwd(g, s, d);
+  }
+  // link U_mu at the site displaced by o (components in {-1, 0, 1}, at most two nonzero)
+  auto L = [&](int mu, int o0, int o1, int o2, int o3) -> Su2<T> {
+    const int o[4] = {o0, o1, o2, o3};
+    int lex = s.lex, odd = 0;
+#pragma unroll
+    for (int d = 0; d < 4; d++) {
+      if (o[d] > 0) lex += fo[d];
+      if (o[d] < 0) lex += bo[d];
+      odd ^= (o[d] != 0);
+    }
+    return ld_link(U + (size_t)mu * V + eo_of(g, lex, p ^ odd));
+  };
+  auto E = [](int d, int k) { return d == k ? 1 : 0; };
+  constexpr int m0 = 2 * HALF, m1 = 2 * HALF + 1;
+  Su2<T> K[2] = {zero_su2<T>(), zero_su2<T>()};
+#pragma unroll
+  for (int j = 0; j < 2; j++) {
+    const int mu = m0 + j;
+#pragma unroll
+    for (int nu = 0; nu < 4; nu++) {
+      if (nu == mu) continue;
+      const bool both = (nu == m0 || nu == m1);
+      if (both && nu < mu) continue;
+      const Su2<T> a = L(nu, E(mu, 0), E(mu, 1), E(mu, 2), E(mu, 3));  // U_nu(x+mu)
+      const Su2<T> b = L(mu, E(nu, 0), E(nu, 1), E(nu, 2), E(nu, 3));  // U_mu(x+nu)
+      Su2<T> A = mul(a, dag(b));
+      if (ANISO) A = scale((mu == 0 || nu == 0) ? wt : ws, A);
+      K[j] = mul_acc(K[j], A, dag(L(nu, 0, 0, 0, 0)));
+      if (both) K[nu - m0] = mul_acc(K[nu - m0], dag(A), dag(L(mu, 0, 0, 0, 0)));
+    }
+  }
+#pragma unroll
+  for (int j = 0; j < 2; j++) {
+    const int mu = m0 + j;
+#pragma unroll
+    for (int nu = 0; nu < 4; nu++) {
+      if (nu == mu) continue;
+      const Su2<T> e = L(nu, E(mu, 0) - E(nu, 0), E(mu, 1) - E(nu, 1), E(mu, 2) - E(nu, 2),
+                         E(mu, 3) - E(nu, 3));                           // U_nu(x+mu-nu)
+      const Su2<T> h = L(mu, -E(nu, 0), -E(nu, 1), -E(nu, 2), -E(nu, 3));  // U_mu(x-nu)
+      const Su2<T> c = L(nu, -E(nu, 0), -E(nu, 1), -E(nu, 2), -E(nu, 3));  // U_nu(x-nu)
+      Su2<T> eh = mul(dag(e), dag(h));
+      if (ANISO) eh = scale((mu == 0 || nu == 0) ? wt : ws, eh);
+      K[j] = mul_acc(K[j], eh, c);
+    }
+  }
+  const size_t self = (size_t)p * g.Vh + cb;
+  double k2 = 0.;
+#pragma unroll
+  for (int j = 0; j < 2; j++)
+    k2 += finish_link<T>(L(m0 + j, 0, 0, 0, 0), K[j], (m0 + j) * V + self, NL, P, extra, f,
+                         scale_, mode, Uout, dt_upd);
+  return k2;
+}
+
+template <class T>
+__device__ __forceinline__ double force_half(const Geom &g, const LinkT<T> *__restrict__ U,
+                                             T *__restrict__ P, const T *__restrict__ extra, T f,
+                                             T scale_, int mode, int aniso, T wt, T ws,
+                                             LinkT<T> *__restrict__ Uout, T dt_upd, int half,
+                                             int p, int cb) {
+  if (half == 0)
+    return aniso ? force_half_impl<T, 0, true>(g, U, P, extra, f, scale_, mode, wt, ws, Uout,
+                                               dt_upd, p, cb)
+                 : force_half_impl<T, 0, false>(g, U, P, extra, f, scale_, mode, wt, ws, Uout,
+                                                dt_upd, p, cb);
+  return aniso ? force_half_impl<T, 1, true>(g, U, P, extra, f, scale_, mode, wt, ws, Uout,
+                                             dt_upd, p, cb)
+               : force_half_impl<T, 1, false>(g, U, P, extra, f, scale_, mode, wt, ws, Uout,
+                                              dt_upd, p, cb);
+}
+
 template <class T, int ND>
 __device__ __forceinline__ double force_site(const Geom &g, const LinkT<T> *__restrict__ U,
                                              T *__restrict__ P, const T *__restrict__ extra, T f,

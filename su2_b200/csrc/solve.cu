@@ -121,6 +121,25 @@ int cg64(su2b_ctx *ctx, double m, double tol, int max_iter, su2b_solve_stats *st
     SU2B_CK(cudaMemcpyAsync(p, r, n * sizeof(double2), cudaMemcpyDeviceToDevice, s));
     SU2B_CKS(upload_state(ctx, h));
     int done = h.done;
+    if (!done) {
+      // the whole solve in one cooperative launch (two grid barriers per iteration)
+      double *slot = ctx->part_slot(5);
+      void *bar = slot + 3 * ctx->part_cap - 4;
+      const cudaError_t e = cg_persistent(g, ctx->ph, m, x, r, p, t, slot, ctx->st, bar,
+                                          (int)(3 * ctx->part_cap - 8), s);
+      if (e != cudaErrorNotSupported) {
+        SU2B_CK(e);
+        ctx->launches++;
+        int failed = 0;
+        if (cg_barrier_failed(bar, s, &failed))
+          return su2b_fail(ctx, SU2B_ERR_CUDA, "persistent CG: %s",
+                           cudaGetErrorString(cudaGetLastError()));
+        if (failed)
+          return su2b_fail(ctx, SU2B_ERR_TIMEOUT, "persistent CG: a grid barrier gave up");
+        SU2B_CKS(fetch_state(ctx));
+        done = ctx->h_st->done;
+      }
+    }
     while (!done) {
       for (int k = 0; k < CHUNK; k++) {
         SU2B_LAUNCH(SU2B_K_STAGGERED, hop64(g, ctx->ph, m, 1, p, t, nullptr, nullptr, nullptr, ctx->st, 0, s));

@@ -55,6 +55,12 @@ cudaError_t m_resid(int n, const double2 *b, const double2 *Ax, double2 *r, floa
 cudaError_t m_after(const double *part, int n, SolverState *st, cudaStream_t s);
 cudaError_t m_p(int n, const float2 *rs, float2 *ps, SolverState *st, cudaStream_t s);
 
+cudaError_t cg_persistent(const Geom &g, const double2 *ph, double m, double2 *x, double2 *r,
+                          double2 *p, double2 *t, double *part, SolverState *st, void *bar_mem,
+                          int part_cap, cudaStream_t s);
+int cg_barrier_failed(const void *bar_mem, cudaStream_t s, int *failed);
+size_t cg_barrier_bytes();
+
 cudaError_t resid64(int n, const double2 *b, const double2 *Ax, double2 *r, double *part,
                     cudaStream_t s);
 cudaError_t to32(int n, const double2 *a, float2 *b, cudaStream_t s);

@@ -228,6 +228,178 @@ __global__ void k_cg_p(int n, const double2 *__restrict__ r, double2 *__restrict
   }
 }
 
+// ---- persistent CG on D D^+ (one cooperative launch for the whole solve) ----
+//
+// For small lattices every CG iteration is a handful of microsecond-long kernels and the
+// launches dominate.  This kernel keeps all blocks resident (cooperative launch: the runtime
+// refuses the launch unless every block can be resident at once) and separates the phases by
+// a grid barrier.  It uses D D^+ = A with <p, A p> = |D^+ p|^2 and, by linearity,
+// D^+ p_new = D^+ r + beta D^+ p, so one iteration needs two barriers:
+//   [t = D^+ p held]  alpha = rr / |t|^2;  Ap = D t;  x += alpha p;  r -= alpha Ap   | barrier
+//   beta = |r|^2 / rr;  p = r + beta p;  t = D^+ r + beta t                         | barrier
+// The scalars follow CG.hpp:51-64 in FP64 (complex alpha/beta with zero imaginary parts).
+// Every block reduces the per-block partials itself in one fixed order, so all blocks take
+// the same decisions and leave the loop together.  Barrier waits are bounded: a wait that
+// gives up sets *err and every block returns.
+__device__ __forceinline__ double2 hop_site64(const Geom &g, const double2 *__restrict__ ph,
+                                              double m, double sgn,
+                                              const double2 *__restrict__ in, int p, int cb) {
+  const Site s = site_from_eo(g, p, cb);
+  double accr = 0, acci = 0;
+  int esum = 0;
+  for (int mu = 0; mu < g.nd; mu++) {
+    const double eta = (esum & 1) ? -0.5 : 0.5;
+    esum += s.c[mu];
+    const int lp = s.lex + fwd(g, s, mu), lm = s.lex + bwd(g, s, mu);
+    const double2 up = ph[(size_t)mu * g.V + (size_t)p * g.Vh + cb];
+    const double2 um = ph[(size_t)mu * g.V + eo_of(g, lm, 1 - p)];
+    // neighbours belong to other blocks and change every iteration: read through L2 only
+    // (the SM's L1 is not coherent with the other SMs' stores)
+    const double2 fp = __ldcg(&in[eo_of(g, lp, 1 - p)]), fm = __ldcg(&in[eo_of(g, lm, 1 - p)]);
+    const double tr = (up.x * fp.x - up.y * fp.y) - (um.x * fm.x + um.y * fm.y);
+    const double ti = (up.x * fp.y + up.y * fp.x) - (um.x * fm.y - um.y * fm.x);
+    accr += eta * tr;
+    acci += eta * ti;
+  }
+  const double2 self = __ldcg(&in[(size_t)p * g.Vh + cb]);
+  return make_double2(m * self.x + sgn * accr, m * self.y + sgn * acci);
+}
+
+struct GridBarrier {
+  unsigned count;
+  unsigned gen;
+  int err;
+};
+
+constexpr long BARRIER_SPIN_LIMIT = 1L << 24;  // x >= 32 ns: gives up after about a second
+
+__device__ __forceinline__ bool grid_sync(GridBarrier *b) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    volatile unsigned *gen = &b->gen;
+    volatile int *err = &b->err;
+    const unsigned g0 = *gen;
+    __threadfence();
+    if (atomicAdd(&b->count, 1u) == gridDim.x - 1) {
+      b->count = 0;
+      __threadfence();
+      atomicAdd(&b->gen, 1u);
+    } else {
+      long spins = 0;
+      while (*gen == g0 && *err == 0) {
+        if (++spins > BARRIER_SPIN_LIMIT) {
+          atomicExch(&b->err, 1);
+          break;
+        }
+        __nanosleep(32);
+      }
+    }
+    __threadfence();
+  }
+  __syncthreads();
+  return *(volatile int *)&b->err == 0;
+}
+
+// sum of part[0..n) in one fixed order (lane-strided, then a fixed warp tree), by warp 0;
+// the result is broadcast through shared memory
+// (n <= 32 * FIXED_SUM_PER_LANE; all loads are issued before the first add, so the sum costs
+// one L2 round trip)
+constexpr int FIXED_SUM_PER_LANE = 16;
+template <int NT> __device__ __forceinline__ double fixed_sum(const double *part, int n) {
+  __shared__ double bc;
+  if (threadIdx.x < 32) {
+    double v[FIXED_SUM_PER_LANE];
+#pragma unroll
+    for (int k = 0; k < FIXED_SUM_PER_LANE; k++) {
+      const int i = threadIdx.x + 32 * k;
+      v[k] = i < n ? __ldcg(&part[i]) : 0.0;
+    }
+    double a = 0.;
+#pragma unroll
+    for (int k = 0; k < FIXED_SUM_PER_LANE; k++) a += v[k];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
+    if (threadIdx.x == 0) bc = a;
+  }
+  __syncthreads();
+  const double r = bc;
+  __syncthreads();
+  return r;
+}
+
+template <int NT>
+__global__ void __launch_bounds__(NT)
+  k_cg_persistent(Geom g, const double2 *__restrict__ ph, double m, double2 *x, double2 *r,
+                  double2 *p, double2 *t, double *part_t, double *part_r, SolverState *st,
+                  GridBarrier *bar) {
+  __shared__ double sh[NT / 32];
+  const int n = g.V, G = gridDim.x;
+  const int first = blockIdx.x * NT + threadIdx.x, stride = G * NT;
+  double2 rr = st->rr;
+  double rn = st->rn;
+  long iters = st->iters;
+  const long max_iter = st->max_iter;
+  const double tol = st->tol;
+  int done = st->done;
+  // t = D^+ p, |t|^2
+  double acc = 0.;
+  for (int i = first; i < n; i += stride) {
+    const int pp = i >= g.Vh, cb = i - pp * g.Vh;
+    const double2 v = hop_site64(g, ph, m, -1.0, p, pp, cb);
+    t[i] = v;
+    acc += v.x * v.x + v.y * v.y;
+  }
+  double bs = block_sum<NT>(acc, sh);
+  if (threadIdx.x == 0) part_t[blockIdx.x] = bs;
+  if (!grid_sync(bar)) return;
+  while (!done) {
+    const double2 alpha = cdivs(rr, make_double2(fixed_sum<NT>(part_t, G), 0.0));
+    acc = 0.;
+    for (int i = first; i < n; i += stride) {
+      const int pp = i >= g.Vh, cb = i - pp * g.Vh;
+      const double2 ap = hop_site64(g, ph, m, 1.0, t, pp, cb);  // A p = D t
+      const double2 pv = p[i], xv = x[i], rv = r[i];
+      const double2 a1 = cm(alpha, pv), a2 = cm(alpha, ap);
+      x[i] = make_double2(xv.x + a1.x, xv.y + a1.y);
+      const double2 rnw = make_double2(rv.x - a2.x, rv.y - a2.y);
+      r[i] = rnw;
+      acc += rnw.x * rnw.x + rnw.y * rnw.y;
+    }
+    bs = block_sum<NT>(acc, sh);
+    if (threadIdx.x == 0) part_r[blockIdx.x] = bs;
+    if (!grid_sync(bar)) return;
+    const double rr_new = fixed_sum<NT>(part_r, G);
+    const double2 beta = cdivs(make_double2(rr_new, 0.0), rr);
+    rr = make_double2(rr_new, 0.0);
+    rn = sqrt(rr_new);
+    iters++;
+    if (rn != rn) done = 3;
+    else if (!(rn > tol)) done = 1;
+    else if (iters >= max_iter) done = 2;
+    if (done) break;
+    acc = 0.;
+    for (int i = first; i < n; i += stride) {
+      const int pp = i >= g.Vh, cb = i - pp * g.Vh;
+      const double2 dr = hop_site64(g, ph, m, -1.0, r, pp, cb);  // D^+ r
+      const double2 rv = r[i], pv = p[i], tv = t[i];
+      const double2 bp = cm(beta, pv), bt = cm(beta, tv);
+      p[i] = make_double2(rv.x + bp.x, rv.y + bp.y);
+      const double2 tn = make_double2(dr.x + bt.x, dr.y + bt.y);
+      t[i] = tn;
+      acc += tn.x * tn.x + tn.y * tn.y;
+    }
+    bs = block_sum<NT>(acc, sh);
+    if (threadIdx.x == 0) part_t[blockIdx.x] = bs;
+    if (!grid_sync(bar)) return;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    st->rr = rr;
+    st->rn = rn;
+    st->iters = iters;
+    st->done = done;
+  }
+}
+
 // ---- BiCGStab ----
 template <int NT> __global__ void k_bi_alpha(const double *part, int n, SolverState *st) {
   if (finished(st)) return;
@@ -596,5 +768,46 @@ cudaError_t dot64(int n, const double2 *a, const double2 *b, double *part, cudaS
   k_dot64<NT_V><<<vec_blocks(n), NT_V, 0, s>>>(n, a, b, part);
   return cudaGetLastError();
 }
+
+// the persistent CG: one cooperative launch until convergence or the iteration limit;
+// returns cudaErrorNotSupported where cooperative launches are unavailable (the caller then
+// queues the per-phase kernels) and cudaErrorTimeout when a barrier wait gave up
+cudaError_t cg_persistent(const Geom &g, const double2 *ph, double m, double2 *x, double2 *r,
+                          double2 *p, double2 *t, double *part, SolverState *st, void *bar_mem,
+                          int part_cap, cudaStream_t s) {
+  // one block of 512 threads per SM: the fewer blocks arrive at a barrier, the shorter it is
+  constexpr int NT = 512;
+  static int grid = -1;
+  if (grid < 0) {
+    int dev = 0, coop = 0, sms = 0, per_sm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_cg_persistent<NT>, NT, 0);
+    grid = (coop && per_sm >= 1) ? sms : 0;
+  }
+  const int G = std::min(grid, std::max(1, (g.V + NT - 1) / NT));
+  if (G <= 0 || 2 * G > part_cap || G > 32 * FIXED_SUM_PER_LANE) return cudaErrorNotSupported;
+  GridBarrier *bar = (GridBarrier *)bar_mem;
+  cudaError_t e = cudaMemsetAsync(bar, 0, sizeof(GridBarrier), s);
+  if (e != cudaSuccess) return e;
+  double *part_t = part, *part_r = part + G;
+  Geom gg = g;
+  double mm = m;
+  void *args[] = {&gg, (void *)&ph, &mm, &x, &r, &p, &t, &part_t, &part_r, &st, &bar};
+  e = cudaLaunchCooperativeKernel((const void *)k_cg_persistent<NT>, dim3(G), dim3(NT), args, 0,
+                                  s);
+  return e;
+}
+
+int cg_barrier_failed(const void *bar_mem, cudaStream_t s, int *failed) {
+  GridBarrier h{};
+  if (cudaMemcpyAsync(&h, bar_mem, sizeof h, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+      cudaStreamSynchronize(s) != cudaSuccess)
+    return 1;
+  *failed = h.err;
+  return 0;
+}
+size_t cg_barrier_bytes() { return sizeof(GridBarrier); }
 
 }  // namespace su2b

@@ -157,10 +157,16 @@ class gaugeconfig:
         assert U.size == self.n_links * self.link_reals
         self._c(self.lib.su2b_upload_gauge(self.ctx, _dp(U)))
 
-    def download(self) -> np.ndarray:
-        U = np.empty(self.n_links * self.link_reals)
-        self._c(self.lib.su2b_download_gauge(self.ctx, _dp(U)))
-        return U
+    def download(self, out=None) -> np.ndarray:
+        """The links in the reference's host layout.  out: a C-contiguous float64 buffer of
+        the right size to write into (pinned memory makes the copy a direct DMA)."""
+        n = self.n_links * self.link_reals
+        if out is None:
+            out = np.empty(n)
+        elif out.dtype != np.float64 or out.size != n or not out.flags.c_contiguous:
+            raise ValueError(f"out must be a contiguous float64 array of {n} elements")
+        self._c(self.lib.su2b_download_gauge(self.ctx, _dp(out)))
+        return out
 
     # ---- reductions ----
     def gauge_energy(self, spatial_only=False) -> float:

@@ -314,9 +314,9 @@ def test_rejected_trajectory_keeps_start_field(gpu, orc):
 @pytest.mark.parametrize("dims", [(8, 6, 4, 8), (4, 4, 8, 4), (8, 8, 16, 6)],
                          ids=["8x6x4x8", "4x4x8x4", "8x8x16x6"])
 def test_every_force_launch_shape_is_exact(gpu, orc, precision, dims):
-    """Every launch shape, including the shared-memory brick kernels (which need extents
-    divisible by the brick: 4x4x8 takes the second and third lattice, 2x4x16 the third; the
-    others fall back to the gather kernel), gives the oracle's force and a finite trajectory."""
+    """Every launch shape of the force kernel (threads per block x register cap, including
+    the register-starved ones that spill) gives the oracle's force and a finite trajectory,
+    on lattices whose half volume is and is not a multiple of the block's sites."""
     group, nd = 0, 4
     U = hot(orc, group, dims, nd)
     F = orc.gauge_derivative(group, dims, nd, 2.3, U)
