@@ -238,6 +238,16 @@ SU2B_API int su2b_batch_autotune(su2b_batch *b, double *times_us);
 SU2B_API int su2b_batch_tune_get(su2b_batch *b, int *variant);
 SU2B_API int su2b_batch_tune_set(su2b_batch *b, int variant);
 
+/* ---- observables between trajectories ---------------------------------------------------- */
+/* polyakov_loop_spatial_average (polyakov_loop.hh:48-63): sum over spatial points of ReTr of
+ * the product of the temporal links, divided by the full volume as the reference does. */
+SU2B_API int su2b_polyakov_loop(su2b_ctx *ctx, double *out);
+/* wilsonloop(U, r, t) (wilsonloop.hh:147-157): r x t planar loops in the (mu, 0) planes,
+ * mu >= 1, summed over sites, divided by V Nc ndims. */
+SU2B_API int su2b_wilson_loop(su2b_ctx *ctx, int r, int t, double *out);
+/* APEsmearing(U, alpha, spatial) (smearape.hh:97-131) of the context's links, in place. */
+SU2B_API int su2b_ape_smear(su2b_ctx *ctx, double alpha, int spatial);
+
 /* ---- derivatives (SU(2)) ------------------------------------------------------------------ */
 /* Left Lie-algebra derivatives, the convention of gaugemonomial::derivative
  * (flat-gaugemonomial.hh:105-131): grad(x,mu)_k = d/dw O(exp(w e_k) U_mu(x)) at w = 0 with

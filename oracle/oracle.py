@@ -31,6 +31,9 @@ _SIGS = {
     "random_gauge_trafo": (None, _G + [i32, _D]),
     "retr_sum_plaquettes": (f64, _G + [_D, f64, i32, i32]),
     "gauge_energy": (f64, _G + [_D, i32]),
+    "polyakov_loop": (f64, _G + [_D]),
+    "wilson_loop": (f64, _G + [_D, i32, i32]),
+    "ape_smear": (None, _G + [f64, i32, _D]),
     "S_G_hmc": (f64, _G + [f64, _D, f64, i32]),
     "gauge_derivative": (None, _G + [f64, f64, _D, f64, _D]),
     "md_injected": (f64, _G + [f64, f64, i32, i32, f64, _D, _D, _D]),
@@ -127,6 +130,17 @@ class Oracle:
 
     def gauge_energy(self, group, dims, nd, U, spatial_only=False):
         return self._gauge_energy(group, *dims, nd, dp(U), int(spatial_only))
+
+    def polyakov_loop(self, group, dims, nd, U):
+        return self._polyakov_loop(group, *dims, nd, dp(U))
+
+    def wilson_loop(self, group, dims, nd, U, r, t):
+        return self._wilson_loop(group, *dims, nd, dp(U), r, t)
+
+    def ape_smear(self, group, dims, nd, U, alpha, spatial=True):
+        U = np.ascontiguousarray(U, dtype=np.float64).copy()
+        self._ape_smear(group, *dims, nd, alpha, int(spatial), dp(U))
+        return U
 
     def S_G_hmc(self, group, dims, nd, beta, U, xi=1.0, aniso=False):
         return self._S_G_hmc(group, *dims, nd, beta, dp(U), xi, int(aniso))

@@ -27,6 +27,9 @@
 #include "monomial.hh"
 #include "random_gauge_trafo.hh"
 #include "staggered.hpp"
+#include "polyakov_loop.hh"
+#include "smearape.hh"
+#include "wilsonloop.hh"
 
 #ifdef _USE_OMP_
 #include <omp.h>
@@ -510,4 +513,39 @@ void ref_gaussian_spinor(int Lx, int Ly, int Lz, int Lt, double avr, double sigm
              out);
 }
 
+
+// ---- observables between trajectories -------------------------------------------------
+// polyakov_loop_spatial_average (polyakov_loop.hh:48-63)
+double ref_polyakov_loop(int group, int Lx, int Ly, int Lz, int Lt, int nd, const double *in) {
+  double r = 0.;
+  DISPATCH(group, {
+    gaugeconfig<G> U(Lx, Ly, Lz, Lt, nd, 0.);
+    io<G>::put(U, in);
+    r = polyakov_loop_spatial_average(U);
+  });
+  return r;
+}
+
+// wilsonloop(U, r, t) (wilsonloop.hh:147-157): planar r x t loops in the (mu, 0) planes
+double ref_wilson_loop(int group, int Lx, int Ly, int Lz, int Lt, int nd, const double *in,
+                       int r, int t) {
+  double w = 0.;
+  DISPATCH(group, {
+    gaugeconfig<G> U(Lx, Ly, Lz, Lt, nd, 0.);
+    io<G>::put(U, in);
+    w = wilsonloop(U, (size_t)r, (size_t)t);
+  });
+  return w;
+}
+
+// APEsmearing<double>(U, alpha, spatial) (smearape.hh:97-131), in place
+void ref_ape_smear(int group, int Lx, int Ly, int Lz, int Lt, int nd, double alpha, int spatial,
+                   double *inout) {
+  DISPATCH(group, {
+    gaugeconfig<G> U(Lx, Ly, Lz, Lt, nd, 0.);
+    io<G>::put(U, inout);
+    APEsmearing<double, G>(U, alpha, bool(spatial));
+    io<G>::get(U, inout);
+  });
+}
 } // extern "C"

@@ -559,6 +559,163 @@ void orc_update_gauge(int group, int Lx, int Ly, int Lz, int Lt, int nd, double 
 /* ===================================================================================== */
 
 /* staggered.hpp:41-48 */
+/* ===================================================================================== */
+/* observables between trajectories                                                      */
+/* ===================================================================================== */
+
+/* exp(i a) as std::exp(a * Complex(0., 1.)) evaluates it: (e^0 cos a, e^0 sin a) */
+static inline cplx u1_phase(double a) { return C(cos(a), sin(a)); }
+
+/* polyakov_loop_spatial_average (polyakov_loop.hh:26-63): the product of the temporal links
+ * along t at every spatial point, ReTr, summed and divided by the full volume */
+double orc_polyakov_loop(int group, int Lx, int Ly, int Lz, int Lt, int nd, const double *U) {
+  const lat_t l = mklat(Lx, Ly, Lz, Lt, nd);
+  double ploop = 0.;
+  for (long x1 = 0; x1 < l.L[1]; x1++)
+    for (long x2 = 0; x2 < l.L[2]; x2++)
+      for (long x3 = 0; x3 < l.L[3]; x3++) {
+        long c[4] = {0, x1, x2, x3};
+        if (group == 0) {
+          su2 P;
+          P.a = C(1., 0.);
+          P.b = C(0., 0.);
+          for (c[0] = 0; c[0] < l.L[0]; c[0]++) P = smul(P, sload(U, link(&l, c, 0)));
+          ploop += sretr(P);
+        } else {
+          cplx P = C(1., 0.);
+          for (c[0] = 0; c[0] < l.L[0]; c[0]++) P = cmul(P, u1_phase(U[link(&l, c, 0)]));
+          ploop += P.r;
+        }
+      }
+  return ploop / (double)l.V;
+}
+
+/* planar_wilsonloop_dir (wilsonloop.hh:51-91): sum over sites of ReTr of the r x t loop
+ * x -> x + t nu -> + r mu -> - t nu -> - r mu */
+static double planar_loop_dir(int group, const lat_t *l, const double *U, long r, long t,
+                              int mu, int nu) {
+  double loop = 0.;
+  for (size_t s = 0; s < l->V; s++) {
+    long x[4];
+    coords(l, s, x);
+    if (group == 0) {
+      su2 L;
+      L.a = C(1., 0.);
+      L.b = C(0., 0.);
+      for (long k = 0; k < t; k++) {
+        L = smul(L, sload(U, link(l, x, nu)));
+        x[nu] += 1;
+      }
+      for (long k = 0; k < r; k++) {
+        L = smul(L, sload(U, link(l, x, mu)));
+        x[mu] += 1;
+      }
+      for (long k = 0; k < t; k++) {
+        x[nu] -= 1;
+        L = smul(L, sdag(sload(U, link(l, x, nu))));
+      }
+      for (long k = 0; k < r; k++) {
+        x[mu] -= 1;
+        L = smul(L, sdag(sload(U, link(l, x, mu))));
+      }
+      loop += sretr(L);
+    } else {
+      cplx L = C(1., 0.);
+      for (long k = 0; k < t; k++) {
+        L = cmul(L, u1_phase(U[link(l, x, nu)]));
+        x[nu] += 1;
+      }
+      for (long k = 0; k < r; k++) {
+        L = cmul(L, u1_phase(U[link(l, x, mu)]));
+        x[mu] += 1;
+      }
+      for (long k = 0; k < t; k++) {
+        x[nu] -= 1;
+        L = cmul(L, u1_phase(-U[link(l, x, nu)]));
+      }
+      for (long k = 0; k < r; k++) {
+        x[mu] -= 1;
+        L = cmul(L, u1_phase(-U[link(l, x, mu)]));
+      }
+      loop += L.r;
+    }
+  }
+  return loop;
+}
+
+/* wilsonloop(U, r, t) (wilsonloop.hh:147-157): planar loops in the (mu, 0) planes, mu >= 1,
+ * normalised by V Nc ndims */
+double orc_wilson_loop(int group, int Lx, int Ly, int Lz, int Lt, int nd, const double *U,
+                       int r, int t) {
+  const lat_t l = mklat(Lx, Ly, Lz, Lt, nd);
+  double loop = 0.;
+  for (int mu = 1; mu < nd; mu++) loop += planar_loop_dir(group, &l, U, r, t, mu, 0);
+  const double Nc = group == 0 ? 2. : 1.;
+  return loop / (double)l.V / Nc / (double)nd;
+}
+
+/* APEsmearing<double>(U, alpha, spatial) (smearape.hh:97-131) with the staples of
+ * get_staples_APE (get_staples.hh:89-110):
+ *   K = sum_{nu != i} U_nu(x) U_i(x+nu) U_nu(x+i)^+ + U_nu(x-nu)^+ U_i(x-nu) U_nu(x+i-nu)
+ *   U_i(x) <- restoreSU(alpha U_i(x) + beta K),  beta = (1 - alpha) / (2 (d - 1 - start))
+ * over nu >= start, for the links i >= start (start = 1 for spatial smearing) */
+void orc_ape_smear(int group, int Lx, int Ly, int Lz, int Lt, int nd, double alpha,
+                   int spatial, double *U) {
+  const lat_t l = mklat(Lx, Ly, Lz, Lt, nd);
+  const size_t n = nlinks(&l) * (group == 0 ? 4 : 1);
+  double *Uold = (double *)malloc(n * sizeof(double));
+  memcpy(Uold, U, n * sizeof(double));
+  const int start = spatial ? 1 : 0;
+  const double beta = (1.0 - alpha) / ((double)(2 * (nd - 1 - start)));
+  for (size_t s = 0; s < l.V; s++) {
+    long x[4];
+    coords(&l, s, x);
+    for (int i = start; i < nd; i++) {
+      long xi[4] = {x[0], x[1], x[2], x[3]};
+      xi[i] += 1;
+      if (group == 0) {
+        su2 K;
+        K.a = C(0., 0.);
+        K.b = C(0., 0.);
+        for (int nu = start; nu < nd; nu++) {
+          if (nu == i) continue;
+          long xn[4] = {x[0], x[1], x[2], x[3]}, xmn[4] = {x[0], x[1], x[2], x[3]},
+               ximn[4] = {xi[0], xi[1], xi[2], xi[3]};
+          xn[nu] += 1;
+          xmn[nu] -= 1;
+          ximn[nu] -= 1;
+          K = sadd(K, smul(smul(sload(Uold, link(&l, x, nu)), sload(Uold, link(&l, xn, i))),
+                           sdag(sload(Uold, link(&l, xi, nu)))));
+          K = sadd(K, smul(smul(sdag(sload(Uold, link(&l, xmn, nu))),
+                                sload(Uold, link(&l, xmn, i))),
+                           sload(Uold, link(&l, ximn, nu))));
+        }
+        const su2 up = sadd(sscale(alpha, sload(Uold, link(&l, x, i))), sscale(beta, K));
+        sstore(U, link(&l, x, i), srestore(up));
+      } else {
+        cplx K = C(0., 0.);
+        for (int nu = start; nu < nd; nu++) {
+          if (nu == i) continue;
+          long xn[4] = {x[0], x[1], x[2], x[3]}, xmn[4] = {x[0], x[1], x[2], x[3]},
+               ximn[4] = {xi[0], xi[1], xi[2], xi[3]};
+          xn[nu] += 1;
+          xmn[nu] -= 1;
+          ximn[nu] -= 1;
+          /* _u1 products are angle sums; K += exp(i angle) */
+          K = cadd(K, u1_phase((Uold[link(&l, x, nu)] + Uold[link(&l, xn, i)]) +
+                               (-Uold[link(&l, xi, nu)])));
+          K = cadd(K, u1_phase(((-Uold[link(&l, xmn, nu)]) + Uold[link(&l, xmn, i)]) +
+                               Uold[link(&l, ximn, nu)]));
+        }
+        const cplx up = cadd(cmul(C(alpha, 0.), u1_phase(Uold[link(&l, x, i)])),
+                             cmul(C(beta, 0.), K));
+        U[link(&l, x, i)] = atan2(up.i, up.r);
+      }
+    }
+  }
+  free(Uold);
+}
+
 double orc_eta(int t, int x, int y, int z, int mu) {
   const int c[4] = {t, x, y, z};
   double s = 0;

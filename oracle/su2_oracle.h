@@ -113,4 +113,9 @@ void orc_metropolis_checkerboard(int group, int Lx, int Ly, int Lz, int Lt, int 
 #ifdef __cplusplus
 }
 #endif
+double orc_polyakov_loop(int group, int Lx, int Ly, int Lz, int Lt, int nd, const double *U);
+double orc_wilson_loop(int group, int Lx, int Ly, int Lz, int Lt, int nd, const double *U,
+                       int r, int t);
+void orc_ape_smear(int group, int Lx, int Ly, int Lz, int Lt, int nd, double alpha,
+                   int spatial, double *U);
 #endif

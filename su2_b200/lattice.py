@@ -190,6 +190,23 @@ class gaugeconfig:
                                              C.byref(Q)))
         return E.value, Q.value
 
+    # ---- observables between trajectories ----
+    def polyakov_loop_spatial_average(self) -> float:
+        """polyakov_loop.hh:48-63 (normalised by the full volume, as the reference)."""
+        out = C.c_double()
+        self._c(self.lib.su2b_polyakov_loop(self.ctx, C.byref(out)))
+        return out.value
+
+    def wilsonloop(self, r, t) -> float:
+        """Planar r x t Wilson loops averaged over the (mu, 0) planes (wilsonloop.hh:147-157)."""
+        out = C.c_double()
+        self._c(self.lib.su2b_wilson_loop(self.ctx, int(r), int(t), C.byref(out)))
+        return out.value
+
+    def APEsmearing(self, alpha, spatial=True):
+        """APE smearing of the links in place (smearape.hh:97-131)."""
+        self._c(self.lib.su2b_ape_smear(self.ctx, alpha, int(spatial)))
+
     # ---- force / updates ----
     def derivative(self, fac=1.0) -> np.ndarray:
         out = np.empty(self.n_links * self.adj_reals)

@@ -12,7 +12,9 @@ Cases (all FP64, small enough that the file stays a few hundred KB):
           derivative at beta 2.4 (flat-gaugemonomial.hh:105-131), one RK3 flow step eps 0.01
           (flat-gradient_flow.hh:17-50), clover E and Q (flat-energy_density.hh:57-164),
           flow records to t = 0.05, and leapfrog (n 10) / omf2 (n 4) trajectories with
-          injected momenta (md_update.hh:18-81 with the momenta given).
+          injected momenta (md_update.hh:18-81 with the momenta given); the Polyakov loop
+          (polyakov_loop.hh:48-63), the 2x3 Wilson loop (wilsonloop.hh:147-157) and spatial
+          APE smearing at alpha 0.6 (smearape.hh:97-131).
   su2d3_* SU(2) d=3 4x4x1x6: plaquette sums and the gauge derivative at beta 2.0.
   u1_*    U(1) d=2 8x1x1x8 hot start: plaquette sum, gauge derivative at beta 4.0, D D^+ psi
           at m 0.05 (staggered.hpp:290-389), the CG solve of D D^+ x = psi (CG.hpp:36-94)
@@ -50,6 +52,9 @@ def main():
     g["su2_E"], g["su2_Q"] = np.array(E), np.array(Q)
     g["su2_flow_rows"] = np.asarray(r.gradient_flow_rows(0, dims, nd, 2.4, U, 0.05, 0.01),
                                     dtype=np.float64)
+    g["su2_polyakov"] = np.array(r.polyakov_loop(0, dims, nd, U))
+    g["su2_wilson_2_3"] = np.array(r.wilson_loop(0, dims, nd, U, 2, 3))
+    g["su2_ape_0.6"] = r.ape_smear(0, dims, nd, U, 0.6, True)
     P = np.random.default_rng(31).normal(size=O.Oracle.nlinks(dims, nd) * 3)
     g["su2_P"] = P
     for name, integ, n in (("leapfrog", 0, 10), ("omf2", 6, 4)):

@@ -207,6 +207,25 @@ def test_metropolis_statistics_match_reference(orc, ref):
     assert abs(np.mean(a) - np.mean(b)) < err + 0.01
 
 
+# ---------------------------------------------------------------- observables
+@pytest.mark.parametrize("group,dims,nd", [(0, (4, 4, 4, 6), 4), (0, (4, 6, 1, 4), 3),
+                                           (1, (4, 4, 4, 4), 4), (1, (8, 1, 1, 6), 2)])
+def test_pin_observables(orc, ref, group, dims, nd):
+    """Polyakov loop, planar Wilson loops and APE smearing against the reference's own
+    polyakov_loop_spatial_average, wilsonloop and APEsmearing.  The reference sums the loops
+    in OpenMP reductions, whose order moves the last bit with the thread count: 1e-13."""
+    U = ref.hotstart(group, dims, nd, 321, 1.0, 654321)
+    assert orc.polyakov_loop(group, dims, nd, U) == pytest.approx(
+        ref.polyakov_loop(group, dims, nd, U), rel=1e-13, abs=1e-15)
+    for r, t in ((1, 1), (2, 3), (3, 2)):
+        assert orc.wilson_loop(group, dims, nd, U, r, t) == pytest.approx(
+            ref.wilson_loop(group, dims, nd, U, r, t), rel=1e-13, abs=1e-15)
+    if nd > 2:
+        for spatial in (True, False):
+            assert np.array_equal(orc.ape_smear(group, dims, nd, U, 0.6, spatial),
+                                  ref.ape_smear(group, dims, nd, U, 0.6, spatial))
+
+
 # ---------------------------------------------------------------- golden fixtures
 def test_golden_fixtures(orc):
     """The restatement against vectors the reference itself produced (make_golden.py)."""
@@ -237,6 +256,11 @@ def test_golden_fixtures(orc):
     assert np.array_equal(orc.hotstart(0, d3, 3, 4711, 1.0, 99), U3)
     assert orc.gauge_energy(0, d3, 3, U3) == pytest.approx(float(g["su2d3_plaq"]), rel=1e-13)
     assert np.array_equal(orc.gauge_derivative(0, d3, 3, 2.0, U3), g["su2d3_force"])
+    assert orc.polyakov_loop(0, dims, nd, U) == pytest.approx(float(g["su2_polyakov"]),
+                                                               rel=1e-13, abs=1e-15)
+    assert orc.wilson_loop(0, dims, nd, U, 2, 3) == pytest.approx(float(g["su2_wilson_2_3"]),
+                                                                  rel=1e-13, abs=1e-15)
+    assert np.array_equal(orc.ape_smear(0, dims, nd, U, 0.6, True), g["su2_ape_0.6"])
     Uu = g["u1_U"]
     du = tuple(int(v) for v in g["u1_dims"])
     assert np.array_equal(orc.hotstart(1, du, 2, 13526463, 1.0, 654321), Uu)
