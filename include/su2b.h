@@ -238,6 +238,15 @@ SU2B_API int su2b_batch_autotune(su2b_batch *b, double *times_us);
 SU2B_API int su2b_batch_tune_get(su2b_batch *b, int *variant);
 SU2B_API int su2b_batch_tune_set(su2b_batch *b, int variant);
 
+/* ---- gauge configurations on disk ------------------------------------------------------- */
+/* gaugeconfig<G>::save / load (gaugeconfig.hh:225-252): the reference's raw binary format, one
+ * in-memory _su2 (40 bytes: size_t N_c = 2, then Re a, Im a, Re b, Im b) or _u1 (16 bytes:
+ * size_t N_c = 1, then the angle) object per link in the host link order.  Records are built
+ * and parsed on the device; load checks every N_c against the group and fails on a file
+ * shorter than the lattice.  FP32 contexts store FP32 links widened to double. */
+SU2B_API int su2b_save_gauge(su2b_ctx *ctx, const char *path);
+SU2B_API int su2b_load_gauge(su2b_ctx *ctx, const char *path);
+
 /* ---- observables between trajectories ---------------------------------------------------- */
 /* polyakov_loop_spatial_average (polyakov_loop.hh:48-63): sum over spatial points of ReTr of
  * the product of the temporal links, divided by the full volume as the reference does. */

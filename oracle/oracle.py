@@ -73,6 +73,8 @@ _REF_ONLY = {
     "sweep": (None, _G + [f64, f64, i32, f64, i32, i64, i64, _D, _D]),
     "gradient_flow": (None, _G + [f64, f64, _D, f64, f64, f64, C.c_char_p]),
     "omp_threads": (i32, []),
+    "save_gauge": (None, _G + [_D, C.c_char_p]),
+    "load_gauge": (i32, _G + [C.c_char_p, _D]),
 }
 
 
@@ -141,6 +143,18 @@ class Oracle:
         U = np.ascontiguousarray(U, dtype=np.float64).copy()
         self._ape_smear(group, *dims, nd, alpha, int(spatial), dp(U))
         return U
+
+    def save_gauge(self, group, dims, nd, U, path):
+        """gaugeconfig::save of the reference (reference harness only)."""
+        self._save_gauge(group, *dims, nd, dp(np.ascontiguousarray(U, dtype=np.float64)),
+                         str(path).encode())
+
+    def load_gauge(self, group, dims, nd, path):
+        out = np.zeros(self.nlinks(dims, nd) * (4 if group == 0 else 1))
+        rc = self._load_gauge(group, *dims, nd, str(path).encode(), dp(out))
+        if rc != 0:
+            raise OSError(f"reference could not load {path}")
+        return out
 
     def S_G_hmc(self, group, dims, nd, beta, U, xi=1.0, aniso=False):
         return self._S_G_hmc(group, *dims, nd, beta, dp(U), xi, int(aniso))

@@ -548,4 +548,24 @@ void ref_ape_smear(int group, int Lx, int Ly, int Lz, int Lt, int nd, double alp
     io<G>::get(U, inout);
   });
 }
+
+// gaugeconfig<G>::save / load (gaugeconfig.hh:225-252), the reference's binary format
+void ref_save_gauge(int group, int Lx, int Ly, int Lz, int Lt, int nd, const double *in,
+                    const char *path) {
+  DISPATCH(group, {
+    gaugeconfig<G> U(Lx, Ly, Lz, Lt, nd, 0.);
+    io<G>::put(U, in);
+    U.save(path);
+  });
+}
+int ref_load_gauge(int group, int Lx, int Ly, int Lz, int Lt, int nd, const char *path,
+                   double *out) {
+  int rc = 1;
+  DISPATCH(group, {
+    gaugeconfig<G> U(Lx, Ly, Lz, Lt, nd, 0.);
+    rc = U.load(path);
+    io<G>::get(U, out);
+  });
+  return rc;
+}
 } // extern "C"

@@ -168,6 +168,14 @@ class gaugeconfig:
         self._c(self.lib.su2b_download_gauge(self.ctx, _dp(out)))
         return out
 
+    def save(self, path):
+        """gaugeconfig::save (gaugeconfig.hh:225-230): the reference's binary format."""
+        self._c(self.lib.su2b_save_gauge(self.ctx, str(path).encode()))
+
+    def load(self, path):
+        """gaugeconfig::load (gaugeconfig.hh:241-252); raises on a short or foreign file."""
+        self._c(self.lib.su2b_load_gauge(self.ctx, str(path).encode()))
+
     # ---- reductions ----
     def gauge_energy(self, spatial_only=False) -> float:
         out = C.c_double()

@@ -273,3 +273,19 @@ def test_golden_fixtures(orc):
     x, it = orc.bicgstab_d(du, 2, Uu, 0.05, g["u1_psi"], g["u1_x0"], 1e-10)
     assert np.array_equal(x, g["u1_bicgstab_x"])
     assert int(g["u1_bicgstab_iter"]) == it + orc._last_solve_calls() - 1
+
+
+# ---------------------------------------------------------------- configuration files
+def test_reference_file_format(ref, tmp_path):
+    """gaugeconfig::save writes one in-memory _su2 (size_t N_c = 2, then Re a, Im a, Re b,
+    Im b) or _u1 (size_t N_c = 1, then the angle) per link in host link order
+    (gaugeconfig.hh:225-230, su2.hh:11-16, u1.hh:11-15); load reads it back."""
+    for group, dims, nd, nc, width in ((0, (4, 4, 4, 6), 4, 2, 4), (1, (8, 1, 1, 6), 2, 1, 1)):
+        U = ref.hotstart(group, dims, nd, 99, 1.0, 654321)
+        path = tmp_path / f"conf{group}"
+        ref.save_gauge(group, dims, nd, U, path)
+        rec = np.fromfile(path, dtype=np.dtype([("nc", "<u8"), ("v", "<f8", (width,))]))
+        assert rec.size == U.size // width
+        assert np.all(rec["nc"] == nc)
+        assert np.array_equal(rec["v"].reshape(-1), U)
+        assert np.array_equal(ref.load_gauge(group, dims, nd, path), U)
