@@ -206,6 +206,13 @@ SU2B_API int su2b_fermion_force(su2b_ctx *ctx, double mass, const double *phi_ho
 SU2B_API int su2b_fermion_action(su2b_ctx *ctx, double mass, const double *phi_host, double tol,
                         int max_iter, const double *x0_host, long seed, double *out);
 
+/* staggered::C_pion (propagator.hpp:25-65): pion correlator at rest, C[t] = sum_x |D^-1(x|0)|^2
+ * / Vs over the time slice t, with D^-1 = D^+ (D D^+)^-1 from one CG solve (tolerance as the
+ * reference's absolute |r| bound, start gaussian_spinor(0, 10, seed)); C[0] = 0 as the
+ * reference skips the contact term.  C_host receives Lt values.  U(1) only. */
+SU2B_API int su2b_pion_correlator(su2b_ctx *ctx, double mass, double tol, int max_iter,
+                                  long seed, double *C_host, long *cg_iterations);
+
 /* ---- batched ensembles of independent SU(2) chains ------------------------------------------ */
 /* Chains of different geometry (d = 3 or 4, even extents), coupling and seed advanced together:
  * every stage of a trajectory is one persistent launch over all chains, a trajectory is one

@@ -34,6 +34,7 @@ _SIGS = {
     "polyakov_loop": (f64, _G + [_D]),
     "wilson_loop": (f64, _G + [_D, i32, i32]),
     "ape_smear": (None, _G + [f64, i32, _D]),
+    "pion_correlator": (None, [i32, i32, i32, i32, i32, _D, f64, f64, i64, _D]),
     "S_G_hmc": (f64, _G + [f64, _D, f64, i32]),
     "gauge_derivative": (None, _G + [f64, f64, _D, f64, _D]),
     "md_injected": (f64, _G + [f64, f64, i32, i32, f64, _D, _D, _D]),
@@ -143,6 +144,11 @@ class Oracle:
         U = np.ascontiguousarray(U, dtype=np.float64).copy()
         self._ape_smear(group, *dims, nd, alpha, int(spatial), dp(U))
         return U
+
+    def pion_correlator(self, dims, nd, U, m, tol, seed):
+        C = np.zeros(dims[3])
+        self._pion_correlator(*dims, nd, dp(U), m, tol, seed, dp(C))
+        return C
 
     def save_gauge(self, group, dims, nd, U, path):
         """gaugeconfig::save of the reference (reference harness only)."""

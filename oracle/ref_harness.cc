@@ -28,6 +28,7 @@
 #include "random_gauge_trafo.hh"
 #include "staggered.hpp"
 #include "polyakov_loop.hh"
+#include "propagator.hpp"
 #include "smearape.hh"
 #include "wilsonloop.hh"
 
@@ -567,5 +568,14 @@ int ref_load_gauge(int group, int Lx, int Ly, int Lz, int Lt, int nd, const char
     io<G>::get(U, out);
   });
   return rc;
+}
+
+// staggered::C_pion<_u1>(U, m, "CG", tol, 0, seed) (propagator.hpp:25-65)
+void ref_pion_correlator(int Lx, int Ly, int Lz, int Lt, int nd, const double *Uin, double m,
+                         double tol, long seed, double *C) {
+  gaugeconfig<_u1> U(Lx, Ly, Lz, Lt, nd, 0.);
+  io<_u1>::put(U, Uin);
+  const std::vector<double> c = staggered::C_pion<_u1>(U, m, "CG", tol, 0, (size_t)seed);
+  for (int t = 0; t < Lt; t++) C[t] = c[t];
 }
 } // extern "C"

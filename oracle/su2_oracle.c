@@ -982,6 +982,31 @@ void orc_ddag_inv(int Lx, int Ly, int Lz, int Lt, int nd, const double *U, doubl
   free(x0);
 }
 
+/* staggered::C_pion (propagator.hpp:25-65): R = (D D^+)^-1 delta_0 by DDdag.inv (CG from
+ * gaussian_spinor(0, 10, seed)), S = D^+ R, C[t] = sum_{x in slice t} |S(x)|^2 / Vs for t >= 1,
+ * C[0] = 0.  The reference repeats the identical solve for every site; once is the same. */
+void orc_pion_correlator(int Lx, int Ly, int Lz, int Lt, int nd, const double *U, double m,
+                         double tol, long seed, double *C) {
+  const size_t V = (size_t)Lx * Ly * Lz * Lt, Vs = V / (size_t)Lt;
+  double *src = calloc(2 * V, sizeof(double)), *R = malloc(2 * V * sizeof(double)),
+         *S = malloc(2 * V * sizeof(double));
+  src[0] = 1.0;
+  orc_ddag_inv(Lx, Ly, Lz, Lt, nd, U, m, src, tol, seed, R);
+  orc_staggered_apply(Lx, Ly, Lz, Lt, nd, U, m, 1, R, S);
+  for (int t = 0; t < Lt; t++) {
+    C[t] = 0.0;
+    if (t == 0) continue;
+    for (size_t i = 0; i < Vs; i++) {
+      const size_t x = (size_t)t * Vs + i;
+      C[t] += S[2 * x] * S[2 * x] + S[2 * x + 1] * S[2 * x + 1];
+    }
+    C[t] /= (double)Vs;
+  }
+  free(src);
+  free(R);
+  free(S);
+}
+
 /* detDDdag_monomial.hh:64-83 with n_traj = 0 */
 double orc_fermion_heatbath(int Lx, int Ly, int Lz, int Lt, int nd, const double *U, double m,
                             long seed_pf, double *phi) {

@@ -118,4 +118,6 @@ double orc_wilson_loop(int group, int Lx, int Ly, int Lz, int Lt, int nd, const 
                        int r, int t);
 void orc_ape_smear(int group, int Lx, int Ly, int Lz, int Lt, int nd, double alpha,
                    int spatial, double *U);
+void orc_pion_correlator(int Lx, int Ly, int Lz, int Lt, int nd, const double *U, double m,
+                         double tol, long seed, double *C);
 #endif

@@ -101,6 +101,7 @@ SIGNATURES = {
     "su2b_batch_autotune": (i32, [_P, _D]),
     "su2b_polyakov_loop": (i32, [_P, _D]),
     "su2b_save_gauge": (i32, [_P, C.c_char_p]),
+    "su2b_pion_correlator": (i32, [_P, f64, f64, i32, i64, _D, C.POINTER(i64)]),
     "su2b_load_gauge": (i32, [_P, C.c_char_p]),
     "su2b_wilson_loop": (i32, [_P, i32, i32, _D]),
     "su2b_ape_smear": (i32, [_P, f64, i32]),

@@ -518,3 +518,35 @@ extern "C" int su2b_fermion_action(su2b_ctx *ctx, double mass, const double *phi
   *out = ctx->h_red[30];
   return SU2B_OK;
 }
+
+// staggered::C_pion (propagator.hpp:25-65).  The reference solves (D D^+) R = delta_0 with
+// DDdag_matrix_lat::inv -- always CG (its BiCGStab branch only declares a type,
+// staggered.hpp:258-263), started from gaussian_spinor(0, 10, seed) -- once for every site
+// with x0 >= 1, each time with the same source and start, then takes S = D^+ R at that site.
+// One solve gives the same R; S = D^+ R over the whole lattice; C[t] sums |S|^2 over the
+// time slice and divides by the spatial volume; C[0] stays 0 (the contact term is skipped).
+extern "C" int su2b_pion_correlator(su2b_ctx *ctx, double mass, double tol, int max_iter,
+                                    long seed, double *C_host, long *cg_iterations) {
+  if (!ctx) return SU2B_ERR_INVALID;
+  ctx->err.clear();
+  SU2B_CK(cudaSetDevice(ctx->device));
+  SU2B_NEED(C_host, "C_host is NULL");
+  SU2B_NEED(max_iter > 0, "max_iter must be positive");
+  SU2B_CKS(su2b_fermion_setup(ctx, false));
+  cudaStream_t s = ctx->stream;
+  double2 *b = ctx->sv[SV_B];
+  SU2B_CK(cudaMemsetAsync(b, 0, ctx->V * sizeof(double2), s));
+  const double2 one = make_double2(1.0, 0.0);  // the origin is even: eo index 0
+  SU2B_CK(cudaMemcpyAsync(b, &one, sizeof(double2), cudaMemcpyHostToDevice, s));
+  SU2B_CKS(set_start(ctx, SU2B_CG_START_REFERENCE, seed));
+  su2b_solve_stats st{};
+  const int rc = cg64(ctx, mass, tol, max_iter, &st);
+  if (cg_iterations) *cg_iterations = st.iterations;
+  if (rc != SU2B_OK) return rc;
+  SU2B_LAUNCH(SU2B_K_STAGGERED, hop64(ctx->g, ctx->ph, mass, 1, ctx->sv[SV_X], ctx->sv[SV_T], nullptr, nullptr, nullptr, nullptr, 0, s));
+  double *C = ctx->part_slot(4);
+  SU2B_LAUNCH(SU2B_K_OTHER, pion_slices(ctx->g, ctx->sv[SV_T], C, s));
+  SU2B_CK(cudaMemcpyAsync(C_host, C, sizeof(double) * ctx->g.L[0], cudaMemcpyDeviceToHost, s));
+  SU2B_CK(cudaStreamSynchronize(s));
+  return SU2B_OK;
+}

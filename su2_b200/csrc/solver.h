@@ -61,6 +61,8 @@ cudaError_t cg_persistent(const Geom &g, const double2 *ph, double m, double2 *x
 int cg_barrier_failed(const void *bar_mem, cudaStream_t s, int *failed);
 size_t cg_barrier_bytes();
 
+cudaError_t pion_slices(const Geom &g, const double2 *S, double *C, cudaStream_t s);
+
 cudaError_t resid64(int n, const double2 *b, const double2 *Ax, double2 *r, double *part,
                     cudaStream_t s);
 cudaError_t to32(int n, const double2 *a, float2 *b, cudaStream_t s);

@@ -228,6 +228,25 @@ __global__ void k_cg_p(int n, const double2 *__restrict__ r, double2 *__restrict
   }
 }
 
+// pion correlator: C[t] = sum over the spatial sites of time slice t of |S(t, x)|^2 / Vs,
+// one block per t summing its slice in a fixed order (propagator.hpp:43-60)
+template <int NT>
+__global__ void __launch_bounds__(NT)
+  k_pion_slices(Geom g, const double2 *__restrict__ S, double *C) {
+  __shared__ double sh[NT / 32];
+  const int t = blockIdx.x;
+  const int Vs = g.V / g.L[0];
+  double acc = 0.;
+  for (int i = threadIdx.x; i < Vs; i += NT) {
+    const int lex = t * Vs + i;
+    const Site s = site_from_lex(g, lex);
+    const double2 v = S[eo_of(g, lex, s.p)];
+    acc += v.x * v.x + v.y * v.y;
+  }
+  const double r = block_sum<NT>(acc, sh);
+  if (threadIdx.x == 0) C[t] = t == 0 ? 0.0 : r / (double)Vs;
+}
+
 // ---- persistent CG on D D^+ (one cooperative launch for the whole solve) ----
 //
 // For small lattices every CG iteration is a handful of microsecond-long kernels and the
@@ -809,5 +828,10 @@ int cg_barrier_failed(const void *bar_mem, cudaStream_t s, int *failed) {
   return 0;
 }
 size_t cg_barrier_bytes() { return sizeof(GridBarrier); }
+
+cudaError_t pion_slices(const Geom &g, const double2 *S, double *C, cudaStream_t s) {
+  k_pion_slices<256><<<g.L[0], 256, 0, s>>>(g, S, C);
+  return cudaGetLastError();
+}
 
 }  // namespace su2b

@@ -349,6 +349,14 @@ class gaugeconfig:
         return SolveResult(x, st.iterations, st.restarts, st.residual, st.true_residual,
                            rc == _abi.OK)
 
+    def C_pion(self, m, tol=1e-10, seed=97234719, max_iter=100000):
+        """staggered::C_pion (propagator.hpp:25-65): the pion correlator at rest, Lt values."""
+        C_ = np.zeros(self.dims[3])
+        it = C.c_long()
+        self._c(self.lib.su2b_pion_correlator(self.ctx, m, tol, max_iter, seed, _dp(C_),
+                                              C.byref(it)))
+        return C_
+
     def fermion_derivative(self, m, phi, tol=1e-10, seed=97234719, x0=None, max_iter=100000):
         phi = _f64(phi)
         out = np.empty(self.n_links)

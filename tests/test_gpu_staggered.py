@@ -125,3 +125,24 @@ def test_pf_source_stream(orc):
     R = orc.philox_pf_source((16, 1, 1, 16), 5, 0)
     assert np.all(R[1::2] == 0.0)
     assert abs(R[0::2].var() - 0.5) < 0.1
+
+
+@pytest.mark.parametrize("dims,nd", U1_GEOMS, ids=IDS)
+def test_pion_correlator(gpu, orc, dims, nd):
+    """C_pion (propagator.hpp:25-65) on the device against the oracle: same CG start, both
+    solves stop at |r| < 1e-12, so the correlators agree to the solver tolerance."""
+    U, _, _ = setup(orc, dims, nd)
+    want = orc.pion_correlator(dims, nd, U, 0.1, 1e-12, 17)
+    with u1(gpu, dims, nd) as c:
+        c.upload(U)
+        got = c.C_pion(0.1, tol=1e-12, seed=17)
+    assert got[0] == 0.0
+    np.testing.assert_allclose(got, want, rtol=1e-9, atol=1e-14)
+
+
+def test_pion_correlator_rejects_su2(gpu):
+    import su2_b200
+    with gpu.gaugeconfig(4, 4, 4, 4, 4, 2.0) as c:
+        with pytest.raises(su2_b200.Su2bError) as e:
+            c.C_pion(0.1)
+        assert e.value.code == 4

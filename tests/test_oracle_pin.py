@@ -289,3 +289,12 @@ def test_reference_file_format(ref, tmp_path):
         assert np.all(rec["nc"] == nc)
         assert np.array_equal(rec["v"].reshape(-1), U)
         assert np.array_equal(ref.load_gauge(group, dims, nd, path), U)
+
+
+def test_pin_pion_correlator(orc, ref):
+    """staggered::C_pion of the reference against the restatement, which solves once where
+    the reference repeats the identical solve for every site."""
+    for dims, nd in (((8, 1, 1, 6), 2), ((4, 4, 1, 4), 3)):
+        U = ref.hotstart(1, dims, nd, 42, 1.0, 654321)
+        assert np.array_equal(orc.pion_correlator(dims, nd, U, 0.1, 1e-12, 17),
+                              ref.pion_correlator(dims, nd, U, 0.1, 1e-12, 17))
