@@ -66,7 +66,7 @@ _ORC_ONLY = {
     "philox_momenta": (None, _G + [u64, u32, _D]),
     "philox_accept_uniform": (f64, [u64, u32]),
     "philox_pf_source": (None, [i32] * 4 + [u64, u32, i32, _D]),
-    "metropolis_checkerboard": (None, _G + [f64, f64, i32, u64, u32, _D, _D]),
+    "metropolis_checkerboard": (None, _G + [f64, f64, f64, i32, u64, u32, _D, _D]),
     "exp_su2": (None, [_D, _D]),
     "last_solve_calls": (i64, []),
 }
@@ -335,11 +335,12 @@ class Oracle:
         self._philox_pf_source(*dims, seed, traj, int(complex_source), dp(R))
         return R
 
-    def metropolis_checkerboard(self, group, dims, nd, beta, delta, N_hit, seed, sweep, U):
+    def metropolis_checkerboard(self, group, dims, nd, beta, delta, N_hit, seed, sweep, U,
+                                xi=1.0):
         U = U.copy()
         rates = np.zeros(2)
-        self._metropolis_checkerboard(group, *dims, nd, beta, delta, N_hit, seed, sweep, dp(U),
-                                      dp(rates))
+        self._metropolis_checkerboard(group, *dims, nd, beta, xi, delta, N_hit, seed, sweep,
+                                      dp(U), dp(rates))
         return U, rates
 
     def exp_su2(self, x):

@@ -1572,7 +1572,7 @@ void orc_philox_pf_source(int Lx, int Ly, int Lz, int Lt, uint64_t seed, uint32_
 /* Site-parity checkerboard sweep: for mu, for parity p, every link (x, mu) with
  * parity(x) = p gets N_hit proposals U -> U R (flat-sweep.hh:97-117 update rule). */
 void orc_metropolis_checkerboard(int group, int Lx, int Ly, int Lz, int Lt, int nd,
-                                 double beta, double delta, int N_hit, uint64_t seed,
+                                 double beta, double xi, double delta, int N_hit, uint64_t seed,
                                  uint32_t sweep, double *U, double *rates) {
   const lat_t l = mklat(Lx, Ly, Lz, Lt, nd);
   const double Nc = group == 0 ? 2. : 1.;
@@ -1585,7 +1585,7 @@ void orc_metropolis_checkerboard(int group, int Lx, int Ly, int Lz, int Lt, int 
         if (((c[0] + c[1] + c[2] + c[3]) & 1) != p) continue;
         const size_t i = link(&l, c, mu);
         if (group == 0) {
-          const su2 K = staples_su2(&l, U, c, mu, 1.0, 0);
+          const su2 K = staples_su2(&l, U, c, mu, xi, xi != 1.0);
           su2 u = sload(U, i);
           for (int n = 0; n < N_hit; n++) {
             uint32_t r[4];
@@ -1609,7 +1609,7 @@ void orc_metropolis_checkerboard(int group, int Lx, int Ly, int Lz, int Lt, int 
           }
           sstore(U, i, u);
         } else {
-          const cplx K = staples_u1(&l, U, c, mu, 1.0, 0);
+          const cplx K = staples_u1(&l, U, c, mu, xi, xi != 1.0);
           double u = U[i];
           for (int n = 0; n < N_hit; n++) {
             uint32_t r[4];

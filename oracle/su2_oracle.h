@@ -107,7 +107,7 @@ double orc_philox_accept_uniform(uint64_t seed, uint32_t traj);
 void orc_philox_pf_source(int Lx, int Ly, int Lz, int Lt, uint64_t seed, uint32_t traj,
                           int complex_source, double *R);
 void orc_metropolis_checkerboard(int group, int Lx, int Ly, int Lz, int Lt, int nd,
-                                 double beta, double delta, int N_hit, uint64_t seed,
+                                 double beta, double xi, double delta, int N_hit, uint64_t seed,
                                  uint32_t sweep, double *U, double *rates);
 
 #ifdef __cplusplus

@@ -466,10 +466,10 @@ extern "C" int su2b_metropolis_sweep(su2b_ctx *ctx, double delta, int N_hit, uin
   for (int mu = 0; mu < ctx->g.nd; mu++)
     for (int p = 0; p < 2; p++) {
       if (ctx->link64)
-        SU2B_LAUNCH(SU2B_K_METROPOLIS, metropolis_pass<double>(ctx->g, ctx->U, ctx->group, mu, p, ctx->beta, delta, N_hit,
+        SU2B_LAUNCH(SU2B_K_METROPOLIS, metropolis_pass<double>(ctx->g, ctx->U, ctx->group, mu, p, ctx->beta, ctx->xi, delta, N_hit,
                                    seed, sweep, ctx->counts, ctx->stream));
       else
-        SU2B_LAUNCH(SU2B_K_METROPOLIS, metropolis_pass<float>(ctx->g, ctx->U, ctx->group, mu, p, ctx->beta, delta, N_hit,
+        SU2B_LAUNCH(SU2B_K_METROPOLIS, metropolis_pass<float>(ctx->g, ctx->U, ctx->group, mu, p, ctx->beta, ctx->xi, delta, N_hit,
                                   seed, sweep, ctx->counts, ctx->stream));
     }
   CK(cudaMemcpyAsync(ctx->h_counts, ctx->counts, 2 * sizeof(unsigned long long),

@@ -19,7 +19,8 @@ template <class T> using LinkT = typename LinkOf<T>::type;
 template <class T, int ND, int NT>
 __global__ void __launch_bounds__(NT)
   k_metro_su2(Geom g, LinkT<T> *__restrict__ U, int mu, int p, double beta_nc, double delta,
-              int N_hit, uint64_t seed, uint32_t sweep, unsigned long long *counts) {
+              int N_hit, uint64_t seed, uint32_t sweep, unsigned long long *counts, double wt,
+              double ws) {
   __shared__ unsigned int sh_acc;
   if (threadIdx.x == 0) sh_acc = 0;
   __syncthreads();
@@ -37,7 +38,7 @@ __global__ void __launch_bounds__(NT)
       const Su2<double> A = to64(ld_link_rw(U + (size_t)nu * g.V + eo_of(g, lpm, 1 - p)));
       const Su2<double> B = to64(ld_link_rw(U + (size_t)mu * g.V + eo_of(g, lpn, 1 - p)));
       const Su2<double> D = to64(ld_link_rw(U + (size_t)nu * g.V + eo_of(g, s.lex, p)));
-      K = add(K, mul(mul(A, dag(B)), dag(D)));
+      K = add(K, scale((nu == 0 || mu == 0) ? wt : ws, mul(mul(A, dag(B)), dag(D))));
     }
 #pragma unroll
     for (int nu = 0; nu < ND; nu++) {
@@ -46,7 +47,7 @@ __global__ void __launch_bounds__(NT)
       const Su2<double> A = to64(ld_link_rw(U + (size_t)nu * g.V + eo_of(g, lpm + b, p)));
       const Su2<double> B = to64(ld_link_rw(U + (size_t)mu * g.V + eo_of(g, s.lex + b, 1 - p)));
       const Su2<double> D = to64(ld_link_rw(U + (size_t)nu * g.V + eo_of(g, s.lex + b, 1 - p)));
-      K = add(K, mul(mul(dag(A), dag(B)), D));
+      K = add(K, scale((nu == 0 || mu == 0) ? wt : ws, mul(mul(dag(A), dag(B)), D)));
     }
     const size_t l = (size_t)mu * g.V + (size_t)p * g.Vh + cb;
     Su2<double> u = to64(ld_link_rw(U + l));
@@ -82,7 +83,8 @@ __global__ void __launch_bounds__(NT)
 template <int ND, int NT>
 __global__ void __launch_bounds__(NT)
   k_metro_u1(Geom g, double *__restrict__ U, int mu, int p, double beta, double delta,
-             int N_hit, uint64_t seed, uint32_t sweep, unsigned long long *counts) {
+             int N_hit, uint64_t seed, uint32_t sweep, unsigned long long *counts, double wt,
+             double ws) {
   __shared__ unsigned int sh_acc;
   if (threadIdx.x == 0) sh_acc = 0;
   __syncthreads();
@@ -101,8 +103,9 @@ __global__ void __launch_bounds__(NT)
       const double D = U[(size_t)nu * g.V + eo_of(g, s.lex, p)];
       double sn, cs;
       sincos((A + (-B)) + (-D), &sn, &cs);
-      Kr += cs;
-      Ki += sn;
+      const double w = (nu == 0 || mu == 0) ? wt : ws;
+      Kr += w * cs;
+      Ki += w * sn;
     }
 #pragma unroll
     for (int nu = 0; nu < ND; nu++) {
@@ -113,8 +116,9 @@ __global__ void __launch_bounds__(NT)
       const double D = U[(size_t)nu * g.V + eo_of(g, s.lex + b, 1 - p)];
       double sn, cs;
       sincos(((-A) + (-B)) + D, &sn, &cs);
-      Kr += cs;
-      Ki += sn;
+      const double w = (nu == 0 || mu == 0) ? wt : ws;
+      Kr += w * cs;
+      Ki += w * sn;
     }
     const size_t l = (size_t)mu * g.V + (size_t)p * g.Vh + cb;
     double u = U[l];
@@ -148,9 +152,12 @@ __global__ void __launch_bounds__(NT)
 
 template <class T>
 cudaError_t metropolis_pass(const Geom &g, void *U, int group, int mu, int parity, double beta,
-                            double delta, int N_hit, uint64_t seed, uint32_t sweep,
+                            double xi, double delta, int N_hit, uint64_t seed, uint32_t sweep,
                             unsigned long long *counts, cudaStream_t s) {
   constexpr int NT = 128;
+  // anisotropic weights of get_staples (get_staples.hh:58-79): 1/xi for planes with
+  // direction 0, xi otherwise; both 1 (exactly) for the isotropic action
+  const double wt = xi == 1.0 ? 1.0 : 1.0 / xi, ws = xi;
   const int grid = (g.Vh + NT - 1) / NT;
   if (group == 0) {
     LinkT<T> *u = (LinkT<T> *)U;
@@ -158,15 +165,15 @@ cudaError_t metropolis_pass(const Geom &g, void *U, int group, int mu, int parit
     switch (g.nd) {
       case 2:
         k_metro_su2<T, 2, NT><<<grid, NT, 0, s>>>(g, u, mu, parity, bn, delta, N_hit, seed,
-                                                  sweep, counts);
+                                                  sweep, counts, wt, ws);
         break;
       case 3:
         k_metro_su2<T, 3, NT><<<grid, NT, 0, s>>>(g, u, mu, parity, bn, delta, N_hit, seed,
-                                                  sweep, counts);
+                                                  sweep, counts, wt, ws);
         break;
       default:
         k_metro_su2<T, 4, NT><<<grid, NT, 0, s>>>(g, u, mu, parity, bn, delta, N_hit, seed,
-                                                  sweep, counts);
+                                                  sweep, counts, wt, ws);
         break;
     }
   } else {
@@ -174,15 +181,15 @@ cudaError_t metropolis_pass(const Geom &g, void *U, int group, int mu, int parit
     switch (g.nd) {
       case 2:
         k_metro_u1<2, NT><<<grid, NT, 0, s>>>(g, u, mu, parity, beta, delta, N_hit, seed, sweep,
-                                              counts);
+                                              counts, wt, ws);
         break;
       case 3:
         k_metro_u1<3, NT><<<grid, NT, 0, s>>>(g, u, mu, parity, beta, delta, N_hit, seed, sweep,
-                                              counts);
+                                              counts, wt, ws);
         break;
       default:
         k_metro_u1<4, NT><<<grid, NT, 0, s>>>(g, u, mu, parity, beta, delta, N_hit, seed, sweep,
-                                              counts);
+                                              counts, wt, ws);
         break;
     }
   }
@@ -190,10 +197,10 @@ cudaError_t metropolis_pass(const Geom &g, void *U, int group, int mu, int parit
 }
 
 template cudaError_t metropolis_pass<double>(const Geom &, void *, int, int, int, double, double,
-                                             int, uint64_t, uint32_t, unsigned long long *,
-                                             cudaStream_t);
+                                             double, int, uint64_t, uint32_t,
+                                             unsigned long long *, cudaStream_t);
 template cudaError_t metropolis_pass<float>(const Geom &, void *, int, int, int, double, double,
-                                            int, uint64_t, uint32_t, unsigned long long *,
-                                            cudaStream_t);
+                                            double, int, uint64_t, uint32_t,
+                                            unsigned long long *, cudaStream_t);
 
 }  // namespace su2b

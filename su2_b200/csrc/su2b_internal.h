@@ -87,7 +87,7 @@ cudaError_t cond_restore(const Geom &g, void *U, const void *U_old, int group,
 // ---- Metropolis ----
 template <class T>
 cudaError_t metropolis_pass(const Geom &g, void *U, int group, int mu, int parity, double beta,
-                            double delta, int N_hit, uint64_t seed, uint32_t sweep,
+                            double xi, double delta, int N_hit, uint64_t seed, uint32_t sweep,
                             unsigned long long *counts, cudaStream_t s);
 
 // ---- clover energy density / charge ----

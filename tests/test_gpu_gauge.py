@@ -194,13 +194,17 @@ def test_device_momentum_stream(gpu, orc, group, dims, nd):
 
 @pytest.mark.parametrize("group,dims,nd", GEOMS, ids=GEOM_IDS)
 def test_metropolis_checkerboard(gpu, orc, group, dims, nd):
+    """The device sweep replayed by the oracle (same Philox stream and update order), for the
+    isotropic and the anisotropic action (staple weights 1/xi and xi, get_staples.hh:58-79)."""
     U = hot(orc, group, dims, nd)
-    U_want, r_want = orc.metropolis_checkerboard(group, dims, nd, 2.3, 0.3, 4, 99, 3, U)
-    with make(gpu, group, dims, nd, beta=2.3) as c:
-        c.upload(U)
-        rates = c.sweep(0.3, 4, 99, 3)
-        assert rel(c.download(), U_want) < 1e-11
-    np.testing.assert_array_equal(rates, r_want)
+    for xi in (1.0, 1.3):
+        U_want, r_want = orc.metropolis_checkerboard(group, dims, nd, 2.3, 0.3, 4, 99, 3, U,
+                                                     xi=xi)
+        with make(gpu, group, dims, nd, beta=2.3, xi=xi) as c:
+            c.upload(U)
+            rates = c.sweep(0.3, 4, 99, 3)
+            assert rel(c.download(), U_want) < 1e-11
+        np.testing.assert_array_equal(rates, r_want)
 
 
 @pytest.mark.parametrize("group,dims,nd", [GEOMS[0], GEOMS[4]], ids=[GEOM_IDS[0], GEOM_IDS[4]])
