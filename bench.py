@@ -115,16 +115,20 @@ class Clocks:
                 self.reasons |= int(get_r(self.h))
             except Exception:
                 pass
+            self.running.set()
             if self.stop_flag.wait(0.002):
                 break
 
     def start(self):
+        """Starts polling and returns once the poller runs (first sample taken)."""
         if self.h is None:
             return
         self.samples, self.reasons = [], 0
         self.stop_flag.clear()
+        self.running = threading.Event()
         self.t = threading.Thread(target=self._poll, daemon=True)
         self.t.start()
+        self.running.wait(5.0)
 
     def stop(self):
         if self.t is None:

@@ -149,6 +149,13 @@ __global__ void __launch_bounds__(NT)
   }
 }
 
+// Programmatic dependent launch between the chained force launches of a trajectory: each
+// block lets the next launch start as soon as it is itself resident, and waits for the
+// previous launch to complete (and its writes to be visible) before it touches global
+// memory.  Both are no-ops for a launch without a programmatic dependency.
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;"); }
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 // fused staple/force/momentum(/link update) kernel: one thread per site, force_site body
 template <class T, int ND, int NT, int MINB>
 __global__ void __launch_bounds__(NT, MINB)
@@ -156,6 +163,8 @@ __global__ void __launch_bounds__(NT, MINB)
               const T *__restrict__ extra, T f, T scale_, int mode, int aniso, T wt, T ws,
               double *kin_part, LinkT<T> *__restrict__ Uout, T dt_upd) {
   __shared__ double sh[NT / 32];
+  pdl_trigger();
+  pdl_wait();
   // warps alternate between the parities of one band of NT/2 sites per parity, so the
   // +-z / +-y neighbours of a site are mostly the own links of another warp of the block
   const int w = threadIdx.x >> 5;
@@ -444,6 +453,8 @@ __global__ void __launch_bounds__(NT, MINB)
                     const T *__restrict__ extra, T f, T scale_, int mode, int aniso, T wt, T ws,
                     double *kin_part, LinkT<T> *__restrict__ Uout, T dt_upd) {
   __shared__ double sh[NT / 32];
+  pdl_trigger();
+  pdl_wait();
   const int w = threadIdx.x >> 5;
   const int half = w & 1, p = (w >> 1) & 1;
   const int cb = blockIdx.x * (NT / 4) + (w >> 2) * 32 + (threadIdx.x & 31);
@@ -456,10 +467,27 @@ __global__ void __launch_bounds__(NT, MINB)
   }
 }
 
+// launch with the programmatic-stream-serialization attribute when pdl is set
+template <typename... KArgs, typename... Args>
+cudaError_t launch_force(void (*kern)(KArgs...), dim3 grid, int nt, cudaStream_t s, bool pdl,
+                         Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = dim3(nt);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = pdl ? 1 : 0;
+  return cudaLaunchKernelEx(&cfg, kern, args...);
+}
+
 template <class T>
 cudaError_t force_update(const Geom &g, const void *U, int group, T *P, const T *extra, double f,
                          double scale, double xi, int mode, double *kin_part, int *nblocks,
-                         void *Uout, double dt_upd, cudaStream_t s, int variant) {
+                         void *Uout, double dt_upd, cudaStream_t s, int variant, bool pdl) {
   constexpr int NT = 128;
   const int aniso = xi != 1.0;
   if (group == 0) {
@@ -468,27 +496,24 @@ cudaError_t force_update(const Geom &g, const void *U, int group, T *P, const T 
     LinkT<T> *uo = (LinkT<T> *)Uout;
     int nb = 0;
     const int v = (variant >= 0 && variant < FORCE_VARIANTS) ? variant : 1;
+#define SU2B_FORCE_ARGS g, u, P, extra, (T)f, (T)scale, mode, aniso, wt, ws, kin_part, uo, (T)dt_upd
 #define SU2B_FORCE_LAUNCH(NTV, MB)                                                           \
   do {                                                                                     \
     const dim3 grid(cdiv(g.Vh, NTV / 2));                                                  \
     nb = grid.x;                                                                           \
+    cudaError_t e_;                                                                        \
     switch (g.nd) {                                                                        \
       case 2:                                                                              \
-        k_force_su2<T, 2, NTV, MB><<<grid, NTV, 0, s>>>(g, u, P, extra, (T)f, (T)scale, mode, \
-                                                        aniso, wt, ws, kin_part, uo,          \
-                                                        (T)dt_upd);                           \
+        e_ = launch_force(k_force_su2<T, 2, NTV, MB>, grid, NTV, s, pdl, SU2B_FORCE_ARGS);  \
         break;                                                                             \
       case 3:                                                                              \
-        k_force_su2<T, 3, NTV, MB><<<grid, NTV, 0, s>>>(g, u, P, extra, (T)f, (T)scale, mode, \
-                                                        aniso, wt, ws, kin_part, uo,          \
-                                                        (T)dt_upd);                           \
+        e_ = launch_force(k_force_su2<T, 3, NTV, MB>, grid, NTV, s, pdl, SU2B_FORCE_ARGS);  \
         break;                                                                             \
       default:                                                                             \
-        k_force_su2<T, 4, NTV, MB><<<grid, NTV, 0, s>>>(g, u, P, extra, (T)f, (T)scale, mode, \
-                                                        aniso, wt, ws, kin_part, uo,          \
-                                                        (T)dt_upd);                           \
+        e_ = launch_force(k_force_su2<T, 4, NTV, MB>, grid, NTV, s, pdl, SU2B_FORCE_ARGS);  \
         break;                                                                             \
     }                                                                                      \
+    if (e_ != cudaSuccess) return e_;                                                      \
   } while (0)
 #define SU2B_FORCE_SPLIT(NTV, MB)                                                            \
   do {                                                                                     \
@@ -498,9 +523,9 @@ cudaError_t force_update(const Geom &g, const void *U, int group, T *P, const T 
     }                                                                                      \
     const dim3 grid(cdiv(g.Vh, NTV / 4));                                                  \
     nb = grid.x;                                                                           \
-    k_force_su2_split<T, NTV, MB><<<grid, NTV, 0, s>>>(g, u, P, extra, (T)f, (T)scale, mode, \
-                                                       aniso, wt, ws, kin_part, uo,          \
-                                                       (T)dt_upd);                           \
+    const cudaError_t e_ =                                                                 \
+      launch_force(k_force_su2_split<T, NTV, MB>, grid, NTV, s, pdl, SU2B_FORCE_ARGS);     \
+    if (e_ != cudaSuccess) return e_;                                                      \
   } while (0)
     switch (v) {
       case 0: SU2B_FORCE_LAUNCH(256, 4); break;
@@ -618,7 +643,7 @@ cudaError_t cond_restore(const Geom &g, void *U, const void *U_old, int group,
                                         int *, cudaStream_t);                                 \
   template cudaError_t force_update<T>(const Geom &, const void *, int, T *, const T *,      \
                                        double, double, double, int, double *, int *, void *,  \
-                                       double, cudaStream_t, int);                            \
+                                       double, cudaStream_t, int, bool);                      \
   template cudaError_t link_update<T>(const Geom &, void *, int, const T *, double,          \
                                       cudaStream_t);                                          \
   template cudaError_t restore_links<T>(const Geom &, void *, int, cudaStream_t);            \

@@ -210,16 +210,19 @@ int enqueue_fused(su2b_ctx *ctx, const std::vector<FOp> &fops, bool host_momenta
       mode |= FM_RESTORE;
       out = F = (cur == S) ? X : next(cur);
     }
+    // chained force launches overlap the next one's launch with the previous one's tail
+    // (programmatic dependent launch; every access waits for the previous launch)
+    const bool pdl = !ctx->prof;
     if (ctx->link64)
       SU2B_LAUNCH(SU2B_K_FORCE,
                   force_update<double>(ctx->g, cur, 0, (double *)ctx->P, nullptr, f, -o.cm,
                                        ctx->xi, mode, ctx->part_slot(1), &nb, out, o.cg, s,
-                                       ctx->tune_force));
+                                       ctx->tune_force, pdl));
     else
       SU2B_LAUNCH(SU2B_K_FORCE,
                   force_update<float>(ctx->g, cur, 0, (float *)ctx->P, nullptr, f, -o.cm,
                                       ctx->xi, mode, ctx->part_slot(1), &nb, out, o.cg, s,
-                                       ctx->tune_force));
+                                      ctx->tune_force, pdl));
     if (o.kinetic) SU2B_LAUNCH(SU2B_K_OTHER, reduce_final(ctx->part_slot(1), nb, 1, ctx->red + 4, s));
     if (o.kind == 1) cur = out;
   }

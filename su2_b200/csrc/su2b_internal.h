@@ -44,7 +44,8 @@ constexpr int FORCE_VARIANTS = 8;
 template <class T>
 cudaError_t force_update(const Geom &g, const void *U, int group, T *P, const T *extra, double f,
                          double scale, double xi, int mode, double *kin_part, int *nblocks,
-                         void *Uout, double dt_upd, cudaStream_t s, int variant = 1);
+                         void *Uout, double dt_upd, cudaStream_t s, int variant = 1,
+                         bool pdl = false);
 
 template <class T>
 cudaError_t link_update(const Geom &g, void *U, int group, const T *P, double dt,
