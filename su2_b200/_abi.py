@@ -118,9 +118,10 @@ BATCH_VARIANTS = 4
 # (threads per block, min blocks per SM) of the batched force kernel
 BATCH_SHAPES = [(64, 8), (128, 4), (128, 6), (256, 3)]
 # (threads per block, min resident blocks per SM) of the force kernel's launch shapes; the
-# "split" shapes run two threads per site (d = 4; other d use (128, 8))
+# "split" shape runs two threads per site (d = 4; other d use (128, 8)); the anisotropic
+# action always runs (128, 6)
 FORCE_SHAPES = [(256, 4), (128, 8), (128, 4), (128, 6), (256, 2), (256, 3), ("split", 128, 8),
-                ("split", 256, 4)]
+                (64, 16)]
 
 K_FORCE, K_UPDATE, K_PLAQUETTE, K_MOMENTA, K_RESTORE, K_METROPOLIS, K_CLOVER, K_STAGGERED, \
     K_OTHER = range(9)

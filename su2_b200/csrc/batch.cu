@@ -74,10 +74,10 @@ __global__ void __launch_bounds__(NT, MINB)
     double k2 = 0.;
     if (cb < d.g.Vh) {
       if (d.g.nd == 4)
-        k2 = force_site<T, 4>(d.g, U, P, nullptr, f, (T)(-cm), mode, 0, T(1), T(1), Uo, (T)cg, p,
+        k2 = force_site_impl<T, 4, false>(d.g, U, P, nullptr, f, (T)(-cm), mode, T(1), T(1), Uo, (T)cg, p,
                               cb);
       else
-        k2 = force_site<T, 3>(d.g, U, P, nullptr, f, (T)(-cm), mode, 0, T(1), T(1), Uo, (T)cg, p,
+        k2 = force_site_impl<T, 3, false>(d.g, U, P, nullptr, f, (T)(-cm), mode, T(1), T(1), Uo, (T)cg, p,
                               cb);
     }
     if (mode & FM_KINETIC) {

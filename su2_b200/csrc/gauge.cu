@@ -157,10 +157,10 @@ __device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.lau
 __device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
 
 // fused staple/force/momentum(/link update) kernel: one thread per site, force_site body
-template <class T, int ND, int NT, int MINB>
+template <class T, int ND, int NT, int MINB, bool ANISO>
 __global__ void __launch_bounds__(NT, MINB)
   k_force_su2(Geom g, const LinkT<T> *__restrict__ U, T *__restrict__ P,
-              const T *__restrict__ extra, T f, T scale_, int mode, int aniso, T wt, T ws,
+              const T *__restrict__ extra, T f, T scale_, int mode, T wt, T ws,
               double *kin_part, LinkT<T> *__restrict__ Uout, T dt_upd) {
   __shared__ double sh[NT / 32];
   pdl_trigger();
@@ -172,7 +172,8 @@ __global__ void __launch_bounds__(NT, MINB)
   const int cb = blockIdx.x * (NT / 2) + (w >> 1) * 32 + (threadIdx.x & 31);
   double k2 = 0.;
   if (cb < g.Vh)
-    k2 = force_site<T, ND>(g, U, P, extra, f, scale_, mode, aniso, wt, ws, Uout, dt_upd, p, cb);
+    k2 = force_site_impl<T, ND, ANISO>(g, U, P, extra, f, scale_, mode, wt, ws, Uout, dt_upd, p,
+                                       cb);
   if (mode & FM_KINETIC) {
     const double r = block_sum<NT>(k2, sh);
     if (threadIdx.x == 0) kin_part[blockIdx.x] = r;
@@ -450,7 +451,7 @@ cudaError_t reduce_final(const double *part, int nblocks, int ncomp, double *out
 template <class T, int NT, int MINB>
 __global__ void __launch_bounds__(NT, MINB)
   k_force_su2_split(Geom g, const LinkT<T> *__restrict__ U, T *__restrict__ P,
-                    const T *__restrict__ extra, T f, T scale_, int mode, int aniso, T wt, T ws,
+                    const T *__restrict__ extra, T f, T scale_, int mode, T wt, T ws,
                     double *kin_part, LinkT<T> *__restrict__ Uout, T dt_upd) {
   __shared__ double sh[NT / 32];
   pdl_trigger();
@@ -460,7 +461,10 @@ __global__ void __launch_bounds__(NT, MINB)
   const int cb = blockIdx.x * (NT / 4) + (w >> 2) * 32 + (threadIdx.x & 31);
   double k2 = 0.;
   if (cb < g.Vh)
-    k2 = force_half<T>(g, U, P, extra, f, scale_, mode, aniso, wt, ws, Uout, dt_upd, half, p, cb);
+    k2 = half == 0 ? force_half_impl<T, 0, false>(g, U, P, extra, f, scale_, mode, wt, ws, Uout,
+                                                  dt_upd, p, cb)
+                   : force_half_impl<T, 1, false>(g, U, P, extra, f, scale_, mode, wt, ws, Uout,
+                                                  dt_upd, p, cb);
   if (mode & FM_KINETIC) {
     const double r = block_sum<NT>(k2, sh);
     if (threadIdx.x == 0) kin_part[blockIdx.x] = r;
@@ -496,21 +500,24 @@ cudaError_t force_update(const Geom &g, const void *U, int group, T *P, const T 
     LinkT<T> *uo = (LinkT<T> *)Uout;
     int nb = 0;
     const int v = (variant >= 0 && variant < FORCE_VARIANTS) ? variant : 1;
-#define SU2B_FORCE_ARGS g, u, P, extra, (T)f, (T)scale, mode, aniso, wt, ws, kin_part, uo, (T)dt_upd
-#define SU2B_FORCE_LAUNCH(NTV, MB)                                                           \
+#define SU2B_FORCE_ARGS g, u, P, extra, (T)f, (T)scale, mode, wt, ws, kin_part, uo, (T)dt_upd
+#define SU2B_FORCE_LAUNCH(NTV, MB, AN)                                                       \
   do {                                                                                     \
     const dim3 grid(cdiv(g.Vh, NTV / 2));                                                  \
     nb = grid.x;                                                                           \
     cudaError_t e_;                                                                        \
     switch (g.nd) {                                                                        \
       case 2:                                                                              \
-        e_ = launch_force(k_force_su2<T, 2, NTV, MB>, grid, NTV, s, pdl, SU2B_FORCE_ARGS);  \
+        e_ = launch_force(k_force_su2<T, 2, NTV, MB, AN>, grid, NTV, s, pdl,               \
+                          SU2B_FORCE_ARGS);                                                \
         break;                                                                             \
       case 3:                                                                              \
-        e_ = launch_force(k_force_su2<T, 3, NTV, MB>, grid, NTV, s, pdl, SU2B_FORCE_ARGS);  \
+        e_ = launch_force(k_force_su2<T, 3, NTV, MB, AN>, grid, NTV, s, pdl,               \
+                          SU2B_FORCE_ARGS);                                                \
         break;                                                                             \
       default:                                                                             \
-        e_ = launch_force(k_force_su2<T, 4, NTV, MB>, grid, NTV, s, pdl, SU2B_FORCE_ARGS);  \
+        e_ = launch_force(k_force_su2<T, 4, NTV, MB, AN>, grid, NTV, s, pdl,               \
+                          SU2B_FORCE_ARGS);                                                \
         break;                                                                             \
     }                                                                                      \
     if (e_ != cudaSuccess) return e_;                                                      \
@@ -518,7 +525,7 @@ cudaError_t force_update(const Geom &g, const void *U, int group, T *P, const T 
 #define SU2B_FORCE_SPLIT(NTV, MB)                                                            \
   do {                                                                                     \
     if (g.nd != 4) {                                                                       \
-      SU2B_FORCE_LAUNCH(128, 8);                                                           \
+      SU2B_FORCE_LAUNCH(128, 8, false);                                                    \
       break;                                                                               \
     }                                                                                      \
     const dim3 grid(cdiv(g.Vh, NTV / 4));                                                  \
@@ -527,18 +534,25 @@ cudaError_t force_update(const Geom &g, const void *U, int group, T *P, const T 
       launch_force(k_force_su2_split<T, NTV, MB>, grid, NTV, s, pdl, SU2B_FORCE_ARGS);     \
     if (e_ != cudaSuccess) return e_;                                                      \
   } while (0)
-    switch (v) {
-      case 0: SU2B_FORCE_LAUNCH(256, 4); break;
-      case 1: SU2B_FORCE_LAUNCH(128, 8); break;
-      case 2: SU2B_FORCE_LAUNCH(128, 4); break;
-      case 3: SU2B_FORCE_LAUNCH(128, 6); break;
-      case 4: SU2B_FORCE_LAUNCH(256, 2); break;
-      case 5: SU2B_FORCE_LAUNCH(256, 3); break;
-      case 6: SU2B_FORCE_SPLIT(128, 8); break;
-      default: SU2B_FORCE_SPLIT(256, 4); break;
+    // the anisotropic action (rare) runs one launch shape; the tuned shapes are isotropic and
+    // carry no code for the plane weights
+    if (aniso) {
+      SU2B_FORCE_LAUNCH(128, 6, true);
+    } else {
+      switch (v) {
+        case 0: SU2B_FORCE_LAUNCH(256, 4, false); break;
+        case 1: SU2B_FORCE_LAUNCH(128, 8, false); break;
+        case 2: SU2B_FORCE_LAUNCH(128, 4, false); break;
+        case 3: SU2B_FORCE_LAUNCH(128, 6, false); break;
+        case 4: SU2B_FORCE_LAUNCH(256, 2, false); break;
+        case 5: SU2B_FORCE_LAUNCH(256, 3, false); break;
+        case 6: SU2B_FORCE_SPLIT(128, 8); break;
+        default: SU2B_FORCE_LAUNCH(64, 16, false); break;
+      }
     }
-#undef SU2B_FORCE_SPLIT
 #undef SU2B_FORCE_LAUNCH
+#undef SU2B_FORCE_SPLIT
+#undef SU2B_FORCE_ARGS
     if (nblocks) *nblocks = nb;
   } else {
     if (sizeof(T) != 8) return cudaErrorNotSupported;

@@ -190,35 +190,7 @@ __device__ __forceinline__ double force_half_impl(const Geom &g, const LinkT<T> 
   return k2;
 }
 
-template <class T>
-__device__ __forceinline__ double force_half(const Geom &g, const LinkT<T> *__restrict__ U,
-                                             T *__restrict__ P, const T *__restrict__ extra, T f,
-                                             T scale_, int mode, int aniso, T wt, T ws,
-                                             LinkT<T> *__restrict__ Uout, T dt_upd, int half,
-                                             int p, int cb) {
-  if (half == 0)
-    return aniso ? force_half_impl<T, 0, true>(g, U, P, extra, f, scale_, mode, wt, ws, Uout,
-                                               dt_upd, p, cb)
-                 : force_half_impl<T, 0, false>(g, U, P, extra, f, scale_, mode, wt, ws, Uout,
-                                                dt_upd, p, cb);
-  return aniso ? force_half_impl<T, 1, true>(g, U, P, extra, f, scale_, mode, wt, ws, Uout,
-                                             dt_upd, p, cb)
-               : force_half_impl<T, 1, false>(g, U, P, extra, f, scale_, mode, wt, ws, Uout,
-                                              dt_upd, p, cb);
-}
 
-template <class T, int ND>
-__device__ __forceinline__ double force_site(const Geom &g, const LinkT<T> *__restrict__ U,
-                                             T *__restrict__ P, const T *__restrict__ extra, T f,
-                                             T scale_, int mode, int aniso, T wt, T ws,
-                                             LinkT<T> *__restrict__ Uout, T dt_upd, int p,
-                                             int cb) {
-  if (aniso)
-    return force_site_impl<T, ND, true>(g, U, P, extra, f, scale_, mode, wt, ws, Uout, dt_upd,
-                                        p, cb);
-  return force_site_impl<T, ND, false>(g, U, P, extra, f, scale_, mode, wt, ws, Uout, dt_upd, p,
-                                       cb);
-}
 
 // plaquettes of one site: sums over planes mu<nu of ReTr U_mu(x) U_nu(x+mu) U_mu(x+nu)^+
 // U_nu(x)^+ (flat-gauge_energy.hpp:31-94), FP64 products; {full, spatial (mu >= 1), xi-weighted}
