@@ -106,13 +106,8 @@ __global__ void __launch_bounds__(NT)
       for (int mu = 0; mu < d.g.nd; mu++) {
         const uint32_t lref = (uint32_t)s.lex * (uint32_t)d.g.nd + (uint32_t)mu;
         const size_t l = (size_t)mu * d.g.V + (size_t)p * d.g.Vh + cb;
-        uint32_t r[4];
-        T n[4];
-        philox(lref, 0u, *traj, TAG_MOMENTA, d.seed, r);
-        gauss_pair<T>(r, n[0], n[1]);
-        philox(lref, 1u, *traj, TAG_MOMENTA, d.seed, r);
-        gauss_pair<T>(r, n[2], n[3]);
-        const T a = n[0], b = n[1], cc = n[2];
+        T a, b, cc;
+        momentum_normals<T>(lref, *traj, d.seed, 3, a, b, cc);
         P[l] = a;
         P[NL + l] = b;
         P[2 * NL + l] = cc;

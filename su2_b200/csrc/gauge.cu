@@ -101,6 +101,46 @@ __global__ void __launch_bounds__(NT)
   if (threadIdx.x == 0) part[3 * b + 2] = r;
 }
 
+// The start of a trajectory in one pass over the sites: the Philox momenta of the site's
+// links (as k_momenta) with their |P|^2, and the site's plaquettes (as k_plaq_su2) for H_old.
+// Per block: {sum |P|^2, plaquettes, spatial plaquettes, xi-weighted plaquettes}.
+template <class T, int ND, int NT>
+__global__ void __launch_bounds__(NT)
+  k_momenta_plaq_su2(Geom g, const LinkT<T> *__restrict__ U, T *__restrict__ P,
+                     const TrajParams *__restrict__ tp, double xi, double *part) {
+  __shared__ double sh[NT / 32];
+  const int w = threadIdx.x >> 5, p = w & 1;
+  const int cb = blockIdx.x * (NT / 2) + (w >> 1) * 32 + (threadIdx.x & 31);
+  double k2 = 0., full = 0., spat = 0., wsum = 0.;
+  if (cb < g.Vh) {
+    const uint64_t seed = tp->seed;
+    const uint32_t traj = tp->traj;
+    const Site s = site_from_eo(g, p, cb);
+    const size_t NL = (size_t)g.V * ND;
+#pragma unroll
+    for (int mu = 0; mu < ND; mu++) {
+      const uint32_t lref = (uint32_t)s.lex * (uint32_t)ND + (uint32_t)mu;
+      const size_t l = (size_t)mu * g.V + (size_t)p * g.Vh + cb;
+      T n0, n1, n2;
+      momentum_normals<T>(lref, traj, seed, 3, n0, n1, n2);
+      P[l] = n0;
+      P[NL + l] = n1;
+      P[2 * NL + l] = n2;
+      k2 += (double)n0 * n0 + (double)n1 * n1 + (double)n2 * n2;
+    }
+    plaq_site<T, ND>(g, U, p, cb, xi, full, spat, wsum);
+  }
+  const int b = blockIdx.x;
+  double r = block_sum<NT>(k2, sh);
+  if (threadIdx.x == 0) part[4 * b] = r;
+  r = block_sum<NT>(full, sh);
+  if (threadIdx.x == 0) part[4 * b + 1] = r;
+  r = block_sum<NT>(spat, sh);
+  if (threadIdx.x == 0) part[4 * b + 2] = r;
+  r = block_sum<NT>(wsum, sh);
+  if (threadIdx.x == 0) part[4 * b + 3] = r;
+}
+
 template <int ND, int NT>
 __global__ void __launch_bounds__(NT)
   k_plaq_u1(Geom g, const double *__restrict__ U, double xi, double *part) {
@@ -137,14 +177,24 @@ __global__ void __launch_bounds__(NT)
   if (threadIdx.x == 0) part[3 * b + 2] = r;
 }
 
+// out[k] = sum over b of part[b*ncomp + k], one block, in an order fixed by n: thread t sums
+// the entries t + i NT into four accumulators (i mod 4), so four loads are in flight at a
+// time, then adds them pairwise and the block reduces in a fixed tree
 template <int NT>
 __global__ void __launch_bounds__(NT)
   k_reduce_final(const double *__restrict__ part, int n, int ncomp, double *out) {
   __shared__ double sh[NT / 32];
   for (int k = 0; k < ncomp; k++) {
-    double v = 0.;
-    for (int b = threadIdx.x; b < n; b += NT) v += part[(size_t)b * ncomp + k];
-    const double r = block_sum<NT>(v, sh);
+    double a0 = 0., a1 = 0., a2 = 0., a3 = 0.;
+    int b = threadIdx.x;
+    for (; b + 3 * NT < n; b += 4 * NT) {
+      a0 += part[(size_t)b * ncomp + k];
+      a1 += part[(size_t)(b + NT) * ncomp + k];
+      a2 += part[(size_t)(b + 2 * NT) * ncomp + k];
+      a3 += part[(size_t)(b + 3 * NT) * ncomp + k];
+    }
+    for (; b < n; b += NT) a0 += part[(size_t)b * ncomp + k];
+    const double r = block_sum<NT>((a0 + a1) + (a2 + a3), sh);
     if (threadIdx.x == 0) out[k] = r;
   }
 }
@@ -277,15 +327,11 @@ __global__ void __launch_bounds__(NT)
     const uint32_t lref = (uint32_t)s.lex * (uint32_t)g.nd + (uint32_t)mu;
     const size_t NL = (size_t)g.V * g.nd;
     const size_t l = (size_t)mu * g.V + (size_t)p * g.Vh + cb;
-    uint32_t r[4];
-    T n0, n1, n2, n3;
-    philox(lref, 0u, traj, TAG_MOMENTA, seed, r);
-    gauss_pair<T>(r, n0, n1);
+    T n0, n1, n2;
+    momentum_normals<T>(lref, traj, seed, na, n0, n1, n2);
     P[l] = n0;
     k2 = (double)n0 * n0;
     if (na == 3) {
-      philox(lref, 1u, traj, TAG_MOMENTA, seed, r);
-      gauss_pair<T>(r, n2, n3);
       P[NL + l] = n1;
       P[2 * NL + l] = n2;
       k2 += (double)n1 * n1 + (double)n2 * n2;
@@ -442,7 +488,7 @@ cudaError_t plaq_partials(const Geom &g, const void *U, int group, double xi, do
 
 cudaError_t reduce_final(const double *part, int nblocks, int ncomp, double *out,
                          cudaStream_t s) {
-  k_reduce_final<512><<<1, 512, 0, s>>>(part, nblocks, ncomp, out);
+  k_reduce_final<1024><<<1, 1024, 0, s>>>(part, nblocks, ncomp, out);
   return cudaGetLastError();
 }
 
@@ -610,6 +656,21 @@ cudaError_t momenta_philox(const Geom &g, T *P, int group, const TrajParams *tp,
 }
 
 template <class T>
+cudaError_t momenta_plaq(const Geom &g, const void *U, T *P, const TrajParams *tp, double xi,
+                         double *part, int *nblocks, cudaStream_t s) {
+  constexpr int NT = 256;
+  const dim3 grid(cdiv(g.Vh, NT / 2));
+  *nblocks = grid.x;
+  const LinkT<T> *u = (const LinkT<T> *)U;
+  switch (g.nd) {
+    case 2: k_momenta_plaq_su2<T, 2, NT><<<grid, NT, 0, s>>>(g, u, P, tp, xi, part); break;
+    case 3: k_momenta_plaq_su2<T, 3, NT><<<grid, NT, 0, s>>>(g, u, P, tp, xi, part); break;
+    default: k_momenta_plaq_su2<T, 4, NT><<<grid, NT, 0, s>>>(g, u, P, tp, xi, part); break;
+  }
+  return cudaGetLastError();
+}
+
+template <class T>
 cudaError_t kinetic_partials(const Geom &g, const T *P, int group, double *part, int *nblocks,
                              cudaStream_t s) {
   constexpr int NT = NT_RED;
@@ -663,6 +724,8 @@ cudaError_t cond_restore(const Geom &g, void *U, const void *U_old, int group,
   template cudaError_t restore_links<T>(const Geom &, void *, int, cudaStream_t);            \
   template cudaError_t momenta_philox<T>(const Geom &, T *, int, const TrajParams *,         \
                                          double *, int *, cudaStream_t);                      \
+  template cudaError_t momenta_plaq<T>(const Geom &, const void *, T *, const TrajParams *,  \
+                                       double, double *, int *, cudaStream_t);                \
   template cudaError_t kinetic_partials<T>(const Geom &, const T *, int, double *, int *,    \
                                            cudaStream_t);                                     \
   template cudaError_t negate_adj<T>(const Geom &, T *, int, cudaStream_t);                  \

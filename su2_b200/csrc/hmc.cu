@@ -174,17 +174,19 @@ int enqueue_fused(su2b_ctx *ctx, const std::vector<FOp> &fops, bool host_momenta
                   void *X, void *Y, void **fin) {
   cudaStream_t s = ctx->stream;
   int nb = 0;
-  if (!host_momenta) {
-    if (ctx->link64)
-      SU2B_LAUNCH(SU2B_K_MOMENTA, momenta_philox<double>(ctx->g, (double *)ctx->P, 0,
-                                                         ctx->tparams, ctx->part_slot(1), &nb, s));
-    else
-      SU2B_LAUNCH(SU2B_K_MOMENTA, momenta_philox<float>(ctx->g, (float *)ctx->P, 0, ctx->tparams,
-                                                        ctx->part_slot(1), &nb, s));
-    SU2B_LAUNCH(SU2B_K_OTHER, reduce_final(ctx->part_slot(1), nb, 1, ctx->red + 0, s));
-  }
   SU2B_CK(cudaMemsetAsync(ctx->red + 8, 0, 2 * sizeof(double), s));
-  SU2B_CKS(su2b_q_plaq(ctx, S, 1));
+  if (!host_momenta) {
+    // momenta, kinetic energy and the plaquettes of the start field in one pass: red[0..3]
+    if (ctx->link64)
+      SU2B_LAUNCH(SU2B_K_MOMENTA, momenta_plaq<double>(ctx->g, S, (double *)ctx->P, ctx->tparams,
+                                                       ctx->xi, ctx->part_slot(1), &nb, s));
+    else
+      SU2B_LAUNCH(SU2B_K_MOMENTA, momenta_plaq<float>(ctx->g, S, (float *)ctx->P, ctx->tparams,
+                                                      ctx->xi, ctx->part_slot(1), &nb, s));
+    SU2B_LAUNCH(SU2B_K_OTHER, reduce_final(ctx->part_slot(1), nb, 4, ctx->red + 0, s));
+  } else {
+    SU2B_CKS(su2b_q_plaq(ctx, S, 1));
+  }
   const double f = ctx->beta / ctx->Nc();
   void *cur = S;
   auto next = [&](void *c) { return c == X ? Y : X; };

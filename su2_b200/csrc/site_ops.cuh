@@ -218,22 +218,50 @@ __device__ __forceinline__ void plaq_site(const Geom &g, const LinkT<T> *__restr
   }
 }
 
-// Box-Muller pair from one Philox draw: FP64 from two 53-bit uniforms; the FP32 (mixed
-// precision) path uses 24-bit uniforms of the same words and FP32 transcendentals.
-template <class T> __device__ __forceinline__ void gauss_pair(const uint32_t r[4], T &a, T &b);
-template <>
-__device__ __forceinline__ void gauss_pair<double>(const uint32_t r[4], double &a, double &b) {
+// Box-Muller pair from one Philox draw: FP64 from two 53-bit uniforms (all four words).
+__device__ __forceinline__ void gauss_pair64(const uint32_t r[4], double &a, double &b) {
   box_muller(u01_53(r[0], r[1]), u01_53(r[2], r[3]), a, b);
 }
-template <>
-__device__ __forceinline__ void gauss_pair<float>(const uint32_t r[4], float &a, float &b) {
-  const float u1 = ((float)(r[0] >> 8) + 1.0f) * 0x1p-24f;  // (0, 1]
-  const float u2 = (float)(r[2] >> 8) * 0x1p-24f;           // [0, 1)
+// FP32 Box-Muller pair from two words: 24-bit uniforms and FP32 transcendentals
+__device__ __forceinline__ void gauss_pair32(uint32_t w1, uint32_t w2, float &a, float &b) {
+  const float u1 = ((float)(w1 >> 8) + 1.0f) * 0x1p-24f;  // (0, 1]
+  const float u2 = (float)(w2 >> 8) * 0x1p-24f;           // [0, 1)
   const float rad = sqrtf(-2.0f * logf(u1));
   float sn, cs;
   sincospif(2.0f * u2, &sn, &cs);
   a = rad * cs;
   b = rad * sn;
+}
+
+// The three standard normals of the SU(2) momentum of link lref (reference link index) for
+// trajectory traj: Philox(seed; {lref, draw, traj, TAG_MOMENTA}).  FP64 uses draws 0 and 1
+// (a 53-bit Box-Muller pair each); FP32 gets four words from draw 0 alone, two pairs of
+// 24-bit uniforms.  U(1) momenta use the first normal.
+template <class T>
+__device__ __forceinline__ void momentum_normals(uint32_t lref, uint32_t traj, uint64_t seed,
+                                                 int na, T &n0, T &n1, T &n2);
+template <>
+__device__ __forceinline__ void momentum_normals<double>(uint32_t lref, uint32_t traj,
+                                                         uint64_t seed, int na, double &n0,
+                                                         double &n1, double &n2) {
+  uint32_t r[4];
+  double n3;
+  philox(lref, 0u, traj, TAG_MOMENTA, seed, r);
+  gauss_pair64(r, n0, n1);
+  if (na == 3) {
+    philox(lref, 1u, traj, TAG_MOMENTA, seed, r);
+    gauss_pair64(r, n2, n3);
+  }
+}
+template <>
+__device__ __forceinline__ void momentum_normals<float>(uint32_t lref, uint32_t traj,
+                                                        uint64_t seed, int na, float &n0,
+                                                        float &n1, float &n2) {
+  uint32_t r[4];
+  float n3;
+  philox(lref, 0u, traj, TAG_MOMENTA, seed, r);
+  gauss_pair32(r[0], r[1], n0, n1);
+  if (na == 3) gauss_pair32(r[2], r[3], n2, n3);
 }
 
 }  // namespace su2b

@@ -63,6 +63,11 @@ struct TrajParams {
 template <class T>
 cudaError_t momenta_philox(const Geom &g, T *P, int group, const TrajParams *tp,
                            double *kin_part, int *nblocks, cudaStream_t s);
+// SU(2): the Philox momenta of every link and the plaquette sums of the field in one pass;
+// partials {|P|^2, plaquettes, spatial, weighted} per block (4 per block)
+template <class T>
+cudaError_t momenta_plaq(const Geom &g, const void *U, T *P, const TrajParams *tp, double xi,
+                         double *part, int *nblocks, cudaStream_t s);
 template <class T>
 cudaError_t kinetic_partials(const Geom &g, const T *P, int group, double *part, int *nblocks,
                              cudaStream_t s);
