@@ -85,7 +85,7 @@ __global__ void k_spinor_to_host(Geom g, const double2 *__restrict__ psi, double
 // plaquettes: per site, sum over planes mu<nu of ReTr U_mu(x) U_nu(x+mu) U_mu(x+nu)^+ U_nu(x)^+
 // (flat-gauge_energy.hpp:31-94), FP64 products.  Partials {full, spatial, xi-weighted}.
 template <class T, int ND, int NT>
-__global__ void __launch_bounds__(NT)
+__global__ void __launch_bounds__(NT, 1024 / NT)
   k_plaq_su2(Geom g, const LinkT<T> *__restrict__ U, double xi, double *part) {
   __shared__ double sh[NT / 32];
   const int w = threadIdx.x >> 5, p = w & 1;
@@ -105,7 +105,7 @@ __global__ void __launch_bounds__(NT)
 // links (as k_momenta) with their |P|^2, and the site's plaquettes (as k_plaq_su2) for H_old.
 // Per block: {sum |P|^2, plaquettes, spatial plaquettes, xi-weighted plaquettes}.
 template <class T, int ND, int NT>
-__global__ void __launch_bounds__(NT)
+__global__ void __launch_bounds__(NT, 1024 / NT)
   k_momenta_plaq_su2(Geom g, const LinkT<T> *__restrict__ U, T *__restrict__ P,
                      const TrajParams *__restrict__ tp, double xi, double *part) {
   __shared__ double sh[NT / 32];
