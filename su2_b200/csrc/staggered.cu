@@ -816,6 +816,10 @@ cudaError_t cg_persistent(const Geom &g, const double2 *ph, double m, double2 *x
   void *args[] = {&gg, (void *)&ph, &mm, &x, &r, &p, &t, &part_t, &part_r, &st, &bar};
   e = cudaLaunchCooperativeKernel((const void *)k_cg_persistent<NT>, dim3(G), dim3(NT), args, 0,
                                   s);
+  if (e == cudaErrorCooperativeLaunchTooLarge) {  // fewer SMs available (shared GPU): queue
+    cudaGetLastError();                           // the per-phase kernels instead
+    return cudaErrorNotSupported;
+  }
   return e;
 }
 
