@@ -316,7 +316,7 @@ def ours(args):
             "config": {"workload": WORKLOAD + " (mixed precision)", "lattice": [L] * 4,
                        "beta": BETA, "integrator": "omf2", "n_steps": NSTEPS, "tau": TAU,
                        "replicas": ws, "parallelism": f"replicas x{ws}",
-                       "l2": "working set per step (U, U_old, P) > 126 MB L2; no flush"},
+                       "l2": "working set per step (three link buffers, P) > 126 MB L2; no flush"},
             "mixed": dict(traj_per_s=value, **stats(res_m, V)),
             "fp64": dict(traj_per_s=ws * K / t_fp64, **stats(res_d, V)),
             "speedup_mixed_vs_fp64": t_fp64 / t_mixed,
@@ -328,6 +328,9 @@ def ours(args):
                          "frac": roof["mixed"]["GB/s"] / hbm, "traffic": traffic,
                          "bytes_per_launch": 56 * NL, "avg_launch_us": roof["mixed"]["avg_us"],
                          "peak_source": peak_src,
+                         "timing": f"CUDA events around every force launch over {max(2, K // 2)} "
+                                   "trajectories right after the timed region (same field, "
+                                   "direct launches instead of the graph)",
                          "fp64_kernel": {"achieved": roof["fp64"]["GB/s"],
                                          "frac": roof["fp64"]["GB/s"] / hbm,
                                          "bytes_per_launch": 112 * NL,
