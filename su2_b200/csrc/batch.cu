@@ -46,10 +46,9 @@ __device__ __forceinline__ int chain_of(const ChainDev *__restrict__ ch, int n, 
   return lo;
 }
 
-// launch shapes of the batched kernels: threads per block (a tile is NT/2 sites of each
-// parity of one chain) and, for the force kernel, the minimum resident blocks per SM
+// threads per block of the batched launch shapes (a tile is NT/2 sites of each parity of one
+// chain); the force kernel's minimum resident blocks per SM are 8, 4, 6, 3 (enqueue_batch)
 constexpr int BATCH_NT[SU2B_BATCH_VARIANTS] = {64, 128, 128, 256};
-constexpr int BATCH_MINB[SU2B_BATCH_VARIANTS] = {8, 4, 6, 3};
 
 template <class T> struct Bufs {
   LinkT<T> *b[3];
