@@ -265,6 +265,33 @@ int cg_mixed(su2b_ctx *ctx, double m, double tol, int max_iter, double delta,
   h.done = (h.rn > tol) ? 0 : 1;
   SU2B_CKS(upload_state(ctx, h));
   int done = h.done;
+  if (!done) {
+    // the whole solve in one cooperative launch
+    double *slot = ctx->part_slot(5);
+    void *bar = slot + 3 * ctx->part_cap - 4;
+    const cudaError_t e = cg_mixed_persistent(g, ctx->ph, ctx->ph32, m, b, x, r, t, xs, rs, ps,
+                                              ts, slot, ctx->st, bar,
+                                              (int)(3 * ctx->part_cap - 8), s);
+    if (e != cudaErrorNotSupported) {
+      SU2B_CK(e);
+      ctx->launches++;
+      int failed = 0;
+      if (cg_barrier_failed(bar, s, &failed))
+        return su2b_fail(ctx, SU2B_ERR_CUDA, "persistent mixed CG: %s",
+                         cudaGetErrorString(cudaGetLastError()));
+      if (failed)
+        return su2b_fail(ctx, SU2B_ERR_TIMEOUT, "persistent mixed CG: a grid barrier gave up");
+      SU2B_CKS(fetch_state(ctx));
+      h = *ctx->h_st;
+      if (stats) {
+        stats->iterations = h.iters;
+        stats->restarts = h.updates;
+        stats->residual = h.rn;
+        stats->true_residual = h.rn;
+      }
+      return finish_status(ctx, h.done);
+    }
+  }
   while (!done) {
     for (int k = 0; k < CHUNK; k++) {
       SU2B_LAUNCH(SU2B_K_STAGGERED, hop32(g, ctx->ph32, m32, 1, ps, ts, nullptr, nullptr, nullptr, ctx->st, s));

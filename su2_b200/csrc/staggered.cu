@@ -284,6 +284,28 @@ __device__ __forceinline__ double2 hop_site64(const Geom &g, const double2 *__re
   return make_double2(m * self.x + sgn * accr, m * self.y + sgn * acci);
 }
 
+__device__ __forceinline__ float2 hop_site32(const Geom &g, const float2 *__restrict__ ph,
+                                             float m, float sgn, const float2 *__restrict__ in,
+                                             int p, int cb) {
+  const Site s = site_from_eo(g, p, cb);
+  float accr = 0.f, acci = 0.f;
+  int esum = 0;
+  for (int mu = 0; mu < g.nd; mu++) {
+    const float eta = (esum & 1) ? -0.5f : 0.5f;
+    esum += s.c[mu];
+    const int lp = s.lex + fwd(g, s, mu), lm = s.lex + bwd(g, s, mu);
+    const float2 up = ph[(size_t)mu * g.V + (size_t)p * g.Vh + cb];
+    const float2 um = ph[(size_t)mu * g.V + eo_of(g, lm, 1 - p)];
+    const float2 fp = __ldcg(&in[eo_of(g, lp, 1 - p)]), fm = __ldcg(&in[eo_of(g, lm, 1 - p)]);
+    const float tr = (up.x * fp.x - up.y * fp.y) - (um.x * fm.x + um.y * fm.y);
+    const float ti = (up.x * fp.y + up.y * fp.x) - (um.x * fm.y - um.y * fm.x);
+    accr += eta * tr;
+    acci += eta * ti;
+  }
+  const float2 self = __ldcg(&in[(size_t)p * g.Vh + cb]);
+  return make_float2(m * self.x + sgn * accr, m * self.y + sgn * acci);
+}
+
 struct GridBarrier {
   unsigned count;
   unsigned gen;
@@ -415,6 +437,137 @@ __global__ void __launch_bounds__(NT)
     st->rr = rr;
     st->rn = rn;
     st->iters = iters;
+    st->done = done;
+  }
+}
+
+// ---- persistent mixed-precision CG: FP32 iterations, FP64 reliable updates ----
+// The iteration of k_cg_persistent in FP32 vectors (ts = D^+ ps kept by linearity).  When the
+// iterated |rs| falls below delta times |r| at the last update, or below the tolerance, every
+// block takes a reliable update: x += xs, xs = 0; r = b - D D^+ x in FP64 (two stencil
+// phases); rs = (float) r; convergence is decided on that true residual.  The decisions come
+// from sums every block forms in the same order, so all blocks take them together.
+template <int NT>
+__global__ void __launch_bounds__(NT)
+  k_cg_mixed_persistent(Geom g, const double2 *__restrict__ ph, const float2 *__restrict__ ph32,
+                        double m, const double2 *__restrict__ b, double2 *x, double2 *r,
+                        double2 *t64, float2 *xs, float2 *rs, float2 *ps, float2 *ts,
+                        double *part_t, double *part_r, SolverState *st, GridBarrier *bar) {
+  __shared__ double sh[NT / 32];
+  const int n = g.V, G = gridDim.x;
+  const int first = blockIdx.x * NT + threadIdx.x, stride = G * NT;
+  const float m32 = (float)m;
+  double rr = st->rr.x, rn = st->rn, maxr = st->maxr;
+  const double delta = st->delta, tol = st->tol;
+  long iters = st->iters, updates = st->updates;
+  const long max_iter = st->max_iter;
+  int done = st->done;
+  // ts = D^+ ps, |ts|^2
+  double acc = 0.;
+  for (int i = first; i < n; i += stride) {
+    const int pp = i >= g.Vh, cb = i - pp * g.Vh;
+    const float2 v = hop_site32(g, ph32, m32, -1.f, ps, pp, cb);
+    ts[i] = v;
+    acc += (double)v.x * v.x + (double)v.y * v.y;
+  }
+  double bs = block_sum<NT>(acc, sh);
+  if (threadIdx.x == 0) part_t[blockIdx.x] = bs;
+  if (!grid_sync(bar)) return;
+  while (!done) {
+    const float alpha = (float)(rr / fixed_sum<NT>(part_t, G));
+    acc = 0.;
+    for (int i = first; i < n; i += stride) {
+      const int pp = i >= g.Vh, cb = i - pp * g.Vh;
+      const float2 aq = hop_site32(g, ph32, m32, 1.f, ts, pp, cb);  // A ps = D ts
+      const float2 pv = ps[i];
+      float2 xv = xs[i], rv = rs[i];
+      xv.x += alpha * pv.x;
+      xv.y += alpha * pv.y;
+      rv.x -= alpha * aq.x;
+      rv.y -= alpha * aq.y;
+      xs[i] = xv;
+      rs[i] = rv;
+      acc += (double)rv.x * rv.x + (double)rv.y * rv.y;
+    }
+    bs = block_sum<NT>(acc, sh);
+    if (threadIdx.x == 0) part_r[blockIdx.x] = bs;
+    if (!grid_sync(bar)) return;
+    double rr_new = fixed_sum<NT>(part_r, G);
+    rn = sqrt(rr_new);
+    iters++;
+    if (rn != rn) {
+      done = 3;
+      break;
+    }
+    const bool update = rn < delta * maxr || !(rn > tol);
+    if (!update && iters >= max_iter) {
+      done = 2;
+      break;
+    }
+    if (update) {
+      for (int i = first; i < n; i += stride) {  // x += xs; xs = 0
+        const float2 v = xs[i];
+        x[i] = make_double2(x[i].x + (double)v.x, x[i].y + (double)v.y);
+        xs[i] = make_float2(0.f, 0.f);
+      }
+      if (!grid_sync(bar)) return;
+      for (int i = first; i < n; i += stride) {  // t64 = D^+ x
+        const int pp = i >= g.Vh, cb = i - pp * g.Vh;
+        t64[i] = hop_site64(g, ph, m, -1.0, x, pp, cb);
+      }
+      if (!grid_sync(bar)) return;
+      acc = 0.;
+      for (int i = first; i < n; i += stride) {  // r = b - D t64; rs = (float) r
+        const int pp = i >= g.Vh, cb = i - pp * g.Vh;
+        const double2 ax = hop_site64(g, ph, m, 1.0, t64, pp, cb);
+        const double2 v = make_double2(b[i].x - ax.x, b[i].y - ax.y);
+        r[i] = v;
+        rs[i] = make_float2((float)v.x, (float)v.y);
+        acc += v.x * v.x + v.y * v.y;
+      }
+      bs = block_sum<NT>(acc, sh);
+      if (threadIdx.x == 0) part_r[blockIdx.x] = bs;
+      if (!grid_sync(bar)) return;
+      rr_new = fixed_sum<NT>(part_r, G);
+      rn = sqrt(rr_new);
+      maxr = rn;
+      updates++;
+      if (!(rn > tol)) {
+        done = 1;
+        break;
+      }
+      if (iters >= max_iter) {
+        done = 2;
+        break;
+      }
+    }
+    const float beta = (float)(rr_new / rr);
+    rr = rr_new;
+    acc = 0.;
+    for (int i = first; i < n; i += stride) {  // ps = rs + beta ps; ts = D^+ rs + beta ts
+      const int pp = i >= g.Vh, cb = i - pp * g.Vh;
+      const float2 dr = hop_site32(g, ph32, m32, -1.f, rs, pp, cb);
+      const float2 rv = rs[i], pv = ps[i], tv = ts[i];
+      ps[i] = make_float2(rv.x + beta * pv.x, rv.y + beta * pv.y);
+      const float2 tn = make_float2(dr.x + beta * tv.x, dr.y + beta * tv.y);
+      ts[i] = tn;
+      acc += (double)tn.x * tn.x + (double)tn.y * tn.y;
+    }
+    bs = block_sum<NT>(acc, sh);
+    if (threadIdx.x == 0) part_t[blockIdx.x] = bs;
+    if (!grid_sync(bar)) return;
+  }
+  if (done == 2 || done == 3)  // fold the FP32 correction into x
+    for (int i = first; i < n; i += stride) {
+      const float2 v = xs[i];
+      x[i] = make_double2(x[i].x + (double)v.x, x[i].y + (double)v.y);
+    }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    st->rr = make_double2(rr, 0.0);
+    st->rn = rn;
+    st->maxr = maxr;
+    st->iters = iters;
+    st->updates = updates;
     st->done = done;
   }
 }
@@ -818,6 +971,41 @@ cudaError_t cg_persistent(const Geom &g, const double2 *ph, double m, double2 *x
                                   s);
   if (e == cudaErrorCooperativeLaunchTooLarge) {  // fewer SMs available (shared GPU): queue
     cudaGetLastError();                           // the per-phase kernels instead
+    return cudaErrorNotSupported;
+  }
+  return e;
+}
+
+// the persistent mixed-precision CG (k_cg_mixed_persistent); the same launch rules as
+// cg_persistent
+cudaError_t cg_mixed_persistent(const Geom &g, const double2 *ph, const float2 *ph32, double m,
+                                const double2 *b, double2 *x, double2 *r, double2 *t64,
+                                float2 *xs, float2 *rs, float2 *ps, float2 *ts, double *part,
+                                SolverState *st, void *bar_mem, int part_cap, cudaStream_t s) {
+  constexpr int NT = 512;
+  static int grid = -1;
+  if (grid < 0) {
+    int dev = 0, coop = 0, sms = 0, per_sm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_cg_mixed_persistent<NT>, NT, 0);
+    grid = (coop && per_sm >= 1) ? sms : 0;
+  }
+  const int G = std::min(grid, std::max(1, (g.V + NT - 1) / NT));
+  if (G <= 0 || 2 * G > part_cap || G > 32 * FIXED_SUM_PER_LANE) return cudaErrorNotSupported;
+  GridBarrier *bar = (GridBarrier *)bar_mem;
+  cudaError_t e = cudaMemsetAsync(bar, 0, sizeof(GridBarrier), s);
+  if (e != cudaSuccess) return e;
+  double *part_t = part, *part_r = part + G;
+  Geom gg = g;
+  double mm = m;
+  void *args[] = {&gg, (void *)&ph, (void *)&ph32, &mm, (void *)&b, &x, &r, &t64,
+                  &xs, &rs, &ps, &ts, &part_t, &part_r, &st, &bar};
+  e = cudaLaunchCooperativeKernel((const void *)k_cg_mixed_persistent<NT>, dim3(G), dim3(NT),
+                                  args, 0, s);
+  if (e == cudaErrorCooperativeLaunchTooLarge) {
+    cudaGetLastError();
     return cudaErrorNotSupported;
   }
   return e;
