@@ -1,7 +1,10 @@
 // solve.cu -- host drivers of the staggered operator and Krylov solvers (U(1) only) and of
 // the det(D Ddag) pseudofermion monomial (detDDdag_monomial.hh).
 //
-// The solvers queue CHUNK iterations at a time; every kernel of an iteration checks the
+// Each solver runs as one persistent cooperative launch (CG, mixed CG, BiCGStab in
+// staggered.cu) that iterates until convergence behind bounded grid barriers.  Where a
+// cooperative launch of one block per SM is not possible, the solvers queue CHUNK iterations
+// of per-phase kernels at a time instead; every kernel of an iteration checks the
 // device-side SolverState and returns at once after convergence, so the host reads the
 // state back once per chunk.  After convergence the true residual |b - A x| is recomputed
 // in FP64 and, as CG.hpp:76-84 / BiCGStab.hpp:79-94 do, the solve restarts from x while the
@@ -199,6 +202,26 @@ int bicgstab64(su2b_ctx *ctx, double m, double tol, int max_iter, su2b_solve_sta
     SU2B_CK(cudaMemcpyAsync(p, r0, n * sizeof(double2), cudaMemcpyDeviceToDevice, s));
     SU2B_CKS(upload_state(ctx, h));
     int done = h.done;
+    if (!done) {
+      // the whole solve in one cooperative launch (three grid barriers per iteration)
+      double *slot = ctx->part_slot(5);
+      void *bar = slot + 3 * ctx->part_cap - 4;
+      const cudaError_t e =
+        bicgstab_persistent(g, ctx->ph, m, x, r, r0, p, ctx->sv[SV_P2], Ap, ctx->sv[SV_AP2], sv,
+                            t, slot, ctx->st, bar, (int)(3 * ctx->part_cap - 8), s);
+      if (e != cudaErrorNotSupported) {
+        SU2B_CK(e);
+        ctx->launches++;
+        int failed = 0;
+        if (cg_barrier_failed(bar, s, &failed))
+          return su2b_fail(ctx, SU2B_ERR_CUDA, "persistent BiCGStab: %s",
+                           cudaGetErrorString(cudaGetLastError()));
+        if (failed)
+          return su2b_fail(ctx, SU2B_ERR_TIMEOUT, "persistent BiCGStab: a grid barrier gave up");
+        SU2B_CKS(fetch_state(ctx));
+        done = ctx->h_st->done;
+      }
+    }
     while (!done) {
       for (int k = 0; k < CHUNK; k++) {
         SU2B_LAUNCH(SU2B_K_STAGGERED, hop64(g, ctx->ph, m, 0, p, Ap, r0, dp, nullptr, ctx->st, 0, s));

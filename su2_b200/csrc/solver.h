@@ -62,6 +62,11 @@ cudaError_t cg_mixed_persistent(const Geom &g, const double2 *ph, const float2 *
                                 const double2 *b, double2 *x, double2 *r, double2 *t64,
                                 float2 *xs, float2 *rs, float2 *ps, float2 *ts, double *part,
                                 SolverState *st, void *bar_mem, int part_cap, cudaStream_t s);
+cudaError_t bicgstab_persistent(const Geom &g, const double2 *ph, double m, double2 *x,
+                                double2 *r, const double2 *r0, double2 *p, double2 *p2,
+                                double2 *Ap, double2 *Ap2, double2 *sv, double2 *t,
+                                double *part, SolverState *st, void *bar_mem, int part_cap,
+                                cudaStream_t s);
 int cg_barrier_failed(const void *bar_mem, cudaStream_t s, int *failed);
 size_t cg_barrier_bytes();
 

@@ -260,9 +260,10 @@ __global__ void __launch_bounds__(NT)
 // Every block reduces the per-block partials itself in one fixed order, so all blocks take
 // the same decisions and leave the loop together.  Barrier waits are bounded: a wait that
 // gives up sets *err and every block returns.
-__device__ __forceinline__ double2 hop_site64(const Geom &g, const double2 *__restrict__ ph,
-                                              double m, double sgn,
-                                              const double2 *__restrict__ in, int p, int cb) {
+// m*in + sgn*hop(in) at one site, with in(j) the input vector's value at even/odd index j
+template <class In>
+__device__ __forceinline__ double2 hop_site64_f(const Geom &g, const double2 *__restrict__ ph,
+                                                double m, double sgn, In in, int p, int cb) {
   const Site s = site_from_eo(g, p, cb);
   double accr = 0, acci = 0;
   int esum = 0;
@@ -272,16 +273,21 @@ __device__ __forceinline__ double2 hop_site64(const Geom &g, const double2 *__re
     const int lp = s.lex + fwd(g, s, mu), lm = s.lex + bwd(g, s, mu);
     const double2 up = ph[(size_t)mu * g.V + (size_t)p * g.Vh + cb];
     const double2 um = ph[(size_t)mu * g.V + eo_of(g, lm, 1 - p)];
-    // neighbours belong to other blocks and change every iteration: read through L2 only
-    // (the SM's L1 is not coherent with the other SMs' stores)
-    const double2 fp = __ldcg(&in[eo_of(g, lp, 1 - p)]), fm = __ldcg(&in[eo_of(g, lm, 1 - p)]);
+    const double2 fp = in(eo_of(g, lp, 1 - p)), fm = in(eo_of(g, lm, 1 - p));
     const double tr = (up.x * fp.x - up.y * fp.y) - (um.x * fm.x + um.y * fm.y);
     const double ti = (up.x * fp.y + up.y * fp.x) - (um.x * fm.y - um.y * fm.x);
     accr += eta * tr;
     acci += eta * ti;
   }
-  const double2 self = __ldcg(&in[(size_t)p * g.Vh + cb]);
+  const double2 self = in((size_t)p * g.Vh + cb);
   return make_double2(m * self.x + sgn * accr, m * self.y + sgn * acci);
+}
+__device__ __forceinline__ double2 hop_site64(const Geom &g, const double2 *__restrict__ ph,
+                                              double m, double sgn,
+                                              const double2 *__restrict__ in, int p, int cb) {
+  // neighbours belong to other blocks and change every iteration: read through L2 only
+  // (the SM's L1 is not coherent with the other SMs' stores)
+  return hop_site64_f(g, ph, m, sgn, [in](size_t j) { return __ldcg(&in[j]); }, p, cb);
 }
 
 __device__ __forceinline__ float2 hop_site32(const Geom &g, const float2 *__restrict__ ph,
@@ -568,6 +574,212 @@ __global__ void __launch_bounds__(NT)
     st->maxr = maxr;
     st->iters = iters;
     st->updates = updates;
+    st->done = done;
+  }
+}
+
+// ---- persistent BiCGStab ----
+// K deterministic block sums in one shared-memory round trip; the results are in thread 0
+template <int NT, int K> __device__ __forceinline__ void block_sums(double (&v)[K], double *sh) {
+#pragma unroll
+  for (int k = 0; k < K; k++)
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_down_sync(0xffffffffu, v[k], o);
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  if (l == 0)
+#pragma unroll
+    for (int k = 0; k < K; k++) sh[k * (NT / 32) + w] = v[k];
+  __syncthreads();
+  if (w == 0)
+#pragma unroll
+    for (int k = 0; k < K; k++) {
+      double r = (l < NT / 32) ? sh[k * (NT / 32) + l] : 0.0;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) r += __shfl_down_sync(0xffffffffu, r, o);
+      v[k] = r;
+    }
+  __syncthreads();
+}
+// fixed_sum of K arrays part[k*n .. k*n+n) at once: one L2 round trip for all of them
+template <int K> __device__ __forceinline__ void fixed_sums(const double *part, int n,
+                                                           double (&out)[K]) {
+  __shared__ double bc[K];
+  if (threadIdx.x < 32) {
+    double v[K][FIXED_SUM_PER_LANE];
+#pragma unroll
+    for (int k = 0; k < K; k++)
+#pragma unroll
+      for (int j = 0; j < FIXED_SUM_PER_LANE; j++) {
+        const int i = threadIdx.x + 32 * j;
+        v[k][j] = i < n ? __ldcg(&part[k * n + i]) : 0.0;
+      }
+#pragma unroll
+    for (int k = 0; k < K; k++) {
+      double a = 0.;
+#pragma unroll
+      for (int j = 0; j < FIXED_SUM_PER_LANE; j++) a += v[k][j];
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
+      if (threadIdx.x == 0) bc[k] = a;
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int k = 0; k < K; k++) out[k] = bc[k];
+  __syncthreads();
+}
+
+// BiCGStab on D (BiCGStab.hpp:50-77) in one cooperative launch: three grid barriers per
+// iteration, one per global reduction.  Where the vector a stencil phase applies D to is a
+// combination of vectors the previous phase left, the combination is formed at every
+// neighbour as it is read instead of being stored first (storing it would cost a barrier):
+//   P1  p = r + beta p - (beta omega) Ap  (formed per site);  Ap = D p;  partial <r0, Ap>
+//   P2  alpha = r0r / <r0, Ap>;  s = r - alpha Ap (formed per site);  t = D s;
+//       partials <t, s>, <t, t>
+//   P3  omega = <t, s> / <t, t>;  r = s - omega t;  x = x + omega s + alpha p;
+//       partials <r0, r>, |r|^2;  beta = (<r0, r> / r0r)(alpha / omega)
+// so A p and A s are applied directly, as in the reference, not carried by recurrences.  P1
+// writes p and Ap while the neighbours still read the previous ones, so both alternate
+// between two buffers.  In the first iteration p is the start residual as given.  The
+// per-element arithmetic is that of the per-phase kernels below (k_bi_s, k_bi_rx, k_bi_p).
+__device__ __forceinline__ double2 bi_comb_p(double2 rv, double2 pv, double2 qv, double2 be,
+                                             double2 bo) {
+  const double2 bp = cm(be, pv), bq = cm(bo, qv);
+  const double2 t = make_double2(rv.x + 1.0 * bp.x, rv.y + 1.0 * bp.y);
+  return make_double2(t.x + (-1.0) * bq.x, t.y + (-1.0) * bq.y);
+}
+__device__ __forceinline__ double2 bi_comb_s(double2 rv, double2 qv, double2 al) {
+  const double2 aq = cm(al, qv);
+  return make_double2(rv.x + (-1.0) * aq.x, rv.y + (-1.0) * aq.y);
+}
+
+template <int NT>
+__global__ void __launch_bounds__(NT)
+  k_bicgstab_persistent(Geom g, const double2 *__restrict__ ph, double m, double2 *x,
+                        double2 *r, const double2 *__restrict__ r0, double2 *p, double2 *pn,
+                        double2 *Ap, double2 *Apn, double2 *s, double2 *t, double *part,
+                        SolverState *st, GridBarrier *bar) {
+  __shared__ double sh[3 * (NT / 32)];
+  const int n = g.V, G = gridDim.x;
+  const int first = blockIdx.x * NT + threadIdx.x, stride = G * NT;
+  // per-phase partial arrays: consecutive phases never share one (a block may write the next
+  // phase's partials while another still reads the previous phase's)
+  double *part1 = part, *part2 = part + 2 * G, *part3 = part + 5 * G;
+  double2 r0r = st->r0r, alpha = make_double2(0., 0.), omega = make_double2(0., 0.),
+          beta = make_double2(0., 0.);
+  double rn = st->rn;
+  long iters = st->iters;
+  const long max_iter = st->max_iter;
+  const double tol = st->tol;
+  int done = st->done;
+  bool start = true;
+  while (!done) {
+    {  // P1
+      double v[2] = {0., 0.};
+      const double2 be = beta, bo = cm(beta, omega);
+      for (int i = first; i < n; i += stride) {
+        const int pp = i >= g.Vh, cb = i - pp * g.Vh;
+        double2 ap, pv;
+        if (start) {
+          ap = hop_site64(g, ph, m, 1.0, p, pp, cb);
+          pv = p[i];
+        } else {
+          const auto pf = [=](size_t j) {
+            return bi_comb_p(__ldcg(&r[j]), __ldcg(&p[j]), __ldcg(&Ap[j]), be, bo);
+          };
+          ap = hop_site64_f(g, ph, m, 1.0, pf, pp, cb);
+          pv = pf(i);
+        }
+        pn[i] = pv;
+        Apn[i] = ap;
+        const double2 d = cmc(r0[i], ap);
+        v[0] += d.x;
+        v[1] += d.y;
+      }
+      block_sums<NT, 2>(v, sh);
+      if (threadIdx.x == 0) {
+        part1[blockIdx.x] = v[0];
+        part1[G + blockIdx.x] = v[1];
+      }
+      if (!grid_sync(bar)) return;
+      double2 *tmp = p;
+      p = pn;
+      pn = tmp;
+      tmp = Ap;
+      Ap = Apn;
+      Apn = tmp;
+      start = false;
+    }
+    {  // P2
+      double q[2];
+      fixed_sums<2>(part1, G, q);
+      alpha = cdivs(r0r, make_double2(q[0], q[1]));
+      const double2 al = alpha;
+      double v[3] = {0., 0., 0.};
+      const auto sf = [=](size_t j) { return bi_comb_s(__ldcg(&r[j]), __ldcg(&Ap[j]), al); };
+      for (int i = first; i < n; i += stride) {
+        const int pp = i >= g.Vh, cb = i - pp * g.Vh;
+        const double2 tv = hop_site64_f(g, ph, m, 1.0, sf, pp, cb);
+        const double2 sv = sf(i);
+        s[i] = sv;
+        t[i] = tv;
+        const double2 d = cmc(tv, sv);
+        v[0] += d.x;
+        v[1] += d.y;
+        v[2] += tv.x * tv.x + tv.y * tv.y;
+      }
+      block_sums<NT, 3>(v, sh);
+      if (threadIdx.x == 0) {
+        part2[blockIdx.x] = v[0];
+        part2[G + blockIdx.x] = v[1];
+        part2[2 * G + blockIdx.x] = v[2];
+      }
+      if (!grid_sync(bar)) return;
+    }
+    {  // P3
+      double q[3];
+      fixed_sums<3>(part2, G, q);
+      omega = cdivs(make_double2(q[0], q[1]), make_double2(q[2], 0.0));
+      const double2 om = omega, al = alpha;
+      double v[3] = {0., 0., 0.};
+      for (int i = first; i < n; i += stride) {
+        const double2 sv = s[i], tv = t[i], pv = p[i], xv = x[i];
+        const double2 ot = cm(om, tv);
+        const double2 rnw = make_double2(sv.x + (-1.0) * ot.x, sv.y + (-1.0) * ot.y);
+        r[i] = rnw;
+        const double2 os = cm(om, sv), ap = cm(al, pv);
+        const double2 x1 = make_double2(xv.x + 1.0 * os.x, xv.y + 1.0 * os.y);
+        x[i] = make_double2(x1.x + 1.0 * ap.x, x1.y + 1.0 * ap.y);
+        const double2 d = cmc(r0[i], rnw);
+        v[0] += d.x;
+        v[1] += d.y;
+        v[2] += rnw.x * rnw.x + rnw.y * rnw.y;
+      }
+      block_sums<NT, 3>(v, sh);
+      if (threadIdx.x == 0) {
+        part3[blockIdx.x] = v[0];
+        part3[G + blockIdx.x] = v[1];
+        part3[2 * G + blockIdx.x] = v[2];
+      }
+      if (!grid_sync(bar)) return;
+      fixed_sums<3>(part3, G, q);
+      const double2 r0r_new = make_double2(q[0], q[1]);
+      beta = cm(cdivs(r0r_new, r0r), cdivs(alpha, omega));
+      r0r = r0r_new;
+      rn = sqrt(q[2]);
+      iters++;
+      if (rn != rn) done = 3;
+      else if (!(rn > tol)) done = 1;
+      else if (iters >= max_iter) done = 2;
+    }
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    st->r0r = r0r;
+    st->alpha = alpha;
+    st->omega = omega;
+    st->beta = beta;
+    st->rn = rn;
+    st->iters = iters;
     st->done = done;
   }
 }
@@ -1003,6 +1215,41 @@ cudaError_t cg_mixed_persistent(const Geom &g, const double2 *ph, const float2 *
   void *args[] = {&gg, (void *)&ph, (void *)&ph32, &mm, (void *)&b, &x, &r, &t64,
                   &xs, &rs, &ps, &ts, &part_t, &part_r, &st, &bar};
   e = cudaLaunchCooperativeKernel((const void *)k_cg_mixed_persistent<NT>, dim3(G), dim3(NT),
+                                  args, 0, s);
+  if (e == cudaErrorCooperativeLaunchTooLarge) {
+    cudaGetLastError();
+    return cudaErrorNotSupported;
+  }
+  return e;
+}
+
+// the persistent BiCGStab (k_bicgstab_persistent); the same launch rules as cg_persistent.
+// p holds the start direction; p2 and Ap2 are the second buffers of p and Ap.
+cudaError_t bicgstab_persistent(const Geom &g, const double2 *ph, double m, double2 *x,
+                                double2 *r, const double2 *r0, double2 *p, double2 *p2,
+                                double2 *Ap, double2 *Ap2, double2 *sv, double2 *t,
+                                double *part, SolverState *st, void *bar_mem, int part_cap,
+                                cudaStream_t s) {
+  constexpr int NT = 512;
+  static int grid = -1;
+  if (grid < 0) {
+    int dev = 0, coop = 0, sms = 0, per_sm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_bicgstab_persistent<NT>, NT, 0);
+    grid = (coop && per_sm >= 1) ? sms : 0;
+  }
+  const int G = std::min(grid, std::max(1, (g.V + NT - 1) / NT));
+  if (G <= 0 || 8 * G > part_cap || G > 32 * FIXED_SUM_PER_LANE) return cudaErrorNotSupported;
+  GridBarrier *bar = (GridBarrier *)bar_mem;
+  cudaError_t e = cudaMemsetAsync(bar, 0, sizeof(GridBarrier), s);
+  if (e != cudaSuccess) return e;
+  Geom gg = g;
+  double mm = m;
+  void *args[] = {&gg, (void *)&ph, &mm, &x, &r, (void *)&r0, &p, &p2, &Ap, &Ap2,
+                  &sv, &t, &part, &st, &bar};
+  e = cudaLaunchCooperativeKernel((const void *)k_bicgstab_persistent<NT>, dim3(G), dim3(NT),
                                   args, 0, s);
   if (e == cudaErrorCooperativeLaunchTooLarge) {
     cudaGetLastError();

@@ -10,7 +10,7 @@
 constexpr int NSLOT = 6;  // partial-sum slots: 0 plaquette, 1 kinetic, 2 clover, 3-5 solvers
 
 // device spinor buffers (U(1) staggered fermions)
-enum { SV_B, SV_X, SV_R, SV_P, SV_T, SV_AP, SV_S, SV_R0, SV_PHI, SV_CHI, SV_CHI1, SV_X0, SV_N };
+enum { SV_B, SV_X, SV_R, SV_P, SV_T, SV_AP, SV_S, SV_R0, SV_PHI, SV_CHI, SV_CHI1, SV_X0, SV_P2, SV_AP2, SV_N };
 enum { SV32_XS, SV32_RS, SV32_PS, SV32_TS, SV32_APS, SV32_N };
 
 struct su2b_ctx {
