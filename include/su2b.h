@@ -253,6 +253,22 @@ SU2B_API int su2b_batch_tune_set(su2b_batch *b, int variant);
  * shorter than the lattice.  FP32 contexts store FP32 links widened to double. */
 SU2B_API int su2b_save_gauge(su2b_ctx *ctx, const char *path);
 SU2B_API int su2b_load_gauge(su2b_ctx *ctx, const char *path);
+/* io::update_nconf_counter (io.hh:294-305): writes conf_dir + "nconf_counter.txt" as the
+ * header line "heat i path_conf" and the line "<heat> <i> <path_conf>" (heat printed as 0 or
+ * 1, no trailing newline).  conf_dir is prefixed as given, as in the reference.  Host only:
+ * needs no context and no GPU. */
+SU2B_API int su2b_update_nconf_counter(const char *conf_dir, int heat, long i,
+                                       const char *path_conf);
+/* io::read_nconf_counter (io.hh:267-285): reads the second line of conf_dir +
+ * "nconf_counter.txt" and splits it at spaces into heat (0 or 1), i and path_conf (copied
+ * into path_buf, at most path_cap bytes with the terminating NUL).  Fails with
+ * SU2B_ERR_INVALID where the reference aborts (a missing file) or would throw (a malformed
+ * line).  Host only. */
+SU2B_API int su2b_read_nconf_counter(const char *conf_dir, int *heat, long *i, char *path_buf,
+                                     size_t path_cap);
+/* the restart of base_program.hpp:284-296: read the counter in conf_dir and load the
+ * configuration it names into the context; heat and i as the counter holds them */
+SU2B_API int su2b_restart(su2b_ctx *ctx, const char *conf_dir, int *heat, long *i);
 
 /* ---- observables between trajectories ---------------------------------------------------- */
 /* polyakov_loop_spatial_average (polyakov_loop.hh:48-63): sum over spatial points of ReTr of

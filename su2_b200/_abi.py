@@ -103,6 +103,10 @@ SIGNATURES = {
     "su2b_save_gauge": (i32, [_P, C.c_char_p]),
     "su2b_pion_correlator": (i32, [_P, f64, f64, i32, i64, _D, C.POINTER(i64)]),
     "su2b_load_gauge": (i32, [_P, C.c_char_p]),
+    "su2b_update_nconf_counter": (i32, [C.c_char_p, i32, C.c_long, C.c_char_p]),
+    "su2b_read_nconf_counter": (i32, [C.c_char_p, C.POINTER(i32), C.POINTER(C.c_long),
+                                      C.c_char_p, C.c_size_t]),
+    "su2b_restart": (i32, [_P, C.c_char_p, C.POINTER(i32), C.POINTER(C.c_long)]),
     "su2b_wilson_loop": (i32, [_P, i32, i32, _D]),
     "su2b_ape_smear": (i32, [_P, f64, i32]),
     "su2b_batch_tune_get": (i32, [_P, C.POINTER(i32)]),

@@ -11,7 +11,9 @@
 // (load: read, copy in, convert, the same way round).  Loading checks every record's N_c.
 #include <algorithm>
 #include <cstdio>
+#include <cstring>
 #include <string>
+#include <vector>
 
 #include "site_ops.cuh"
 #include "su2b.h"
@@ -205,4 +207,63 @@ extern "C" int su2b_load_gauge(su2b_ctx *ctx, const char *path) {
                      "%s: a record's N_c does not match the group (not a %s configuration)",
                      path, ctx->group == 0 ? "SU(2)" : "U(1)");
   return SU2B_OK;
+}
+
+// ---- the restart counter (io.hh:251-305) ----
+static const char *const NCONF_COUNTER = "nconf_counter.txt";
+
+extern "C" int su2b_update_nconf_counter(const char *conf_dir, int heat, long i,
+                                         const char *path_conf) {
+  if (!conf_dir || !path_conf || (heat != 0 && heat != 1) || i < 0) return SU2B_ERR_INVALID;
+  const std::string name = std::string(conf_dir) + NCONF_COUNTER;
+  File out;
+  out.f = fopen(name.c_str(), "w");
+  if (!out.f) return SU2B_ERR_INVALID;
+  const int w = fprintf(out.f, "heat i path_conf\n%d %ld %s", heat, i, path_conf);
+  const int c = fclose(out.f);
+  out.f = nullptr;
+  return (w < 0 || c != 0) ? SU2B_ERR_INVALID : SU2B_OK;
+}
+
+extern "C" int su2b_read_nconf_counter(const char *conf_dir, int *heat, long *i, char *path_buf,
+                                       size_t path_cap) {
+  if (!conf_dir || !heat || !i || !path_buf || path_cap == 0) return SU2B_ERR_INVALID;
+  const std::string name = std::string(conf_dir) + NCONF_COUNTER;
+  File in;
+  in.f = fopen(name.c_str(), "r");
+  if (!in.f) return SU2B_ERR_INVALID;
+  // the second line, whole
+  std::string line[2];
+  for (int k = 0; k < 2; k++) {
+    int ch;
+    while ((ch = fgetc(in.f)) != EOF && ch != '\n') line[k].push_back((char)ch);
+    if (ch == EOF && k == 0) return SU2B_ERR_INVALID;
+  }
+  // split at every space, as boost::split(v, line, is_any_of(" ")) does (empty tokens kept)
+  std::vector<std::string> v(1);
+  for (char ch : line[1]) {
+    if (ch == ' ')
+      v.emplace_back();
+    else
+      v.back().push_back(ch);
+  }
+  if (v.size() < 3) return SU2B_ERR_INVALID;
+  if (v[0] != "0" && v[0] != "1") return SU2B_ERR_INVALID;  // lexical_cast<bool>
+  char *end = nullptr;
+  const long iv = strtol(v[1].c_str(), &end, 10);  // std::stoi: leading digits
+  if (end == v[1].c_str()) return SU2B_ERR_INVALID;
+  if (v[2].size() + 1 > path_cap) return SU2B_ERR_INVALID;
+  *heat = v[0] == "1";
+  *i = iv;
+  memcpy(path_buf, v[2].c_str(), v[2].size() + 1);
+  return SU2B_OK;
+}
+
+extern "C" int su2b_restart(su2b_ctx *ctx, const char *conf_dir, int *heat, long *i) {
+  if (!ctx) return SU2B_ERR_INVALID;
+  SU2B_NEED(conf_dir && heat && i, "NULL argument");
+  std::vector<char> path(4096);
+  if (su2b_read_nconf_counter(conf_dir, heat, i, path.data(), path.size()) != SU2B_OK)
+    return su2b_fail(ctx, SU2B_ERR_INVALID, "cannot read %s%s", conf_dir, NCONF_COUNTER);
+  return su2b_load_gauge(ctx, path.data());
 }

@@ -53,6 +53,22 @@ class SolveResult:
     converged: bool
 
 
+def update_nconf_counter(conf_dir, heat, i, path_conf):
+    """io::update_nconf_counter (io.hh:294-305): conf_dir + "nconf_counter.txt" names the
+    last saved configuration.  Host only."""
+    check(_abi.load().su2b_update_nconf_counter(str(conf_dir).encode(), int(bool(heat)), int(i),
+                                                 str(path_conf).encode()))
+
+
+def read_nconf_counter(conf_dir):
+    """io::read_nconf_counter (io.hh:267-285): (heat, i, path_conf).  Host only."""
+    heat, i = C.c_int(), C.c_long()
+    buf = C.create_string_buffer(4096)
+    check(_abi.load().su2b_read_nconf_counter(str(conf_dir).encode(), C.byref(heat), C.byref(i),
+                                               buf, len(buf)))
+    return bool(heat.value), i.value, buf.value.decode()
+
+
 class gaugeconfig:
     """Device-resident gauge field: gaugeconfig<G>(Lx, Ly, Lz, Lt, ndims, beta)
     (gaugeconfig.hh:49-63).  group: "su2" or "u1"; precision: "fp64" or "mixed"."""
@@ -175,6 +191,14 @@ class gaugeconfig:
     def load(self, path):
         """gaugeconfig::load (gaugeconfig.hh:241-252); raises on a short or foreign file."""
         self._c(self.lib.su2b_load_gauge(self.ctx, str(path).encode()))
+
+    def restart(self, conf_dir):
+        """The restart of base_program.hpp:284-296: reads conf_dir + "nconf_counter.txt" and
+        loads the configuration it names.  Returns (heat, i) as the counter holds them."""
+        heat, i = C.c_int(), C.c_long()
+        self._c(self.lib.su2b_restart(self.ctx, str(conf_dir).encode(), C.byref(heat),
+                                      C.byref(i)))
+        return bool(heat.value), i.value
 
     # ---- reductions ----
     def gauge_energy(self, spatial_only=False) -> float:

@@ -74,3 +74,20 @@ def test_load_rejects_short_and_foreign_files(gpu, orc, ref, tmp_path):
     with make(gpu, 0, (4, 4, 2, 2), 4) as c:  # as many bytes as the U(1) file
         with pytest.raises(su2_b200.Su2bError):
             c.load(tmp_path / "u1.conf")
+
+
+def test_restart_from_the_counter(gpu, orc, tmp_path):
+    # base_program.hpp:284-296 and :440-454: save, update the counter, restart elsewhere
+    dims, nd = (4, 4, 4, 6), 4
+    U = orc.hotstart(0, dims, nd, 9, 1.0, 654321)
+    d = str(tmp_path) + "/"
+    with make(gpu, 0, dims, nd) as c:
+        c.upload(U)
+        c.save(d + "run.conf.50")
+    gpu.update_nconf_counter(d, True, 50, d + "run.conf.50")
+    with make(gpu, 0, dims, nd) as c:
+        assert c.restart(d) == (True, 50)
+        assert np.array_equal(c.download(), U)
+    with make(gpu, 0, dims, nd) as c:
+        with pytest.raises(gpu.Su2bError):
+            c.restart(str(tmp_path / "nowhere") + "/")
