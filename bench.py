@@ -214,6 +214,12 @@ def ours(args):
     for k in range(THERM_TRAJ + max(W, 3)):
         mixed.md_update("omf2", NSTEPS, TAU, seed=seed, traj=100000 + k)
     U_th = mixed.download()
+    # one FP64 start for both arms: FP32 links widened to double are unitary to about 1e-7
+    # only, and the FP64 trajectory's closing restoreSU would then shift S_G by O(1) at 32^4
+    # (a systematic dH of about 5), so the start is reunitarised in FP64 first
+    Uq = U_th.reshape(-1, 4)
+    Uq /= np.sqrt(np.einsum("ij,ij->i", Uq, Uq))[:, None]
+    mixed.upload(U_th)
     tune_m = mixed.autotune()  # launch shape of the force kernel, timed on this field
 
     # ---- headline: mixed precision, K trajectories ----
@@ -413,13 +419,14 @@ def reference(args):
 
 
 def profile_run(args):
-    """--profile-run: the bare timed loop of the headline workload, for ncu.
+    """--profile-run: a bare loop of one operation of the 32^4 workload, for ncu.
 
     A Haar-random 32^4 start (untimed work does not change what a kernel reads or writes),
-    the force kernel's launch shape fixed by --force-variant instead of the tuner, W warm-up
-    and K trajectories of one precision.  Prints one JSON line with the number of kernel
-    launches made before the K trajectories (the ncu ``-s`` to skip to them) and per
-    trajectory.
+    the force kernel's launch shape fixed by --force-variant instead of the tuner, then W
+    warm-up and K steps of one precision.  --profile-op picks the step: an omf2 trajectory
+    (hmc), a Metropolis sweep (delta 0.15, 8 hits) or an RK3 Wilson-flow step (eps 0.01).
+    Prints one JSON line with the number of kernel launches made before the K steps (the ncu
+    ``-s`` to skip to them) and per step.
     """
     import torch
 
@@ -428,17 +435,27 @@ def profile_run(args):
     c = su2_b200.gaugeconfig(L, L, L, L, 4, BETA, precision=args.precision)
     c.upload(haar_links(V * 4, 20240))
     c.force_variant = args.force_variant
+
+    def step(k):
+        if args.profile_op == "hmc":
+            c.md_update("omf2", NSTEPS, TAU, seed=20240, traj=k)
+        elif args.profile_op == "metropolis":
+            c.sweep(0.15, 8, 20240, k)
+        else:
+            c.runge_kutta(0.01)
+
     for k in range(args.warmup):
-        c.md_update("omf2", NSTEPS, TAU, seed=20240, traj=k)
+        step(k)
     c.synchronize()
     n0 = c.kernel_launches()
     for k in range(args.steps):
-        c.md_update("omf2", NSTEPS, TAU, seed=20240, traj=args.warmup + k)
+        step(args.warmup + k)
     c.synchronize()
     n1 = c.kernel_launches()
-    print(json.dumps({"profile_run": WORKLOAD, "precision": args.precision,
+    print(json.dumps({"profile_run": f"SU(2) d=4 {L}^4, beta={BETA}", "op": args.profile_op,
+                      "precision": args.precision,
                       "force_variant": su2_b200._abi.FORCE_SHAPES[args.force_variant],
-                      "setup_launches": n0, "launches_per_traj": (n1 - n0) / max(1, args.steps),
+                      "setup_launches": n0, "launches_per_step": (n1 - n0) / max(1, args.steps),
                       "steps": args.steps, "warmup": args.warmup}), flush=True)
     c.close()
     torch.cuda.synchronize()
@@ -797,6 +814,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile-run", action="store_true",
                     help="only the timed loop of one precision, for ncu (no bench line)")
+    ap.add_argument("--profile-op", default="hmc", choices=["hmc", "metropolis", "flow"],
+                    help="with --profile-run: the step of the loop")
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--force-variant", type=int, default=3)
     ap.add_argument("--config", type=int, default=2, choices=[1, 2, 3, 4, 5],

@@ -23,6 +23,7 @@
 // left-trivialised differential of exp (for su(2): ad_x v = -2 x cross v, theta = 2|x|,
 // J = 1 + (1 - cos th)/th^2 ad + (th - sin th)/th^3 ad^2).
 #include <cmath>
+#include <utility>
 #include <vector>
 
 #include "su2b.h"
@@ -173,18 +174,40 @@ cudaError_t exp_adjoint(const Geom &g, const T *Z, double b, T *lam, T *mu, int 
 }
 
 // device scratch of one adjoint computation, freed on return
+// Scratch carved from the context's arena.  The arena stays allocated between calls (one
+// gradient at 24^4 needs about 1.4 GB; allocating and freeing that per call costs
+// milliseconds, and cudaFree synchronises the device) and only grows.
 struct Scratch {
-  std::vector<void *> p;
-  ~Scratch() {
-    for (void *q : p) cudaFree(q);
-  }
-  void *get(size_t bytes, cudaError_t *e) {
-    void *q = nullptr;
-    *e = cudaMalloc(&q, bytes);
-    if (*e == cudaSuccess) p.push_back(q);
+  char *base = nullptr;
+  size_t off = 0, cap = 0;
+  void *get(size_t bytes) {
+    const size_t b = (bytes + 255) & ~(size_t)255;
+    if (off + b > cap) return nullptr;
+    void *q = base + off;
+    off += b;
     return q;
   }
 };
+int arena(su2b_ctx *ctx, size_t bytes, Scratch *sc) {
+  if (ctx->arena_bytes < bytes) {
+    if (ctx->arena) {
+      cudaFree(ctx->arena);
+      ctx->arena = nullptr;
+      ctx->arena_bytes = 0;
+    }
+    const cudaError_t e = cudaMalloc(&ctx->arena, bytes);
+    if (e != cudaSuccess) {
+      ctx->arena = nullptr;
+      return su2b_fail(ctx, SU2B_ERR_NOMEM, "flow adjoint scratch (%zu bytes): %s", bytes,
+                       cudaGetErrorString(e));
+    }
+    ctx->arena_bytes = bytes;
+  }
+  sc->base = (char *)ctx->arena;
+  sc->off = 0;
+  sc->cap = ctx->arena_bytes;
+  return SU2B_OK;
+}
 
 struct FlowCoef {
   double a[3], b[3];
@@ -211,29 +234,35 @@ int flow_adjoint_t(su2b_ctx *ctx, double eps, int n, int every, double *objectiv
   const size_t NL = ctx->NL, lb = ctx->link_bytes() * NL, ab = ctx->adj_bytes() * NL;
   if (every <= 0) every = std::max(1, (int)std::lround(std::sqrt((double)n)));
   const int nseg = (n + every - 1) / every;
+  const size_t lb_a = (lb + 255) & ~(size_t)255, ab_a = (ab + 255) & ~(size_t)255;
   Scratch sc;
-  cudaError_t e = cudaSuccess;
+  SU2B_CKS(arena(ctx, (nseg + every + 3) * lb_a + 5 * ab_a, &sc));
   std::vector<void *> ck(nseg), seg(every);
-  for (int i = 0; i < nseg && e == cudaSuccess; i++) ck[i] = sc.get(lb, &e);
-  for (int i = 0; i < every && e == cudaSuccess; i++) seg[i] = sc.get(lb, &e);
-  void *W1 = sc.get(lb, &e), *W2 = sc.get(lb, &e), *cur = sc.get(lb, &e);
+  for (int i = 0; i < nseg; i++) ck[i] = sc.get(lb);
+  for (int i = 0; i < every; i++) seg[i] = sc.get(lb);
+  void *W1 = sc.get(lb), *W2 = sc.get(lb), *cur = sc.get(lb);
   T *Zs[3], *lam, *mu;
-  for (int f = 0; f < 3; f++) Zs[f] = (T *)sc.get(ab, &e);
-  lam = (T *)sc.get(ab, &e);
-  mu = (T *)sc.get(ab, &e);
-  if (e != cudaSuccess)
-    return su2b_fail(ctx, SU2B_ERR_NOMEM, "flow adjoint scratch: %s", cudaGetErrorString(e));
+  for (int f = 0; f < 3; f++) Zs[f] = (T *)sc.get(ab);
+  lam = (T *)sc.get(ab);
+  mu = (T *)sc.get(ab);
   const FlowCoef c = flow_coef(ctx, eps);
-  auto force = [&](const void *W, T *Z, double a, int mode) {
-    return su2b_q_force(ctx, W, Z, nullptr, a, 1.0, mode, nullptr, nullptr);
+  // Z = a g(W) (+ Z with FM_HAS_IN); with Wn, also Wn = exp(b Z) W from the same kernel
+  auto force = [&](const void *W, T *Z, double a, int mode, void *Wn = nullptr,
+                   double b = 0.0) {
+    return su2b_q_force(ctx, W, Z, nullptr, a, 1.0, Wn ? (mode | FM_UPDATE) : mode, nullptr,
+                        nullptr, Wn, b);
   };
-  // forward with checkpoints every `every` steps
+  // forward with checkpoints every `every` steps; the field alternates between cur and W1
+  // (W1 is free until the backward pass), so every stage is fused with its link update
   SU2B_CK(cudaMemcpyAsync(cur, ctx->U, lb, cudaMemcpyDeviceToDevice, s));
+  void *fa = cur, *fb = W1;
   for (int st = 0; st < n; st++) {
     if (st % every == 0)
-      SU2B_CK(cudaMemcpyAsync(ck[st / every], cur, lb, cudaMemcpyDeviceToDevice, s));
-    SU2B_CKS(su2b_q_flow_step(ctx, cur, eps));
+      SU2B_CK(cudaMemcpyAsync(ck[st / every], fa, lb, cudaMemcpyDeviceToDevice, s));
+    SU2B_CKS(su2b_q_flow_step_to(ctx, fa, fb, eps));
+    std::swap(fa, fb);
   }
+  cur = fa;
   // objective t^2 E_p(t), E_p = d(d-1)/2 - P/(V Nc) (flat-gradient_flow.hh:151)
   SU2B_CKS(su2b_q_plaq(ctx, cur, 40));
   SU2B_CKS(su2b_fetch_red(ctx, 43));
@@ -245,20 +274,18 @@ int flow_adjoint_t(su2b_ctx *ctx, double eps, int n, int every, double *objectiv
   for (int sg = nseg - 1; sg >= 0; sg--) {
     const int s0 = sg * every, s1 = std::min(n, s0 + every);
     SU2B_CK(cudaMemcpyAsync(seg[0], ck[sg], lb, cudaMemcpyDeviceToDevice, s));
-    for (int j = 1; j < s1 - s0; j++) {
-      SU2B_CK(cudaMemcpyAsync(seg[j], seg[j - 1], lb, cudaMemcpyDeviceToDevice, s));
-      SU2B_CKS(su2b_q_flow_step(ctx, seg[j], eps));
+    for (int j = 1; j < s1 - s0; j++) {  // seg[j-1] -> seg[j] through W2, seg[j-1] kept
+      SU2B_CKS(force(seg[j - 1], Zs[0], c.a[0], 0, seg[j], c.b[0]));
+      SU2B_CKS(force(seg[j], Zs[0], c.a[1], FM_HAS_IN, W2, c.b[1]));
+      SU2B_CKS(force(W2, Zs[0], c.a[2], FM_HAS_IN, seg[j], c.b[2]));
+      if (!ctx->link64) SU2B_CKS(su2b_q_restore(ctx, seg[j]));
     }
     for (int j = s1 - s0 - 1; j >= 0; j--) {
       const void *W0 = seg[j];
-      // stages of this step
-      SU2B_CKS(force(W0, Zs[0], c.a[0], 0));
-      SU2B_CK(cudaMemcpyAsync(W1, W0, lb, cudaMemcpyDeviceToDevice, s));
-      SU2B_CKS(su2b_q_update(ctx, W1, Zs[0], c.b[0]));
+      // stages of this step, each fused with its link update
+      SU2B_CKS(force(W0, Zs[0], c.a[0], 0, W1, c.b[0]));
       SU2B_CK(cudaMemcpyAsync(Zs[1], Zs[0], ab, cudaMemcpyDeviceToDevice, s));
-      SU2B_CKS(force(W1, Zs[1], c.a[1], FM_HAS_IN));
-      SU2B_CK(cudaMemcpyAsync(W2, W1, lb, cudaMemcpyDeviceToDevice, s));
-      SU2B_CKS(su2b_q_update(ctx, W2, Zs[1], c.b[1]));
+      SU2B_CKS(force(W1, Zs[1], c.a[1], FM_HAS_IN, W2, c.b[1]));
       SU2B_CK(cudaMemcpyAsync(Zs[2], Zs[1], ab, cudaMemcpyDeviceToDevice, s));
       SU2B_CKS(force(W2, Zs[2], c.a[2], FM_HAS_IN));
       // reverse

@@ -177,6 +177,7 @@ extern "C" int su2b_ctx_destroy(su2b_ctx *ctx) {
   for (cudaEvent_t e : ctx->ev_pool) cudaEventDestroy(e);
   for (auto &kv : ctx->graphs) cudaGraphExecDestroy(kv.second.exec);
   for (void *p : ctx->allocs) cudaFree(p);
+  if (ctx->arena) cudaFree(ctx->arena);
   if (ctx->h_red) cudaFreeHost(ctx->h_red);
   if (ctx->h_traj) cudaFreeHost(ctx->h_traj);
   if (ctx->h_counts) cudaFreeHost(ctx->h_counts);
@@ -404,18 +405,19 @@ extern "C" int su2b_energy_density(su2b_ctx *ctx, int cloverdef, int ss, double 
 // force and updates
 template <class T>
 static int q_force(su2b_ctx *ctx, const void *U, T *P, const T *extra, double f, double scale,
-                   int mode, double *kin_part, int *nb) {
+                   int mode, double *kin_part, int *nb, void *Uout, double dt_upd) {
   SU2B_LAUNCH(SU2B_K_FORCE, force_update<T>(ctx->g, U, ctx->group, P, extra, f, scale, ctx->xi,
-                                            mode, kin_part, nb, nullptr, 0.0, ctx->stream,
+                                            mode, kin_part, nb, Uout, dt_upd, ctx->stream,
                                             ctx->tune_force));
   return SU2B_OK;
 }
 int su2b_q_force(su2b_ctx *ctx, const void *U, void *P, const void *extra, double f,
-                 double scale, int mode, double *kin_part, int *nb) {
+                 double scale, int mode, double *kin_part, int *nb, void *Uout, double dt_upd) {
   if (ctx->link64)
     return q_force<double>(ctx, U, (double *)P, (const double *)extra, f, scale, mode,
-                           kin_part, nb);
-  return q_force<float>(ctx, U, (float *)P, (const float *)extra, f, scale, mode, kin_part, nb);
+                           kin_part, nb, Uout, dt_upd);
+  return q_force<float>(ctx, U, (float *)P, (const float *)extra, f, scale, mode, kin_part, nb,
+                        Uout, dt_upd);
 }
 int su2b_q_update(su2b_ctx *ctx, void *U, const void *P, double dt) {
   if (ctx->link64)
@@ -485,23 +487,51 @@ extern "C" int su2b_metropolis_sweep(su2b_ctx *ctx, double delta, int N_hit, uin
 
 // ------------------------------------------------------------------------------------
 // Wilson flow: runge_kutta (flat-gradient_flow.hh:17-50)
-int su2b_q_flow_step(su2b_ctx *ctx, void *U, double eps) {
+int su2b_q_flow_step_to(su2b_ctx *ctx, void *src, void *dst, double eps) {
   const double zfac[3] = {(-17.0) / (36.0), (8.0) / (9.0), (-3.0) / (4.0)};
   const double expfac[3] = {-36.0 / 4. / 17.0, 1., -1.};
   const int Nc = ctx->group == 0 ? 2 : 1;
+  // SU(2): a stage's link update W' = exp(c Z) W is written by the force kernel itself into
+  // the other link buffer, as the fused trajectory steps do, so W is read once per stage
+  // instead of twice.  src != dst: all three stages fused, src -> dst -> src -> dst (src is
+  // left holding W2).  In place: src -> U2 -> src fused, then the third stage's force and
+  // update in place (U2 holds no field between calls: it is the trajectory's spare).  The
+  // update arithmetic is the separate update kernel's, so the flowed field is the same bit
+  // for bit either way.
+  const bool su2 = ctx->group == SU2B_GROUP_SU2;
+  if (!su2 && src != dst) {  // U(1): the steps run in place, on a copy in dst
+    CK(cudaMemcpyAsync(dst, src, ctx->link_bytes() * ctx->NL, cudaMemcpyDeviceToDevice,
+                       ctx->stream));
+    src = dst;
+  }
+  const bool in_place = src == dst;
+  void *other = in_place ? ctx->U2 : dst;
+  const int nfused = !su2 || (in_place && src == ctx->U2) ? 0 : (in_place ? 2 : 3);
+  void *W = src;
   for (int f = 0; f < 3; f++) {
     const double fac = 2. * Nc * zfac[f] / ctx->beta;
     const double ff = fac * ctx->beta / (double)Nc;
-    CKS(su2b_q_force(ctx, U, ctx->Z, nullptr, ff, 1.0, f == 0 ? 0 : FM_HAS_IN, nullptr,
-                     nullptr));
-    CKS(su2b_q_update(ctx, U, ctx->Z, -eps * expfac[f]));
+    const int mode = f == 0 ? 0 : FM_HAS_IN;
+    if (f < nfused) {
+      void *next = W == src ? other : src;
+      CKS(su2b_q_force(ctx, W, ctx->Z, nullptr, ff, 1.0, mode | FM_UPDATE, nullptr, nullptr,
+                       next, -eps * expfac[f]));
+      W = next;
+      ctx->phases_valid = false;
+    } else {
+      CKS(su2b_q_force(ctx, W, ctx->Z, nullptr, ff, 1.0, mode, nullptr, nullptr));
+      CKS(su2b_q_update(ctx, W, ctx->Z, -eps * expfac[f]));
+    }
   }
   // FP32 links: every exp(.)U product rounds |U| by about one ulp in a direction that does not
   // average out over hundreds of steps, and the flowed plaquette (close to 1) amplifies that
   // drift in E = d(d-1)/2 - P/(V Nc).  Reunitarise in FP64 after each step, as the trajectory
   // does at its end; FP64 links keep the reference's step unchanged.
-  if (!ctx->link64 && ctx->group == SU2B_GROUP_SU2) CKS(su2b_q_restore(ctx, U));
+  if (!ctx->link64 && su2) CKS(su2b_q_restore(ctx, W));
   return SU2B_OK;
+}
+int su2b_q_flow_step(su2b_ctx *ctx, void *U, double eps) {
+  return su2b_q_flow_step_to(ctx, U, U, eps);
 }
 
 extern "C" int su2b_flow_step(su2b_ctx *ctx, double eps) {
@@ -535,12 +565,13 @@ extern "C" int su2b_gradient_flow(su2b_ctx *ctx, double tmax, double eps, double
   while (t[1] < tmax - eps) {
     t[0] = t[2];
     t[1] = t[0] + eps;
-    CKS(su2b_q_flow_step(ctx, Vt, eps));
+    // two steps per record, Vt -> U2 -> Vt, every stage fused with its link update
+    CKS(su2b_q_flow_step_to(ctx, Vt, ctx->U2, eps));
     // the reference prints the observables of the middle step only
-    CKS(su2b_q_plaq(ctx, Vt, 0));
-    CKS(su2b_q_clover(ctx, Vt, 1, 3));
+    CKS(su2b_q_plaq(ctx, ctx->U2, 0));
+    CKS(su2b_q_clover(ctx, ctx->U2, 1, 3));
     t[2] = t[1] + eps;
-    CKS(su2b_q_flow_step(ctx, Vt, eps));
+    CKS(su2b_q_flow_step_to(ctx, ctx->U2, Vt, eps));
     CKS(su2b_fetch_red(ctx, 6));
     const double *r = ctx->h_red;
     const double P1 = r[0] / den, Pss1 = r[1] / den;

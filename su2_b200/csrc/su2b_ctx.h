@@ -27,6 +27,9 @@ struct su2b_ctx {
   // trajectory (the start configuration stays untouched in one of them until accept/reject)
   void *U = nullptr, *U_old = nullptr, *U2 = nullptr, *U_aux = nullptr, *U_rev = nullptr;
   void *P = nullptr, *Z = nullptr;
+  // scratch arena of the flow adjoint, kept between calls and grown on demand
+  void *arena = nullptr;
+  size_t arena_bytes = 0;
   double *stage = nullptr;  // host-layout staging buffer on the device
   double *part = nullptr;   // NSLOT slots of 3*part_cap partial sums
   size_t part_cap = 0;
@@ -88,11 +91,15 @@ int su2b_adj_download(su2b_ctx *ctx, const void *dev, double *host);
 int su2b_q_plaq(su2b_ctx *ctx, const void *U, int red_slot);
 int su2b_q_clover(su2b_ctx *ctx, const void *U, int cloverdef, int red_slot);
 int su2b_fetch_red(su2b_ctx *ctx, int n);
+// mode FM_UPDATE / FM_RESTORE: the force kernel also writes the next link buffer Uout
 int su2b_q_force(su2b_ctx *ctx, const void *U, void *P, const void *extra, double f,
-                 double scale, int mode, double *kin_part, int *nb);
+                 double scale, int mode, double *kin_part, int *nb, void *Uout = nullptr,
+                 double dt_upd = 0.0);
 int su2b_q_update(su2b_ctx *ctx, void *U, const void *P, double dt);
 int su2b_q_restore(su2b_ctx *ctx, void *U);
 int su2b_q_flow_step(su2b_ctx *ctx, void *U, double eps);
+// one flow step from src into dst (dst == src: in place); src != dst leaves src clobbered
+int su2b_q_flow_step_to(su2b_ctx *ctx, void *src, void *dst, double eps);
 int su2b_ensure_aux(su2b_ctx *ctx);
 int su2b_links_to_stage(su2b_ctx *ctx, const void *U);
 int su2b_prof_fold(su2b_ctx *ctx);
