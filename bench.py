@@ -308,6 +308,37 @@ def ours(args):
     metro = 5 / (ev[0].elapsed_time(ev[1]) / 1e3)
     flow = 10 / (ev[2].elapsed_time(ev[3]) / 1e3)
 
+    # ---- the measurements taken between trajectories (FP64 context, thermalised field):
+    #      wall time per call, each call returns its value to the host ----
+    def per_call(fn, n=5):
+        fn()
+        fp64.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(n):
+            fn()
+        fp64.synchronize()
+        return 1e3 * (time.perf_counter() - t0) / n
+
+    fp64.upload(U_th)
+    obs = {"plaquette_ms": per_call(fp64.gauge_energy),
+           "clover_E_Q_ms": per_call(fp64.energy_density),
+           "polyakov_loop_ms": per_call(fp64.polyakov_loop_spatial_average),
+           "wilson_loop_4x4_ms": per_call(lambda: fp64.wilsonloop(4, 4)),
+           "ape_smear_spatial_ms": per_call(lambda: fp64.APEsmearing(0.5))}
+    fp64.upload(U_th)
+    with tempfile.TemporaryDirectory() as td:
+        path = os.path.join(td, "conf.0")
+        t0 = time.perf_counter()
+        fp64.save(path)
+        t_save = time.perf_counter() - t0
+        nbytes = os.path.getsize(path)
+        t0 = time.perf_counter()
+        fp64.load(path)
+        t_load = time.perf_counter() - t0
+    obs["gaugeconfig_file_bytes"] = nbytes
+    obs["save_GB_per_s"] = nbytes / t_save / 1e9
+    obs["load_GB_per_s"] = nbytes / t_load / 1e9
+
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(U_th)
@@ -349,6 +380,7 @@ def ours(args):
                                   "chosen": {"mixed": su2_b200._abi.FORCE_SHAPES[mixed.force_variant],
                                              "fp64": su2_b200._abi.FORCE_SHAPES[fp64.force_variant]}},
             "metropolis_sweeps_per_s": metro, "flow_rk3_steps_per_s_fp64": flow,
+            "between_trajectories_fp64": obs,
             "e2e": {"value": ws * K / t_e2e, "unit": "traj/s",
                     "h2d_bytes_per_step": int(NL * 4 * 8), "d2h_bytes_per_step": int(NL * 4 * 8),
                     "note": "upload of the host gaugeconfig (reference layout, FP64, pinned) "
@@ -587,6 +619,16 @@ def config3(args):
                           "acceptance": sum(a.accepted for a in acc) / nt,
                           "cg_iterations_per_traj": float(np.mean([a.cg_iterations
                                                                    for a in acc]))}
+            # pion correlator (propagator.hpp:25-65): one CG solve and the time-slice sums
+            c.upload(U)
+            C_pi = c.C_pion(m, tol=1e-10)
+            npi = max(2, args.steps // 2)
+            t0 = time.perf_counter()
+            for _ in range(npi):
+                C_pi = c.C_pion(m, tol=1e-10)
+            out["pion"] = {"ms_per_correlator": 1e3 * (time.perf_counter() - t0) / npi,
+                           "C1": float(C_pi[1]), "timeslices": len(C_pi),
+                           "note": "C(0) is skipped, as the reference does (contact term)"}
         c.close()
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
@@ -608,7 +650,7 @@ def config3(args):
               ws, solves["cg_fp64"]["ms_per_solve"],
               {"workload": "U(1) d=2 256x256 beta=4.0 staggered m=0.05, hot start",
                "replicas": ws}, dtype="fp64 (and fp32-inner mixed CG)", solvers=solves,
-              fermion_hmc=out.get("hmc"), cpu_baseline=cpu)
+              fermion_hmc=out.get("hmc"), pion_correlator=out.get("pion"), cpu_baseline=cpu)
 
 
 def ensemble_chains(n=64, seed=20250):
