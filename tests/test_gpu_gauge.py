@@ -315,19 +315,20 @@ def test_rejected_trajectory_keeps_start_field(gpu, orc):
 
 
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
-@pytest.mark.parametrize("dims", [(8, 6, 4, 8), (4, 4, 8, 4), (8, 8, 16, 6)],
-                         ids=["8x6x4x8", "4x4x8x4", "8x8x16x6"])
+@pytest.mark.parametrize("dims", [(8, 6, 4, 8), (4, 4, 8, 4), (8, 8, 16, 6), (6, 6, 6, 6)],
+                         ids=["8x6x4x8", "4x4x8x4", "8x8x16x6", "6x6x6x6"])
 def test_every_force_launch_shape_is_exact(gpu, orc, precision, dims):
     """Every launch shape of the force kernel (threads per block x register cap, including
     the register-starved ones that spill) gives the oracle's force and a finite trajectory,
-    on lattices whose half volume is and is not a multiple of the block's sites."""
+    on lattices whose half volume is and is not a multiple of the block's sites (6^4: 648
+    sites per parity, not a multiple of 32)."""
     group, nd = 0, 4
     U = hot(orc, group, dims, nd)
     F = orc.gauge_derivative(group, dims, nd, 2.3, U)
     tol = 1e-12 if precision == "fp64" else 1e-5
     with make(gpu, group, dims, nd, beta=2.3, precision=precision) as c:
         c.upload(U)
-        for v in range(8):
+        for v in range(gpu._abi.FORCE_VARIANTS):
             c.force_variant = v
             assert rel(c.derivative(), F) < tol, v
             r = c.md_update("omf2", 3, 0.3, momenta=orc.initnormal(group, dims, nd, 5)[0],
@@ -349,6 +350,6 @@ def test_autotune_cache(gpu, orc, tmp_path):
     line = open(path).read().split()
     assert int(line[1]) == best and "/force/fp32/16x16x16x16/d4" in line[0]
     with make(gpu, group, dims, nd, beta=2.4, precision="mixed") as c:
-        c.force_variant = (best + 1) % 8
+        c.force_variant = (best + 1) % gpu._abi.FORCE_VARIANTS
         t2 = c.autotune(path)  # cached: no measurement
         assert all(v < 0 for v in t2.values()) and c.force_variant == best
