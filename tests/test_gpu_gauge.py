@@ -140,6 +140,13 @@ def test_gradient_flow_records(gpu, orc, group, dims, nd):
     fin = np.isfinite(want)
     assert np.array_equal(fin, np.isfinite(got))
     np.testing.assert_allclose(got[fin], want[fin], rtol=1e-11, atol=1e-13)
+    if group == 0:  # FP32 links: the step pairs between two buffers, reunitarised each step
+        with make(gpu, group, dims, nd, beta=2.3, precision="mixed") as c:
+            c.upload(U)
+            got32 = c.gradient_flow(0.2, 0.01)
+        # columns t, xi_R, P, P_ss, E_p, E_p_ss, E_c, E_c_ss, Q: FP32 link rounding only
+        cols = [0, 2, 3, 4, 5, 6, 7]
+        np.testing.assert_allclose(got32[:, cols], want[:, cols], rtol=1e-5, atol=1e-5)
 
 
 @pytest.mark.parametrize("group,dims,nd", GEOMS, ids=GEOM_IDS)
