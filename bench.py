@@ -526,7 +526,7 @@ def config1(args):
     K, W = args.steps, args.warmup
     c = su2_b200.gaugeconfig(8, 8, 8, 8, 4, 2.3, precision="fp64", device=local)
     c.upload(haar_links(8 ** 4 * 4, seed))
-    c.autotune()  # the launch shape that suits 8^4 is not the one of 32^4
+    tune = c.autotune()  # the launch shape that suits 8^4 is not the one of 32^4
     c.upload(haar_links(8 ** 4 * 4, seed))
     for k in range(W):
         c.md_update("leapfrog", 10, 1.0, seed=seed, traj=k)
@@ -559,7 +559,9 @@ def config1(args):
                                         "Haar start", "replicas": ws},
               dtype="fp64", acceptance=sum(r.accepted for r in res) / K,
               plaquette_mean=float(np.mean(plaq)), plaquette_last=plaq[-1],
-              gpu_launches=c.kernel_launches() - n0, cpu_baseline=cpu)
+              gpu_launches=c.kernel_launches() - n0, cpu_baseline=cpu,
+              autotune_force_us={str(su2_b200._abi.FORCE_SHAPES[k]): v for k, v in tune.items()},
+              force_shape=su2_b200._abi.FORCE_SHAPES[c.force_variant])
     c.close()
 
 

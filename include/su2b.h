@@ -307,7 +307,7 @@ SU2B_API int su2b_flow_adjoint(su2b_ctx *ctx, double eps, int n_steps, int check
  * with cache_path it first looks the choice up in that text file (unless retune) and writes
  * new measurements to it.  times_us (optional, SU2B_FORCE_VARIANTS entries) receives the
  * average launch time of each shape (-1 when not measured). */
-#define SU2B_FORCE_VARIANTS 9
+#define SU2B_FORCE_VARIANTS 10
 enum { SU2B_TUNE_FORCE = 0 };
 SU2B_API int su2b_autotune(su2b_ctx *ctx, const char *cache_path, int retune, double *times_us);
 SU2B_API int su2b_tune_get(su2b_ctx *ctx, int kernel, int *variant);

@@ -231,6 +231,40 @@ __global__ void __launch_bounds__(NT, MINB)
 }
 
 
+// the fused force step with one thread per link (force_link_impl): warp mu of block b takes
+// the links in direction mu of 32 sites of parity b & 1, so a block holds all d links of its
+// sites; for lattices too small to fill the GPU one thread per site
+template <class T, int ND, int MINB>
+__global__ void __launch_bounds__(32 * ND, MINB)
+  k_force_su2_link(Geom g, const LinkT<T> *__restrict__ U, T *__restrict__ P,
+                   const T *__restrict__ extra, T f, T scale_, int mode, T wt, T ws,
+                   double *kin_part, LinkT<T> *__restrict__ Uout, T dt_upd) {
+  constexpr int NT = 32 * ND;
+  __shared__ double sh[NT / 32];
+  pdl_trigger();
+  pdl_wait();
+  const int mu = threadIdx.x >> 5, p = blockIdx.x & 1;
+  const int cb = (blockIdx.x >> 1) * 32 + (threadIdx.x & 31);
+  double k2 = 0.;
+  // the direction is a compile-time constant in each warp's body (static site indexing)
+#define SU2B_LINK_BODY(M)                                                                     \
+  k2 = force_link_impl<T, ND, (M < ND ? M : 0)>(g, U, P, extra, f, scale_, mode, Uout, dt_upd, \
+                                                 p, cb)
+  if (cb < g.Vh) {
+    switch (mu) {
+      case 0: SU2B_LINK_BODY(0); break;
+      case 1: SU2B_LINK_BODY(1); break;
+      case 2: SU2B_LINK_BODY(2); break;
+      default: SU2B_LINK_BODY(3); break;
+    }
+  }
+#undef SU2B_LINK_BODY
+  if (mode & FM_KINETIC) {
+    const double r = block_sum<NT>(k2, sh);
+    if (threadIdx.x == 0) kin_part[blockIdx.x] = r;
+  }
+}
+
 template <int ND, int NT>
 __global__ void __launch_bounds__(NT)
   k_force_u1(Geom g, const double *__restrict__ U, double *__restrict__ P,
@@ -610,6 +644,24 @@ cudaError_t force_update(const Geom &g, const void *U, int group, T *P, const T 
       launch_force(k_force_su2_split<T, NTV, MB>, grid, NTV, s, pdl, SU2B_FORCE_ARGS);     \
     if (e_ != cudaSuccess) return e_;                                                      \
   } while (0)
+#define SU2B_FORCE_LINK(MB)                                                                  \
+  do {                                                                                     \
+    const dim3 grid(2 * cdiv(g.Vh, 32));                                                   \
+    nb = grid.x;                                                                           \
+    cudaError_t e_;                                                                        \
+    switch (g.nd) {                                                                        \
+      case 2:                                                                              \
+        e_ = launch_force(k_force_su2_link<T, 2, MB>, grid, 64, s, pdl, SU2B_FORCE_ARGS);  \
+        break;                                                                             \
+      case 3:                                                                              \
+        e_ = launch_force(k_force_su2_link<T, 3, MB>, grid, 96, s, pdl, SU2B_FORCE_ARGS);  \
+        break;                                                                             \
+      default:                                                                             \
+        e_ = launch_force(k_force_su2_link<T, 4, MB>, grid, 128, s, pdl, SU2B_FORCE_ARGS); \
+        break;                                                                             \
+    }                                                                                      \
+    if (e_ != cudaSuccess) return e_;                                                      \
+  } while (0)
 #define SU2B_FORCE_XSPLIT(NTV, MB)                                                           \
   do {                                                                                     \
     if (g.nd != 4) {                                                                       \
@@ -636,12 +688,14 @@ cudaError_t force_update(const Geom &g, const void *U, int group, T *P, const T 
         case 5: SU2B_FORCE_LAUNCH(256, 3, false); break;
         case 6: SU2B_FORCE_SPLIT(128, 8); break;
         case 8: SU2B_FORCE_XSPLIT(128, 8); break;
+        case 9: SU2B_FORCE_LINK(6); break;
         default: SU2B_FORCE_LAUNCH(64, 16, false); break;
       }
     }
 #undef SU2B_FORCE_LAUNCH
 #undef SU2B_FORCE_SPLIT
 #undef SU2B_FORCE_XSPLIT
+#undef SU2B_FORCE_LINK
 #undef SU2B_FORCE_ARGS
     if (nblocks) *nblocks = nb;
   } else {

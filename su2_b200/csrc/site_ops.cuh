@@ -192,6 +192,40 @@ __device__ __forceinline__ double force_half_impl(const Geom &g, const LinkT<T> 
 
 
 
+// The fused force step for one link U_mu(x), one thread per link: its 2(d-1) staples,
+//   K = sum_{nu != mu} U_nu(x+mu) U_mu(x+nu)^+ U_nu(x)^+ + U_nu(x+mu-nu)^+ U_mu(x-nu)^+ U_nu(x-nu),
+// then finish_link.  6(d-1)+1 link loads and no product shared with another link: more work
+// per link than the site bodies, but d times the threads, for lattices too small to fill the
+// GPU with one thread per site.  Isotropic action.
+template <class T, int ND, int mu>
+__device__ __forceinline__ double force_link_impl(const Geom &g, const LinkT<T> *__restrict__ U,
+                                                  T *__restrict__ P,
+                                                  const T *__restrict__ extra, T f, T scale_,
+                                                  int mode, LinkT<T> *__restrict__ Uout,
+                                                  T dt_upd, int p, int cb) {
+  const int q = 1 - p;
+  const Site s = site_from_eo(g, p, cb);
+  const size_t V = (size_t)g.V, NL = V * ND;
+  const size_t self = (size_t)p * g.Vh + cb;
+  const int lpm = s.lex + fwd(g, s, mu);
+  Su2<T> K = zero_su2<T>();
+#pragma unroll
+  for (int nu = 0; nu < ND; nu++) {
+    if (nu == mu) continue;
+    const int lpn = s.lex + fwd(g, s, nu), bn = bwd(g, s, nu);
+    const Su2<T> a = ld_link(U + nu * V + eo_of(g, lpm, q));         // U_nu(x+mu)
+    const Su2<T> b = ld_link(U + mu * V + eo_of(g, lpn, q));         // U_mu(x+nu)
+    const Su2<T> c = ld_link(U + nu * V + self);                     // U_nu(x)
+    const Su2<T> e = ld_link(U + nu * V + eo_of(g, lpm + bn, p));    // U_nu(x+mu-nu)
+    const Su2<T> h = ld_link(U + mu * V + eo_of(g, s.lex + bn, q));  // U_mu(x-nu)
+    const Su2<T> d = ld_link(U + nu * V + eo_of(g, s.lex + bn, q));  // U_nu(x-nu)
+    K = mul_acc(K, mul(a, dag(b)), dag(c));
+    K = mul_acc(K, mul(dag(e), dag(h)), d);
+  }
+  return finish_link<T>(ld_link(U + mu * V + self), K, mu * V + self, NL, P, extra, f, scale_,
+                        mode, Uout, dt_upd);
+}
+
 // The split force step with each of the four planes that cross the halves formed once per
 // site instead of once per half.  With A_{mu,nu} = U_nu(x+mu) U_mu(x+nu)^+ the forward staples
 // of a plane are K_mu += A_{mu,nu} U_nu(x)^+ and K_nu += A_{mu,nu}^+ U_mu(x)^+.  The two

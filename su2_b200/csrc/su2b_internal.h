@@ -40,7 +40,7 @@ enum ForceMode : int {
 // launch shapes of the SU(2) force kernel (threads per block, minimum resident blocks per
 // SM, which caps registers): 0 (64,8) 1 (128,1) 2 (128,4) 3 (128,6) 4 (256,2) 5 (256,3);
 // 6, 7: neighbour links staged in shared memory by cp.async, 64 / 128 threads per block
-constexpr int FORCE_VARIANTS = 9;
+constexpr int FORCE_VARIANTS = 10;
 template <class T>
 cudaError_t force_update(const Geom &g, const void *U, int group, T *P, const T *extra, double f,
                          double scale, double xi, int mode, double *kin_part, int *nblocks,

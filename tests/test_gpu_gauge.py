@@ -344,6 +344,28 @@ def test_every_force_launch_shape_is_exact(gpu, orc, precision, dims):
             c.upload(U)
 
 
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+@pytest.mark.parametrize("dims,nd", [((6, 1, 1, 4), 2), ((4, 6, 1, 4), 3), ((6, 4, 1, 6), 3)],
+                         ids=["6x4-d2", "4x6x4-d3", "6x4x6-d3"])
+def test_every_force_launch_shape_below_four_dims(gpu, orc, precision, dims, nd):
+    """d = 2 and 3: every launch shape, including the one-thread-per-link kernel and the
+    two-threads-per-site shapes (which fall back to a site shape below d = 4), gives the
+    oracle's force and a finite trajectory."""
+    group = 0
+    U = hot(orc, group, dims, nd)
+    F = orc.gauge_derivative(group, dims, nd, 2.3, U)
+    tol = 1e-12 if precision == "fp64" else 1e-5
+    with make(gpu, group, dims, nd, beta=2.3, precision=precision) as c:
+        c.upload(U)
+        for v in range(gpu._abi.FORCE_VARIANTS):
+            c.force_variant = v
+            assert rel(c.derivative(), F) < tol, v
+            r = c.md_update("omf2", 3, 0.3, momenta=orc.initnormal(group, dims, nd, 5)[0],
+                            accept_reject=False)
+            assert np.isfinite(r.dH)
+            c.upload(U)
+
+
 def test_autotune_cache(gpu, orc, tmp_path):
     group, dims, nd = 0, (16, 16, 16, 16), 4
     U = hot(orc, group, dims, nd)
