@@ -181,9 +181,8 @@ __global__ void __launch_bounds__(NT)
 // the entries t + i NT into four accumulators (i mod 4), so four loads are in flight at a
 // time, then adds them pairwise and the block reduces in a fixed tree
 template <int NT>
-__global__ void __launch_bounds__(NT)
-  k_reduce_final(const double *__restrict__ part, int n, int ncomp, double *out) {
-  __shared__ double sh[NT / 32];
+__device__ __forceinline__ void reduce_into(const double *__restrict__ part, int n, int ncomp,
+                                            double *out, double *sh) {
   for (int k = 0; k < ncomp; k++) {
     double a0 = 0., a1 = 0., a2 = 0., a3 = 0.;
     int b = threadIdx.x;
@@ -197,6 +196,12 @@ __global__ void __launch_bounds__(NT)
     const double r = block_sum<NT>((a0 + a1) + (a2 + a3), sh);
     if (threadIdx.x == 0) out[k] = r;
   }
+}
+template <int NT>
+__global__ void __launch_bounds__(NT)
+  k_reduce_final(const double *__restrict__ part, int n, int ncomp, double *out) {
+  __shared__ double sh[NT / 32];
+  reduce_into<NT>(part, n, ncomp, out, sh);
 }
 
 // Programmatic dependent launch between the chained force launches of a trajectory: each
@@ -402,8 +407,8 @@ template <class T> __global__ void k_negate(size_t n, T *P) {
 
 // ------------------------------------------------------------------------------------
 // accept/reject (md_update.hh:45-60), one thread
-__global__ void k_accept(const double *__restrict__ red, const TrajParams *__restrict__ tp,
-                         TrajDev *out) {
+__device__ __forceinline__ void accept_body(const double *red, const TrajParams *__restrict__ tp,
+                                            TrajDev *out) {
   const TrajParams in = *tp;
   TrajDev t;
   t.H_old[0] = 0.5 * red[0];
@@ -431,6 +436,24 @@ __global__ void k_accept(const double *__restrict__ red, const TrajParams *__res
   }
   t.pad = 0;
   *out = t;
+}
+__global__ void k_accept(const double *__restrict__ red, const TrajParams *__restrict__ tp,
+                         TrajDev *out) {
+  accept_body(red, tp, out);
+}
+// the closing reductions of a fused trajectory and its accept/reject in one launch: the
+// start partials (momenta pass, 4 components, skipped when ns = 0) into red[0..3], the final
+// kinetic partials into red[4] (skipped when nk = 0), the end plaquette partials into
+// red[5..7], in the order of k_reduce_final, then the accept step on thread 0
+__global__ void __launch_bounds__(1024)
+  k_reduce_accept(const double *__restrict__ ps, int ns, const double *__restrict__ pk, int nk,
+                  const double *__restrict__ pp, int np, double *red,
+                  const TrajParams *__restrict__ tp, TrajDev *out) {
+  __shared__ double sh[32];
+  if (ns > 0) reduce_into<1024>(ps, ns, 4, red + 0, sh);
+  if (nk > 0) reduce_into<1024>(pk, nk, 1, red + 4, sh);
+  reduce_into<1024>(pp, np, 3, red + 5, sh);
+  if (threadIdx.x == 0) accept_body(red, tp, out);  // red[] as thread 0 itself wrote it
 }
 
 template <class T>
@@ -786,6 +809,12 @@ template <class T> cudaError_t negate_adj(const Geom &g, T *P, int group, cudaSt
 
 cudaError_t accept_step(const double *red, const TrajParams *tp, TrajDev *out, cudaStream_t s) {
   k_accept<<<1, 1, 0, s>>>(red, tp, out);
+  return cudaGetLastError();
+}
+cudaError_t reduce_accept(const double *ps, int ns, const double *pk, int nk, const double *pp,
+                          int np, double *red, const TrajParams *tp, TrajDev *out,
+                          cudaStream_t s) {
+  k_reduce_accept<<<1, 1024, 0, s>>>(ps, ns, pk, nk, pp, np, red, tp, out);
   return cudaGetLastError();
 }
 

@@ -174,16 +174,18 @@ int enqueue_fused(su2b_ctx *ctx, const std::vector<FOp> &fops, bool host_momenta
                   void *X, void *Y, void **fin) {
   cudaStream_t s = ctx->stream;
   int nb = 0;
+  // partial sums: the start pass in slot 1, the final kinetic energy in slot 2, the end
+  // plaquettes in slot 0; all three are reduced by the accept launch
+  int nb_start = 0, nb_kin = 0, nb_plaq = 0;
   SU2B_CK(cudaMemsetAsync(ctx->red + 8, 0, 2 * sizeof(double), s));
   if (!host_momenta) {
-    // momenta, kinetic energy and the plaquettes of the start field in one pass: red[0..3]
+    // momenta, kinetic energy and the plaquettes of the start field in one pass
     if (ctx->link64)
       SU2B_LAUNCH(SU2B_K_MOMENTA, momenta_plaq<double>(ctx->g, S, (double *)ctx->P, ctx->tparams,
-                                                       ctx->xi, ctx->part_slot(1), &nb, s));
+                                                       ctx->xi, ctx->part_slot(1), &nb_start, s));
     else
       SU2B_LAUNCH(SU2B_K_MOMENTA, momenta_plaq<float>(ctx->g, S, (float *)ctx->P, ctx->tparams,
-                                                      ctx->xi, ctx->part_slot(1), &nb, s));
-    SU2B_LAUNCH(SU2B_K_OTHER, reduce_final(ctx->part_slot(1), nb, 4, ctx->red + 0, s));
+                                                      ctx->xi, ctx->part_slot(1), &nb_start, s));
   } else {
     SU2B_CKS(su2b_q_plaq(ctx, S, 1));
   }
@@ -218,14 +220,14 @@ int enqueue_fused(su2b_ctx *ctx, const std::vector<FOp> &fops, bool host_momenta
     if (ctx->link64)
       SU2B_LAUNCH(SU2B_K_FORCE,
                   force_update<double>(ctx->g, cur, 0, (double *)ctx->P, nullptr, f, -o.cm,
-                                       ctx->xi, mode, ctx->part_slot(1), &nb, out, o.cg, s,
+                                       ctx->xi, mode, ctx->part_slot(2), &nb, out, o.cg, s,
                                        ctx->tune_force, pdl));
     else
       SU2B_LAUNCH(SU2B_K_FORCE,
                   force_update<float>(ctx->g, cur, 0, (float *)ctx->P, nullptr, f, -o.cm,
-                                      ctx->xi, mode, ctx->part_slot(1), &nb, out, o.cg, s,
+                                      ctx->xi, mode, ctx->part_slot(2), &nb, out, o.cg, s,
                                       ctx->tune_force, pdl));
-    if (o.kinetic) SU2B_LAUNCH(SU2B_K_OTHER, reduce_final(ctx->part_slot(1), nb, 1, ctx->red + 4, s));
+    if (o.kinetic) nb_kin = nb;
     if (o.kind == 1) cur = out;
   }
   if (!F) {  // the schedule ended with a gauge step: restore in place in a scratch buffer
@@ -236,8 +238,15 @@ int enqueue_fused(su2b_ctx *ctx, const std::vector<FOp> &fops, bool host_momenta
     SU2B_CKS(su2b_q_restore(ctx, cur));
     F = cur;
   }
-  SU2B_CKS(su2b_q_plaq(ctx, F, 5));
-  SU2B_LAUNCH(SU2B_K_OTHER, accept_step(ctx->red, ctx->tparams, ctx->traj, s));
+  if (ctx->link64)
+    SU2B_LAUNCH(SU2B_K_PLAQUETTE, plaq_partials<double>(ctx->g, F, ctx->group, ctx->xi,
+                                                        ctx->part_slot(0), &nb_plaq, s));
+  else
+    SU2B_LAUNCH(SU2B_K_PLAQUETTE, plaq_partials<float>(ctx->g, F, ctx->group, ctx->xi,
+                                                       ctx->part_slot(0), &nb_plaq, s));
+  SU2B_LAUNCH(SU2B_K_OTHER, reduce_accept(ctx->part_slot(1), nb_start, ctx->part_slot(2), nb_kin,
+                                          ctx->part_slot(0), nb_plaq, ctx->red, ctx->tparams,
+                                          ctx->traj, s));
   SU2B_CK(cudaMemcpyAsync(ctx->h_traj, ctx->traj, sizeof(TrajDev), cudaMemcpyDeviceToHost, s));
   SU2B_CK(cudaMemcpyAsync(ctx->h_red, ctx->red, 20 * sizeof(double), cudaMemcpyDeviceToHost, s));
   *fin = F;

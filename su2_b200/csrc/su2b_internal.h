@@ -86,6 +86,9 @@ struct TrajDev {
   int pad;
 };
 cudaError_t accept_step(const double *red, const TrajParams *tp, TrajDev *out, cudaStream_t s);
+cudaError_t reduce_accept(const double *ps, int ns, const double *pk, int nk, const double *pp,
+                          int np, double *red, const TrajParams *tp, TrajDev *out,
+                          cudaStream_t s);
 template <class T>
 cudaError_t cond_restore(const Geom &g, void *U, const void *U_old, int group,
                          const TrajDev *flag, cudaStream_t s);
