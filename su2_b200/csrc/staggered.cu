@@ -1153,6 +1153,23 @@ cudaError_t dot64(int n, const double2 *a, const double2 *b, double *part, cudaS
   return cudaGetLastError();
 }
 
+// One block per SM on the current device when it supports cooperative launches and one
+// block of `nt` threads of `kern` fits an SM, else 0.  Computed once per device and kernel:
+// slots[dev] holds the grid + 1 (0: not yet known).
+constexpr int COOP_MAX_DEVICES = 64;
+static int coop_blocks(const void *kern, int nt, int *slots) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= COOP_MAX_DEVICES) return 0;
+  if (slots[dev] == 0) {
+    int coop = 0, sms = 0, per_sm = 0;
+    cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, nt, 0);
+    slots[dev] = 1 + ((coop && per_sm >= 1) ? sms : 0);
+  }
+  return slots[dev] - 1;
+}
+
 // the persistent CG: one cooperative launch until convergence or the iteration limit;
 // returns cudaErrorNotSupported where cooperative launches are unavailable (the caller then
 // queues the per-phase kernels) and cudaErrorTimeout when a barrier wait gave up
@@ -1161,15 +1178,8 @@ cudaError_t cg_persistent(const Geom &g, const double2 *ph, double m, double2 *x
                           int part_cap, cudaStream_t s) {
   // one block of 512 threads per SM: the fewer blocks arrive at a barrier, the shorter it is
   constexpr int NT = 512;
-  static int grid = -1;
-  if (grid < 0) {
-    int dev = 0, coop = 0, sms = 0, per_sm = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_cg_persistent<NT>, NT, 0);
-    grid = (coop && per_sm >= 1) ? sms : 0;
-  }
+  static int slots[COOP_MAX_DEVICES];
+  const int grid = coop_blocks((const void *)k_cg_persistent<NT>, NT, slots);
   const int G = std::min(grid, std::max(1, (g.V + NT - 1) / NT));
   if (G <= 0 || 2 * G > part_cap || G > 32 * FIXED_SUM_PER_LANE) return cudaErrorNotSupported;
   GridBarrier *bar = (GridBarrier *)bar_mem;
@@ -1195,15 +1205,8 @@ cudaError_t cg_mixed_persistent(const Geom &g, const double2 *ph, const float2 *
                                 float2 *xs, float2 *rs, float2 *ps, float2 *ts, double *part,
                                 SolverState *st, void *bar_mem, int part_cap, cudaStream_t s) {
   constexpr int NT = 512;
-  static int grid = -1;
-  if (grid < 0) {
-    int dev = 0, coop = 0, sms = 0, per_sm = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_cg_mixed_persistent<NT>, NT, 0);
-    grid = (coop && per_sm >= 1) ? sms : 0;
-  }
+  static int slots[COOP_MAX_DEVICES];
+  const int grid = coop_blocks((const void *)k_cg_mixed_persistent<NT>, NT, slots);
   const int G = std::min(grid, std::max(1, (g.V + NT - 1) / NT));
   if (G <= 0 || 2 * G > part_cap || G > 32 * FIXED_SUM_PER_LANE) return cudaErrorNotSupported;
   GridBarrier *bar = (GridBarrier *)bar_mem;
@@ -1231,15 +1234,8 @@ cudaError_t bicgstab_persistent(const Geom &g, const double2 *ph, double m, doub
                                 double *part, SolverState *st, void *bar_mem, int part_cap,
                                 cudaStream_t s) {
   constexpr int NT = 512;
-  static int grid = -1;
-  if (grid < 0) {
-    int dev = 0, coop = 0, sms = 0, per_sm = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_bicgstab_persistent<NT>, NT, 0);
-    grid = (coop && per_sm >= 1) ? sms : 0;
-  }
+  static int slots[COOP_MAX_DEVICES];
+  const int grid = coop_blocks((const void *)k_bicgstab_persistent<NT>, NT, slots);
   const int G = std::min(grid, std::max(1, (g.V + NT - 1) / NT));
   if (G <= 0 || 8 * G > part_cap || G > 32 * FIXED_SUM_PER_LANE) return cudaErrorNotSupported;
   GridBarrier *bar = (GridBarrier *)bar_mem;
