@@ -105,3 +105,37 @@ def test_su2_4d_hmc_plaquette(gpu, precision):
           f"{np.mean(acc):.3f} (published {ref})")
     assert np.mean(acc) > 0.5
     assert abs(m - ref) < 4 * np.hypot(e, ref_err), (m, e, ref)
+
+
+def test_mixed_precision_keeps_the_dH_distribution(gpu):
+    """Mixed precision (FP32 links and forces, FP64 sums and accept/reject) against the FP64
+    path on the same start: the Delta H distribution (two-sample Kolmogorov-Smirnov), its
+    mean and the acceptance agree within statistical error, and both satisfy
+    <exp(-Delta H)> = 1 (Creutz's equality for an area-preserving, reversible integrator).
+    The two precisions draw different momenta, so they agree in distribution only."""
+    from scipy.stats import ks_2samp
+    L, beta = 10, 2.0
+    start = haar(L ** 4 * 4, 16)
+    dH, acc = {}, {}
+    for precision in ("fp64", "mixed"):
+        with gpu.gaugeconfig(L, L, L, L, 4, beta, precision=precision) as c:
+            c.upload(start)
+            for k in range(100):
+                c.sweep(0.3, 8, 17, k)
+            rs = [c.md_update("omf2", 8, 1.0, seed=18, traj=k) for k in range(1600)][100:]
+        dH[precision] = np.array([r.dH for r in rs])
+        acc[precision] = np.array([float(r.accepted) for r in rs])
+    for p in dH:
+        m, e = blocked(np.exp(-dH[p]))
+        print(f"{p}: <dH> = {dH[p].mean():.4f}, acceptance {acc[p].mean():.3f}, "
+              f"<exp(-dH)> = {m:.4f} +- {e:.4f}")
+        assert abs(m - 1.0) < 5 * e + 0.02, (p, m, e)
+    ks = ks_2samp(dH["fp64"], dH["mixed"])
+    print(f"KS two-sample: statistic {ks.statistic:.4f}, p {ks.pvalue:.3g}")
+    assert ks.pvalue > 1e-3
+    m64, e64 = blocked(dH["fp64"])
+    m32, e32 = blocked(dH["mixed"])
+    assert abs(m64 - m32) < 5 * np.hypot(e64, e32), (m64, e64, m32, e32)
+    a64, ea64 = blocked(acc["fp64"])
+    a32, ea32 = blocked(acc["mixed"])
+    assert abs(a64 - a32) < 5 * np.hypot(ea64, ea32), (a64, ea64, a32, ea32)
