@@ -456,7 +456,11 @@ def profile_run(args):
     A Haar-random 32^4 start (untimed work does not change what a kernel reads or writes),
     the force kernel's launch shape fixed by --force-variant instead of the tuner, then W
     warm-up and K steps of one precision.  --profile-op picks the step: an omf2 trajectory
-    (hmc), a Metropolis sweep (delta 0.15, 8 hits) or an RK3 Wilson-flow step (eps 0.01).
+    (hmc), a Metropolis sweep (delta 0.15, 8 hits), an RK3 Wilson-flow step (eps 0.01), or
+    (all) each of these plus every other kernel of the path once: plaquette, clover, Polyakov
+    and Wilson loops, APE smearing, gauge-file save/load, download, CG / BiCGStab (and the
+    mixed CG, or in FP64 a pseudofermion trajectory) on the U(1) 256^2 staggered workload,
+    and a leapfrog trajectory of eight chains of the batched ensemble.
     Prints one JSON line with the number of kernel launches made before the K steps (the ncu
     ``-s`` to skip to them) and per step.
     """
@@ -468,13 +472,45 @@ def profile_run(args):
     c.upload(haar_links(V * 4, 20240))
     c.force_variant = args.force_variant
 
+    u1 = batch = None
+    if args.profile_op == "all":
+        # the staggered solvers run on the U(1) 256^2 workload (vectors of 65,536 sites)
+        u1 = su2_b200.gaugeconfig(256, 1, 1, 256, 2, 4.0, group="u1", precision=args.precision)
+        u1.upload(np.random.default_rng(4242).uniform(-np.pi, np.pi, size=256 * 256 * 2))
+        b = np.random.default_rng(4243).normal(size=2 * 256 * 256)
+        # the batched kernels on the first eight chains of the 64-chain ensemble
+        from su2_b200.batch import chain_batch
+        from su2_b200 import replicas
+        chains = ensemble_chains()[:8]
+        batch = chain_batch(chains, precision="mixed")
+        for i, ch in enumerate(chains):
+            batch.upload(i, haar_links(replicas.chain_cost(ch) * ch["ndims"], ch["seed"]))
+    td = tempfile.mkdtemp()
+
     def step(k):
-        if args.profile_op == "hmc":
+        if args.profile_op in ("hmc", "all"):
             c.md_update("omf2", NSTEPS, TAU, seed=20240, traj=k)
-        elif args.profile_op == "metropolis":
+        if args.profile_op in ("metropolis", "all"):
             c.sweep(0.15, 8, 20240, k)
-        else:
+        if args.profile_op in ("flow", "all"):
             c.runge_kutta(0.01)
+        if args.profile_op == "all":  # every other kernel of the path, once
+            c.gauge_energy()
+            c.energy_density()
+            c.polyakov_loop_spatial_average()
+            c.wilsonloop(2, 2)
+            path = os.path.join(td, "conf")
+            c.save(path)
+            c.load(path)
+            c.APEsmearing(0.5)
+            c.download()
+            u1.solve(b, 0.05, tol=1e-10, solver="CG", tol_mode="rel")
+            u1.solve(b, 0.05, tol=1e-10, solver="BiCGStab", tol_mode="rel")
+            if args.precision == "mixed":
+                u1.solve(b, 0.05, tol=1e-10, solver="CG_mixed", tol_mode="rel")
+            else:  # pseudofermion trajectory (det D D^+ monomial, FP64 U(1) only)
+                u1.md_update("omf2", 2, 0.2, seed=7, traj=k, fermion_mass=0.05, cg_tol=1e-10)
+            batch.md_update("leapfrog", 10, 1.0, traj=k)
 
     for k in range(args.warmup):
         step(k)
@@ -490,6 +526,9 @@ def profile_run(args):
                       "setup_launches": n0, "launches_per_step": (n1 - n0) / max(1, args.steps),
                       "steps": args.steps, "warmup": args.warmup}), flush=True)
     c.close()
+    if u1 is not None:
+        u1.close()
+        batch.close()
     torch.cuda.synchronize()
 
 
@@ -858,7 +897,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile-run", action="store_true",
                     help="only the timed loop of one precision, for ncu (no bench line)")
-    ap.add_argument("--profile-op", default="hmc", choices=["hmc", "metropolis", "flow"],
+    ap.add_argument("--profile-op", default="hmc", choices=["hmc", "metropolis", "flow", "all"],
                     help="with --profile-run: the step of the loop")
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--force-variant", type=int, default=3)
