@@ -444,16 +444,48 @@ __global__ void k_accept(const double *__restrict__ red, const TrajParams *__res
 // the closing reductions of a fused trajectory and its accept/reject in one launch: the
 // start partials (momenta pass, 4 components, skipped when ns = 0) into red[0..3], the final
 // kinetic partials into red[4] (skipped when nk = 0), the end plaquette partials into
-// red[5..7], in the order of k_reduce_final, then the accept step on thread 0
+// red[5..7], then the accept step on thread 0.  Every thread strides over all three partial
+// arrays at once with eight accumulators (the loads of one stride are independent), then a
+// fixed shuffle tree per warp and the warp sums in order.
 __global__ void __launch_bounds__(1024)
   k_reduce_accept(const double *__restrict__ ps, int ns, const double *__restrict__ pk, int nk,
                   const double *__restrict__ pp, int np, double *red,
                   const TrajParams *__restrict__ tp, TrajDev *out) {
-  __shared__ double sh[32];
-  if (ns > 0) reduce_into<1024>(ps, ns, 4, red + 0, sh);
-  if (nk > 0) reduce_into<1024>(pk, nk, 1, red + 4, sh);
-  reduce_into<1024>(pp, np, 3, red + 5, sh);
-  if (threadIdx.x == 0) accept_body(red, tp, out);  // red[] as thread 0 itself wrote it
+  constexpr int NT = 1024, NC = 8;
+  __shared__ double sh[NC][NT / 32];
+  double acc[NC];
+#pragma unroll
+  for (int c = 0; c < NC; c++) acc[c] = 0.;
+  const int nmax = max(ns, max(nk, np));
+  for (int b = threadIdx.x; b < nmax; b += NT) {
+    if (b < ns) {
+#pragma unroll
+      for (int k = 0; k < 4; k++) acc[k] += ps[(size_t)b * 4 + k];
+    }
+    if (b < nk) acc[4] += pk[b];
+    if (b < np) {
+#pragma unroll
+      for (int k = 0; k < 3; k++) acc[5 + k] += pp[(size_t)b * 3 + k];
+    }
+  }
+#pragma unroll
+  for (int c = 0; c < NC; c++) {
+    double v = acc[c];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    if ((threadIdx.x & 31) == 0) sh[c][threadIdx.x >> 5] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < 32 * NC) {  // warp c sums component c over the 32 warp partials
+    const int c = threadIdx.x >> 5, l = threadIdx.x & 31;
+    double v = sh[c][l];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    const bool skip = (c < 4 && ns <= 0) || (c == 4 && nk <= 0);
+    if (l == 0 && !skip) red[c] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) accept_body(red, tp, out);
 }
 
 template <class T>
