@@ -27,7 +27,7 @@ __device__ __forceinline__ Su2<double> L(const Geom &g, const LinkT<T> *U, int m
 template <class T, int ND, int NT>
 __global__ void __launch_bounds__(NT)
   k_clover_su2(Geom g, const LinkT<T> *__restrict__ U, int cloverdef, double *part) {
-  __shared__ double sh[NT / 32];
+  __shared__ double shk[4 * (NT / 32)];
   const int p = blockIdx.x & 1;
   const int cb = (blockIdx.x >> 1) * NT + threadIdx.x;
   double e_all = 0., e_ss = 0., q = 0.;
@@ -74,18 +74,19 @@ __global__ void __launch_bounds__(NT)
     }
   }
   const int b = blockIdx.x;
-  double r = block_sum<NT>(e_all, sh);
-  if (threadIdx.x == 0) part[3 * b] = r;
-  r = block_sum<NT>(e_ss, sh);
-  if (threadIdx.x == 0) part[3 * b + 1] = r;
-  r = block_sum<NT>(q, sh);
-  if (threadIdx.x == 0) part[3 * b + 2] = r;
+  double v[3] = {e_all, e_ss, q};
+  block_sums<NT, 3>(v, shk);
+  if (threadIdx.x == 0) {
+    part[3 * b] = v[0];
+    part[3 * b + 1] = v[1];
+    part[3 * b + 2] = v[2];
+  }
 }
 
 template <int ND, int NT>
 __global__ void __launch_bounds__(NT)
   k_clover_u1(Geom g, const double *__restrict__ U, int cloverdef, double *part) {
-  __shared__ double sh[NT / 32];
+  __shared__ double shk[4 * (NT / 32)];
   const int p = blockIdx.x & 1;
   const int cb = (blockIdx.x >> 1) * NT + threadIdx.x;
   double e_all = 0., e_ss = 0., q = 0.;
@@ -126,12 +127,13 @@ __global__ void __launch_bounds__(NT)
     if (ND == 2) q += -G[0][1];
   }
   const int b = blockIdx.x;
-  double r = block_sum<NT>(e_all, sh);
-  if (threadIdx.x == 0) part[3 * b] = r;
-  r = block_sum<NT>(e_ss, sh);
-  if (threadIdx.x == 0) part[3 * b + 1] = r;
-  r = block_sum<NT>(q, sh);
-  if (threadIdx.x == 0) part[3 * b + 2] = r;
+  double v[3] = {e_all, e_ss, q};
+  block_sums<NT, 3>(v, shk);
+  if (threadIdx.x == 0) {
+    part[3 * b] = v[0];
+    part[3 * b + 1] = v[1];
+    part[3 * b + 2] = v[2];
+  }
 }
 
 }  // namespace

@@ -87,18 +87,19 @@ __global__ void k_spinor_to_host(Geom g, const double2 *__restrict__ psi, double
 template <class T, int ND, int NT>
 __global__ void __launch_bounds__(NT, 1024 / NT)
   k_plaq_su2(Geom g, const LinkT<T> *__restrict__ U, double xi, double *part) {
-  __shared__ double sh[NT / 32];
+  __shared__ double shk[4 * (NT / 32)];
   const int w = threadIdx.x >> 5, p = w & 1;
   const int cb = blockIdx.x * (NT / 2) + (w >> 1) * 32 + (threadIdx.x & 31);
   double full = 0., spat = 0., wsum = 0.;
   if (cb < g.Vh) plaq_site<T, ND>(g, U, p, cb, xi, full, spat, wsum);
   const int b = blockIdx.x;
-  double r = block_sum<NT>(full, sh);
-  if (threadIdx.x == 0) part[3 * b] = r;
-  r = block_sum<NT>(spat, sh);
-  if (threadIdx.x == 0) part[3 * b + 1] = r;
-  r = block_sum<NT>(wsum, sh);
-  if (threadIdx.x == 0) part[3 * b + 2] = r;
+  double v[3] = {full, spat, wsum};
+  block_sums<NT, 3>(v, shk);
+  if (threadIdx.x == 0) {
+    part[3 * b] = v[0];
+    part[3 * b + 1] = v[1];
+    part[3 * b + 2] = v[2];
+  }
 }
 
 // The start of a trajectory in one pass over the sites: the Philox momenta of the site's
@@ -108,7 +109,7 @@ template <class T, int ND, int NT>
 __global__ void __launch_bounds__(NT, 1024 / NT)
   k_momenta_plaq_su2(Geom g, const LinkT<T> *__restrict__ U, T *__restrict__ P,
                      const TrajParams *__restrict__ tp, double xi, double *part) {
-  __shared__ double sh[NT / 32];
+  __shared__ double shk[4 * (NT / 32)];
   const int w = threadIdx.x >> 5, p = w & 1;
   const int cb = blockIdx.x * (NT / 2) + (w >> 1) * 32 + (threadIdx.x & 31);
   double k2 = 0., full = 0., spat = 0., wsum = 0.;
@@ -131,20 +132,20 @@ __global__ void __launch_bounds__(NT, 1024 / NT)
     plaq_site<T, ND>(g, U, p, cb, xi, full, spat, wsum);
   }
   const int b = blockIdx.x;
-  double r = block_sum<NT>(k2, sh);
-  if (threadIdx.x == 0) part[4 * b] = r;
-  r = block_sum<NT>(full, sh);
-  if (threadIdx.x == 0) part[4 * b + 1] = r;
-  r = block_sum<NT>(spat, sh);
-  if (threadIdx.x == 0) part[4 * b + 2] = r;
-  r = block_sum<NT>(wsum, sh);
-  if (threadIdx.x == 0) part[4 * b + 3] = r;
+  double v[4] = {k2, full, spat, wsum};
+  block_sums<NT, 4>(v, shk);
+  if (threadIdx.x == 0) {
+    part[4 * b] = v[0];
+    part[4 * b + 1] = v[1];
+    part[4 * b + 2] = v[2];
+    part[4 * b + 3] = v[3];
+  }
 }
 
 template <int ND, int NT>
 __global__ void __launch_bounds__(NT)
   k_plaq_u1(Geom g, const double *__restrict__ U, double xi, double *part) {
-  __shared__ double sh[NT / 32];
+  __shared__ double shk[4 * (NT / 32)];
   const int w = threadIdx.x >> 5, p = w & 1;
   const int cb = blockIdx.x * (NT / 2) + (w >> 1) * 32 + (threadIdx.x & 31);
   double full = 0., spat = 0., wsum = 0.;
@@ -169,12 +170,13 @@ __global__ void __launch_bounds__(NT)
     }
   }
   const int b = blockIdx.x;
-  double r = block_sum<NT>(full, sh);
-  if (threadIdx.x == 0) part[3 * b] = r;
-  r = block_sum<NT>(spat, sh);
-  if (threadIdx.x == 0) part[3 * b + 1] = r;
-  r = block_sum<NT>(wsum, sh);
-  if (threadIdx.x == 0) part[3 * b + 2] = r;
+  double v[3] = {full, spat, wsum};
+  block_sums<NT, 3>(v, shk);
+  if (threadIdx.x == 0) {
+    part[3 * b] = v[0];
+    part[3 * b + 1] = v[1];
+    part[3 * b + 2] = v[2];
+  }
 }
 
 // out[k] = sum over b of part[b*ncomp + k], one block, in an order fixed by n: thread t sums

@@ -579,27 +579,6 @@ __global__ void __launch_bounds__(NT)
 }
 
 // ---- persistent BiCGStab ----
-// K deterministic block sums in one shared-memory round trip; the results are in thread 0
-template <int NT, int K> __device__ __forceinline__ void block_sums(double (&v)[K], double *sh) {
-#pragma unroll
-  for (int k = 0; k < K; k++)
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_down_sync(0xffffffffu, v[k], o);
-  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
-  if (l == 0)
-#pragma unroll
-    for (int k = 0; k < K; k++) sh[k * (NT / 32) + w] = v[k];
-  __syncthreads();
-  if (w == 0)
-#pragma unroll
-    for (int k = 0; k < K; k++) {
-      double r = (l < NT / 32) ? sh[k * (NT / 32) + l] : 0.0;
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) r += __shfl_down_sync(0xffffffffu, r, o);
-      v[k] = r;
-    }
-  __syncthreads();
-}
 // fixed_sum of K arrays part[k*n .. k*n+n) at once: one L2 round trip for all of them
 template <int K> __device__ __forceinline__ void fixed_sums(const double *part, int n,
                                                            double (&out)[K]) {

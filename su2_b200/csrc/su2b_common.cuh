@@ -338,5 +338,28 @@ template <int NT> __device__ __forceinline__ double block_sum(double v, double *
   __syncthreads();
   return r;  // valid in thread 0
 }
+// K block sums with one pair of barriers instead of K: each component is summed exactly as
+// block_sum sums it (the same shuffle tree, then the warp sums in order), so the results are
+// those of K calls of block_sum.  sh holds K * NT / 32 doubles; the sums are in thread 0.
+template <int NT, int K> __device__ __forceinline__ void block_sums(double (&v)[K], double *sh) {
+#pragma unroll
+  for (int k = 0; k < K; k++)
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_down_sync(0xffffffffu, v[k], o);
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  if (l == 0)
+#pragma unroll
+    for (int k = 0; k < K; k++) sh[k * (NT / 32) + w] = v[k];
+  __syncthreads();
+  if (w == 0)
+#pragma unroll
+    for (int k = 0; k < K; k++) {
+      double r = (l < NT / 32) ? sh[k * (NT / 32) + l] : 0.0;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) r += __shfl_down_sync(0xffffffffu, r, o);
+      v[k] = r;
+    }
+  __syncthreads();
+}
 
 }  // namespace su2b
