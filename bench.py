@@ -744,27 +744,33 @@ def config4(args):
         t_b = allmax(dist, e0.elapsed_time(e1) / 1e3)
         launches = b.kernel_launches() - n0
     total_sites = replicas.sum_over_ranks(sites) if dist is not None else sites
-    # one by one: every chain its own context and trajectory graph, run back to back
-    ctxs = []
-    for c, U in zip(mine, starts):
-        Lx, Ly, Lz, Lt = c["dims"]
-        g = su2_b200.gaugeconfig(Lx, Ly, Lz, Lt, c["ndims"], c["beta"], precision="mixed",
-                                 device=local)
-        g.upload(U)
-        g.autotune(os.path.join(tempfile.gettempdir(), "su2b_tune_cache.txt"))
-        for k in range(W):
-            g.md_update("leapfrog", 10, 1.0, seed=c["seed"], traj=k)
-        ctxs.append(g)
-    torch.cuda.synchronize()
-    barrier(dist)
-    t0 = time.perf_counter()
-    for k in range(K):
-        for c, g in zip(mine, ctxs):
-            g.md_update("leapfrog", 10, 1.0, seed=c["seed"], traj=W + k)
-    torch.cuda.synchronize()
-    t_1 = allmax(dist, time.perf_counter() - t0)
-    for g in ctxs:
-        g.close()
+    # one by one: every chain its own context and trajectory graph, run back to back, in the
+    # same precision (mixed) and in the plain form (FP64)
+    def one_by_one(precision):
+        ctxs = []
+        for c, U in zip(mine, starts):
+            Lx, Ly, Lz, Lt = c["dims"]
+            g = su2_b200.gaugeconfig(Lx, Ly, Lz, Lt, c["ndims"], c["beta"],
+                                     precision=precision, device=local)
+            g.upload(U)
+            g.autotune(os.path.join(tempfile.gettempdir(), "su2b_tune_cache.txt"))
+            for k in range(W):
+                g.md_update("leapfrog", 10, 1.0, seed=c["seed"], traj=k)
+            ctxs.append(g)
+        torch.cuda.synchronize()
+        barrier(dist)
+        t0 = time.perf_counter()
+        for k in range(K):
+            for c, g in zip(mine, ctxs):
+                g.md_update("leapfrog", 10, 1.0, seed=c["seed"], traj=W + k)
+        torch.cuda.synchronize()
+        t = allmax(dist, time.perf_counter() - t0)
+        for g in ctxs:
+            g.close()
+        return t
+
+    t_1 = one_by_one("mixed")
+    t_64 = one_by_one("fp64")
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         from oracle import oracle as O
@@ -792,6 +798,8 @@ def config4(args):
               batch_autotune_force_us={str(su2_b200._abi.BATCH_SHAPES[v]): us
                                        for v, us in tune.items()},
               batched_over_one_by_one=t_1 / t_b,
+              one_by_one_fp64_site_updates_per_s=total_sites * K / t_64,
+              batched_mixed_over_one_by_one_fp64=t_64 / t_b,
               acceptance=float(np.mean([r.accepted for rr in res for r in rr])),
               gpu_launches=int(launches), cpu_baseline=cpu)
 
