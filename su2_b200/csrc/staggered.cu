@@ -313,35 +313,37 @@ __device__ __forceinline__ float2 hop_site32(const Geom &g, const float2 *__rest
 }
 
 struct GridBarrier {
-  unsigned count;
-  unsigned gen;
+  unsigned long long count;  // arrivals since the launch; the host zeroes it before each launch
   int err;
 };
 
 constexpr long BARRIER_SPIN_LIMIT = 1L << 24;  // x >= 32 ns: gives up after about a second
 
+// One atomic per block and barrier: block b's k-th arrival draws a ticket from the running
+// 64-bit count, and the barrier of that round is complete when the count reaches the
+// round's end, (ticket / G + 1) G.  The arrival has release semantics (after the block barrier it
+// publishes every write of the block), the polling load acquire semantics.  No block resets
+// anything, so no second round trip is needed.
 __device__ __forceinline__ bool grid_sync(GridBarrier *b) {
   __syncthreads();
   if (threadIdx.x == 0) {
-    volatile unsigned *gen = &b->gen;
-    volatile int *err = &b->err;
-    const unsigned g0 = *gen;
-    __threadfence();
-    if (atomicAdd(&b->count, 1u) == gridDim.x - 1) {
-      b->count = 0;
-      __threadfence();
-      atomicAdd(&b->gen, 1u);
-    } else {
-      long spins = 0;
-      while (*gen == g0 && *err == 0) {
-        if (++spins > BARRIER_SPIN_LIMIT) {
-          atomicExch(&b->err, 1);
-          break;
-        }
-        __nanosleep(32);
+    unsigned long long ticket;
+    asm volatile("atom.add.release.gpu.u64 %0, [%1], 1;"
+                 : "=l"(ticket)
+                 : "l"(&b->count)
+                 : "memory");
+    const unsigned long long target = (ticket / gridDim.x + 1) * gridDim.x;
+    long spins = 0;
+    for (;;) {
+      unsigned long long cur;
+      asm volatile("ld.acquire.gpu.u64 %0, [%1];" : "=l"(cur) : "l"(&b->count) : "memory");
+      if (cur >= target || *(volatile int *)&b->err != 0) break;
+      if (++spins > BARRIER_SPIN_LIMIT) {
+        atomicExch(&b->err, 1);
+        break;
       }
+      __nanosleep(32);
     }
-    __threadfence();
   }
   __syncthreads();
   return *(volatile int *)&b->err == 0;
