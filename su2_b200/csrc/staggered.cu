@@ -337,8 +337,10 @@ __device__ __forceinline__ bool grid_sync(GridBarrier *b) {
     for (;;) {
       unsigned long long cur;
       asm volatile("ld.acquire.gpu.u64 %0, [%1];" : "=l"(cur) : "l"(&b->count) : "memory");
-      if (cur >= target || *(volatile int *)&b->err != 0) break;
-      if (++spins > BARRIER_SPIN_LIMIT) {
+      if (cur >= target) break;
+      // another block's wait gave up: checked every 64 polls (a load per poll costs time)
+      if ((++spins & 63) == 0 && *(volatile int *)&b->err != 0) break;
+      if (spins > BARRIER_SPIN_LIMIT) {
         atomicExch(&b->err, 1);
         break;
       }
