@@ -272,10 +272,13 @@ def ours(args):
                     d["GB/s"] = nb[kname] * NL / (kms / 1e3 / kn) / 1e9
                 per[kname] = d
         kernels[name] = per
+    # measured DRAM bytes of the launch shape the tuner chose, from an ncu capture
     traffic = None
     tp = os.path.join(ROOT, "profiles", "force_kernel_traffic.json")
     if os.path.exists(tp):
-        traffic = json.load(open(tp)).get("mixed_bytes_per_launch")
+        shape = su2_b200._abi.FORCE_SHAPES[mixed.force_variant]
+        key = shape[0] if isinstance(shape[0], str) else str(shape)
+        traffic = json.load(open(tp)).get("mixed_bytes_per_launch", {}).get(key)
 
     # ---- e2e through the C ABI with host buffers (pinned), per trajectory:
     #      upload the host gaugeconfig, one trajectory, download the gaugeconfig ----
