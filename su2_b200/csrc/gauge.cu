@@ -36,11 +36,7 @@ __global__ void k_links_to_host_su2(Geom g, const LinkT<T> *__restrict__ U, doub
     const int lex = (int)(i / g.nd), mu = (int)(i - (long)lex * g.nd);
     const Site s = site_from_lex(g, lex);
     const Su2<double> u = to64(ld_link_rw(U + (size_t)mu * g.V + eo_of(g, lex, s.p)));
-    double *dst = aos + 4 * i;
-    dst[0] = u.ar;
-    dst[1] = u.ai;
-    dst[2] = u.br;
-    dst[3] = u.bi;
+    st_link((Link64 *)aos + i, u);  // one 32-byte store (aos is 32-byte aligned)
   }
 }
 // U(1) angles and adjoint fields: na reals per link, SoA on the device
