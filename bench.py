@@ -215,8 +215,7 @@ def ours(args):
         mixed.md_update("omf2", NSTEPS, TAU, seed=seed, traj=100000 + k)
     U_th = mixed.download()
     # one FP64 start for both arms: FP32 links widened to double are unitary to about 1e-7
-    # only, and the FP64 trajectory's closing restoreSU would then shift S_G by O(1) at 32^4
-    # (a systematic dH of about 5), so the start is reunitarised in FP64 first
+    # only, so the thermalised field is reunitarised in FP64 first
     Uq = U_th.reshape(-1, 4)
     Uq /= np.sqrt(np.einsum("ij,ij->i", Uq, Uq))[:, None]
     mixed.upload(U_th)
@@ -341,6 +340,16 @@ def ours(args):
     obs["gaugeconfig_file_bytes"] = nbytes
     obs["save_GB_per_s"] = nbytes / t_save / 1e9
     obs["load_GB_per_s"] = nbytes / t_load / 1e9
+    # the workload's flow measurement: Wilson flow to t = 4 with eps = 0.01 on the thermalised
+    # field, records every second step (flat-gradient_flow.hh:70-197), t^2 E_clover at the end
+    fp64.upload(U_th)
+    fp64.synchronize()
+    t0 = time.perf_counter()
+    rows = fp64.gradient_flow(4.0, 0.01)
+    t_flow = time.perf_counter() - t0
+    obs["flow_to_t4"] = {"s": t_flow, "records": int(len(rows)), "t_last": float(rows[-1, 0]),
+                         "t2_Ec_last": float(rows[-1, 0] ** 2 * rows[-1, 6]),
+                         "t2_Ep_last": float(rows[-1, 0] ** 2 * rows[-1, 4])}
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
