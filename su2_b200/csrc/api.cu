@@ -7,6 +7,7 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <utility>
 #include <cstring>
 #include <random>
 #include <string>
@@ -536,7 +537,14 @@ int su2b_q_flow_step(su2b_ctx *ctx, void *U, double eps) {
 
 extern "C" int su2b_flow_step(su2b_ctx *ctx, double eps) {
   CKS(enter(ctx));
-  CKS(su2b_q_flow_step(ctx, ctx->U, eps));
+  if (ctx->group == SU2B_GROUP_SU2) {
+    // all three stages fused, U -> U2 -> U -> U2; the spare buffer becomes the current field
+    // (as a trajectory's accept rotates its buffers) and the old one the spare
+    CKS(su2b_q_flow_step_to(ctx, ctx->U, ctx->U2, eps));
+    std::swap(ctx->U, ctx->U2);
+  } else {
+    CKS(su2b_q_flow_step(ctx, ctx->U, eps));
+  }
   CK(cudaStreamSynchronize(ctx->stream));
   return SU2B_OK;
 }
