@@ -139,32 +139,65 @@ __global__ void __launch_bounds__(NT)
     double r = block_sum<NT>(full, sh);
     if (threadIdx.x == 0) part[3 * tile] = r;
     r = block_sum<NT>(spat, sh);
-    if (threadIdx.x == 0) part[3 * tile + 1] = r;
+    if (threadIdx.x == 0) {
+      part[3 * tile + 1] = r;
+      part[3 * tile + 2] = 0.0;
+    }
   }
 }
 
-// per chain: red[c*RS + slot + k] = sum of part[tile*ncomp + k] over the chain's tiles
-__global__ void __launch_bounds__(256)
-  k_batch_reduce(const ChainDev *__restrict__ ch, const double *__restrict__ part, int ncomp,
-                 double *red, int slot) {
-  __shared__ double sh[8];
-  const ChainDev &d = ch[blockIdx.x];
-  for (int k = 0; k < ncomp; k++) {
-    double v = 0.;
-    for (int t = threadIdx.x; t < d.ntiles; t += 256) v += part[(size_t)(d.tile0 + t) * ncomp + k];
-    const double r = block_sum<256>(v, sh);
-    if (threadIdx.x == 0) red[blockIdx.x * RS + slot + k] = r;
+// the start of a batched trajectory in one pass, as in the single-lattice path: each
+// site's Philox momenta with their |P|^2 and its start plaquettes; per tile the partials
+// {sum |P|^2, plaquettes, spatial plaquettes}
+template <class T, int NT>
+__global__ void __launch_bounds__(NT)
+  k_batch_momenta_plaq(const ChainDev *__restrict__ ch, int nchains, int ntiles, Bufs<T> bufs,
+                       const int *__restrict__ cur, T *__restrict__ Pall,
+                       const uint32_t *__restrict__ traj, double *part) {
+  __shared__ double shk[3 * (NT / 32)];
+  const int w = threadIdx.x >> 5, p = w & 1;
+  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const int c = chain_of(ch, nchains, tile);
+    const ChainDev &d = ch[c];
+    const int cb = (tile - d.tile0) * (NT / 2) + (w >> 1) * 32 + (threadIdx.x & 31);
+    double v[3] = {0., 0., 0.};
+    if (cb < d.g.Vh) {
+      const Site s = site_from_eo(d.g, p, cb);
+      const size_t NL = (size_t)d.g.V * d.g.nd;
+      T *P = Pall + d.off_adj;
+      for (int mu = 0; mu < d.g.nd; mu++) {
+        const uint32_t lref = (uint32_t)s.lex * (uint32_t)d.g.nd + (uint32_t)mu;
+        const size_t l = (size_t)mu * d.g.V + (size_t)p * d.g.Vh + cb;
+        T a, b, cc;
+        momentum_normals<T>(lref, *traj, d.seed, 3, a, b, cc);
+        P[l] = a;
+        P[NL + l] = b;
+        P[2 * NL + l] = cc;
+        v[0] += (double)a * a + (double)b * b + (double)cc * cc;
+      }
+      const LinkT<T> *U = bufs.b[cur[c] % 3] + d.off_link;
+      double wsum = 0.;
+      if (d.g.nd == 4)
+        plaq_site<T, 4>(d.g, U, p, cb, 1.0, v[1], v[2], wsum);
+      else
+        plaq_site<T, 3>(d.g, U, p, cb, 1.0, v[1], v[2], wsum);
+    }
+    block_sums<NT, 3>(v, shk);
+    if (threadIdx.x == 0) {
+      part[3 * tile] = v[0];
+      part[3 * tile + 1] = v[1];
+      part[3 * tile + 2] = v[2];
+    }
   }
 }
 
-// per chain accept/reject (md_update.hh:45-60) and advance of the buffer rotation
-__global__ void k_batch_accept(const ChainDev *__restrict__ ch, int nchains,
-                               const double *__restrict__ red, const uint32_t *__restrict__ traj,
-                               int rel_final, int *cur, TrajDev *out) {
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= nchains) return;
-  const ChainDev &d = ch[c];
-  const double *r = red + c * RS;
+// the closing reductions and the accept/reject of every chain in one launch, one block per
+// chain: the start partials (3 per tile) into red[0..2], the final kinetic partials into
+// red[4], the end plaquette partials (3 per tile, the third unused) into red[5..7], each in
+// a fixed order; then the chain's accept step (accept_chain) on thread 0
+__device__ __forceinline__ void accept_chain(const ChainDev &d, const double *r,
+                                             const uint32_t *__restrict__ traj, int rel_final,
+                                             int *cur_c, TrajDev *out) {
   TrajDev t;
   t.H_old[0] = 0.5 * r[0];
   t.H_old[1] = -d.beta * r[1] / 2.0;
@@ -185,8 +218,38 @@ __global__ void k_batch_accept(const ChainDev *__restrict__ ch, int nchains,
     if (t.u > exp(-dH)) t.accepted = 0;
   }
   t.pad = 0;
-  out[c] = t;
-  if (t.accepted) cur[c] = (cur[c] + rel_final) % 3;
+  *out = t;
+  if (t.accepted) *cur_c = (*cur_c + rel_final) % 3;
+}
+__global__ void __launch_bounds__(256)
+  k_batch_reduce_accept(const ChainDev *__restrict__ ch, const double *__restrict__ ps,
+                        const double *__restrict__ pk, const double *__restrict__ pe,
+                        double *red, const uint32_t *__restrict__ traj, int rel_final, int *cur,
+                        TrajDev *out) {
+  __shared__ double shk[7 * 8];
+  const int c = blockIdx.x;
+  const ChainDev &d = ch[c];
+  double v[7] = {0., 0., 0., 0., 0., 0., 0.};
+  for (int t = threadIdx.x; t < d.ntiles; t += 256) {
+    const size_t tt = (size_t)(d.tile0 + t);
+#pragma unroll
+    for (int k = 0; k < 3; k++) v[k] += ps[tt * 3 + k];
+    v[3] += pk[tt];
+#pragma unroll
+    for (int k = 0; k < 3; k++) v[4 + k] += pe[tt * 3 + k];
+  }
+  block_sums<256, 7>(v, shk);
+  if (threadIdx.x == 0) {
+    double *r = red + c * RS;
+    r[0] = v[0];
+    r[1] = v[1];
+    r[2] = v[2];
+    r[4] = v[3];
+    r[5] = v[4];
+    r[6] = v[5];
+    r[7] = v[6];
+    accept_chain(d, r, traj, rel_final, cur + c, out + c);
+  }
 }
 
 }  // namespace
@@ -202,6 +265,7 @@ struct su2b_batch {
   int ntiles[SU2B_BATCH_VARIANTS] = {};
   int variant = 2;
   size_t total_links = 0;
+  int maxtiles = 0;  // tiles of the launch shape with the most (sizes the partial buffer)
   void *buf[3] = {};
   void *P = nullptr;
   double *part = nullptr, *red = nullptr, *stage = nullptr;
@@ -291,6 +355,7 @@ extern "C" int su2b_batch_create(int n_chains, const su2b_chain_desc *chains, in
     maxtiles = std::max(maxtiles, tile);
   }
   b->total_links = off_l;
+  b->maxtiles = maxtiles;
   const int tile = maxtiles;
   if (cudaSetDevice(device) != cudaSuccess) return fin(SU2B_ERR_CUDA);
   if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess)
@@ -305,7 +370,7 @@ extern "C" int su2b_batch_create(int n_chains, const su2b_chain_desc *chains, in
   for (auto &c : b->hch[0]) maxNL = std::max(maxNL, (size_t)c.g.V * c.g.nd);
   bool ok = dal(&b->buf[0], lb * off_l) && dal(&b->buf[1], lb * off_l) &&
             dal(&b->buf[2], lb * off_l) && dal(&b->P, ab * off_a) &&
-            dal((void **)&b->part, sizeof(double) * 3 * (size_t)tile) &&
+            dal((void **)&b->part, sizeof(double) * 7 * (size_t)tile) &&
             dal((void **)&b->red, sizeof(double) * RS * n_chains) &&
             dal((void **)&b->stage, sizeof(double) * 4 * maxNL) &&
             dal((void **)&b->cur, sizeof(int) * n_chains) &&
@@ -463,14 +528,15 @@ int enqueue_batch_v(su2b_batch *b, const std::vector<BOp> &ops, int *rel_final) 
   Bufs<T> bufs{{(LinkT<T> *)b->buf[0], (LinkT<T> *)b->buf[1], (LinkT<T> *)b->buf[2]}};
   T *P = (T *)b->P;
   const int gF = grid_for<NT>((const void *)k_batch_force<T, NT, MINB>, ntiles);
-  const int gM = grid_for<NT>((const void *)k_batch_momenta<T, NT>, ntiles);
+  const int gM = grid_for<NT>((const void *)k_batch_momenta_plaq<T, NT>, ntiles);
   const int gP = grid_for<NT>((const void *)k_batch_plaq<T, NT>, ntiles);
+  // partial sums: the start pass, the final kinetic energy and the end plaquettes in three
+  // regions, all reduced by the closing accept launch
+  double *ps = b->part, *pk = b->part + 3 * (size_t)b->maxtiles,
+         *pe = b->part + 4 * (size_t)b->maxtiles;
   long nl = 0;
-  k_batch_momenta<T, NT><<<gM, NT, 0, s>>>(ch, b->n, ntiles, P, b->traj, b->part);
-  k_batch_reduce<<<b->n, 256, 0, s>>>(ch, b->part, 1, b->red, 0);
-  k_batch_plaq<T, NT><<<gP, NT, 0, s>>>(ch, b->n, ntiles, bufs, b->cur, 0, b->part);
-  k_batch_reduce<<<b->n, 256, 0, s>>>(ch, b->part, 3, b->red, 1);
-  nl += 4;
+  k_batch_momenta_plaq<T, NT><<<gM, NT, 0, s>>>(ch, b->n, ntiles, bufs, b->cur, P, b->traj, ps);
+  nl += 1;
   int cur = 0;
   auto next = [](int c) { return c == 1 ? 2 : 1; };
   int fin = -1;
@@ -486,20 +552,15 @@ int enqueue_batch_v(su2b_batch *b, const std::vector<BOp> &ops, int *rel_final) 
       out = fin = (cur == 0) ? 1 : next(cur);
     }
     k_batch_force<T, NT, MINB><<<gF, NT, 0, s>>>(ch, b->n, ntiles, bufs, P, b->cur, cur, out,
-                                                 o.cm, o.cg, mode, b->part);
+                                                 o.cm, o.cg, mode, pk);
     nl++;
-    if (o.kinetic) {
-      k_batch_reduce<<<b->n, 256, 0, s>>>(ch, b->part, 1, b->red, 4);
-      nl++;
-    }
     if (o.kind == 1) cur = out;
   }
   if (fin < 0) return bfail(b, SU2B_ERR_UNSUPPORTED, "schedule must end with a momentum step");
-  k_batch_plaq<T, NT><<<gP, NT, 0, s>>>(ch, b->n, ntiles, bufs, b->cur, fin, b->part);
-  k_batch_reduce<<<b->n, 256, 0, s>>>(ch, b->part, 3, b->red, 5);
-  k_batch_accept<<<(b->n + 63) / 64, 64, 0, s>>>(ch, b->n, b->red, b->traj, fin, b->cur,
-                                                 b->res);
-  nl += 3;
+  k_batch_plaq<T, NT><<<gP, NT, 0, s>>>(ch, b->n, ntiles, bufs, b->cur, fin, pe);
+  k_batch_reduce_accept<<<b->n, 256, 0, s>>>(ch, ps, pk, pe, b->red, b->traj, fin, b->cur,
+                                             b->res);
+  nl += 2;
   BCK(cudaGetLastError());
   BCK(cudaMemcpyAsync(b->h_res, b->res, sizeof(TrajDev) * b->n, cudaMemcpyDeviceToHost, s));
   BCK(cudaMemcpyAsync(b->h_red, b->red, sizeof(double) * RS * b->n, cudaMemcpyDeviceToHost, s));
