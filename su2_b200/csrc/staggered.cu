@@ -379,7 +379,7 @@ template <int NT> __device__ __forceinline__ double fixed_sum(const double *part
 }
 
 template <int NT>
-__global__ void __launch_bounds__(NT)
+__global__ void __launch_bounds__(NT, 1)
   k_cg_persistent(Geom g, const double2 *__restrict__ ph, double m, double2 *x, double2 *r,
                   double2 *p, double2 *t, double *part_t, double *part_r, SolverState *st,
                   GridBarrier *bar) {
@@ -403,13 +403,29 @@ __global__ void __launch_bounds__(NT)
   double bs = block_sum<NT>(acc, sh);
   if (threadIdx.x == 0) part_t[blockIdx.x] = bs;
   if (!grid_sync(bar)) return;
+  // Each phase reads its first site's stencil and own values before the global sum it
+  // waits for, so the two L2 round trips overlap (at 256^2 every thread has one site).
+  const bool has0 = first < n;
+  const int pp0 = first >= g.Vh, cb0 = first - pp0 * g.Vh;
   while (!done) {
+    double2 ap0{}, pv0{}, xv0{}, rv0{};
+    if (has0) {
+      ap0 = hop_site64(g, ph, m, 1.0, t, pp0, cb0);  // A p = D t
+      pv0 = p[first];
+      xv0 = x[first];
+      rv0 = r[first];
+    }
     const double2 alpha = cdivs(rr, make_double2(fixed_sum<NT>(part_t, G), 0.0));
     acc = 0.;
     for (int i = first; i < n; i += stride) {
-      const int pp = i >= g.Vh, cb = i - pp * g.Vh;
-      const double2 ap = hop_site64(g, ph, m, 1.0, t, pp, cb);  // A p = D t
-      const double2 pv = p[i], xv = x[i], rv = r[i];
+      double2 ap, pv, xv, rv;
+      if (i == first) {
+        ap = ap0, pv = pv0, xv = xv0, rv = rv0;
+      } else {
+        const int pp = i >= g.Vh, cb = i - pp * g.Vh;
+        ap = hop_site64(g, ph, m, 1.0, t, pp, cb);
+        pv = p[i], xv = x[i], rv = r[i];
+      }
       const double2 a1 = cm(alpha, pv), a2 = cm(alpha, ap);
       x[i] = make_double2(xv.x + a1.x, xv.y + a1.y);
       const double2 rnw = make_double2(rv.x - a2.x, rv.y - a2.y);
@@ -419,6 +435,13 @@ __global__ void __launch_bounds__(NT)
     bs = block_sum<NT>(acc, sh);
     if (threadIdx.x == 0) part_r[blockIdx.x] = bs;
     if (!grid_sync(bar)) return;
+    double2 dr0{}, rw0{}, pw0{}, tw0{};
+    if (has0) {
+      dr0 = hop_site64(g, ph, m, -1.0, r, pp0, cb0);  // D^+ r
+      rw0 = r[first];
+      pw0 = p[first];
+      tw0 = t[first];
+    }
     const double rr_new = fixed_sum<NT>(part_r, G);
     const double2 beta = cdivs(make_double2(rr_new, 0.0), rr);
     rr = make_double2(rr_new, 0.0);
@@ -430,9 +453,14 @@ __global__ void __launch_bounds__(NT)
     if (done) break;
     acc = 0.;
     for (int i = first; i < n; i += stride) {
-      const int pp = i >= g.Vh, cb = i - pp * g.Vh;
-      const double2 dr = hop_site64(g, ph, m, -1.0, r, pp, cb);  // D^+ r
-      const double2 rv = r[i], pv = p[i], tv = t[i];
+      double2 dr, rv, pv, tv;
+      if (i == first) {
+        dr = dr0, rv = rw0, pv = pw0, tv = tw0;
+      } else {
+        const int pp = i >= g.Vh, cb = i - pp * g.Vh;
+        dr = hop_site64(g, ph, m, -1.0, r, pp, cb);
+        rv = r[i], pv = p[i], tv = t[i];
+      }
       const double2 bp = cm(beta, pv), bt = cm(beta, tv);
       p[i] = make_double2(rv.x + bp.x, rv.y + bp.y);
       const double2 tn = make_double2(dr.x + bt.x, dr.y + bt.y);
@@ -458,7 +486,7 @@ __global__ void __launch_bounds__(NT)
 // phases); rs = (float) r; convergence is decided on that true residual.  The decisions come
 // from sums every block forms in the same order, so all blocks take them together.
 template <int NT>
-__global__ void __launch_bounds__(NT)
+__global__ void __launch_bounds__(NT, 1)
   k_cg_mixed_persistent(Geom g, const double2 *__restrict__ ph, const float2 *__restrict__ ph32,
                         double m, const double2 *__restrict__ b, double2 *x, double2 *r,
                         double2 *t64, float2 *xs, float2 *rs, float2 *ps, float2 *ts,
@@ -483,14 +511,29 @@ __global__ void __launch_bounds__(NT)
   double bs = block_sum<NT>(acc, sh);
   if (threadIdx.x == 0) part_t[blockIdx.x] = bs;
   if (!grid_sync(bar)) return;
+  // as in k_cg_persistent, each phase reads its first site's stencil and own values before
+  // the global sum it waits for
+  const bool has0 = first < n;
+  const int pp0 = first >= g.Vh, cb0 = first - pp0 * g.Vh;
   while (!done) {
+    float2 aq0{}, pv0{}, xv0{}, rv0{};
+    if (has0) {
+      aq0 = hop_site32(g, ph32, m32, 1.f, ts, pp0, cb0);  // A ps = D ts
+      pv0 = ps[first];
+      xv0 = xs[first];
+      rv0 = rs[first];
+    }
     const float alpha = (float)(rr / fixed_sum<NT>(part_t, G));
     acc = 0.;
     for (int i = first; i < n; i += stride) {
-      const int pp = i >= g.Vh, cb = i - pp * g.Vh;
-      const float2 aq = hop_site32(g, ph32, m32, 1.f, ts, pp, cb);  // A ps = D ts
-      const float2 pv = ps[i];
-      float2 xv = xs[i], rv = rs[i];
+      float2 aq, pv, xv, rv;
+      if (i == first) {
+        aq = aq0, pv = pv0, xv = xv0, rv = rv0;
+      } else {
+        const int pp = i >= g.Vh, cb = i - pp * g.Vh;
+        aq = hop_site32(g, ph32, m32, 1.f, ts, pp, cb);
+        pv = ps[i], xv = xs[i], rv = rs[i];
+      }
       xv.x += alpha * pv.x;
       xv.y += alpha * pv.y;
       rv.x -= alpha * aq.x;
@@ -502,6 +545,14 @@ __global__ void __launch_bounds__(NT)
     bs = block_sum<NT>(acc, sh);
     if (threadIdx.x == 0) part_r[blockIdx.x] = bs;
     if (!grid_sync(bar)) return;
+    // read before the sum; a reliable update below rewrites rs and forces a re-read
+    float2 dr0{}, rw0{}, pw0{}, tw0{};
+    if (has0) {
+      dr0 = hop_site32(g, ph32, m32, -1.f, rs, pp0, cb0);
+      rw0 = rs[first];
+      pw0 = ps[first];
+      tw0 = ts[first];
+    }
     double rr_new = fixed_sum<NT>(part_r, G);
     rn = sqrt(rr_new);
     iters++;
@@ -550,14 +601,23 @@ __global__ void __launch_bounds__(NT)
         done = 2;
         break;
       }
+      if (has0) {  // rs changed everywhere
+        dr0 = hop_site32(g, ph32, m32, -1.f, rs, pp0, cb0);
+        rw0 = rs[first];
+      }
     }
     const float beta = (float)(rr_new / rr);
     rr = rr_new;
     acc = 0.;
     for (int i = first; i < n; i += stride) {  // ps = rs + beta ps; ts = D^+ rs + beta ts
-      const int pp = i >= g.Vh, cb = i - pp * g.Vh;
-      const float2 dr = hop_site32(g, ph32, m32, -1.f, rs, pp, cb);
-      const float2 rv = rs[i], pv = ps[i], tv = ts[i];
+      float2 dr, rv, pv, tv;
+      if (i == first) {
+        dr = dr0, rv = rw0, pv = pw0, tv = tw0;
+      } else {
+        const int pp = i >= g.Vh, cb = i - pp * g.Vh;
+        dr = hop_site32(g, ph32, m32, -1.f, rs, pp, cb);
+        rv = rs[i], pv = ps[i], tv = ts[i];
+      }
       ps[i] = make_float2(rv.x + beta * pv.x, rv.y + beta * pv.y);
       const float2 tn = make_float2(dr.x + beta * tv.x, dr.y + beta * tv.y);
       ts[i] = tn;
