@@ -304,7 +304,7 @@ int flow_adjoint_t(su2b_ctx *ctx, double eps, int n, int every, double *objectiv
 
 extern "C" int su2b_action_backward(su2b_ctx *ctx, double grad_out, double *S, double *dS_host) {
   if (!ctx) return SU2B_ERR_INVALID;
-  ctx->err.clear();
+  ctx->begin_call();
   SU2B_CK(cudaSetDevice(ctx->device));
   if (S) {
     SU2B_CKS(su2b_q_plaq(ctx, ctx->U, 40));
@@ -319,7 +319,7 @@ extern "C" int su2b_action_backward(su2b_ctx *ctx, double grad_out, double *S, d
 
 extern "C" int su2b_force_vjp(su2b_ctx *ctx, const double *mu_host, double *out_host) {
   if (!ctx) return SU2B_ERR_INVALID;
-  ctx->err.clear();
+  ctx->begin_call();
   SU2B_CK(cudaSetDevice(ctx->device));
   SU2B_NEED(mu_host && out_host, "NULL buffer");
   if (ctx->group != SU2B_GROUP_SU2)
@@ -337,7 +337,7 @@ extern "C" int su2b_force_vjp(su2b_ctx *ctx, const double *mu_host, double *out_
 extern "C" int su2b_flow_adjoint(su2b_ctx *ctx, double eps, int n_steps, int checkpoint_every,
                                  double *objective, double *grad_host) {
   if (!ctx) return SU2B_ERR_INVALID;
-  ctx->err.clear();
+  ctx->begin_call();
   SU2B_CK(cudaSetDevice(ctx->device));
   SU2B_NEED(n_steps >= 1 && eps > 0, "n_steps >= 1 and eps > 0 required");
   if (ctx->group != SU2B_GROUP_SU2)

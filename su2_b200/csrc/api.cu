@@ -51,7 +51,7 @@ int su2b_fail(su2b_ctx *ctx, int code, const char *fmt, ...) {
 
 static int enter(su2b_ctx *ctx) {
   if (!ctx) return SU2B_ERR_INVALID;
-  ctx->err.clear();
+  ctx->begin_call();
   CK(cudaSetDevice(ctx->device));
   return SU2B_OK;
 }

@@ -69,7 +69,7 @@ void cache_store(const char *path, const std::string &key, int variant, double u
 extern "C" int su2b_autotune(su2b_ctx *ctx, const char *cache_path, int retune,
                              double *times_us) {
   if (!ctx) return SU2B_ERR_INVALID;
-  ctx->err.clear();
+  ctx->begin_call();
   SU2B_CK(cudaSetDevice(ctx->device));
   if (times_us)
     for (int v = 0; v < FORCE_VARIANTS; v++) times_us[v] = -1.0;

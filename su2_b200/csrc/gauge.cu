@@ -101,7 +101,9 @@ __global__ void __launch_bounds__(NT, 1024 / NT)
 // The start of a trajectory in one pass over the sites: the Philox momenta of the site's
 // links (as k_momenta) with their |P|^2, and the site's plaquettes (as k_plaq_su2) for H_old.
 // Per block: {sum |P|^2, plaquettes, spatial plaquettes, xi-weighted plaquettes}.
-template <class T, int ND, int NT>
+// Without PLAQ only the momenta and |P|^2 (the start plaquettes are known from the previous
+// trajectory); the partial layout stays the same, so the kinetic sums are identical.
+template <class T, int ND, int NT, bool PLAQ = true>
 __global__ void __launch_bounds__(NT, 1024 / NT)
   k_momenta_plaq_su2(Geom g, const LinkT<T> *__restrict__ U, T *__restrict__ P,
                      const TrajParams *__restrict__ tp, double xi, double *part) {
@@ -125,7 +127,7 @@ __global__ void __launch_bounds__(NT, 1024 / NT)
       P[2 * NL + l] = n2;
       k2 += (double)n0 * n0 + (double)n1 * n1 + (double)n2 * n2;
     }
-    plaq_site<T, ND>(g, U, p, cb, xi, full, spat, wsum);
+    if (PLAQ) plaq_site<T, ND>(g, U, p, cb, xi, full, spat, wsum);
   }
   const int b = blockIdx.x;
   double v[4] = {k2, full, spat, wsum};
@@ -445,12 +447,17 @@ __global__ void k_accept(const double *__restrict__ red, const TrajParams *__res
 // red[5..7], then the accept step on thread 0.  Every thread strides over all three partial
 // arrays at once with eight accumulators (the loads of one stride are independent), then a
 // fixed shuffle tree per warp and the warp sums in order.
+// cached_start: the momenta pass summed no plaquettes (its components 1..3 are zero); the
+// start field is the previous trajectory's result, whose plaquette sums are still in red[]:
+// red[5..7] if that trajectory was accepted (out->accepted), else red[1..3].  They are taken
+// before the end plaquettes overwrite red[5..7].
 __global__ void __launch_bounds__(1024)
   k_reduce_accept(const double *__restrict__ ps, int ns, const double *__restrict__ pk, int nk,
                   const double *__restrict__ pp, int np, double *red,
-                  const TrajParams *__restrict__ tp, TrajDev *out) {
+                  const TrajParams *__restrict__ tp, TrajDev *out, int cached_start) {
   constexpr int NT = 1024, NC = 8;
   __shared__ double sh[NC][NT / 32];
+  __shared__ double sum[NC];
   double acc[NC];
 #pragma unroll
   for (int c = 0; c < NC; c++) acc[c] = 0.;
@@ -479,11 +486,24 @@ __global__ void __launch_bounds__(1024)
     double v = sh[c][l];
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-    const bool skip = (c < 4 && ns <= 0) || (c == 4 && nk <= 0);
-    if (l == 0 && !skip) red[c] = v;
+    if (l == 0) sum[c] = v;
   }
   __syncthreads();
-  if (threadIdx.x == 0) accept_body(red, tp, out);
+  if (threadIdx.x == 0) {
+    if (cached_start) {
+      const bool prev_accepted = out->accepted != 0;
+#pragma unroll
+      for (int k = 1; k < 4; k++) red[k] = prev_accepted ? red[4 + k] : red[k];
+      red[0] = sum[0];
+    } else if (ns > 0) {
+#pragma unroll
+      for (int k = 0; k < 4; k++) red[k] = sum[k];
+    }
+    if (nk > 0) red[4] = sum[4];
+#pragma unroll
+    for (int k = 5; k < 8; k++) red[k] = sum[k];
+    accept_body(red, tp, out);
+  }
 }
 
 template <class T>
@@ -808,16 +828,20 @@ cudaError_t momenta_philox(const Geom &g, T *P, int group, const TrajParams *tp,
 
 template <class T>
 cudaError_t momenta_plaq(const Geom &g, const void *U, T *P, const TrajParams *tp, double xi,
-                         double *part, int *nblocks, cudaStream_t s) {
+                         double *part, int *nblocks, cudaStream_t s, bool plaq) {
   constexpr int NT = 256;
   const dim3 grid(cdiv(g.Vh, NT / 2));
   *nblocks = grid.x;
   const LinkT<T> *u = (const LinkT<T> *)U;
+#define SU2B_MP(ND)                                                                          \
+  (plaq ? (k_momenta_plaq_su2<T, ND, NT, true><<<grid, NT, 0, s>>>(g, u, P, tp, xi, part), 0) \
+        : (k_momenta_plaq_su2<T, ND, NT, false><<<grid, NT, 0, s>>>(g, u, P, tp, xi, part), 0))
   switch (g.nd) {
-    case 2: k_momenta_plaq_su2<T, 2, NT><<<grid, NT, 0, s>>>(g, u, P, tp, xi, part); break;
-    case 3: k_momenta_plaq_su2<T, 3, NT><<<grid, NT, 0, s>>>(g, u, P, tp, xi, part); break;
-    default: k_momenta_plaq_su2<T, 4, NT><<<grid, NT, 0, s>>>(g, u, P, tp, xi, part); break;
+    case 2: SU2B_MP(2); break;
+    case 3: SU2B_MP(3); break;
+    default: SU2B_MP(4); break;
   }
+#undef SU2B_MP
   return cudaGetLastError();
 }
 
@@ -843,8 +867,8 @@ cudaError_t accept_step(const double *red, const TrajParams *tp, TrajDev *out, c
 }
 cudaError_t reduce_accept(const double *ps, int ns, const double *pk, int nk, const double *pp,
                           int np, double *red, const TrajParams *tp, TrajDev *out,
-                          cudaStream_t s) {
-  k_reduce_accept<<<1, 1024, 0, s>>>(ps, ns, pk, nk, pp, np, red, tp, out);
+                          bool cached_start, cudaStream_t s) {
+  k_reduce_accept<<<1, 1024, 0, s>>>(ps, ns, pk, nk, pp, np, red, tp, out, (int)cached_start);
   return cudaGetLastError();
 }
 
@@ -882,7 +906,7 @@ cudaError_t cond_restore(const Geom &g, void *U, const void *U_old, int group,
   template cudaError_t momenta_philox<T>(const Geom &, T *, int, const TrajParams *,         \
                                          double *, int *, cudaStream_t);                      \
   template cudaError_t momenta_plaq<T>(const Geom &, const void *, T *, const TrajParams *,  \
-                                       double, double *, int *, cudaStream_t);                \
+                                       double, double *, int *, cudaStream_t, bool);          \
   template cudaError_t kinetic_partials<T>(const Geom &, const T *, int, double *, int *,    \
                                            cudaStream_t);                                     \
   template cudaError_t negate_adj<T>(const Geom &, T *, int, cudaStream_t);                  \

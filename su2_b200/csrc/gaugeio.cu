@@ -105,7 +105,7 @@ using namespace su2b;
 
 static int io_enter(su2b_ctx *ctx) {
   if (!ctx) return SU2B_ERR_INVALID;
-  ctx->err.clear();
+  ctx->begin_call();
   SU2B_CK(cudaSetDevice(ctx->device));
   return SU2B_OK;
 }

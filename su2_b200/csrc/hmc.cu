@@ -170,8 +170,10 @@ std::vector<FOp> fuse(const std::vector<Op> &ops) {
 }
 
 // queues the trajectory; returns the buffer that holds the final field in *fin
-int enqueue_fused(su2b_ctx *ctx, const std::vector<FOp> &fops, bool host_momenta, void *S,
-                  void *X, void *Y, void **fin) {
+// cached: the start plaquettes are those the previous trajectory left in red[] (its start
+// or its end field, by its accept flag), so the start pass skips the plaquette sums
+int enqueue_fused(su2b_ctx *ctx, const std::vector<FOp> &fops, bool host_momenta, bool cached,
+                  void *S, void *X, void *Y, void **fin) {
   cudaStream_t s = ctx->stream;
   int nb = 0;
   // partial sums: the start pass in slot 1, the final kinetic energy in slot 2, the end
@@ -182,10 +184,12 @@ int enqueue_fused(su2b_ctx *ctx, const std::vector<FOp> &fops, bool host_momenta
     // momenta, kinetic energy and the plaquettes of the start field in one pass
     if (ctx->link64)
       SU2B_LAUNCH(SU2B_K_MOMENTA, momenta_plaq<double>(ctx->g, S, (double *)ctx->P, ctx->tparams,
-                                                       ctx->xi, ctx->part_slot(1), &nb_start, s));
+                                                       ctx->xi, ctx->part_slot(1), &nb_start, s,
+                                                       !cached));
     else
       SU2B_LAUNCH(SU2B_K_MOMENTA, momenta_plaq<float>(ctx->g, S, (float *)ctx->P, ctx->tparams,
-                                                      ctx->xi, ctx->part_slot(1), &nb_start, s));
+                                                      ctx->xi, ctx->part_slot(1), &nb_start, s,
+                                                      !cached));
   } else {
     SU2B_CKS(su2b_q_plaq(ctx, S, 1));
   }
@@ -246,14 +250,14 @@ int enqueue_fused(su2b_ctx *ctx, const std::vector<FOp> &fops, bool host_momenta
                                                        ctx->part_slot(0), &nb_plaq, s));
   SU2B_LAUNCH(SU2B_K_OTHER, reduce_accept(ctx->part_slot(1), nb_start, ctx->part_slot(2), nb_kin,
                                           ctx->part_slot(0), nb_plaq, ctx->red, ctx->tparams,
-                                          ctx->traj, s));
+                                          ctx->traj, cached && !host_momenta, s));
   SU2B_CK(cudaMemcpyAsync(ctx->h_traj, ctx->traj, sizeof(TrajDev), cudaMemcpyDeviceToHost, s));
   SU2B_CK(cudaMemcpyAsync(ctx->h_red, ctx->red, 20 * sizeof(double), cudaMemcpyDeviceToHost, s));
   *fin = F;
   return SU2B_OK;
 }
 
-int traj_fused(su2b_ctx *ctx, const su2b_hmc_params *prm, su2b_traj_result *res) {
+int traj_fused(su2b_ctx *ctx, const su2b_hmc_params *prm, bool cached, su2b_traj_result *res) {
   cudaStream_t s = ctx->stream;
   const std::vector<FOp> fops = fuse(schedule(prm->integrator, prm->n_steps, prm->tau));
   void *S = ctx->U, *X = ctx->U_old, *Y = ctx->U2, *F = nullptr;
@@ -263,19 +267,19 @@ int traj_fused(su2b_ctx *ctx, const su2b_hmc_params *prm, su2b_traj_result *res)
     SU2B_CKS(kinetic_now(ctx, 0));
   }
   if (ctx->prof || host_momenta) {
-    SU2B_CKS(enqueue_fused(ctx, fops, host_momenta, S, X, Y, &F));
+    SU2B_CKS(enqueue_fused(ctx, fops, host_momenta, cached && !host_momenta, S, X, Y, &F));
   } else {
     // one CUDA graph per schedule, coupling and buffer assignment; seed, trajectory index
     // and accept uniform come from ctx->tparams, so the graph replays for every trajectory
     char key[256];
-    snprintf(key, sizeof key, "%d/%d/%.17g/%.17g/%p/%p/%p/%d", prm->integrator, prm->n_steps,
-             prm->tau, ctx->beta, S, X, Y, ctx->tune_force);
+    snprintf(key, sizeof key, "%d/%d/%.17g/%.17g/%p/%p/%p/%d/%d", prm->integrator, prm->n_steps,
+             prm->tau, ctx->beta, S, X, Y, ctx->tune_force, (int)cached);
     auto it = ctx->graphs.find(key);
     if (it == ctx->graphs.end()) {
       const long n0 = ctx->launches;
       cudaGraph_t graph = nullptr;
       SU2B_CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
-      const int rc = enqueue_fused(ctx, fops, false, S, X, Y, &F);
+      const int rc = enqueue_fused(ctx, fops, false, cached, S, X, Y, &F);
       const cudaError_t ec = cudaStreamEndCapture(s, &graph);
       if (rc != SU2B_OK) {
         if (graph) cudaGraphDestroy(graph);
@@ -312,6 +316,9 @@ int traj_fused(su2b_ctx *ctx, const su2b_hmc_params *prm, su2b_traj_result *res)
   res->plaquette = t.accepted ? r[5] : r[1];
   res->cg_iterations = 0;
   if (ctx->pend.size() > 4096) SU2B_CKS(su2b_prof_fold(ctx));
+  // red[1..3] and red[5..7] now hold the start and end plaquettes; the next trajectory of an
+  // uninterrupted sequence takes its start plaquettes from them (any other call clears this)
+  ctx->start_plaq_cached = true;
   return SU2B_OK;
 }
 
@@ -320,7 +327,8 @@ int traj_fused(su2b_ctx *ctx, const su2b_hmc_params *prm, su2b_traj_result *res)
 extern "C" int su2b_hmc_trajectory(su2b_ctx *ctx, const su2b_hmc_params *prm,
                                    su2b_traj_result *res) {
   if (!ctx) return SU2B_ERR_INVALID;
-  ctx->err.clear();
+  const bool cached = ctx->start_plaq_cached;
+  ctx->begin_call();
   SU2B_CK(cudaSetDevice(ctx->device));
   SU2B_NEED(prm && res, "params or result is NULL");
   SU2B_NEED(prm->n_steps >= 1, "n_steps must be >= 1");
@@ -343,7 +351,7 @@ extern "C" int su2b_hmc_trajectory(su2b_ctx *ctx, const su2b_hmc_params *prm,
   SU2B_CK(cudaMemcpyAsync(ctx->tparams, ctx->h_tparams, sizeof(TrajParams),
                           cudaMemcpyHostToDevice, s));
   if (ctx->group == SU2B_GROUP_SU2 && !ferm && !prm->revtest)
-    return traj_fused(ctx, prm, res);
+    return traj_fused(ctx, prm, cached, res);
 
   // generic path: U(1), fermions, reversibility test
   const std::vector<Op> ops = schedule(prm->integrator, prm->n_steps, prm->tau);

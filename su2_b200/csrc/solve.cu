@@ -466,7 +466,7 @@ int su2b_fermion_heatbath_q(su2b_ctx *ctx, double mass, const double *R_host, ui
 extern "C" int su2b_staggered_apply(su2b_ctx *ctx, int op, double mass, const double *psi_host,
                                     double *out_host) {
   if (!ctx) return SU2B_ERR_INVALID;
-  ctx->err.clear();
+  ctx->begin_call();
   SU2B_CK(cudaSetDevice(ctx->device));
   SU2B_NEED(psi_host && out_host, "NULL buffer");
   SU2B_NEED(op == SU2B_OP_D || op == SU2B_OP_DDAG || op == SU2B_OP_DDDAG, "bad op %d", op);
@@ -483,7 +483,7 @@ extern "C" int su2b_staggered_apply(su2b_ctx *ctx, int op, double mass, const do
 extern "C" int su2b_solve(su2b_ctx *ctx, const su2b_solve_params *prm, const double *b_host,
                           const double *x0_host, double *x_host, su2b_solve_stats *stats) {
   if (!ctx) return SU2B_ERR_INVALID;
-  ctx->err.clear();
+  ctx->begin_call();
   SU2B_CK(cudaSetDevice(ctx->device));
   SU2B_NEED(prm && b_host && x_host, "NULL argument");
   SU2B_NEED(prm->max_iter > 0, "max_iter must be positive");
@@ -539,7 +539,7 @@ extern "C" int su2b_fermion_force(su2b_ctx *ctx, double mass, const double *phi_
                                   double tol, int max_iter, const double *x0_host, long seed,
                                   double *deriv_host, long *cg_iterations) {
   if (!ctx) return SU2B_ERR_INVALID;
-  ctx->err.clear();
+  ctx->begin_call();
   SU2B_CK(cudaSetDevice(ctx->device));
   SU2B_NEED(deriv_host, "deriv_host is NULL");
   long it = 0;
@@ -556,7 +556,7 @@ extern "C" int su2b_fermion_action(su2b_ctx *ctx, double mass, const double *phi
                                    double tol, int max_iter, const double *x0_host, long seed,
                                    double *out) {
   if (!ctx) return SU2B_ERR_INVALID;
-  ctx->err.clear();
+  ctx->begin_call();
   SU2B_CK(cudaSetDevice(ctx->device));
   SU2B_NEED(out, "out is NULL");
   long it = 0;
@@ -578,7 +578,7 @@ extern "C" int su2b_fermion_action(su2b_ctx *ctx, double mass, const double *phi
 extern "C" int su2b_pion_correlator(su2b_ctx *ctx, double mass, double tol, int max_iter,
                                     long seed, double *C_host, long *cg_iterations) {
   if (!ctx) return SU2B_ERR_INVALID;
-  ctx->err.clear();
+  ctx->begin_call();
   SU2B_CK(cudaSetDevice(ctx->device));
   SU2B_NEED(C_host, "C_host is NULL");
   SU2B_NEED(max_iter > 0, "max_iter must be positive");

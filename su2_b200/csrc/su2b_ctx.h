@@ -54,6 +54,16 @@ struct su2b_ctx {
   su2b::SolverState *st = nullptr;
   long x0_seed = -1;  // seed of the reference CG start held in sv[SV_X0]
 
+  // set at the end of a fused trajectory: red[] then holds the plaquette sums of both the
+  // trajectory's start field and its final field, so the next fused trajectory takes its
+  // start plaquettes from there instead of summing them again.  Every entry point clears it
+  // on entry (begin_call), so any call between trajectories forces a fresh sum.
+  bool start_plaq_cached = false;
+  void begin_call() {
+    err.clear();
+    start_plaq_cached = false;
+  }
+
   // launch shape of the SU(2) force kernel (su2b_autotune)
   int tune_force = 3;  // (128 threads, 6 blocks/SM) until tuned; FP64 contexts start at 2
 

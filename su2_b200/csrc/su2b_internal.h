@@ -64,10 +64,12 @@ template <class T>
 cudaError_t momenta_philox(const Geom &g, T *P, int group, const TrajParams *tp,
                            double *kin_part, int *nblocks, cudaStream_t s);
 // SU(2): the Philox momenta of every link and the plaquette sums of the field in one pass;
-// partials {|P|^2, plaquettes, spatial, weighted} per block (4 per block)
+// partials {|P|^2, plaquettes, spatial, weighted} per block (4 per block); with plaq false the
+// plaquette components are zero (the start plaquettes are carried over from the previous
+// trajectory)
 template <class T>
 cudaError_t momenta_plaq(const Geom &g, const void *U, T *P, const TrajParams *tp, double xi,
-                         double *part, int *nblocks, cudaStream_t s);
+                         double *part, int *nblocks, cudaStream_t s, bool plaq = true);
 template <class T>
 cudaError_t kinetic_partials(const Geom &g, const T *P, int group, double *part, int *nblocks,
                              cudaStream_t s);
@@ -88,7 +90,7 @@ struct TrajDev {
 cudaError_t accept_step(const double *red, const TrajParams *tp, TrajDev *out, cudaStream_t s);
 cudaError_t reduce_accept(const double *ps, int ns, const double *pk, int nk, const double *pp,
                           int np, double *red, const TrajParams *tp, TrajDev *out,
-                          cudaStream_t s);
+                          bool cached_start, cudaStream_t s);
 template <class T>
 cudaError_t cond_restore(const Geom &g, void *U, const void *U_old, int group,
                          const TrajDev *flag, cudaStream_t s);

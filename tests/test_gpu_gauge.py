@@ -303,6 +303,39 @@ def test_trajectory_graph_replay(gpu, orc, precision):
     assert 0 < sum(r.accepted for r in runs["graph"][0])
 
 
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_start_plaquettes_carried_over(gpu, orc, precision):
+    """Consecutive trajectories take their start plaquettes from the previous trajectory's
+    sums (its end field if accepted, else its start field); a chain with a read-only call
+    between trajectories (which drops that carry-over) evolves the same field bit for bit,
+    with the same accept decisions and energies to rounding."""
+    group, dims, nd = 0, (8, 8, 8, 8), 4
+    U = hot(orc, group, dims, nd)
+    runs = {}
+    for mode in ("chain", "interleaved"):
+        with make(gpu, group, dims, nd, beta=2.3, precision=precision) as c:
+            c.upload(U)
+            out = []
+            for k in range(12):
+                # uniform 1e-300 accepts; 0.999999 rejects whenever dH > 1e-6
+                u = 1e-300 if k % 3 == 0 else 0.999999
+                out.append(c.md_update("omf2", 3, 1.0, seed=5, traj=k, uniform=u))
+                if mode == "interleaved":
+                    c.gauge_energy()
+            runs[mode] = (out, c.download())
+    chain, inter = runs["chain"][0], runs["interleaved"][0]
+    for a, b in zip(chain, inter):
+        assert a.accepted == b.accepted
+        assert a.dH == pytest.approx(b.dH, abs=1e-9)
+        assert a.plaquette == pytest.approx(b.plaquette, rel=1e-13)
+    assert np.array_equal(runs["chain"][1], runs["interleaved"][1])
+    acc = [r.accepted for r in chain]
+    assert any(acc) and not all(acc)
+    # the carried-over start energy is the previous trajectory's end or start energy exactly
+    for a, b in zip(chain, chain[1:]):
+        assert b.H_old[1] == (a.H_new[1] if a.accepted else a.H_old[1])
+
+
 def test_rejected_trajectory_keeps_start_field(gpu, orc):
     group, dims, nd = 0, (6, 6, 6, 6), 4
     U = hot(orc, group, dims, nd)
