@@ -44,9 +44,9 @@ __device__ __forceinline__ double finish_link(const Su2<T> &u, const Su2<T> &k, 
     p1 = P[NL + l];
     p2 = P[2 * NL + l];
   }
-  p0 = p0 + scale_ * d0;
-  p1 = p1 + scale_ * d1;
-  p2 = p2 + scale_ * d2;
+  p0 = fm(scale_, d0, p0);
+  p1 = fm(scale_, d1, p1);
+  p2 = fm(scale_, d2, p2);
   P[l] = p0;
   P[NL + l] = p1;
   P[2 * NL + l] = p2;
