@@ -306,9 +306,10 @@ def test_trajectory_graph_replay(gpu, orc, precision):
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
 def test_start_plaquettes_carried_over(gpu, orc, precision):
     """Consecutive trajectories take their start plaquettes from the previous trajectory's
-    sums (its end field if accepted, else its start field); a chain with a read-only call
-    between trajectories (which drops that carry-over) evolves the same field bit for bit,
-    with the same accept decisions and energies to rounding."""
+    sums (its end field if accepted, else its start field), also after a trajectory with
+    host momenta; a chain with a read-only call between trajectories (which drops that
+    carry-over) evolves the same field bit for bit, with the same accept decisions and
+    energies to rounding."""
     group, dims, nd = 0, (8, 8, 8, 8), 4
     U = hot(orc, group, dims, nd)
     runs = {}
@@ -317,9 +318,11 @@ def test_start_plaquettes_carried_over(gpu, orc, precision):
             c.upload(U)
             out = []
             for k in range(12):
-                # uniform 1e-300 accepts; 0.999999 rejects whenever dH > 1e-6
+                # uniform 1e-300 accepts; 0.999999 rejects whenever dH > 1e-6; trajectory 6
+                # takes host momenta (its start sums come from the separate plaquette pass)
                 u = 1e-300 if k % 3 == 0 else 0.999999
-                out.append(c.md_update("omf2", 3, 1.0, seed=5, traj=k, uniform=u))
+                mom = orc.initnormal(group, dims, nd, 77)[0] if k == 6 else None
+                out.append(c.md_update("omf2", 3, 1.0, seed=5, traj=k, uniform=u, momenta=mom))
                 if mode == "interleaved":
                     c.gauge_energy()
             runs[mode] = (out, c.download())
@@ -332,8 +335,12 @@ def test_start_plaquettes_carried_over(gpu, orc, precision):
     acc = [r.accepted for r in chain]
     assert any(acc) and not all(acc)
     # the carried-over start energy is the previous trajectory's end or start energy exactly
-    for a, b in zip(chain, chain[1:]):
-        assert b.H_old[1] == (a.H_new[1] if a.accepted else a.H_old[1])
+    for k, (a, b) in enumerate(zip(chain, chain[1:])):
+        if k + 1 == 6:  # summed afresh by the host-momenta path
+            assert b.H_old[1] == pytest.approx(a.H_new[1] if a.accepted else a.H_old[1],
+                                               rel=1e-13)
+        else:
+            assert b.H_old[1] == (a.H_new[1] if a.accepted else a.H_old[1])
 
 
 def test_rejected_trajectory_keeps_start_field(gpu, orc):
