@@ -65,3 +65,16 @@ def test_transfer_requires_context(fn):
     from su2_b200 import _abi
     lib = _abi.load()
     assert getattr(lib, fn)(None, None) == _abi.ERR_INVALID
+
+
+def test_launch_shape_tables_agree_with_the_header():
+    """The Python tables of launch shapes have one entry per variant the C ABI accepts, and
+    the variant counts equal the header's (and the library's) constants."""
+    from su2_b200 import _abi
+    text = open(os.path.join(ROOT, "include", "su2b.h")).read()
+    nf = int(re.search(r"#define SU2B_FORCE_VARIANTS (\d+)", text).group(1))
+    nb = int(re.search(r"#define SU2B_BATCH_VARIANTS (\d+)", text).group(1))
+    assert _abi.FORCE_VARIANTS == nf == len(_abi.FORCE_SHAPES)
+    assert _abi.BATCH_VARIANTS == nb == len(_abi.BATCH_SHAPES)
+    src = open(os.path.join(ROOT, "su2_b200", "csrc", "su2b_internal.h")).read()
+    assert int(re.search(r"constexpr int FORCE_VARIANTS = (\d+);", src).group(1)) == nf
