@@ -62,7 +62,9 @@ enum { SU2B_PREC_FP64 = 0, SU2B_PREC_MIXED = 1 };
 /* integrator ids as the reference enum (integrator.hh:15) */
 enum {
   SU2B_LEAPFROG = 0,
+  SU2B_LP_LEAPFROG = 1, /* leapfrog with rounding (integrator.hh:53-80) */
   SU2B_OMF4 = 2,
+  SU2B_LP_OMF4 = 3,     /* omf4 with rounding (integrator.hh:158-199) */
   SU2B_EULER = 4,
   SU2B_RUTH = 5,
   SU2B_OMF2 = 6
@@ -135,6 +137,12 @@ typedef struct {
   int pf_complex;         /* 0: real R as the reference (staggered.hpp:188-191) */
   int cg_start;           /* SU2B_CG_START_*: start vector of every inner CG */
   long pf_seed;           /* seed of the reference's sigma=10 Gaussian CG start */
+  /* SU2B_LP_LEAPFROG / SU2B_LP_OMF4 only, 0..19: before each momentum step the summed
+   * derivative, and before each gauge step every link, is rounded componentwise to
+   * round(x * 10^e) / 10^e (update_momenta.hh:36-58, update_gauge.hh:20-26; a U(1) link
+   * angle a becomes round(a) * 10^e / 10^e as u1.hh:31-33 writes it).  The reference's
+   * command-line default is 0. */
+  int round_exponent;
 } su2b_hmc_params;
 
 typedef struct {

@@ -38,6 +38,7 @@ _SIGS = {
     "S_G_hmc": (f64, _G + [f64, _D, f64, i32]),
     "gauge_derivative": (None, _G + [f64, f64, _D, f64, _D]),
     "md_injected": (f64, _G + [f64, f64, i32, i32, f64, _D, _D, _D]),
+    "md_injected_lp": (f64, _G + [f64, f64, i32, i32, f64, _D, _D, _D, i32]),
     "hmc_run": (None, _G + [f64, f64, i32, i32, f64, i64, i32, i32, _D, _I, _D, _D]),
     "energy_density": (None, _G + [_D, i32, i32, _D, _D]),
     "runge_kutta": (None, _G + [f64, f64, f64, _D]),
@@ -170,12 +171,21 @@ class Oracle:
         self._gauge_derivative(group, *dims, nd, beta, xi, dp(U), fac, dp(out))
         return out
 
-    def md_injected(self, group, dims, nd, beta, integ, nsteps, tau, U, P, xi=1.0):
+    def md_injected(self, group, dims, nd, beta, integ, nsteps, tau, U, P, xi=1.0,
+                    exponent=None):
+        """exponent: the rounding exponent of the low-precision integrators (ids 1 and 3);
+        None uses 16, the reference's default when the integrator is built without one."""
         U = U.copy()
         P = P.copy()
         H = np.zeros(4)
-        dH = self._md_injected(group, *dims, nd, beta, xi, integ, nsteps, tau, dp(U), dp(P),
-                               dp(H))
+        if exponent is None and integ in (1, 3):
+            exponent = 16
+        if exponent is None:
+            dH = self._md_injected(group, *dims, nd, beta, xi, integ, nsteps, tau, dp(U),
+                                   dp(P), dp(H))
+        else:
+            dH = self._md_injected_lp(group, *dims, nd, beta, xi, integ, nsteps, tau, dp(U),
+                                      dp(P), dp(H), exponent)
         return dH, U, P, H
 
     def hmc_run(self, group, dims, nd, beta, integ, nsteps, tau, seed, i0, ntraj, U, xi=1.0):

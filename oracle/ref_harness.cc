@@ -130,8 +130,9 @@ namespace {
     return l;
   }
 
-  template <class G> integrator<double, G> *make_integrator(int id) {
-    return set_integrator<double, G>(static_cast<size_t>(id), 16);
+  // the exponent matters to the low-precision integrators (ids 1, 3) only
+  template <class G> integrator<double, G> *make_integrator(int id, int exponent = 16) {
+    return set_integrator<double, G>(static_cast<size_t>(id), static_cast<size_t>(exponent));
   }
 
 } // namespace
@@ -232,9 +233,9 @@ void ref_gauge_derivative(int group, int Lx, int Ly, int Lz, int Lt, int nd, dou
 // md_update (md_update.hh:18-81) with the momentum draw replaced by injected momenta and
 // no accept/reject: heatbath -> integrate -> accept.  U, P updated in place.
 // H[0..3] = {kinetic Hold, gauge Hold, kinetic Hnew, gauge Hnew}; returns delta H.
-double ref_md_injected(int group, int Lx, int Ly, int Lz, int Lt, int nd, double beta,
-                       double xi, int integ, int nsteps, double tau, double *U_io,
-                       double *P_io, double *H) {
+double ref_md_injected_lp(int group, int Lx, int Ly, int Lz, int Lt, int nd, double beta,
+                          double xi, int integ, int nsteps, double tau, double *U_io,
+                          double *P_io, double *H, int exponent) {
   double dH = 0.;
   DISPATCH(group, {
     gaugeconfig<G> U(Lx, Ly, Lz, Lt, nd, beta);
@@ -246,7 +247,7 @@ double ref_md_injected(int group, int Lx, int Ly, int Lz, int Lt, int nd, double
     auto ml = gauge_monomials(km, gm);
     hamiltonian_field<double, G> h(P, U);
     for (auto m : ml) m->heatbath(h);
-    integrator<double, G> *it = make_integrator<G>(integ);
+    integrator<double, G> *it = make_integrator<G>(integ, exponent);
     md_params p(nsteps, tau);
     it->integrate(ml, h, p);
     for (auto m : ml) {
@@ -262,6 +263,12 @@ double ref_md_injected(int group, int Lx, int Ly, int Lz, int Lt, int nd, double
     io<G>::getP(P, P_io);
   });
   return dH;
+}
+double ref_md_injected(int group, int Lx, int Ly, int Lz, int Lt, int nd, double beta,
+                       double xi, int integ, int nsteps, double tau, double *U_io,
+                       double *P_io, double *H) {
+  return ref_md_injected_lp(group, Lx, Ly, Lz, Lt, nd, beta, xi, integ, nsteps, tau, U_io, P_io,
+                            H, 16);
 }
 
 // The reference HMC chain: for i in [i0, i0+ntraj): std::mt19937 engine(seed+i);

@@ -1080,7 +1080,15 @@ typedef struct {
   double m, tol;
   long seed;
   const double *phi;
+  /* lp_leapfrog / lp_omf4: 10^exponent (> 0), else 0 */
+  double round_dn;
 } md_sys;
+
+/* x.round(n) of the low-precision integrators, componentwise std::round(x*dn)/dn:
+ * adjointsu2 / adjointu1 (adjointfield.hh:28-31, 67-69) and _su2 (su2.hh:29-33) */
+static inline double round_dn(double x, double dn) { return round(x * dn) / dn; }
+/* _u1::round (u1.hh:31-33) rounds the angle before scaling: (round(a)*dn)/dn */
+static inline double round_u1_link(double a, double dn) { return (round(a) * dn) / dn; }
 
 /* update_momenta.hh:10-33: deriv = 0; gauge (+ fermion) derivative; P -= dtau*deriv */
 static void md_update_momenta(const md_sys *s, double *U, double *P, double dtau) {
@@ -1092,16 +1100,30 @@ static void md_update_momenta(const md_sys *s, double *U, double *P, double dtau
   if (s->fermions)
     orc_fermion_derivative((int)l->L[1], (int)l->L[2], (int)l->L[3], (int)l->L[0], l->nd, U,
                            s->m, s->phi, s->tol, s->seed, deriv);
-  for (size_t i = 0; i < N * na; i++) P[i] -= dtau * deriv[i];
+  if (s->round_dn > 0.) /* round_and_update_momenta (update_momenta.hh:36-58) */
+    for (size_t i = 0; i < N * na; i++) P[i] -= dtau * round_dn(deriv[i], s->round_dn);
+  else
+    for (size_t i = 0; i < N * na; i++) P[i] -= dtau * deriv[i];
   free(deriv);
 }
 static void md_update_gauge(const md_sys *s, double *U, const double *P, double dtau) {
   const lat_t *l = &s->l;
+  if (s->round_dn > 0.) { /* round_and_update_gauge (update_gauge.hh:20-26): U = e * round(U) */
+    const size_t N = nlinks(l);
+    for (size_t i = 0; i < N; i++) {
+      if (s->group == 0)
+        for (int k = 0; k < 4; k++) U[4 * i + k] = round_dn(U[4 * i + k], s->round_dn);
+      else
+        U[i] = round_u1_link(U[i], s->round_dn);
+    }
+  }
   orc_update_gauge(s->group, (int)l->L[1], (int)l->L[2], (int)l->L[3], (int)l->L[0], l->nd, U,
                    P, dtau);
 }
 
-/* integrator.hh:26-50 (0), :83-116 (6), :119-156 (2), :201-217 (4), :220-241 (5) */
+/* integrator.hh:26-50 (0), :83-116 (6), :119-156 (2), :201-217 (4), :220-241 (5); the
+ * low-precision lp_leapfrog (1, :53-80) and lp_omf4 (3, :158-199) take the schedules of 0 and
+ * 2 with the rounding of md_sys.round_dn */
 static void md_integrate(const md_sys *s, int integ, int nsteps, double tau, double *U,
                          double *P) {
   const double dtau = tau / (double)nsteps;
@@ -1119,7 +1141,7 @@ static void md_integrate(const md_sys *s, int integ, int nsteps, double tau, dou
     md_update_momenta(s, U, P, om2l * dtau);
     md_update_gauge(s, U, P, 0.5 * dtau);
     md_update_momenta(s, U, P, lambda * dtau);
-  } else if (integ == 2) { /* omf4 */
+  } else if (integ == 2 || integ == 3) { /* omf4, lp_omf4 */
     const double rho = 0.2539785108410595, theta = -0.03230286765269967,
                  vartheta = 0.08398315262876693, lambda = 0.6822365335719091;
     const double eps[10] = {rho * dtau,
@@ -1171,10 +1193,15 @@ static void md_integrate(const md_sys *s, int integ, int nsteps, double tau, dou
   orc_restore_su(s->group, (int)l->L[1], (int)l->L[2], (int)l->L[3], (int)l->L[0], l->nd, U);
 }
 
+static void integrate_r(int group, int Lx, int Ly, int Lz, int Lt, int nd, double beta,
+                        double xi, int integ, int nsteps, double tau, double *U, double *P,
+                        double dn) {
+  md_sys s = {group, mklat(Lx, Ly, Lz, Lt, nd), beta, xi, 0, 0., 0., 0, NULL, dn};
+  md_integrate(&s, integ, nsteps, tau, U, P);
+}
 void orc_integrate(int group, int Lx, int Ly, int Lz, int Lt, int nd, double beta, double xi,
                    int integ, int nsteps, double tau, double *U, double *P) {
-  md_sys s = {group, mklat(Lx, Ly, Lz, Lt, nd), beta, xi, 0, 0., 0., 0, NULL};
-  md_integrate(&s, integ, nsteps, tau, U, P);
+  integrate_r(group, Lx, Ly, Lz, Lt, nd, beta, xi, integ, nsteps, tau, U, P, 0.);
 }
 
 /* adjointfield.hh:219-238: P*P */
@@ -1194,20 +1221,33 @@ static double kinetic(int group, const double *P, size_t nl) {
 }
 
 /* md_update.hh:18-61 with injected momenta, without the accept/reject */
-double orc_md_injected(int group, int Lx, int Ly, int Lz, int Lt, int nd, double beta,
-                       double xi, int integ, int nsteps, double tau, double *U, double *P,
-                       double *H) {
+static double md_injected_r(int group, int Lx, int Ly, int Lz, int Lt, int nd, double beta,
+                            double xi, int integ, int nsteps, double tau, double *U, double *P,
+                            double *H, double dn) {
   const lat_t l = mklat(Lx, Ly, Lz, Lt, nd);
   const int aniso = (xi != 1.0);
   H[0] = kinetic(group, P, nlinks(&l));
   H[1] = orc_S_G_hmc(group, Lx, Ly, Lz, Lt, nd, beta, U, xi, aniso);
-  orc_integrate(group, Lx, Ly, Lz, Lt, nd, beta, xi, integ, nsteps, tau, U, P);
+  integrate_r(group, Lx, Ly, Lz, Lt, nd, beta, xi, integ, nsteps, tau, U, P, dn);
   H[2] = kinetic(group, P, nlinks(&l));
   H[3] = orc_S_G_hmc(group, Lx, Ly, Lz, Lt, nd, beta, U, xi, aniso);
   double dH = 0.;
   dH += H[2] - H[0];
   dH += H[3] - H[1];
   return dH;
+}
+double orc_md_injected(int group, int Lx, int Ly, int Lz, int Lt, int nd, double beta,
+                       double xi, int integ, int nsteps, double tau, double *U, double *P,
+                       double *H) {
+  return md_injected_r(group, Lx, Ly, Lz, Lt, nd, beta, xi, integ, nsteps, tau, U, P, H, 0.);
+}
+/* md_injected with a low-precision integrator (1 or 3): N = pow(10, exponent) converted to
+ * size_t as integrator.hh:59,168 does, so dn = 10^exponent exactly for exponent <= 19 */
+double orc_md_injected_lp(int group, int Lx, int Ly, int Lz, int Lt, int nd, double beta,
+                          double xi, int integ, int nsteps, double tau, double *U, double *P,
+                          double *H, int exponent) {
+  const double dn = (double)(size_t)pow(10, exponent);
+  return md_injected_r(group, Lx, Ly, Lz, Lt, nd, beta, xi, integ, nsteps, tau, U, P, H, dn);
 }
 
 /* initnormal (adjointfield.hh:240-258) from std::mt19937(seed) + the next uniform draw */
@@ -1262,7 +1302,7 @@ double orc_md_injected_fermion(int Lx, int Ly, int Lz, int Lt, int nd, double be
   H[0] = kinetic(1, P, nlinks(&l));
   H[1] = orc_S_G_hmc(1, Lx, Ly, Lz, Lt, nd, beta, U, 1.0, 0);
   H[2] = vdot(l.V, R, R).r;
-  md_sys s = {1, l, beta, 1.0, 1, m, tol, seed, phi};
+  md_sys s = {1, l, beta, 1.0, 1, m, tol, seed, phi, 0.};
   md_integrate(&s, integ, nsteps, tau, U, P);
   H[3] = kinetic(1, P, nlinks(&l));
   H[4] = orc_S_G_hmc(1, Lx, Ly, Lz, Lt, nd, beta, U, 1.0, 0);

@@ -54,6 +54,9 @@ void orc_integrate(int group, int Lx, int Ly, int Lz, int Lt, int nd, double bet
 double orc_md_injected(int group, int Lx, int Ly, int Lz, int Lt, int nd, double beta,
                        double xi, int integ, int nsteps, double tau, double *U, double *P,
                        double *H);
+double orc_md_injected_lp(int group, int Lx, int Ly, int Lz, int Lt, int nd, double beta,
+                          double xi, int integ, int nsteps, double tau, double *U, double *P,
+                          double *H, int exponent);
 double orc_initnormal(int group, int Lx, int Ly, int Lz, int Lt, int nd, long seed, double *P);
 void orc_hmc_run(int group, int Lx, int Ly, int Lz, int Lt, int nd, double beta, double xi,
                  int integ, int nsteps, double tau, long seed, int i0, int ntraj, double *U,

@@ -14,7 +14,7 @@ LIB_PATH = os.path.join(HERE, "libsu2b.so")
 OK, ERR_INVALID, ERR_CUDA, ERR_NOT_CONVERGED, ERR_UNSUPPORTED, ERR_NOMEM, ERR_TIMEOUT = range(7)
 GROUP_SU2, GROUP_U1 = 0, 1
 PREC_FP64, PREC_MIXED = 0, 1
-LEAPFROG, OMF4, EULER, RUTH, OMF2 = 0, 2, 4, 5, 6
+LEAPFROG, LP_LEAPFROG, OMF4, LP_OMF4, EULER, RUTH, OMF2 = 0, 1, 2, 3, 4, 5, 6
 OP_D, OP_DDAG, OP_DDDAG = 0, 1, 2
 SOLVER_CG, SOLVER_BICGSTAB, SOLVER_CG_MIXED = 0, 1, 2
 TOL_ABS, TOL_REL = 0, 1
@@ -33,7 +33,7 @@ class HmcParams(C.Structure):
                 ("accept_reject", C.c_int), ("momenta_host", _D), ("uniform_host", C.c_double),
                 ("fermion_mass", C.c_double), ("cg_tol", C.c_double), ("cg_max_iter", C.c_int),
                 ("pf_source_host", _D), ("pf_complex", C.c_int), ("cg_start", C.c_int),
-                ("pf_seed", C.c_long)]
+                ("pf_seed", C.c_long), ("round_exponent", C.c_int)]
 
 
 class TrajResult(C.Structure):

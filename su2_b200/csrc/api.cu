@@ -420,11 +420,13 @@ int su2b_q_force(su2b_ctx *ctx, const void *U, void *P, const void *extra, doubl
   return q_force<float>(ctx, U, (float *)P, (const float *)extra, f, scale, mode, kin_part, nb,
                         Uout, dt_upd);
 }
-int su2b_q_update(su2b_ctx *ctx, void *U, const void *P, double dt) {
+int su2b_q_update(su2b_ctx *ctx, void *U, const void *P, double dt, double round_dn) {
   if (ctx->link64)
-    SU2B_LAUNCH(SU2B_K_UPDATE, link_update<double>(ctx->g, U, ctx->group, (const double *)P, dt, ctx->stream));
+    SU2B_LAUNCH(SU2B_K_UPDATE, link_update<double>(ctx->g, U, ctx->group, (const double *)P, dt,
+                                                   ctx->stream, round_dn));
   else
-    SU2B_LAUNCH(SU2B_K_UPDATE, link_update<float>(ctx->g, U, ctx->group, (const float *)P, dt, ctx->stream));
+    SU2B_LAUNCH(SU2B_K_UPDATE, link_update<float>(ctx->g, U, ctx->group, (const float *)P, dt,
+                                                  ctx->stream, round_dn));
   ctx->phases_valid = false;
   return SU2B_OK;
 }

@@ -341,6 +341,41 @@ __global__ void k_update_u1(size_t NL, double *__restrict__ U, const double *__r
        l += (size_t)gridDim.x * blockDim.x)
     U[l] = dt * P[l] + U[l];
 }
+// The rounding of the low-precision integrators, round(x dn) / dn with an IEEE multiply and
+// divide in FP64 (std::round and a division: adjointfield.hh:28-31, su2.hh:29-33).
+__device__ __forceinline__ double round_dn(double x, double dn) {
+  return __ddiv_rn(round(__dmul_rn(x, dn)), dn);
+}
+// round_and_update_gauge (update_gauge.hh:20-26): U = exp(dt P) round(U)
+template <class T>
+__global__ void k_update_su2_round(size_t NL, LinkT<T> *__restrict__ U, const T *__restrict__ P,
+                                   T dt, double dn) {
+  for (size_t l = blockIdx.x * (size_t)blockDim.x + threadIdx.x; l < NL;
+       l += (size_t)gridDim.x * blockDim.x) {
+    const Su2<T> u = ld_link_rw(U + l);
+    const Su2<double> r{round_dn((double)u.ar, dn), round_dn((double)u.ai, dn),
+                        round_dn((double)u.br, dn), round_dn((double)u.bi, dn)};
+    const Su2<T> e = exp_alg(dt * P[l], dt * P[NL + l], dt * P[2 * NL + l]);
+    st_link(U + l, mul(e, from64<T>(r)));
+  }
+}
+// U(1): the angle as _u1::round writes it (u1.hh:31-33), round(a) * dn / dn
+__global__ void k_update_u1_round(size_t NL, double *__restrict__ U,
+                                  const double *__restrict__ P, double dt, double dn) {
+  for (size_t l = blockIdx.x * (size_t)blockDim.x + threadIdx.x; l < NL;
+       l += (size_t)gridDim.x * blockDim.x)
+    U[l] = dt * P[l] + __ddiv_rn(__dmul_rn(round(U[l]), dn), dn);
+}
+// round_and_update_momenta (update_momenta.hh:36-58): P -= dt * round(D), multiply and
+// subtract rounded separately as there
+template <class T>
+__global__ void k_adj_round_axpy(size_t n, T *__restrict__ P, const T *__restrict__ D,
+                                 double dt, double dn) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x)
+    P[i] = (T)__dsub_rn((double)P[i], __dmul_rn(dt, round_dn((double)D[i], dn)));
+}
+
 // restoreSU in FP64 (gaugeconfig.hh:115-120)
 template <class T> __global__ void k_restore(size_t NL, LinkT<T> *__restrict__ U) {
   for (size_t l = blockIdx.x * (size_t)blockDim.x + threadIdx.x; l < NL;
@@ -798,14 +833,30 @@ cudaError_t force_update(const Geom &g, const void *U, int group, T *P, const T 
 
 template <class T>
 cudaError_t link_update(const Geom &g, void *U, int group, const T *P, double dt,
-                        cudaStream_t s) {
+                        cudaStream_t s, double round_dn) {
   const size_t NL = (size_t)g.V * g.nd;
-  if (group == 0)
-    k_update_su2<T><<<flat_grid(NL, 256), 256, 0, s>>>(NL, (LinkT<T> *)U, P, (T)dt);
-  else {
+  if (group == 0) {
+    if (round_dn > 0.)
+      k_update_su2_round<T><<<flat_grid(NL, 256), 256, 0, s>>>(NL, (LinkT<T> *)U, P, (T)dt,
+                                                               round_dn);
+    else
+      k_update_su2<T><<<flat_grid(NL, 256), 256, 0, s>>>(NL, (LinkT<T> *)U, P, (T)dt);
+  } else {
     if (sizeof(T) != 8) return cudaErrorNotSupported;
-    k_update_u1<<<flat_grid(NL, 256), 256, 0, s>>>(NL, (double *)U, (const double *)P, dt);
+    if (round_dn > 0.)
+      k_update_u1_round<<<flat_grid(NL, 256), 256, 0, s>>>(NL, (double *)U, (const double *)P,
+                                                           dt, round_dn);
+    else
+      k_update_u1<<<flat_grid(NL, 256), 256, 0, s>>>(NL, (double *)U, (const double *)P, dt);
   }
+  return cudaGetLastError();
+}
+
+template <class T>
+cudaError_t adj_round_axpy(const Geom &g, T *P, const T *D, int group, double dt, double dn,
+                           cudaStream_t s) {
+  const size_t n = (size_t)g.V * g.nd * (group == 0 ? 3 : 1);
+  k_adj_round_axpy<T><<<flat_grid(n, 256), 256, 0, s>>>(n, P, D, dt, dn);
   return cudaGetLastError();
 }
 
@@ -901,7 +952,9 @@ cudaError_t cond_restore(const Geom &g, void *U, const void *U_old, int group,
                                        double, double, double, int, double *, int *, void *,  \
                                        double, cudaStream_t, int, bool);                      \
   template cudaError_t link_update<T>(const Geom &, void *, int, const T *, double,          \
-                                      cudaStream_t);                                          \
+                                      cudaStream_t, double);                                  \
+  template cudaError_t adj_round_axpy<T>(const Geom &, T *, const T *, int, double, double,  \
+                                         cudaStream_t);                                       \
   template cudaError_t restore_links<T>(const Geom &, void *, int, cudaStream_t);            \
   template cudaError_t momenta_philox<T>(const Geom &, T *, int, const TrajParams *,         \
                                          double *, int *, cudaStream_t);                      \

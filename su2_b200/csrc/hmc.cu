@@ -46,7 +46,9 @@ std::vector<Op> schedule(int integ, int n, double tau) {
     M(om2l * dtau);
     G(0.5 * dtau);
     M(lambda * dtau);
-  } else if (integ == SU2B_OMF4) {  // integrator.hh:119-156 (loop from i = 1 as there)
+  } else if (integ == SU2B_OMF4 || integ == SU2B_LP_OMF4) {
+    // integrator.hh:119-156 and the same schedule of lp_omf4, :158-199 (loop from i = 1 as
+    // there)
     const double rho = 0.2539785108410595, theta = -0.03230286765269967,
                  vartheta = 0.08398315262876693, lambda = 0.6822365335719091;
     const double eps[10] = {rho * dtau,
@@ -85,7 +87,7 @@ std::vector<Op> schedule(int integ, int n, double tau) {
       M(2. / 3. * dtau);
       G(7. / 24. * dtau);
     }
-  } else {  // leapfrog, also the reference's fallback (integrator.hh:274-277)
+  } else {  // leapfrog and lp_leapfrog (integrator.hh:26-80), the fallback (:274-277)
     M(dtau / 2.);
     G(dtau);
     for (int i = 0; i < n - 1; i++) {
@@ -97,9 +99,17 @@ std::vector<Op> schedule(int integ, int n, double tau) {
   return o;
 }
 
+int kinetic_now(su2b_ctx *ctx, int slot);
+
+bool low_precision(int integ) { return integ == SU2B_LP_LEAPFROG || integ == SU2B_LP_OMF4; }
+
 int integrate(su2b_ctx *ctx, const std::vector<Op> &ops, const su2b_hmc_params *prm,
               int kin_slot, long *cg_iters) {
   const bool ferm = prm->fermion_mass > 0.0;
+  // lp_leapfrog / lp_omf4: dn = N = pow(10, exponent) as a size_t (integrator.hh:59, 168);
+  // each momentum step rounds the summed derivative, each gauge step the links
+  const bool lp = low_precision(prm->integrator);
+  const double dn = lp ? (double)(size_t)std::pow(10.0, (double)prm->round_exponent) : 0.0;
   int last_m = -1;
   for (int i = 0; i < (int)ops.size(); i++)
     if (ops[i].kind == 0) last_m = i;
@@ -116,15 +126,29 @@ int integrate(su2b_ctx *ctx, const std::vector<Op> &ops, const su2b_hmc_params *
         extra = ctx->fderiv;
         mode |= FM_EXTRA;
       }
+      if (lp) {  // the derivative into Z (no momentum input), then P -= c round(Z)
+        SU2B_CKS(su2b_q_force(ctx, ctx->U, ctx->Z, extra, f, 1.0, mode & FM_EXTRA, nullptr,
+                              nullptr));
+        if (ctx->link64)
+          SU2B_LAUNCH(SU2B_K_OTHER, adj_round_axpy<double>(ctx->g, (double *)ctx->P,
+                                                           (const double *)ctx->Z, ctx->group,
+                                                           ops[i].c, dn, ctx->stream));
+        else
+          SU2B_LAUNCH(SU2B_K_OTHER, adj_round_axpy<float>(ctx->g, (float *)ctx->P,
+                                                          (const float *)ctx->Z, ctx->group,
+                                                          ops[i].c, dn, ctx->stream));
+        continue;
+      }
       int nb = 0;
       SU2B_CKS(su2b_q_force(ctx, ctx->U, ctx->P, extra, f, -ops[i].c, mode, ctx->part_slot(1),
                             &nb));
       if (mode & FM_KINETIC)
         SU2B_LAUNCH(SU2B_K_OTHER, reduce_final(ctx->part_slot(1), nb, 1, ctx->red + kin_slot, ctx->stream));
     } else {
-      SU2B_CKS(su2b_q_update(ctx, ctx->U, ctx->P, ops[i].c));
+      SU2B_CKS(su2b_q_update(ctx, ctx->U, ctx->P, ops[i].c, dn));
     }
   }
+  if (lp) SU2B_CKS(kinetic_now(ctx, kin_slot));
   return su2b_q_restore(ctx, ctx->U);  // integrator.hh:48
 }
 
@@ -332,9 +356,9 @@ extern "C" int su2b_hmc_trajectory(su2b_ctx *ctx, const su2b_hmc_params *prm,
   SU2B_CK(cudaSetDevice(ctx->device));
   SU2B_NEED(prm && res, "params or result is NULL");
   SU2B_NEED(prm->n_steps >= 1, "n_steps must be >= 1");
-  if (prm->integrator == 1 || prm->integrator == 3)
-    return su2b_fail(ctx, SU2B_ERR_UNSUPPORTED,
-                     "decimal-rounding integrators (lp_leapfrog, lp_omf4) are not provided");
+  const bool lp = low_precision(prm->integrator);
+  SU2B_NEED(!lp || (prm->round_exponent >= 0 && prm->round_exponent <= 19),
+            "round_exponent must be in 0..19 (10^e as a size_t)");
   const bool ferm = prm->fermion_mass > 0.0;
   if (ferm && ctx->group != SU2B_GROUP_U1)
     return su2b_fail(ctx, SU2B_ERR_UNSUPPORTED,
@@ -350,7 +374,7 @@ extern "C" int su2b_hmc_trajectory(su2b_ctx *ctx, const su2b_hmc_params *prm,
   *ctx->h_tparams = tp;
   SU2B_CK(cudaMemcpyAsync(ctx->tparams, ctx->h_tparams, sizeof(TrajParams),
                           cudaMemcpyHostToDevice, s));
-  if (ctx->group == SU2B_GROUP_SU2 && !ferm && !prm->revtest)
+  if (ctx->group == SU2B_GROUP_SU2 && !ferm && !prm->revtest && !lp)
     return traj_fused(ctx, prm, cached, res);
 
   // generic path: U(1), fermions, reversibility test

@@ -105,7 +105,7 @@ int su2b_fetch_red(su2b_ctx *ctx, int n);
 int su2b_q_force(su2b_ctx *ctx, const void *U, void *P, const void *extra, double f,
                  double scale, int mode, double *kin_part, int *nb, void *Uout = nullptr,
                  double dt_upd = 0.0);
-int su2b_q_update(su2b_ctx *ctx, void *U, const void *P, double dt);
+int su2b_q_update(su2b_ctx *ctx, void *U, const void *P, double dt, double round_dn = 0.0);
 int su2b_q_restore(su2b_ctx *ctx, void *U);
 int su2b_q_flow_step(su2b_ctx *ctx, void *U, double eps);
 // one flow step from src into dst (dst == src: in place); src != dst leaves src clobbered

@@ -47,9 +47,16 @@ cudaError_t force_update(const Geom &g, const void *U, int group, T *P, const T 
                          void *Uout, double dt_upd, cudaStream_t s, int variant = 1,
                          bool pdl = false);
 
+// U = exp(dt P) U (update_gauge.hh:8-16); with round_dn > 0 the links are rounded first,
+// U = exp(dt P) round(U) (round_and_update_gauge, update_gauge.hh:20-26)
 template <class T>
 cudaError_t link_update(const Geom &g, void *U, int group, const T *P, double dt,
-                        cudaStream_t s);
+                        cudaStream_t s, double round_dn = 0.0);
+// P -= dt * round(D) componentwise, round(x) = round(x dn) / dn in FP64
+// (round_and_update_momenta, update_momenta.hh:36-58); D, P of na components per link
+template <class T>
+cudaError_t adj_round_axpy(const Geom &g, T *P, const T *D, int group, double dt, double dn,
+                           cudaStream_t s);
 template <class T> cudaError_t restore_links(const Geom &g, void *U, int group, cudaStream_t s);
 // per-trajectory parameters read by the kernels from device memory, so that a captured
 // trajectory graph can be replayed with a new seed and trajectory index

@@ -20,8 +20,9 @@ from ._abi import check
 
 _D = C.POINTER(C.c_double)
 
-INTEGRATORS = {"leapfrog": _abi.LEAPFROG, "omf4": _abi.OMF4, "euler": _abi.EULER,
-               "ruth": _abi.RUTH, "omf2": _abi.OMF2}
+INTEGRATORS = {"leapfrog": _abi.LEAPFROG, "lp_leapfrog": _abi.LP_LEAPFROG, "omf4": _abi.OMF4,
+               "lp_omf4": _abi.LP_OMF4, "euler": _abi.EULER, "ruth": _abi.RUTH,
+               "omf2": _abi.OMF2}
 
 
 def _dp(a: np.ndarray):
@@ -278,9 +279,11 @@ class gaugeconfig:
     def md_update(self, integrator="leapfrog", n_steps=10, tau=1.0, seed=0, traj=0,
                   momenta=None, uniform=None, revtest=False, accept_reject=True,
                   fermion_mass=0.0, cg_tol=1e-10, cg_max_iter=100000, pf_source=None,
-                  pf_complex=False, cg_start="reference", pf_seed=97234719) -> TrajectoryResult:
+                  pf_complex=False, cg_start="reference", pf_seed=97234719,
+                  exponent=0) -> TrajectoryResult:
         """One HMC trajectory (md_update, md_update.hh:18-81).  momenta/uniform replay a host
-        random stream; otherwise the device Philox streams keyed by (seed, traj) are used."""
+        random stream; otherwise the device Philox streams keyed by (seed, traj) are used.
+        exponent: rounding exponent of lp_leapfrog / lp_omf4 (the reference's default 0)."""
         p = _abi.HmcParams()
         p.integrator = INTEGRATORS[integrator] if isinstance(integrator, str) else integrator
         p.n_steps = n_steps
@@ -305,6 +308,7 @@ class gaugeconfig:
         p.pf_complex = int(pf_complex)
         p.cg_start = _abi.CG_START_REFERENCE if cg_start == "reference" else _abi.CG_START_ZERO
         p.pf_seed = pf_seed
+        p.round_exponent = exponent
         r = _abi.TrajResult()
         self._c(self.lib.su2b_hmc_trajectory(self.ctx, C.byref(p), C.byref(r)))
         return TrajectoryResult(bool(r.accepted), r.dH, r.ddH, tuple(r.H_old), tuple(r.H_new),

@@ -165,6 +165,26 @@ def test_md_trajectory_injected_momenta(gpu, orc, group, dims, nd, integ):
         assert rel(c.download(), U_want) < 1e-10
 
 
+@pytest.mark.parametrize("group,dims,nd", GEOMS, ids=GEOM_IDS)
+@pytest.mark.parametrize("integ,exponent", [(1, 16), (1, 6), (3, 8)],
+                         ids=["lp_leapfrog-e16", "lp_leapfrog-e6", "lp_omf4-e8"])
+def test_md_trajectory_low_precision_integrators(gpu, orc, group, dims, nd, integ, exponent):
+    """lp_leapfrog / lp_omf4 (integrator.hh:53-80, 158-199): the derivative rounded to
+    10^-e before each momentum step and the links before each gauge step, against the
+    oracle (pinned bit for bit to the reference's integrators)."""
+    U = hot(orc, group, dims, nd)
+    P, _ = orc.initnormal(group, dims, nd, 4242)
+    dH, U_want, _, H = orc.md_injected(group, dims, nd, 2.3, integ, 6, 1.0, U, P,
+                                       exponent=exponent)
+    with make(gpu, group, dims, nd, beta=2.3) as c:
+        c.upload(U)
+        r = c.md_update(integ, 6, 1.0, momenta=P, accept_reject=False, exponent=exponent)
+        assert r.accepted
+        assert r.dH == pytest.approx(dH, abs=1e-9 * max(1.0, abs(H[1])))
+        assert r.H_new[1] == pytest.approx(H[3], rel=1e-12)
+        assert rel(c.download(), U_want) < 1e-10
+
+
 def test_reference_chain_replay(gpu, orc):
     """Replaying the reference's own random stream (std::mt19937(seed+i) momenta and accept
     uniform), the device chain takes the same accept decisions with the same Delta H as the
@@ -252,8 +272,8 @@ def test_error_paths(gpu):
         gpu.gaugeconfig(4, 4, 2, 4, 3, 2.0)  # inactive extent != 1
     with gpu.gaugeconfig(4, 4, 4, 4, 4, 2.0) as c:
         with pytest.raises(su2_b200.Su2bError) as e:
-            c.md_update(1, 4, 1.0)  # lp_leapfrog
-        assert e.value.code == 4
+            c.md_update("lp_leapfrog", 4, 1.0, exponent=20)  # 10^20 overflows a size_t
+        assert e.value.code == 1
         with pytest.raises(su2_b200.Su2bError) as e:
             c.md_update("leapfrog", 4, 1.0, fermion_mass=0.1)  # SU(2) fermions
         assert e.value.code == 4

@@ -133,6 +133,12 @@ def test_pin_gauge_path(orc, ref, group, dims, nd):
         b = ref.md_injected(group, dims, nd, 2.3, integ, 5, 1.0, U, P)
         assert np.array_equal(a[1], b[1]) and np.array_equal(a[2], b[2])
         assert a[0] == pytest.approx(b[0], abs=1e-9 * max(1, abs(b[3][1])))
+    # the low-precision integrators (lp_leapfrog 1, lp_omf4 3) with rounding exponents
+    for integ, e in ((1, 16), (1, 6), (3, 8), (3, 16)):
+        a = orc.md_injected(group, dims, nd, 2.3, integ, 5, 1.0, U, P, exponent=e)
+        b = ref.md_injected(group, dims, nd, 2.3, integ, 5, 1.0, U, P, exponent=e)
+        assert np.array_equal(a[1], b[1]) and np.array_equal(a[2], b[2]), (integ, e)
+        assert a[0] == pytest.approx(b[0], abs=1e-9 * max(1, abs(b[3][1])))
 
 
 @pytest.mark.parametrize("group,dims,nd", [GEOMS[0], GEOMS[3], GEOMS[4]],
