@@ -496,7 +496,7 @@ def profile_run(args):
         chains = ensemble_chains()[:8]
         batch = chain_batch(chains, precision="mixed")
         for i, ch in enumerate(chains):
-            batch.upload(i, haar_links(replicas.chain_cost(ch) * ch["ndims"], ch["seed"]))
+            batch.upload(i, haar_links(replicas.chain_sites(ch) * ch["ndims"], ch["seed"]))
     td = tempfile.mkdtemp()
 
     def step(k):
@@ -737,8 +737,8 @@ def config4(args):
     torch.cuda.set_device(local)
     chains = ensemble_chains()
     mine = [chains[i] for i in replicas.partition_chains(chains, ws, rank)]
-    sites = sum(replicas.chain_cost(c) for c in mine)
-    starts = [haar_links(replicas.chain_cost(c) * c["ndims"], c["seed"]) for c in mine]
+    sites = sum(replicas.chain_sites(c) for c in mine)
+    starts = [haar_links(replicas.chain_sites(c) * c["ndims"], c["seed"]) for c in mine]
     K, W = args.steps, args.warmup
     with chain_batch(mine, precision="mixed", device=local) as b:
         for i, U in enumerate(starts):
@@ -790,12 +790,12 @@ def config4(args):
             r = O.Oracle("ref")
             c = max(chains, key=replicas.chain_cost)
             Lx, Ly, Lz, Lt = c["dims"]
-            U = haar_links(replicas.chain_cost(c) * c["ndims"], 1)
+            U = haar_links(replicas.chain_sites(c) * c["ndims"], 1)
             with quiet_stdout():
                 t0 = time.perf_counter()
                 r.hmc_run(0, c["dims"], c["ndims"], c["beta"], 0, 10, 1.0, 1, 0, 1, U)
                 dt = time.perf_counter() - t0
-            cpu = {"value": replicas.chain_cost(c) / dt, "unit": "site-updates/s",
+            cpu = {"value": replicas.chain_sites(c) / dt, "unit": "site-updates/s",
                    "cores": r._omp_threads(), "kind": "reference",
                    "sample": f"1 leapfrog trajectory of the largest chain {c['dims']} "
                              f"d={c['ndims']}"}

@@ -137,7 +137,8 @@ typedef struct {
   int pf_complex;         /* 0: real R as the reference (staggered.hpp:188-191) */
   int cg_start;           /* SU2B_CG_START_*: start vector of every inner CG */
   long pf_seed;           /* seed of the reference's sigma=10 Gaussian CG start */
-  /* SU2B_LP_LEAPFROG / SU2B_LP_OMF4 only, 0..19: before each momentum step the summed
+  /* SU2B_LP_LEAPFROG / SU2B_LP_OMF4 only (FP64 links: a context with FP32 SU(2) links
+   * returns SU2B_ERR_UNSUPPORTED for them), 0..19: before each momentum step the summed
    * derivative, and before each gauge step every link, is rounded componentwise to
    * round(x * 10^e) / 10^e (update_momenta.hh:36-58, update_gauge.hh:20-26; a U(1) link
    * angle a becomes round(a) * 10^e / 10^e as u1.hh:31-33 writes it).  The reference's
@@ -331,9 +332,11 @@ SU2B_API int su2b_tune_set(su2b_ctx *ctx, int kernel, int variant);
  * context is created and nothing is allocated: the only scratch is a fixed array of
  * 16384 partial-sum pairs inside the library, so the lattice may have at most 4,194,304
  * sites (larger sizes return SU2B_ERR_INVALID).  All calls share that array: calls that
- * overlap on the GPU race and must be ordered by the caller.  The first call on a device
- * looks up the array's device address and should come before any stream capture.  Returns
- * without waiting for the kernels; errors are reported only through the status code. */
+ * overlap on the GPU race and must be ordered by the caller.  Each call outside a stream
+ * capture looks up the array's device address in the current context; a call during a
+ * capture reuses the address found by the last call outside one, so the first call on a
+ * device should come before any stream capture.  Returns without waiting for the kernels;
+ * errors are reported only through the status code. */
 SU2B_API int su2b_gauge_energy_noalloc(int group, int Lx, int Ly, int Lz, int Lt, int ndims,
                                        const double *U_dev, double *out_dev, void *stream);
 

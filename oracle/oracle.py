@@ -50,6 +50,8 @@ _SIGS = {
     "fermion_accept": (f64, _L + [_D, f64, _D, f64, i64]),
     "fermion_derivative": (None, _L + [_D, f64, _D, f64, i64, _D]),
     "md_injected_fermion": (f64, _L + [f64, f64, f64, i64, i32, i32, f64, _D, _D, _D, _D]),
+    "md_injected_fermion_lp": (f64, _L + [f64, f64, f64, i64, i32, i32, f64, _D, _D, _D, _D,
+                                          i32]),
     "eta": (f64, [i32] * 5),
     "initnormal": (f64, _G + [i64, _D]),
     "gaussian_spinor": (None, [i32] * 4 + [f64, f64, i64, _D]),
@@ -83,6 +85,18 @@ _REF_ONLY = {
 def build(which: str = "oracle") -> None:
     """Compile a checker with oracle/Makefile (``oracle`` or ``ref``)."""
     subprocess.run(["make", "-s", "-C", HERE, which], check=True)
+
+
+def reference_dir() -> str | None:
+    """The reference checkout oracle/Makefile reads ($SU2_REFERENCE overrides its default),
+    or None where it is absent (the GPU box, a fresh clone without the reference)."""
+    try:
+        r = subprocess.run(["make", "-s", "-C", HERE, "refdir"], capture_output=True,
+                           text=True, check=True)
+    except (OSError, subprocess.CalledProcessError):
+        return None
+    d = r.stdout.strip()
+    return d or None
 
 
 def available(kind: str) -> bool:
@@ -249,12 +263,20 @@ class Oracle:
         self._fermion_derivative(*dims, nd, dp(U), m, dp(phi), tol, seed, dp(out))
         return out
 
-    def md_injected_fermion(self, dims, nd, beta, m, tol, seed, integ, nsteps, tau, U, P, R):
+    def md_injected_fermion(self, dims, nd, beta, m, tol, seed, integ, nsteps, tau, U, P, R,
+                            exponent=None):
+        """exponent: as md_injected (the low-precision integrators, ids 1 and 3)."""
         U = U.copy()
         P = P.copy()
         H = np.zeros(6)
-        dH = self._md_injected_fermion(*dims, nd, beta, m, tol, seed, integ, nsteps, tau,
-                                       dp(U), dp(P), dp(R), dp(H))
+        if exponent is None and integ in (1, 3):
+            exponent = 16
+        if exponent is None:
+            dH = self._md_injected_fermion(*dims, nd, beta, m, tol, seed, integ, nsteps, tau,
+                                           dp(U), dp(P), dp(R), dp(H))
+        else:
+            dH = self._md_injected_fermion_lp(*dims, nd, beta, m, tol, seed, integ, nsteps, tau,
+                                              dp(U), dp(P), dp(R), dp(H), exponent)
         return dH, U, P, H
 
     def gaussian_spinor(self, dims, avr, sigma, seed):

@@ -452,10 +452,12 @@ void ref_fermion_derivative(int Lx, int Ly, int Lz, int Lt, int nd, const double
 
 // U(1) md_update with gauge + detDDdag monomials, injected momenta and injected R
 // (phi = D R, Hold = |R|^2 exactly as heatbath sets them, detDDdag_monomial.hh:64-83).
-double ref_md_injected_fermion(int Lx, int Ly, int Lz, int Lt, int nd, double beta,
-                               double m, double tol, long seed, int integ, int nsteps,
-                               double tau, double *U_io, double *P_io, const double *R,
-                               double *H) {
+// exponent: the rounding exponent of the low-precision integrators (ids 1, 3); the
+// round_and_update_momenta of those integrators rounds the summed gauge + fermion derivative.
+double ref_md_injected_fermion_lp(int Lx, int Ly, int Lz, int Lt, int nd, double beta,
+                                  double m, double tol, long seed, int integ, int nsteps,
+                                  double tau, double *U_io, double *P_io, const double *R,
+                                  double *H, int exponent) {
   gaugeconfig<_u1> U(Lx, Ly, Lz, Lt, nd, beta);
   io<_u1>::put(U, U_io);
   adjointfield<double, _u1> P(Lx, Ly, Lz, Lt, nd);
@@ -471,7 +473,7 @@ double ref_md_injected_fermion(int Lx, int Ly, int Lz, int Lt, int nd, double be
   const spinor Rs = make_spinor(U, R);
   f.phi = staggered::apply_D<double, Complex>(U, m, Rs);
   f.Hold = Rs.norm_squared();
-  integrator<double, _u1> *it = make_integrator<_u1>(integ);
+  integrator<double, _u1> *it = make_integrator<_u1>(integ, exponent);
   md_params p(nsteps, tau);
   it->integrate(ml, h, p);
   double dH = 0.;
@@ -489,6 +491,14 @@ double ref_md_injected_fermion(int Lx, int Ly, int Lz, int Lt, int nd, double be
   io<_u1>::get(U, U_io);
   io<_u1>::getP(P, P_io);
   return dH;
+}
+
+double ref_md_injected_fermion(int Lx, int Ly, int Lz, int Lt, int nd, double beta,
+                               double m, double tol, long seed, int integ, int nsteps,
+                               double tau, double *U_io, double *P_io, const double *R,
+                               double *H) {
+  return ref_md_injected_fermion_lp(Lx, Ly, Lz, Lt, nd, beta, m, tol, seed, integ, nsteps, tau,
+                                    U_io, P_io, R, H, 16);
 }
 
 // staggered::eta (staggered.hpp:41-48)

@@ -1292,17 +1292,19 @@ void orc_hmc_run(int group, int Lx, int Ly, int Lz, int Lt, int nd, double beta,
   free(U_old);
 }
 
-/* U(1) gauge + staggered pseudofermion trajectory with injected P and R */
-double orc_md_injected_fermion(int Lx, int Ly, int Lz, int Lt, int nd, double beta, double m,
-                               double tol, long seed, int integ, int nsteps, double tau,
-                               double *U, double *P, const double *R, double *H) {
+/* U(1) gauge + staggered pseudofermion trajectory with injected P and R; dn > 0 rounds as
+ * the low-precision integrators do (the summed gauge + fermion derivative and the links) */
+static double md_injected_fermion_r(int Lx, int Ly, int Lz, int Lt, int nd, double beta,
+                                    double m, double tol, long seed, int integ, int nsteps,
+                                    double tau, double *U, double *P, const double *R,
+                                    double *H, double dn) {
   const lat_t l = mklat(Lx, Ly, Lz, Lt, nd);
   double *phi = malloc(2 * l.V * sizeof(double));
   apply_D_or_Ddag(&l, U, m, 0, R, phi);
   H[0] = kinetic(1, P, nlinks(&l));
   H[1] = orc_S_G_hmc(1, Lx, Ly, Lz, Lt, nd, beta, U, 1.0, 0);
   H[2] = vdot(l.V, R, R).r;
-  md_sys s = {1, l, beta, 1.0, 1, m, tol, seed, phi, 0.};
+  md_sys s = {1, l, beta, 1.0, 1, m, tol, seed, phi, dn};
   md_integrate(&s, integ, nsteps, tau, U, P);
   H[3] = kinetic(1, P, nlinks(&l));
   H[4] = orc_S_G_hmc(1, Lx, Ly, Lz, Lt, nd, beta, U, 1.0, 0);
@@ -1313,6 +1315,22 @@ double orc_md_injected_fermion(int Lx, int Ly, int Lz, int Lt, int nd, double be
   dH += H[4] - H[1];
   dH += H[5] - H[2];
   return dH;
+}
+double orc_md_injected_fermion(int Lx, int Ly, int Lz, int Lt, int nd, double beta, double m,
+                               double tol, long seed, int integ, int nsteps, double tau,
+                               double *U, double *P, const double *R, double *H) {
+  return md_injected_fermion_r(Lx, Ly, Lz, Lt, nd, beta, m, tol, seed, integ, nsteps, tau, U, P,
+                               R, H, 0.);
+}
+/* the same with a low-precision integrator (1 or 3) and N = pow(10, exponent) as a size_t
+ * (integrator.hh:59,168) */
+double orc_md_injected_fermion_lp(int Lx, int Ly, int Lz, int Lt, int nd, double beta,
+                                  double m, double tol, long seed, int integ, int nsteps,
+                                  double tau, double *U, double *P, const double *R, double *H,
+                                  int exponent) {
+  const double dn = (double)(size_t)pow(10, exponent);
+  return md_injected_fermion_r(Lx, Ly, Lz, Lt, nd, beta, m, tol, seed, integ, nsteps, tau, U, P,
+                               R, H, dn);
 }
 
 /* ===================================================================================== */

@@ -95,6 +95,10 @@ void orc_fermion_force_from_chi(int Lx, int Ly, int Lz, int Lt, int nd, const do
 double orc_md_injected_fermion(int Lx, int Ly, int Lz, int Lt, int nd, double beta, double m,
                                double tol, long seed, int integ, int nsteps, double tau,
                                double *U, double *P, const double *R, double *H);
+double orc_md_injected_fermion_lp(int Lx, int Ly, int Lz, int Lt, int nd, double beta,
+                                  double m, double tol, long seed, int integ, int nsteps,
+                                  double tau, double *U, double *P, const double *R, double *H,
+                                  int exponent);
 /* number of solve() passes of the last Krylov solve (1 + restarts, CG.hpp:78-84) */
 long orc_last_solve_calls(void);
 /* dense complex n x n (row-major interleaved) solvers for the reference's 3x3 tests */

@@ -359,6 +359,11 @@ extern "C" int su2b_hmc_trajectory(su2b_ctx *ctx, const su2b_hmc_params *prm,
   const bool lp = low_precision(prm->integrator);
   SU2B_NEED(!lp || (prm->round_exponent >= 0 && prm->round_exponent <= 19),
             "round_exponent must be in 0..19 (10^e as a size_t)");
+  // the rounding to 10^-e is defined on FP64 links and momenta (integrator.hh:53-80,
+  // 158-199); on FP32 storage it would round nothing past e = 7
+  if (lp && !ctx->link64)
+    return su2b_fail(ctx, SU2B_ERR_UNSUPPORTED,
+                     "lp_leapfrog / lp_omf4 need FP64 links (SU2B_PREC_FP64)");
   const bool ferm = prm->fermion_mass > 0.0;
   if (ferm && ctx->group != SU2B_GROUP_U1)
     return su2b_fail(ctx, SU2B_ERR_UNSUPPORTED,

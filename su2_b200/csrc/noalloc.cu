@@ -15,9 +15,11 @@
 // without ordering) race on it and must be serialised by the caller.
 //
 // Host code cannot use the array's name as a device address (in host code it names a host
-// shadow object).  The device address is looked up once per device with
-// cudaGetSymbolAddress, with that device current, on the first call made on that device; that
-// first call should therefore happen before any stream capture begins.
+// shadow object).  The device address is looked up with cudaGetSymbolAddress, with the
+// device current, on every call made outside a stream capture, and remembered per device;
+// a call made while its stream is being captured uses the remembered address.  So the first
+// call on a device should happen before any stream capture begins, and a capture uses the
+// address of the context that was current at the last call outside a capture.
 #include <mutex>
 
 #include "su2b.h"
@@ -85,13 +87,20 @@ __global__ void __launch_bounds__(512) k_noalloc_final(const double *part, int n
   }
 }
 
-// device address of the scratch array on the current device (looked up once per device)
-int scratch_address(double **ptr) {
+// device address of the scratch array in the current context.  Outside a stream capture it
+// is looked up afresh (a host-side lookup that allocates nothing), so a context recreated
+// after cudaDeviceReset, or another context made current, gets its own address; during a
+// capture the address remembered for the device is used.
+int scratch_address(cudaStream_t s, double **ptr) {
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) return SU2B_ERR_CUDA;
   if (dev < 0 || dev >= NOALLOC_MAX_DEVICES) return SU2B_ERR_UNSUPPORTED;
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  const bool capturing =
+    cudaStreamIsCapturing(s, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone;
+  if (capturing) cudaGetLastError();  // a refused query leaves no sticky error behind
   std::lock_guard<std::mutex> lock(g_mutex);
-  if (!g_scratch[dev]) {
+  if (!capturing || !g_scratch[dev]) {
     void *p = nullptr;
     if (cudaGetSymbolAddress(&p, g_noalloc_partials) != cudaSuccess || !p)
       return SU2B_ERR_CUDA;
@@ -109,13 +118,17 @@ extern "C" int su2b_gauge_energy_noalloc(int group, int Lx, int Ly, int Lz, int 
   if (group != SU2B_GROUP_SU2 && group != SU2B_GROUP_U1) return SU2B_ERR_INVALID;
   if (ndims < 2 || ndims > 4) return SU2B_ERR_INVALID;
   const int L[4] = {Lt, Lx, Ly, Lz};
+  // the volume is formed one extent at a time and checked against the scratch array's
+  // limit at each step, so no product of extents can wrap before the check
+  constexpr long max_sites = (long)NOALLOC_MAX_BLOCKS * NOALLOC_NT;
+  long V = 1;
   for (int k = 0; k < 4; k++) {
-    if (L[k] < 1) return SU2B_ERR_INVALID;
+    if (L[k] < 1 || L[k] > max_sites) return SU2B_ERR_INVALID;
     if (k >= ndims && L[k] != 1) return SU2B_ERR_INVALID;
+    V *= L[k];
+    if (V > max_sites) return SU2B_ERR_INVALID;  // beyond the scratch array
   }
-  const long V = (long)Lx * Ly * Lz * Lt;
   const long nblocks = (V + NOALLOC_NT - 1) / NOALLOC_NT;
-  if (nblocks > NOALLOC_MAX_BLOCKS) return SU2B_ERR_INVALID;  // beyond the scratch array
   Geom g{};
   g.nd = ndims;
   for (int k = 0; k < 4; k++) g.L[k] = L[k];
@@ -124,10 +137,10 @@ extern "C" int su2b_gauge_energy_noalloc(int group, int Lx, int Ly, int Lz, int 
   g.V = (int)V;
   g.Vh = (int)(V / 2);
   for (int k = 0; k < 4; k++) g.dv[k] = su2b::make_fastdiv((uint32_t)L[k]);
-  double *part = nullptr;
-  const int rc = scratch_address(&part);
-  if (rc != SU2B_OK) return rc;
   cudaStream_t s = (cudaStream_t)stream;
+  double *part = nullptr;
+  const int rc = scratch_address(s, &part);
+  if (rc != SU2B_OK) return rc;
   const int grid = (int)nblocks;
   switch (group * 8 + ndims) {
     case 2: k_plaq_reference_layout<0, 2><<<grid, NOALLOC_NT, 0, s>>>(g, U_dev, part); break;

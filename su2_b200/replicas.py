@@ -12,10 +12,19 @@ from __future__ import annotations
 from typing import Any, Sequence
 
 
-def chain_cost(chain: dict) -> int:
-    """Work of one chain per trajectory, in sites (the kernels are site-parallel)."""
+def chain_sites(chain: dict) -> int:
+    """Lattice sites of one chain."""
     Lx, Ly, Lz, Lt = chain["dims"]
     return Lx * Ly * Lz * Lt
+
+
+def chain_cost(chain: dict) -> int:
+    """Work of one chain per trajectory, in staple evaluations: V d links with 2(d-1) staples
+    each (get_staples.hh:26-80).  The force dominates a trajectory and its cost per site grows
+    with d(d-1): a d = 4 site carries four links of six staples, a d = 3 site three links of
+    four, so counting sites alone would weigh a d = 3 chain twice as heavy as it is."""
+    d = int(chain["ndims"])
+    return chain_sites(chain) * d * 2 * (d - 1)
 
 
 def partition_chains(chains: Sequence[dict], world_size: int, rank: int) -> list[int]:

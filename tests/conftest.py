@@ -29,7 +29,7 @@ def orc():
 def ref():
     """The reference's own headers behind a C ABI; only where the reference was built."""
     if not _oracle.available("ref"):
-        if os.path.isdir("/root/reference/include"):
+        if _oracle.reference_dir():
             _oracle.build("ref")
         else:
             pytest.skip("reference harness not built here")

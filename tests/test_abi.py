@@ -54,10 +54,21 @@ def test_null_context_is_an_error():
 
 
 def test_product_does_not_link_the_oracle():
-    """The CUDA library is self-contained: no oracle or reference symbols inside."""
+    """The CUDA library is self-contained: its dynamic symbol table neither defines nor
+    imports an oracle (orc_*) or reference-harness (ref_*) symbol, and it names neither
+    checker library among the libraries it needs."""
+    import subprocess
+
     from su2_b200 import _abi
-    data = open(_abi.LIB_PATH, "rb").read()
-    assert b"orc_" not in data and b"ref_hotstart" not in data
+    syms = subprocess.run(["nm", "-D", _abi.LIB_PATH], capture_output=True, text=True,
+                          check=True).stdout.split("\n")
+    names = [ln.split()[-1] for ln in syms if ln.strip()]
+    assert any(n.startswith("su2b_") for n in names)
+    assert not [n for n in names if n.startswith(("orc_", "ref_"))]
+    dyn = subprocess.run(["readelf", "-d", _abi.LIB_PATH], capture_output=True, text=True,
+                         check=True).stdout
+    needed = [ln for ln in dyn.split("\n") if "(NEEDED)" in ln]
+    assert not [ln for ln in needed if "su2oracle" in ln or "su2ref" in ln]
 
 
 @pytest.mark.parametrize("fn", ["su2b_upload_gauge", "su2b_download_gauge"])
@@ -78,3 +89,21 @@ def test_launch_shape_tables_agree_with_the_header():
     assert _abi.BATCH_VARIANTS == nb == len(_abi.BATCH_SHAPES)
     src = open(os.path.join(ROOT, "su2_b200", "csrc", "su2b_internal.h")).read()
     assert int(re.search(r"constexpr int FORCE_VARIANTS = (\d+);", src).group(1)) == nf
+
+
+def test_noalloc_rejects_bad_sizes_before_touching_a_device():
+    """su2b_gauge_energy_noalloc validates its geometry on the host: lattices beyond its
+    fixed scratch array, extents whose product would wrap, bad ids and NULL buffers are
+    refused before any CUDA call (the pointer below is never dereferenced)."""
+    from su2_b200 import _abi
+    lib = _abi.load()
+    p = ctypes.c_void_p(16)
+    f = lib.su2b_gauge_energy_noalloc
+    assert f(0, 48, 48, 48, 48, 4, p, p, None) == _abi.ERR_INVALID         # 5.3 M sites
+    assert f(0, 65536, 65536, 65536, 65536, 4, p, p, None) == _abi.ERR_INVALID  # 2^64
+    assert f(1, 2 ** 30, 1, 1, 4, 2, p, p, None) == _abi.ERR_INVALID
+    assert f(0, 8, 8, 8, 8, 4, None, p, None) == _abi.ERR_INVALID
+    assert f(0, 8, 8, 8, 8, 4, p, None, None) == _abi.ERR_INVALID
+    assert f(2, 8, 8, 8, 8, 4, p, p, None) == _abi.ERR_INVALID
+    assert f(0, 8, 8, 8, 8, 5, p, p, None) == _abi.ERR_INVALID
+    assert f(0, 8, 8, 2, 8, 3, p, p, None) == _abi.ERR_INVALID             # inactive Lz != 1

@@ -280,6 +280,11 @@ def test_error_paths(gpu):
         with pytest.raises(su2_b200.Su2bError) as e:
             c.apply_D(0.1, np.zeros(2 * 256))
         assert e.value.code == 4
+    # the decimal rounding of lp_leapfrog / lp_omf4 is defined on FP64 storage only
+    with gpu.gaugeconfig(4, 4, 4, 4, 4, 2.0, precision="mixed") as c:
+        with pytest.raises(su2_b200.Su2bError) as e:
+            c.md_update("lp_leapfrog", 4, 1.0, exponent=6)
+        assert e.value.code == 4
 
 
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])

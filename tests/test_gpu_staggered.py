@@ -121,6 +121,29 @@ def test_fermion_hmc_trajectory(gpu, orc, dims, nd):
     assert r.cg_iterations > 0
 
 
+@pytest.mark.parametrize("exponent", [6, 12])
+def test_fermion_trajectory_low_precision_leapfrog(gpu, orc, exponent):
+    """lp_leapfrog with the det(D D^+) monomial: each momentum step rounds the summed gauge +
+    fermion derivative (round_and_update_momenta, update_momenta.hh:36-58) and each gauge step
+    the link angles (update_gauge.hh:20-26), against the oracle (pinned to the reference's
+    own integrator with fermions).  The fermion derivative shares the scratch field of the
+    gauge derivative, which this covers."""
+    dims, nd = U1_GEOMS[0]
+    U, _, V = setup(orc, dims, nd)
+    P, _ = orc.initnormal(1, dims, nd, 3)
+    R = orc.gaussian_spinor(dims, 0.0, 2 ** -0.5, 11)
+    dH, U_want, _, H = orc.md_injected_fermion(dims, nd, 4.0, 0.1, 1e-12, 97234719, 1, 4, 0.5,
+                                               U, P, R, exponent=exponent)
+    with u1(gpu, dims, nd) as c:
+        c.upload(U)
+        r = c.md_update("lp_leapfrog", 4, 0.5, momenta=P, pf_source=R, fermion_mass=0.1,
+                        cg_tol=1e-12, accept_reject=False, pf_seed=97234719, exponent=exponent)
+        assert rel(c.download(), U_want) < 1e-9
+    assert r.H_old[2] == pytest.approx(H[2], rel=1e-12)
+    assert r.H_new[2] == pytest.approx(H[5], rel=1e-9)
+    assert r.dH == pytest.approx(dH, abs=1e-7)
+
+
 def test_pf_source_stream(orc):
     R = orc.philox_pf_source((16, 1, 1, 16), 5, 0)
     assert np.all(R[1::2] == 0.0)

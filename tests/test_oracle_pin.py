@@ -192,6 +192,14 @@ def test_pin_staggered(orc, ref):
     b = ref.md_injected_fermion(dims, nd, 4.0, 0.05, 1e-10, 97, 6, 3, 1.0, U, P, R)
     assert np.array_equal(a[1], b[1])
     assert a[0] == pytest.approx(b[0], abs=1e-9)
+    # lp_leapfrog with fermions: the rounding applies to the summed gauge + fermion derivative
+    for exponent in (6, 12):
+        a = orc.md_injected_fermion(dims, nd, 4.0, 0.05, 1e-10, 97, 1, 3, 1.0, U, P, R,
+                                    exponent=exponent)
+        b = ref.md_injected_fermion(dims, nd, 4.0, 0.05, 1e-10, 97, 1, 3, 1.0, U, P, R,
+                                    exponent=exponent)
+        assert np.array_equal(a[1], b[1])
+        assert a[0] == pytest.approx(b[0], abs=1e-9)
 
 
 def test_metropolis_statistics_match_reference(orc, ref):

@@ -50,3 +50,7 @@ def test_noalloc_rejects_lattices_beyond_its_scratch(gpu):
     # 48^4 = 5,308,416 sites > 4,194,304
     assert lib.su2b_gauge_energy_noalloc(0, 48, 48, 48, 48, 4, p, p, None) == _abi.ERR_INVALID
     assert lib.su2b_gauge_energy_noalloc(0, 8, 8, 8, 8, 4, None, p, None) == _abi.ERR_INVALID
+    # extents whose product wraps a 64-bit integer (65536^4 = 2^64) or an int stride
+    assert lib.su2b_gauge_energy_noalloc(0, 65536, 65536, 65536, 65536, 4, p, p,
+                                         None) == _abi.ERR_INVALID
+    assert lib.su2b_gauge_energy_noalloc(1, 2 ** 30, 1, 1, 4, 2, p, p, None) == _abi.ERR_INVALID
