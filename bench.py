@@ -193,6 +193,86 @@ def stats(res, V):
             "plaquette": float(np.mean([r.plaquette for r in res])) / (V * 6 * 2)}
 
 
+def blocked(x, nblocks=20):
+    """Mean and its standard error from nblocks consecutive blocks of a chain's series."""
+    x = np.asarray(x, dtype=np.float64)
+    n = len(x) // nblocks * nblocks
+    b = x[:n].reshape(nblocks, -1).mean(axis=1)
+    return float(x.mean()), float(b.std(ddof=1) / np.sqrt(nblocks))
+
+
+def chain_statistics(c, U_start, n, seed, V):
+    """n untimed trajectories of one precision from U_start (a Markov chain with Philox
+    momenta and accept uniforms keyed by seed): Delta H, acceptance, exp(-Delta H) and the
+    plaquette after each trajectory, each with its 20-block standard error."""
+    c.upload(U_start)
+    res = [c.md_update("omf2", NSTEPS, TAU, seed=seed, traj=k) for k in range(n)]
+    dH = np.array([r.dH for r in res])
+    out = {"dH": blocked(dH), "acc": blocked([float(r.accepted) for r in res]),
+           "exp_mdH": blocked(np.exp(-dH)),
+           "plaq": blocked([r.plaquette / (V * 6 * 2) for r in res])}
+    return out, dH
+
+
+def equal_dH_plaq(mixed, fp64, U_start, n, pairs, seed, V):
+    """The metric's comparison of the two precisions at equal Delta H and plaquette.
+
+    Chains: each precision runs n trajectories from the same thermalised field with its own
+    seed (independent samples); the observables are compared by their difference in combined
+    standard errors (z) and the Delta H samples by a two-sample Kolmogorov-Smirnov test;
+    <exp(-Delta H)> = 1 (Creutz) is checked in each arm.
+    Pairs: from the same field with the same seed and trajectory index both precisions draw
+    the same momenta (FP32 storage evaluates the FP64 stream's uniforms in FP32) and the same
+    accept uniform, so their Delta H differ only by the FP32 arithmetic of the trajectory."""
+    from scipy import stats as st
+    sm, dm = chain_statistics(mixed, U_start, n, seed + 11, V)
+    sd, dd = chain_statistics(fp64, U_start, n, seed + 12, V)
+    z = {k: (sm[k][0] - sd[k][0]) / float(np.hypot(sm[k][1], sd[k][1])) for k in sm}
+    creutz = {a: (s_["exp_mdH"][0] - 1.0) / s_["exp_mdH"][1] for a, s_ in (("mixed", sm),
+                                                                           ("fp64", sd))}
+    diff, same = [], 0
+    for k in range(pairs):
+        r = []
+        for c in (mixed, fp64):
+            c.upload(U_start)
+            r.append(c.md_update("omf2", NSTEPS, TAU, seed=seed + 13, traj=k))
+        diff.append(r[0].dH - r[1].dH)
+        same += r[0].accepted == r[1].accepted
+    diff = np.array(diff)
+    rnd = lambda v: [float(f"{v[0]:.6g}"), float(f"{v[1]:.2g}")]  # noqa: E731
+    return {"trajectories_per_arm": n, "errors": "20-block standard errors",
+            "mixed": {k: rnd(v) for k, v in sm.items()},
+            "fp64": {k: rnd(v) for k, v in sd.items()},
+            "z_mixed_minus_fp64": {k: round(v, 2) for k, v in z.items()},
+            "creutz_z": {k: round(v, 2) for k, v in creutz.items()},
+            "ks_p_dH": float(f"{st.ks_2samp(dm, dd).pvalue:.3g}"),
+            "paired": {"pairs": pairs, "same_momenta": True,
+                       "dH_diff_mean": float(f"{diff.mean():.3g}"),
+                       "dH_diff_rms": float(f"{np.sqrt(np.mean(diff ** 2)):.3g}"),
+                       "dH_diff_max": float(f"{np.abs(diff).max():.3g}"),
+                       "same_decision": same / pairs}}
+
+
+def force_in_graph(c, t_traj, n_traj, bytes_per_link, NL, seed):
+    """Device time of one force launch inside the captured trajectory: the trajectory's
+    device time (graph replay, CUDA events) minus the device time of its other kernels (each
+    timed with CUDA events in a direct-launch run of the same trajectory), shared over its
+    force launches.  Launch gaps stay in the figure, so it is an upper bound on the kernel."""
+    c.profile(True)
+    for k in range(n_traj):
+        c.md_update("omf2", NSTEPS, TAU, seed=seed, traj=300000 + k)
+    prof = c.profile_read()
+    c.profile(False)
+    n_force = prof["force"][0] / n_traj
+    other_ms = sum(ms for name, (n, ms) in prof.items() if name != "force") / n_traj
+    t_force = (t_traj * 1e3 - other_ms) / n_force / 1e3
+    per = {name: {"launches": n // n_traj, "us": round(ms * 1e3 / n, 2)}
+           for name, (n, ms) in prof.items() if n}
+    return {"avg_launch_us": t_force * 1e6, "GB/s": bytes_per_link * NL / t_force / 1e9,
+            "force_launches_per_traj": n_force, "other_kernels_ms_per_traj": other_ms,
+            "direct_launch_us": prof["force"][1] * 1e3 / prof["force"][0]}, per
+
+
 def ours(args):
     import torch
 
@@ -214,12 +294,16 @@ def ours(args):
     for k in range(THERM_TRAJ + max(W, 3)):
         mixed.md_update("omf2", NSTEPS, TAU, seed=seed, traj=100000 + k)
     U_th = mixed.download()
-    # one FP64 start for both arms: FP32 links widened to double are unitary to about 1e-7
+    # one FP64 start for all arms: FP32 links widened to double are unitary to about 1e-7
     # only, so the thermalised field is reunitarised in FP64 first
     Uq = U_th.reshape(-1, 4)
     Uq /= np.sqrt(np.einsum("ij,ij->i", Uq, Uq))[:, None]
     mixed.upload(U_th)
     tune_m = mixed.autotune()  # launch shape of the force kernel, timed on this field
+    mixed.upload(U_th)
+    for k in range(W):
+        mixed.md_update("omf2", NSTEPS, TAU, seed=seed + 5, traj=k)
+    mixed.upload(U_th)
 
     # ---- headline: mixed precision, K trajectories ----
     clocks = Clocks(local)
@@ -232,45 +316,40 @@ def ours(args):
     t_mixed = allmax(dist, t_mixed)
     value = ws * K / t_mixed
 
-    # ---- FP64 path, same start and seeds ----
+    # ---- FP64, fused and graph-captured, same start and seeds ----
     fp64 = su2_b200.gaugeconfig(L, L, L, L, 4, BETA, precision="fp64", device=local)
     fp64.upload(U_th)
     tune_d = fp64.autotune()
     fp64.upload(U_th)
-    for k in range(min(W, 2)):
+    for k in range(W):
         fp64.md_update("omf2", NSTEPS, TAU, seed=seed + 7, traj=200000 + k)
     fp64.upload(U_th)
     barrier(dist)
     t_fp64, res_d = run_chain(fp64, K, seed, 0, None)
     t_fp64 = allmax(dist, t_fp64)
 
-    # ---- roofline of the dominant kernel (fused staple/force/momentum), live timers ----
-    roof = {}
-    kernels = {}
+    # ---- the plain form: FP64, integrator steps launched one by one (no graph, no link
+    #      update fused into the force launch, a copy of the start field), the default force
+    #      launch shape (no autotuning) ----
+    plain = su2_b200.gaugeconfig(L, L, L, L, 4, BETA, precision="fp64", device=local)
+    plain.plain_trajectory = True
+    plain.upload(U_th)
+    for k in range(W):
+        plain.md_update("omf2", NSTEPS, TAU, seed=seed + 9, traj=200000 + k)
+    plain.upload(U_th)
+    barrier(dist)
+    t_plain, res_p = run_chain(plain, K, seed, 0, None)
+    t_plain = allmax(dist, t_plain)
+    plain_shape = su2_b200._abi.FORCE_SHAPES[plain.force_variant]
+    plain.close()
+
+    # ---- roofline of the dominant kernel (fused staples/force/momentum/link update) ----
     hbm, peak_src = peaks()
-    # every force launch of the fused trajectory reads U and P, writes P and writes the next
-    # link buffer (exp(dt P) U, or restoreSU(U) after the last step): 56 B/link in FP32
-    # storage, 112 B/link in FP64
-    for name, c, bpl in (("mixed", mixed, 56), ("fp64", fp64, 112)):
+    nprof = max(2, K // 2)
+    roof, kernels = {}, {}
+    for name, c, bpl, t in (("mixed", mixed, 56, t_mixed / K), ("fp64", fp64, 112, t_fp64 / K)):
         c.upload(U_th)
-        c.profile(True)
-        for k in range(max(2, K // 2)):
-            c.md_update("omf2", NSTEPS, TAU, seed=seed, traj=300000 + k)
-        prof = c.profile_read()
-        c.profile(False)
-        n, ms = prof["force"]
-        avg = ms / 1e3 / n
-        roof[name] = {"avg_us": avg * 1e6, "GB/s": bpl * NL / avg / 1e9}
-        per = {}
-        nb = {"force": bpl, "plaquette": 32 if name == "fp64" else 16,
-              "momenta": 24 if name == "fp64" else 12}
-        for kname, (kn, kms) in prof.items():
-            if kn:
-                d = {"launches": kn, "avg_us": kms * 1e3 / kn}
-                if kname in nb:
-                    d["GB/s"] = nb[kname] * NL / (kms / 1e3 / kn) / 1e9
-                per[kname] = d
-        kernels[name] = per
+        roof[name], kernels[name] = force_in_graph(c, t, nprof, bpl, NL, seed)
     # measured DRAM bytes of the launch shape the tuner chose, from an ncu capture
     traffic = None
     tp = os.path.join(ROOT, "profiles", "force_kernel_traffic.json")
@@ -278,6 +357,9 @@ def ours(args):
         shape = su2_b200._abi.FORCE_SHAPES[mixed.force_variant]
         key = shape[0] if isinstance(shape[0], str) else str(shape)
         traffic = json.load(open(tp)).get("mixed_bytes_per_launch", {}).get(key)
+
+    # ---- mixed against FP64 at equal Delta H and plaquette (untimed statistics) ----
+    eq = equal_dH_plaq(mixed, fp64, U_th, args.stat_traj, args.pairs, seed, V)
 
     # ---- e2e through the C ABI with host buffers (pinned), per trajectory:
     #      upload the host gaugeconfig, one trajectory, download the gaugeconfig ----
@@ -288,11 +370,11 @@ def ours(args):
     t0 = time.perf_counter()
     for k in range(K):
         mixed.upload(Uh)
-        r = mixed.md_update("omf2", NSTEPS, TAU, seed=seed, traj=400000 + k)
+        mixed.md_update("omf2", NSTEPS, TAU, seed=seed, traj=400000 + k)
         mixed.download(out=Uh)
     t_e2e = allmax(dist, time.perf_counter() - t0)
 
-    # ---- side measurements of config 2 (Metropolis sweep, flow step) ----
+    # ---- side measurements of the workload (Metropolis sweep, flow step) ----
     mixed.upload(U_th)
     s = torch.cuda.ExternalStream(mixed.stream())
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
@@ -356,6 +438,19 @@ def ours(args):
         cpu = cpu_baseline(U_th)
 
     if rank == 0:
+        shapes = su2_b200._abi.FORCE_SHAPES
+        # details first (one JSON line of their own); the headline line comes last
+        print(json.dumps({
+            "detail": "bench.py headline run: per-kernel timers, tuner and side measurements",
+            "kernels_us": kernels, "roofline_fp64_kernel": roof["fp64"],
+            "roofline_mixed_kernel": roof["mixed"],
+            "autotune_force_us": {"mixed": {str(shapes[k]): v for k, v in tune_m.items()},
+                                  "fp64": {str(shapes[k]): v for k, v in tune_d.items()}},
+            "timed_chain_stats": {"mixed": stats(res_m, V), "fp64": stats(res_d, V),
+                                  "plain_fp64": stats(res_p, V)},
+            "metropolis_sweeps_per_s": metro, "flow_rk3_steps_per_s_fp64": flow,
+            "between_trajectories_fp64": obs}), flush=True)
+        r3 = lambda v: float(f"{v:.4g}")  # noqa: E731
         line = {
             "metric": METRIC, "value": value, "unit": "traj/s", "n_gpus": ws, "steps": K,
             "warmup": W, "ms_per_step": 1e3 * t_mixed / K, "higher_is_better": True,
@@ -363,40 +458,28 @@ def ours(args):
             "dtype": "fp32 links/forces + fp64 reductions/accept",
             "data": "synthetic: seeded Haar-random start, Metropolis-thermalised on device",
             "config": {"workload": WORKLOAD + " (mixed precision)", "lattice": [L] * 4,
-                       "beta": BETA, "integrator": "omf2", "n_steps": NSTEPS, "tau": TAU,
                        "replicas": ws, "parallelism": f"replicas x{ws}",
-                       "l2": "working set per step (three link buffers, P) > 126 MB L2; no flush"},
-            "mixed": dict(traj_per_s=value, **stats(res_m, V)),
-            "fp64": dict(traj_per_s=ws * K / t_fp64, **stats(res_d, V)),
-            "speedup_mixed_vs_fp64": t_fp64 / t_mixed,
-            "roofline": {"bound": "hbm",
-                         "kernel": "fused staples, force, momentum step and following link "
-                                   "update (FP32 storage), launch shape "
-                                   f"{su2_b200._abi.FORCE_SHAPES[mixed.force_variant]}",
-                         "achieved": roof["mixed"]["GB/s"], "peak": hbm, "unit": "GB/s",
-                         "frac": roof["mixed"]["GB/s"] / hbm, "traffic": traffic,
-                         "bytes_per_launch": 56 * NL, "avg_launch_us": roof["mixed"]["avg_us"],
+                       "l2": "working set (three link buffers, P) > 126 MB L2; no flush"},
+            "fp64": {"traj_per_s": r3(ws * K / t_fp64), "form": "fused, graph, tuned"},
+            "plain_fp64": {"traj_per_s": r3(ws * K / t_plain), "form": "steps launched one by "
+                           f"one, no graph, default shape {plain_shape}"},
+            "speedup_mixed_vs_fp64": r3(t_fp64 / t_mixed),
+            "speedup_mixed_vs_plain_fp64": r3(t_plain / t_mixed),
+            "fp64_gpu_over_reference_cpu": r3(ws * K / t_fp64 / cpu["value"]) if cpu else None,
+            "equal_dH_plaq": eq,
+            "roofline": {"bound": "hbm", "kernel": "fused staple/force/momentum/link update "
+                                                   f"FP32 {shapes[mixed.force_variant]}",
+                         "achieved": r3(roof["mixed"]["GB/s"]), "peak": hbm, "unit": "GB/s",
+                         "frac": r3(roof["mixed"]["GB/s"] / hbm), "traffic": traffic,
+                         "bytes_per_launch": 56 * NL,
+                         "avg_launch_us": r3(roof["mixed"]["avg_launch_us"]),
+                         "timing": "in-graph: trajectory device time minus its other kernels, "
+                                   "per force launch",
                          "peak_source": peak_src,
-                         "timing": f"CUDA events around every force launch over {max(2, K // 2)} "
-                                   "trajectories right after the timed region (same field, "
-                                   "direct launches instead of the graph)",
-                         "fp64_kernel": {"achieved": roof["fp64"]["GB/s"],
-                                         "frac": roof["fp64"]["GB/s"] / hbm,
-                                         "bytes_per_launch": 112 * NL,
-                                         "avg_launch_us": roof["fp64"]["avg_us"]}},
-            "kernels": kernels,
-            "autotune_force_us": {"mixed": {str(su2_b200._abi.FORCE_SHAPES[k]): v
-                                            for k, v in tune_m.items()},
-                                  "fp64": {str(su2_b200._abi.FORCE_SHAPES[k]): v
-                                           for k, v in tune_d.items()},
-                                  "chosen": {"mixed": su2_b200._abi.FORCE_SHAPES[mixed.force_variant],
-                                             "fp64": su2_b200._abi.FORCE_SHAPES[fp64.force_variant]}},
-            "metropolis_sweeps_per_s": metro, "flow_rk3_steps_per_s_fp64": flow,
-            "between_trajectories_fp64": obs,
+                         "fp64_frac": r3(roof["fp64"]["GB/s"] / hbm)},
             "e2e": {"value": ws * K / t_e2e, "unit": "traj/s",
                     "h2d_bytes_per_step": int(NL * 4 * 8), "d2h_bytes_per_step": int(NL * 4 * 8),
-                    "note": "upload of the host gaugeconfig (reference layout, FP64, pinned) "
-                            "+ trajectory + download, wall clock"},
+                    "note": "host FP64 gaugeconfig up, trajectory, down; wall clock"},
             "gpu_launches": int(launches),
             "clocks": clk,
             "cpu_baseline": cpu,
@@ -914,6 +997,11 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--therm-sweeps", type=int, default=300)
+    ap.add_argument("--stat-traj", type=int, default=1000,
+                    help="untimed trajectories per precision for the Delta H / plaquette "
+                         "comparison")
+    ap.add_argument("--pairs", type=int, default=32,
+                    help="paired trajectories (same start, same momenta) per precision")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile-run", action="store_true",
                     help="only the timed loop of one precision, for ncu (no bench line)")

@@ -317,7 +317,17 @@ SU2B_API int su2b_flow_adjoint(su2b_ctx *ctx, double eps, int n_steps, int check
  * new measurements to it.  times_us (optional, SU2B_FORCE_VARIANTS entries) receives the
  * average launch time of each shape (-1 when not measured). */
 #define SU2B_FORCE_VARIANTS 10
-enum { SU2B_TUNE_FORCE = 0 };
+/* SU2B_TUNE_TRAJECTORY selects how su2b_hmc_trajectory runs an SU(2) trajectory without
+ * fermions, reversibility test or rounding:
+ *   SU2B_TRAJ_FUSED_GRAPH (default): each momentum step fused with the gauge step after it,
+ *     three link buffers (no copy of the start field), the whole trajectory one CUDA graph;
+ *   SU2B_TRAJ_PLAIN: the plain form, as md_update is written -- the start field copied, the
+ *     integrator's momentum steps (staples, force and momentum update in one kernel) and
+ *     gauge steps launched one by one, restoreSU, the plaquette sums, the accept launch.  It
+ *     keeps the context's force launch shape (an untuned context has the default one).
+ * Both give the same trajectory up to rounding. */
+enum { SU2B_TUNE_FORCE = 0, SU2B_TUNE_TRAJECTORY = 1 };
+enum { SU2B_TRAJ_FUSED_GRAPH = 0, SU2B_TRAJ_PLAIN = 1 };
 SU2B_API int su2b_autotune(su2b_ctx *ctx, const char *cache_path, int retune, double *times_us);
 SU2B_API int su2b_tune_get(su2b_ctx *ctx, int kernel, int *variant);
 SU2B_API int su2b_tune_set(su2b_ctx *ctx, int kernel, int variant);

@@ -130,14 +130,26 @@ extern "C" int su2b_autotune(su2b_ctx *ctx, const char *cache_path, int retune,
 }
 
 extern "C" int su2b_tune_get(su2b_ctx *ctx, int kernel, int *variant) {
-  if (!ctx || !variant || kernel != SU2B_TUNE_FORCE) return SU2B_ERR_INVALID;
-  *variant = ctx->tune_force;
+  if (!ctx || !variant) return SU2B_ERR_INVALID;
+  if (kernel == SU2B_TUNE_FORCE)
+    *variant = ctx->tune_force;
+  else if (kernel == SU2B_TUNE_TRAJECTORY)
+    *variant = ctx->traj_path;
+  else
+    return SU2B_ERR_INVALID;
   return SU2B_OK;
 }
 
 extern "C" int su2b_tune_set(su2b_ctx *ctx, int kernel, int variant) {
-  if (!ctx || kernel != SU2B_TUNE_FORCE || variant < 0 || variant >= FORCE_VARIANTS)
-    return SU2B_ERR_INVALID;
-  ctx->tune_force = variant;
-  return SU2B_OK;
+  if (!ctx) return SU2B_ERR_INVALID;
+  if (kernel == SU2B_TUNE_FORCE && variant >= 0 && variant < FORCE_VARIANTS) {
+    ctx->tune_force = variant;
+    return SU2B_OK;
+  }
+  if (kernel == SU2B_TUNE_TRAJECTORY &&
+      (variant == SU2B_TRAJ_FUSED_GRAPH || variant == SU2B_TRAJ_PLAIN)) {
+    ctx->traj_path = variant;
+    return SU2B_OK;
+  }
+  return SU2B_ERR_INVALID;
 }

@@ -379,10 +379,12 @@ extern "C" int su2b_hmc_trajectory(su2b_ctx *ctx, const su2b_hmc_params *prm,
   *ctx->h_tparams = tp;
   SU2B_CK(cudaMemcpyAsync(ctx->tparams, ctx->h_tparams, sizeof(TrajParams),
                           cudaMemcpyHostToDevice, s));
-  if (ctx->group == SU2B_GROUP_SU2 && !ferm && !prm->revtest && !lp)
+  if (ctx->group == SU2B_GROUP_SU2 && !ferm && !prm->revtest && !lp &&
+      ctx->traj_path == SU2B_TRAJ_FUSED_GRAPH)
     return traj_fused(ctx, prm, cached, res);
 
-  // generic path: U(1), fermions, reversibility test
+  // generic path: U(1), fermions, reversibility test, the low-precision integrators and the
+  // plain form (SU2B_TRAJ_PLAIN)
   const std::vector<Op> ops = schedule(prm->integrator, prm->n_steps, prm->tau);
   long cg_iters = 0;
   int nb = 0;

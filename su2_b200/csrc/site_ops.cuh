@@ -361,10 +361,16 @@ __device__ __forceinline__ void plaq_site(const Geom &g, const LinkT<T> *__restr
 __device__ __forceinline__ void gauss_pair64(const uint32_t r[4], double &a, double &b) {
   box_muller(u01_53(r[0], r[1]), u01_53(r[2], r[3]), a, b);
 }
-// FP32 Box-Muller pair from two words: 24-bit uniforms and FP32 transcendentals
-__device__ __forceinline__ void gauss_pair32(uint32_t w1, uint32_t w2, float &a, float &b) {
-  const float u1 = ((float)(w1 >> 8) + 1.0f) * 0x1p-24f;  // (0, 1]
-  const float u2 = (float)(w2 >> 8) * 0x1p-24f;           // [0, 1)
+// The same pair in FP32 arithmetic: the same two 53-bit uniforms (exact integers scaled by
+// 2^-53, rounded once to float) through FP32 log, sqrt and sincospi.  The radius keeps the
+// FP64 pair's range: u1 >= 2^-53 is a normal float, so |z| reaches sqrt(106 ln 2) = 8.57
+// sigma in both precisions (a 24-bit uniform would cut the tail at 5.77 sigma).  The normals
+// agree with the FP64 pair to FP32 rounding, so both precisions draw the same momenta.
+__device__ __forceinline__ void gauss_pair32(const uint32_t r[4], float &a, float &b) {
+  const uint64_t k1 = ((uint64_t)r[0] << 21) ^ (uint64_t)(r[1] >> 11);
+  const uint64_t k2 = ((uint64_t)r[2] << 21) ^ (uint64_t)(r[3] >> 11);
+  const float u1 = (float)(k1 + 1) * 0x1p-53f;  // (0, 1]
+  const float u2 = (float)(k2 + 1) * 0x1p-53f;
   const float rad = sqrtf(-2.0f * logf(u1));
   float sn, cs;
   sincospif(2.0f * u2, &sn, &cs);
@@ -373,9 +379,9 @@ __device__ __forceinline__ void gauss_pair32(uint32_t w1, uint32_t w2, float &a,
 }
 
 // The three standard normals of the SU(2) momentum of link lref (reference link index) for
-// trajectory traj: Philox(seed; {lref, draw, traj, TAG_MOMENTA}).  FP64 uses draws 0 and 1
-// (a 53-bit Box-Muller pair each); FP32 gets four words from draw 0 alone, two pairs of
-// 24-bit uniforms.  U(1) momenta use the first normal.
+// trajectory traj: Philox(seed; {lref, draw, traj, TAG_MOMENTA}), draws 0 and 1, one
+// Box-Muller pair of 53-bit uniforms each; FP32 storage evaluates the same pairs in FP32
+// arithmetic.  U(1) momenta use the first normal.
 template <class T>
 __device__ __forceinline__ void momentum_normals(uint32_t lref, uint32_t traj, uint64_t seed,
                                                  int na, T &n0, T &n1, T &n2);
@@ -399,8 +405,11 @@ __device__ __forceinline__ void momentum_normals<float>(uint32_t lref, uint32_t 
   uint32_t r[4];
   float n3;
   philox(lref, 0u, traj, TAG_MOMENTA, seed, r);
-  gauss_pair32(r[0], r[1], n0, n1);
-  if (na == 3) gauss_pair32(r[2], r[3], n2, n3);
+  gauss_pair32(r, n0, n1);
+  if (na == 3) {
+    philox(lref, 1u, traj, TAG_MOMENTA, seed, r);
+    gauss_pair32(r, n2, n3);
+  }
 }
 
 }  // namespace su2b

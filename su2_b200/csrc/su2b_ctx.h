@@ -66,6 +66,7 @@ struct su2b_ctx {
 
   // launch shape of the SU(2) force kernel (su2b_autotune)
   int tune_force = 3;  // (128 threads, 6 blocks/SM) until tuned; FP64 contexts start at 2
+  int traj_path = 0;   // SU2B_TRAJ_FUSED_GRAPH or SU2B_TRAJ_PLAIN
 
   // kernel launch counter and the per-class device timers (su2b_profile)
   long launches = 0;

@@ -159,6 +159,18 @@ class gaugeconfig:
     def force_variant(self, v):
         self._c(self.lib.su2b_tune_set(self.ctx, 0, int(v)))
 
+    @property
+    def plain_trajectory(self) -> bool:
+        """True: SU(2) trajectories run in the plain form (start-field copy, integrator steps
+        launched one by one, no graph); False (default): the fused, graph-captured form."""
+        v = C.c_int()
+        self._c(self.lib.su2b_tune_get(self.ctx, 1, C.byref(v)))
+        return v.value == 1
+
+    @plain_trajectory.setter
+    def plain_trajectory(self, on):
+        self._c(self.lib.su2b_tune_set(self.ctx, 1, 1 if on else 0))
+
     def kernel_launches(self) -> int:
         n = C.c_long()
         self._c(self.lib.su2b_kernel_launches(self.ctx, C.byref(n)))

@@ -219,6 +219,27 @@ def test_device_momentum_stream(gpu, orc, group, dims, nd):
     assert P.size == c.n_links * na
 
 
+def test_mixed_momenta_are_the_fp64_stream(gpu, orc):
+    """FP32 storage draws the same momenta as FP64 (the same two Philox draws and 53-bit
+    uniforms per link, Box-Muller in FP32 arithmetic): the kinetic energy agrees to FP32
+    rounding, and a trajectory from the same start and seed lands on the FP64 one within
+    FP32 accuracy, so both precisions sample the same momenta trajectory by trajectory."""
+    dims, nd = (8, 8, 8, 8), 4
+    U = hot(orc, 0, dims, nd)
+    P = orc.philox_momenta(0, dims, nd, 777, 5)
+    out = {}
+    for prec in ("fp64", "mixed"):
+        with gpu.gaugeconfig(*dims, nd, 2.3, precision=prec) as c:
+            c.upload(U)
+            r = c.md_update("omf2", 4, 0.5, seed=777, traj=5, accept_reject=False)
+            out[prec] = (r, c.download())
+    kin = 0.5 * float(np.sum(P * P))
+    assert out["fp64"][0].H_old[0] == pytest.approx(kin, rel=1e-13)
+    assert out["mixed"][0].H_old[0] == pytest.approx(kin, rel=2e-7)
+    assert out["mixed"][0].dH == pytest.approx(out["fp64"][0].dH, abs=5e-3)
+    assert rel(out["mixed"][1], out["fp64"][1]) < 1e-5
+
+
 @pytest.mark.parametrize("group,dims,nd", GEOMS, ids=GEOM_IDS)
 def test_metropolis_checkerboard(gpu, orc, group, dims, nd):
     """The device sweep replayed by the oracle (same Philox stream and update order), for the
@@ -262,6 +283,29 @@ def test_reversibility(gpu, orc):
     # one: the same arithmetic up to rounding
     assert a.dH == pytest.approx(b.dH, abs=1e-9)
     assert abs(a.ddH) < 1e-8
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_plain_trajectory_matches_fused(gpu, orc, precision):
+    """The plain form (start-field copy, integrator steps launched one by one, no graph) and
+    the fused graph-captured trajectory are the same discrete map: the same accept decisions,
+    Delta H and links up to rounding, over a chain of Philox trajectories."""
+    dims, nd = (6, 6, 6, 6), 4
+    U = hot(orc, 0, dims, nd)
+    out = {}
+    for plain in (False, True):
+        with gpu.gaugeconfig(*dims, nd, 2.3, precision=precision) as c:
+            c.upload(U)
+            c.plain_trajectory = plain
+            assert c.plain_trajectory == plain
+            res = [c.md_update("omf2", 5, 1.0, seed=41, traj=k) for k in range(5)]
+            out[plain] = (res, c.download())
+    tol = 1e-9 if precision == "fp64" else 1e-3
+    for a, b in zip(out[False][0], out[True][0]):
+        assert a.accepted == b.accepted
+        assert a.dH == pytest.approx(b.dH, abs=tol)
+        assert a.plaquette == pytest.approx(b.plaquette, rel=1e-12 if precision == "fp64" else 1e-6)
+    assert rel(out[False][1], out[True][1]) < (1e-11 if precision == "fp64" else 1e-5)
 
 
 def test_error_paths(gpu):

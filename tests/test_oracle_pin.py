@@ -312,3 +312,26 @@ def test_pin_pion_correlator(orc, ref):
         U = ref.hotstart(1, dims, nd, 42, 1.0, 654321)
         assert np.array_equal(orc.pion_correlator(dims, nd, U, 0.1, 1e-12, 17),
                               ref.pion_correlator(dims, nd, U, 0.1, 1e-12, 17))
+
+
+def test_oracle_at_full_sizes_against_reference_digests(orc):
+    """The restatement at the workloads' full sizes against the reference's own results
+    (tests/golden/config_sizes.npz): D D^+ on U(1) 256^2, the gauge derivative and action on
+    SU(2) 24^4, the start plaquette and one RK3 flow step on SU(2) 32^4."""
+    import os
+    import sys
+    here = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+    sys.path.insert(0, here)
+    from digest import check
+    from make_config_sizes import SU2_24, SU2_32, U1_DIMS, inputs
+    fx = np.load(os.path.join(here, "config_sizes.npz"))
+    x = inputs(orc)
+    check(orc.staggered_apply(U1_DIMS, 2, x["u1_U"], 0.05, 2, x["u1_b"]), fx, "u1_DDdag_b",
+          1e-13)
+    check(orc.gauge_derivative(0, SU2_24, 4, 2.4, x["su2_24_U"]), fx, "su2_24_force", 1e-13)
+    assert -1.2 * orc.gauge_energy(0, SU2_24, 4, x["su2_24_U"]) == \
+        pytest.approx(float(fx["su2_24_S"]), rel=1e-13)
+    U = x["su2_32_U"]
+    assert orc.gauge_energy(0, SU2_32, 4, U) / (32 ** 4 * 12) == \
+        pytest.approx(float(fx["su2_32_plaq"]), rel=1e-13)
+    check(orc.runge_kutta(0, SU2_32, 4, 2.4, 0.01, U), fx, "su2_32_flow", 1e-13)
