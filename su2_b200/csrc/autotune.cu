@@ -95,9 +95,11 @@ extern "C" int su2b_autotune(su2b_ctx *ctx, const char *cache_path, int retune,
     auto launch = [&]() -> cudaError_t {
       if (ctx->link64)
         return force_update<double>(ctx->g, ctx->U, 0, (double *)ctx->Z, nullptr, f, -1e-3,
-                                    ctx->xi, mode, nullptr, nullptr, ctx->U2, 0.0, s, var);
+                                    ctx->xi, mode, nullptr, nullptr, ctx->U2, 0.0, s, var,
+                                    false, ctx->sched);
       return force_update<float>(ctx->g, ctx->U, 0, (float *)ctx->Z, nullptr, f, -1e-3, ctx->xi,
-                                 mode, nullptr, nullptr, ctx->U2, 0.0, s, var);
+                                 mode, nullptr, nullptr, ctx->U2, 0.0, s, var, false,
+                                 ctx->sched);
     };
     cudaError_t e = cudaSuccess;
     for (int k = 0; k < 2 && e == cudaSuccess; k++) e = launch();

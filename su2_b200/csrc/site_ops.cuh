@@ -54,6 +54,8 @@ __device__ __forceinline__ double finish_link(const Su2<T> &u, const Su2<T> &k, 
     st_link(Uout + l, mul(exp_alg(dt_upd * p0, dt_upd * p1, dt_upd * p2), u));
   else if (mode & FM_RESTORE)
     st_link(Uout + l, from64<T>(restore_su(to64(u))));
+  // |P|^2 in FP64 only where the launch sums it (a uniform branch)
+  if (!(mode & FM_KINETIC)) return 0.;
   return (double)p0 * p0 + (double)p1 * p1 + (double)p2 * p2;
 }
 
@@ -328,6 +330,112 @@ __device__ __forceinline__ double force_half_x(const Geom &g, const LinkT<T> *__
   for (int j = 0; j < 2; j++)
     k2 += finish_link<T>(L(m0 + j, 0, 0, 0, 0), K[j], (m0 + j) * V + self, NL, P, extra, f,
                          scale_, mode, Uout, dt_upd);
+  return k2;
+}
+
+// Neighbour addressing by half-index offsets.  With h = lex/2 (= cb, the site's index within
+// its parity) the site displaced by +-e_d has half-index h + Df[d] (forward) or h + Db[d]
+// (backward), periodic wrap included; a displacement by e_mu - e_nu (mu != nu) has
+// h + Df[mu] + Db[nu], because at most one of the two lexicographic offsets is odd (only the
+// stride-1 direction has odd offsets) and floor((a + even + odd)/2) = floor((a + odd)/2) +
+// even/2.  So every link a thread reads is base[parity] + mu V + (a sum of at most two
+// per-thread offsets), formed once per thread instead of once per load.
+struct NbrOffsets {
+  int f[4], b[4];
+};
+__device__ __forceinline__ NbrOffsets nbr_offsets(const Geom &g, const Site &s, int cb) {
+  NbrOffsets o;
+#pragma unroll
+  for (int d = 0; d < 4; d++) {
+    o.f[d] = ((s.lex + fwd(g, s, d)) >> 1) - cb;
+    o.b[d] = ((s.lex + bwd(g, s, d)) >> 1) - cb;
+  }
+  return o;
+}
+
+// force_half_x with the links addressed through NbrOffsets: the same loads, products and
+// results (bit for bit), fewer integer instructions per load.
+template <class T, int HALF>
+__device__ __forceinline__ double force_half_xd(const Geom &g, const LinkT<T> *__restrict__ U,
+                                                T *__restrict__ P, const T *__restrict__ extra,
+                                                T f, T scale_, int mode,
+                                                LinkT<T> *__restrict__ Uout, T dt_upd, int p,
+                                                int cb, bool valid, Su2<T> (*xs)[2],
+                                                int bar_id) {
+  const Site s = site_from_eo(g, p, cb);
+  const int V = g.V;
+  const NbrOffsets no = nbr_offsets(g, s, cb);
+  // the links of this parity and of the other one, at this thread's half-index
+  const LinkT<T> *__restrict__ Bp = U + (size_t)p * g.Vh + cb;
+  const LinkT<T> *__restrict__ Bq = U + (size_t)(1 - p) * g.Vh + cb;
+  // link U_mu at the site displaced by o (components in {-1, 0, 1}, at most two nonzero)
+  auto L = [&](int mu, int o0, int o1, int o2, int o3) -> Su2<T> {
+    const int o[4] = {o0, o1, o2, o3};
+    int delta = mu * V, odd = 0;
+#pragma unroll
+    for (int d = 0; d < 4; d++) {
+      if (o[d] > 0) delta += no.f[d];
+      if (o[d] < 0) delta += no.b[d];
+      odd ^= (o[d] != 0);
+    }
+    return ld_link((odd ? Bq : Bp) + delta);
+  };
+  auto E = [](int d, int k) { return d == k ? 1 : 0; };
+  constexpr int m0 = 2 * HALF, m1 = 2 * HALF + 1;
+  Su2<T> X0, X1;
+  if (HALF == 0) {
+    X0 = mul(L(2, 1, 0, 0, 0), dag(L(0, 0, 0, 1, 0)));  // A_{0,2}
+    X1 = mul(L(3, 1, 0, 0, 0), dag(L(0, 0, 0, 0, 1)));  // A_{0,3}
+  } else {
+    X0 = mul(L(1, 0, 0, 1, 0), dag(L(2, 0, 1, 0, 0)));  // A_{2,1}
+    X1 = mul(L(1, 0, 0, 0, 1), dag(L(3, 0, 1, 0, 0)));  // A_{3,1}
+  }
+  const int t = threadIdx.x;
+  xs[t][0] = X0;
+  xs[t][1] = X1;
+  Su2<T> K[2];
+  {
+    const Su2<T> A = mul(L(m1, E(m0, 0), E(m0, 1), E(m0, 2), E(m0, 3)),
+                         dag(L(m0, E(m1, 0), E(m1, 1), E(m1, 2), E(m1, 3))));
+    K[0] = mul(A, dag(L(m1, 0, 0, 0, 0)));
+    K[1] = mul(dag(A), dag(L(m0, 0, 0, 0, 0)));
+  }
+#pragma unroll
+  for (int j = 0; j < 2; j++) {
+    const int mu = m0 + j;
+#pragma unroll
+    for (int nu = 0; nu < 4; nu++) {
+      if (nu == mu) continue;
+      const Su2<T> e = L(nu, E(mu, 0) - E(nu, 0), E(mu, 1) - E(nu, 1), E(mu, 2) - E(nu, 2),
+                         E(mu, 3) - E(nu, 3));
+      const Su2<T> h = L(mu, -E(nu, 0), -E(nu, 1), -E(nu, 2), -E(nu, 3));
+      const Su2<T> c = L(nu, -E(nu, 0), -E(nu, 1), -E(nu, 2), -E(nu, 3));
+      K[j] = mul_acc(K[j], mul(dag(e), dag(h)), c);
+    }
+  }
+  warp_pair_sync(bar_id);
+  const Su2<T> Y0 = xs[t ^ 32][0], Y1 = xs[t ^ 32][1];
+  if (HALF == 0) {
+    const Su2<T> u2 = L(2, 0, 0, 0, 0), u3 = L(3, 0, 0, 0, 0);
+    K[0] = mul_acc(K[0], X0, dag(u2));
+    K[0] = mul_acc(K[0], X1, dag(u3));
+    K[1] = mul_acc(K[1], dag(Y0), dag(u2));
+    K[1] = mul_acc(K[1], dag(Y1), dag(u3));
+  } else {
+    const Su2<T> u0 = L(0, 0, 0, 0, 0), u1 = L(1, 0, 0, 0, 0);
+    K[0] = mul_acc(K[0], dag(Y0), dag(u0));
+    K[0] = mul_acc(K[0], X0, dag(u1));
+    K[1] = mul_acc(K[1], dag(Y1), dag(u0));
+    K[1] = mul_acc(K[1], X1, dag(u1));
+  }
+  if (!valid) return 0.;
+  const size_t self = (size_t)p * g.Vh + cb;
+  const size_t NL = 4 * (size_t)V;
+  double k2 = 0.;
+#pragma unroll
+  for (int j = 0; j < 2; j++)
+    k2 += finish_link<T>(L(m0 + j, 0, 0, 0, 0), K[j], (m0 + j) * (size_t)V + self, NL, P, extra,
+                         f, scale_, mode, Uout, dt_upd);
   return k2;
 }
 

@@ -454,6 +454,31 @@ def test_every_force_launch_shape_is_exact(gpu, orc, precision, dims):
 
 
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
+@pytest.mark.parametrize("dims", [(8, 8, 8, 8), (6, 6, 6, 6), (16, 8, 8, 16)],
+                         ids=["8^4", "6^4", "16x8x8x16"])
+def test_offset_addressed_and_sm_local_shapes_equal_xsplit(gpu, orc, precision, dims):
+    """The xsplit force with per-thread neighbour offsets, and the same on persistent blocks
+    with the SM-local tile schedule, perform xsplit's arithmetic: a chain of graph-replayed
+    trajectories (accepts and rejects, the schedule reset between every pair of chained
+    launches) ends on bit-identical links with identical Delta H."""
+    shapes = gpu._abi.FORCE_SHAPES
+    v_ref = shapes.index(("xsplit", 128, 8))
+    U = hot(orc, 0, dims, 4)
+    out = {}
+    for name in ("xsplit", "xsplit_d", "xsplit_sm"):
+        v = shapes.index((name, 128, 8))
+        with make(gpu, 0, dims, 4, beta=2.3, precision=precision) as c:
+            c.upload(U)
+            c.force_variant = v
+            res = [c.md_update("omf2", 4, 1.0, seed=3, traj=k) for k in range(12)]
+            out[v] = ([(r.accepted, r.dH) for r in res], c.download(), c.derivative())
+    for v in out:
+        assert out[v][0] == out[v_ref][0], v
+        assert np.array_equal(out[v][1], out[v_ref][1]), v
+        assert np.array_equal(out[v][2], out[v_ref][2]), v
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
 @pytest.mark.parametrize("dims,nd", [((6, 1, 1, 4), 2), ((4, 6, 1, 4), 3), ((6, 4, 1, 6), 3)],
                          ids=["6x4-d2", "4x6x4-d3", "6x4x6-d3"])
 def test_every_force_launch_shape_below_four_dims(gpu, orc, precision, dims, nd):
