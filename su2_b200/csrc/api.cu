@@ -154,8 +154,7 @@ extern "C" int su2b_ctx_create(int group, int Lx, int Ly, int Lz, int Lt, int nd
       (st = dalloc(ctx, &ctx->part, sizeof(double) * 3 * ctx->part_cap * NSLOT)) ||
       (st = dalloc(ctx, &ctx->red, sizeof(double) * 64)) ||
       (st = dalloc(ctx, &ctx->traj, sizeof(TrajDev))) ||
-      (st = dalloc(ctx, &ctx->counts, sizeof(unsigned long long) * 4)) ||
-      (st = dalloc(ctx, &ctx->sched, sizeof(unsigned) * SCHED_WORDS)))
+      (st = dalloc(ctx, &ctx->counts, sizeof(unsigned long long) * 4)))
     return fin(st);
   if (cudaMallocHost((void **)&ctx->h_red, sizeof(double) * 64) != cudaSuccess ||
       cudaMallocHost((void **)&ctx->h_traj, sizeof(TrajDev)) != cudaSuccess ||
@@ -163,9 +162,7 @@ extern "C" int su2b_ctx_create(int group, int Lx, int Ly, int Lz, int Lt, int nd
       cudaMallocHost((void **)&ctx->h_st, sizeof(SolverState)) != cudaSuccess ||
       cudaMallocHost((void **)&ctx->h_tparams, sizeof(TrajParams)) != cudaSuccess)
     return fin(SU2B_ERR_NOMEM);
-  if (cudaMemsetAsync(ctx->U, 0, lb * NL, ctx->stream) != cudaSuccess ||
-      cudaMemsetAsync(ctx->sched, 0, sizeof(unsigned) * SCHED_WORDS, ctx->stream) != cudaSuccess)
-    return fin(SU2B_ERR_CUDA);
+  if (cudaMemsetAsync(ctx->U, 0, lb * NL, ctx->stream) != cudaSuccess) return fin(SU2B_ERR_CUDA);
   if (cudaStreamSynchronize(ctx->stream) != cudaSuccess) return fin(SU2B_ERR_CUDA);
   return fin(SU2B_OK);
 }
@@ -412,7 +409,7 @@ static int q_force(su2b_ctx *ctx, const void *U, T *P, const T *extra, double f,
                    int mode, double *kin_part, int *nb, void *Uout, double dt_upd) {
   SU2B_LAUNCH(SU2B_K_FORCE, force_update<T>(ctx->g, U, ctx->group, P, extra, f, scale, ctx->xi,
                                             mode, kin_part, nb, Uout, dt_upd, ctx->stream,
-                                            ctx->tune_force, false, ctx->sched));
+                                            ctx->tune_force));
   return SU2B_OK;
 }
 int su2b_q_force(su2b_ctx *ctx, const void *U, void *P, const void *extra, double f,

@@ -95,11 +95,9 @@ extern "C" int su2b_autotune(su2b_ctx *ctx, const char *cache_path, int retune,
     auto launch = [&]() -> cudaError_t {
       if (ctx->link64)
         return force_update<double>(ctx->g, ctx->U, 0, (double *)ctx->Z, nullptr, f, -1e-3,
-                                    ctx->xi, mode, nullptr, nullptr, ctx->U2, 0.0, s, var,
-                                    false, ctx->sched);
+                                    ctx->xi, mode, nullptr, nullptr, ctx->U2, 0.0, s, var);
       return force_update<float>(ctx->g, ctx->U, 0, (float *)ctx->Z, nullptr, f, -1e-3, ctx->xi,
-                                 mode, nullptr, nullptr, ctx->U2, 0.0, s, var, false,
-                                 ctx->sched);
+                                 mode, nullptr, nullptr, ctx->U2, 0.0, s, var);
     };
     cudaError_t e = cudaSuccess;
     for (int k = 0; k < 2 && e == cudaSuccess; k++) e = launch();

@@ -669,7 +669,7 @@ __global__ void __launch_bounds__(NT, MINB)
                      double *kin_part, LinkT<T> *__restrict__ Uout, T dt_upd) {
   static_assert(NT == 128, "two warp pairs per block, hardware barriers 1 and 2");
   __shared__ double sh[NT / 32];
-  __shared__ Su2<T> xs[NT][2];
+  __shared__ LinkT<T> xs[2][NT];
   pdl_trigger();
   pdl_wait();
   const int w = threadIdx.x >> 5;
@@ -689,15 +689,15 @@ __global__ void __launch_bounds__(NT, MINB)
   }
 }
 
-// xsplit with the links addressed through per-thread neighbour offsets (force_half_xd)
+// xsplit with the pair's exchange at the start of the body (force_half_xe)
 template <class T, int NT, int MINB>
 __global__ void __launch_bounds__(NT, MINB)
-  k_force_su2_xsplit_d(Geom g, const LinkT<T> *__restrict__ U, T *__restrict__ P,
+  k_force_su2_xsplit_e(Geom g, const LinkT<T> *__restrict__ U, T *__restrict__ P,
                        const T *__restrict__ extra, T f, T scale_, int mode, T wt, T ws,
                        double *kin_part, LinkT<T> *__restrict__ Uout, T dt_upd) {
   static_assert(NT == 128, "two warp pairs per block, hardware barriers 1 and 2");
   __shared__ double sh[NT / 32];
-  __shared__ Su2<T> xs[NT][2];
+  __shared__ LinkT<T> xs[2][NT];
   pdl_trigger();
   pdl_wait();
   const int w = threadIdx.x >> 5;
@@ -707,141 +707,14 @@ __global__ void __launch_bounds__(NT, MINB)
   const int cbc = valid ? cb : g.Vh - 1;
   const int bar_id = 1 + (w >> 1);
   const double k2 =
-    half == 0 ? force_half_xd<T, 0>(g, U, P, extra, f, scale_, mode, Uout, dt_upd, p, cbc,
+    half == 0 ? force_half_xe<T, 0>(g, U, P, extra, f, scale_, mode, Uout, dt_upd, p, cbc,
                                     valid, xs, bar_id)
-              : force_half_xd<T, 1>(g, U, P, extra, f, scale_, mode, Uout, dt_upd, p, cbc,
+              : force_half_xe<T, 1>(g, U, P, extra, f, scale_, mode, Uout, dt_upd, p, cbc,
                                     valid, xs, bar_id);
   if (mode & FM_KINETIC) {
     const double r = block_sum<NT>(k2, sh);
     if (threadIdx.x == 0) kin_part[blockIdx.x] = r;
   }
-}
-
-// ---- SM-local schedule of the force tiles ----
-// The tiles (32 sites of each parity, the work of one xsplit block) are split into one
-// contiguous region per SM.  A persistent block takes the tiles of the region of the SM it
-// runs on, in order, by an atomic counter per region; so the blocks resident on an SM work
-// on neighbouring tiles at the same time and their +-z / +-y neighbour links come from the
-// SM's L1 instead of L2.  A block whose region is exhausted takes tiles from any region with
-// work left (a flag per region, scanned by one warp), so every tile is processed exactly
-// once whichever SMs the blocks land on.  The last block to finish resets the counters for
-// the next launch.  sched: nreg counters, nreg flags, one count of finished blocks.
-__device__ __forceinline__ unsigned sm_id() {
-  unsigned r;
-  asm volatile("mov.u32 %0, %%smid;" : "=r"(r));
-  return r;
-}
-
-// the next tile for this block (called by warp 0; the result is valid in lane 0), or -1
-__device__ __forceinline__ int claim_tile(unsigned *sched, int nreg, int ntiles, int &reg) {
-  unsigned *cnt = sched, *flag = sched + nreg;
-  const int lane = threadIdx.x & 31;
-  for (int attempt = 0; attempt <= nreg; attempt++) {
-    int tile = -1;
-    if (lane == 0) {
-      if (!((volatile unsigned *)flag)[reg]) {
-        const int lo = (int)((long)reg * ntiles / nreg);
-        const int hi = (int)((long)(reg + 1) * ntiles / nreg);
-        const unsigned k = atomicAdd(cnt + reg, 1u);
-        if ((long)lo + k < (long)hi)
-          tile = lo + (int)k;
-        else
-          flag[reg] = 1u;
-      }
-    }
-    tile = __shfl_sync(0xffffffffu, tile, 0);
-    if (tile >= 0) return tile;
-    // this region is exhausted: the first region after it with work left, if any
-    int next = -1;
-    for (int base = 0; base < nreg && next < 0; base += 32) {
-      const int j = base + lane;
-      const int rr = (reg + 1 + j) % nreg;
-      const bool open = j < nreg - 1 && !((volatile unsigned *)flag)[rr];
-      const unsigned m = __ballot_sync(0xffffffffu, open);
-      if (m) next = (reg + 1 + base + __ffs(m) - 1) % nreg;
-    }
-    if (next < 0) return -1;
-    reg = next;
-  }
-  return -1;
-}
-
-template <class T, int NT, int MINB>
-__global__ void __launch_bounds__(NT, MINB)
-  k_force_su2_xsplit_sm(Geom g, const LinkT<T> *__restrict__ U, T *__restrict__ P,
-                        const T *__restrict__ extra, T f, T scale_, int mode, T wt, T ws,
-                        double *kin_part, LinkT<T> *__restrict__ Uout, T dt_upd,
-                        unsigned *sched, int nreg) {
-  static_assert(NT == 128, "two warp pairs per block, hardware barriers 1 and 2");
-  __shared__ double sh[NT / 32];
-  __shared__ Su2<T> xs[NT][2];
-  __shared__ int s_tile, s_last;
-  pdl_trigger();
-  pdl_wait();
-  const int ntiles = (g.Vh + NT / 4 - 1) / (NT / 4);
-  int reg = (int)(sm_id() % (unsigned)nreg);
-  const int w = threadIdx.x >> 5;
-  const int half = w & 1, p = (w >> 1) & 1;
-  const int bar_id = 1 + (w >> 1);
-  for (;;) {
-    if (w == 0) {
-      const int t = claim_tile(sched, nreg, ntiles, reg);
-      if (threadIdx.x == 0) s_tile = t;
-    }
-    __syncthreads();
-    const int tile = s_tile;
-    __syncthreads();
-    if (tile < 0) break;
-    const int cb = tile * (NT / 4) + (w >> 2) * 32 + (threadIdx.x & 31);
-    const bool valid = cb < g.Vh;
-    const int cbc = valid ? cb : g.Vh - 1;
-    const double k2 =
-      half == 0 ? force_half_xd<T, 0>(g, U, P, extra, f, scale_, mode, Uout, dt_upd, p, cbc,
-                                      valid, xs, bar_id)
-                : force_half_xd<T, 1>(g, U, P, extra, f, scale_, mode, Uout, dt_upd, p, cbc,
-                                      valid, xs, bar_id);
-    if (mode & FM_KINETIC) {
-      const double r = block_sum<NT>(k2, sh);
-      if (threadIdx.x == 0) kin_part[tile] = r;
-    }
-  }
-  // the last block to finish resets the schedule for the next launch
-  if (threadIdx.x == 0) {
-    __threadfence();
-    s_last = atomicAdd(sched + 2 * nreg, 1u) == gridDim.x - 1;
-  }
-  __syncthreads();
-  if (s_last) {
-    __threadfence();
-    for (int r = threadIdx.x; r < 2 * nreg; r += NT) sched[r] = 0u;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      sched[2 * nreg] = 0u;
-      __threadfence();
-    }
-  }
-}
-
-// persistent grid of the SM-local force kernel: resident blocks per SM x SMs (per device and
-// precision, found once)
-template <class T> int xsplit_sm_grid(int *nsm_out) {
-  static int cached_dev[2][64] = {};
-  static int cached_nsm[2][64] = {};
-  int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 0;
-  const int ti = sizeof(T) == 8 ? 1 : 0;
-  if (!cached_dev[ti][dev]) {
-    int nsm = 0, occ = 0;
-    if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
-      return 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_force_su2_xsplit_sm<T, 128, 8>,
-                                                      128, 0) != cudaSuccess)
-      return 0;
-    cached_dev[ti][dev] = occ * nsm;
-    cached_nsm[ti][dev] = nsm;
-  }
-  *nsm_out = cached_nsm[ti][dev];
-  return cached_dev[ti][dev];
 }
 
 // launch with the programmatic-stream-serialization attribute when pdl is set
@@ -864,8 +737,7 @@ cudaError_t launch_force(void (*kern)(KArgs...), dim3 grid, int nt, cudaStream_t
 template <class T>
 cudaError_t force_update(const Geom &g, const void *U, int group, T *P, const T *extra, double f,
                          double scale, double xi, int mode, double *kin_part, int *nblocks,
-                         void *Uout, double dt_upd, cudaStream_t s, int variant, bool pdl,
-                         unsigned *sched) {
+                         void *Uout, double dt_upd, cudaStream_t s, int variant, bool pdl) {
   constexpr int NT = 128;
   const int aniso = xi != 1.0;
   if (group == 0) {
@@ -938,7 +810,7 @@ cudaError_t force_update(const Geom &g, const void *U, int group, T *P, const T 
       launch_force(k_force_su2_xsplit<T, NTV, MB>, grid, NTV, s, pdl, SU2B_FORCE_ARGS);    \
     if (e_ != cudaSuccess) return e_;                                                      \
   } while (0)
-#define SU2B_FORCE_XSPLIT_D(NTV, MB)                                                         \
+#define SU2B_FORCE_XSPLIT_E(NTV, MB)                                                         \
   do {                                                                                     \
     if (g.nd != 4) {                                                                       \
       SU2B_FORCE_LAUNCH(128, 8, false);                                                    \
@@ -947,20 +819,7 @@ cudaError_t force_update(const Geom &g, const void *U, int group, T *P, const T 
     const dim3 grid(cdiv(g.Vh, NTV / 4));                                                  \
     nb = grid.x;                                                                           \
     const cudaError_t e_ =                                                                 \
-      launch_force(k_force_su2_xsplit_d<T, NTV, MB>, grid, NTV, s, pdl, SU2B_FORCE_ARGS);  \
-    if (e_ != cudaSuccess) return e_;                                                      \
-  } while (0)
-#define SU2B_FORCE_XSPLIT_SM()                                                               \
-  do {                                                                                     \
-    int nsm_ = 0;                                                                          \
-    const int nblk_ = xsplit_sm_grid<T>(&nsm_);                                            \
-    if (g.nd != 4 || !sched || nblk_ <= 0 || nsm_ > SCHED_MAX_REGIONS) {                   \
-      SU2B_FORCE_XSPLIT_D(128, 8);                                                         \
-      break;                                                                               \
-    }                                                                                      \
-    nb = cdiv(g.Vh, 32);                                                                   \
-    const cudaError_t e_ = launch_force(k_force_su2_xsplit_sm<T, 128, 8>, dim3(nblk_), 128, \
-                                        s, pdl, SU2B_FORCE_ARGS, sched, nsm_);             \
+      launch_force(k_force_su2_xsplit_e<T, NTV, MB>, grid, NTV, s, pdl, SU2B_FORCE_ARGS);  \
     if (e_ != cudaSuccess) return e_;                                                      \
   } while (0)
     // the anisotropic action (rare) runs one launch shape; the tuned shapes are isotropic and
@@ -978,8 +837,7 @@ cudaError_t force_update(const Geom &g, const void *U, int group, T *P, const T 
         case 6: SU2B_FORCE_SPLIT(128, 8); break;
         case 8: SU2B_FORCE_XSPLIT(128, 8); break;
         case 9: SU2B_FORCE_LINK(6); break;
-        case 10: SU2B_FORCE_XSPLIT_D(128, 8); break;
-        case 11: SU2B_FORCE_XSPLIT_SM(); break;
+        case 10: SU2B_FORCE_XSPLIT_E(128, 8); break;
         default: SU2B_FORCE_LAUNCH(64, 16, false); break;
       }
     }
@@ -987,8 +845,7 @@ cudaError_t force_update(const Geom &g, const void *U, int group, T *P, const T 
 #undef SU2B_FORCE_SPLIT
 #undef SU2B_FORCE_XSPLIT
 #undef SU2B_FORCE_LINK
-#undef SU2B_FORCE_XSPLIT_D
-#undef SU2B_FORCE_XSPLIT_SM
+#undef SU2B_FORCE_XSPLIT_E
 #undef SU2B_FORCE_ARGS
     if (nblocks) *nblocks = nb;
   } else {
@@ -1135,7 +992,7 @@ cudaError_t cond_restore(const Geom &g, void *U, const void *U_old, int group,
                                         int *, cudaStream_t);                                 \
   template cudaError_t force_update<T>(const Geom &, const void *, int, T *, const T *,      \
                                        double, double, double, int, double *, int *, void *,  \
-                                       double, cudaStream_t, int, bool, unsigned *);          \
+                                       double, cudaStream_t, int, bool);                      \
   template cudaError_t link_update<T>(const Geom &, void *, int, const T *, double,          \
                                       cudaStream_t, double);                                  \
   template cudaError_t adj_round_axpy<T>(const Geom &, T *, const T *, int, double, double,  \

@@ -249,12 +249,12 @@ int enqueue_fused(su2b_ctx *ctx, const std::vector<FOp> &fops, bool host_momenta
       SU2B_LAUNCH(SU2B_K_FORCE,
                   force_update<double>(ctx->g, cur, 0, (double *)ctx->P, nullptr, f, -o.cm,
                                        ctx->xi, mode, ctx->part_slot(2), &nb, out, o.cg, s,
-                                       ctx->tune_force, pdl, ctx->sched));
+                                       ctx->tune_force, pdl));
     else
       SU2B_LAUNCH(SU2B_K_FORCE,
                   force_update<float>(ctx->g, cur, 0, (float *)ctx->P, nullptr, f, -o.cm,
                                       ctx->xi, mode, ctx->part_slot(2), &nb, out, o.cg, s,
-                                      ctx->tune_force, pdl, ctx->sched));
+                                      ctx->tune_force, pdl));
     if (o.kinetic) nb_kin = nb;
     if (o.kind == 1) cur = out;
   }

@@ -228,6 +228,22 @@ __device__ __forceinline__ double force_link_impl(const Geom &g, const LinkT<T> 
                         mode, Uout, dt_upd);
 }
 
+// SU(2) elements through shared memory as the aligned storage type (one 128-bit access per
+// FP32 element), laid out [2][threads] so that a warp's accesses are consecutive
+__device__ __forceinline__ Link32 as_link(const Su2<float> &u) {
+  return make_float4(u.ar, u.ai, u.br, u.bi);
+}
+__device__ __forceinline__ Link64 as_link(const Su2<double> &u) {
+  return Link64{u.ar, u.ai, u.br, u.bi};
+}
+__device__ __forceinline__ Su2<float> from_link(const Link32 &v) {
+  return Su2<float>{v.x, v.y, v.z, v.w};
+}
+__device__ __forceinline__ Su2<double> from_link(const Link64 &v) {
+  return Su2<double>{v.ar, v.ai, v.br, v.bi};
+}
+template <class T> using XchgT = LinkT<T> (*)[128];
+
 // The split force step with each of the four planes that cross the halves formed once per
 // site instead of once per half.  With A_{mu,nu} = U_nu(x+mu) U_mu(x+nu)^+ the forward staples
 // of a plane are K_mu += A_{mu,nu} U_nu(x)^+ and K_nu += A_{mu,nu}^+ U_mu(x)^+.  The two
@@ -250,7 +266,7 @@ __device__ __forceinline__ double force_half_x(const Geom &g, const LinkT<T> *__
                                                T *__restrict__ P, const T *__restrict__ extra,
                                                T f, T scale_, int mode,
                                                LinkT<T> *__restrict__ Uout, T dt_upd, int p,
-                                               int cb, bool valid, Su2<T> (*xs)[2],
+                                               int cb, bool valid, XchgT<T> xs,
                                                int bar_id) {
   const Site s = site_from_eo(g, p, cb);
   const size_t V = (size_t)g.V, NL = 4 * V;
@@ -283,8 +299,8 @@ __device__ __forceinline__ double force_half_x(const Geom &g, const LinkT<T> *__
     X1 = mul(L(1, 0, 0, 0, 1), dag(L(3, 0, 1, 0, 0)));  // A_{3,1}
   }
   const int t = threadIdx.x;
-  xs[t][0] = X0;
-  xs[t][1] = X1;
+  xs[0][t] = as_link(X0);
+  xs[1][t] = as_link(X1);
   // the plane inside the half
   Su2<T> K[2];
   {
@@ -309,7 +325,7 @@ __device__ __forceinline__ double force_half_x(const Geom &g, const LinkT<T> *__
   }
   // the partner's cross products
   warp_pair_sync(bar_id);
-  const Su2<T> Y0 = xs[t ^ 32][0], Y1 = xs[t ^ 32][1];
+  const Su2<T> Y0 = from_link(xs[0][t ^ 32]), Y1 = from_link(xs[1][t ^ 32]);
   if (HALF == 0) {  // K_0 += A_{0,k} U_k^+;  K_1 += A_{1,k} U_k^+ with A_{1,k} = Y^+  (k = 2, 3)
     const Su2<T> u2 = L(2, 0, 0, 0, 0), u3 = L(3, 0, 0, 0, 0);
     K[0] = mul_acc(K[0], X0, dag(u2));
@@ -333,109 +349,95 @@ __device__ __forceinline__ double force_half_x(const Geom &g, const LinkT<T> *__
   return k2;
 }
 
-// Neighbour addressing by half-index offsets.  With h = lex/2 (= cb, the site's index within
-// its parity) the site displaced by +-e_d has half-index h + Df[d] (forward) or h + Db[d]
-// (backward), periodic wrap included; a displacement by e_mu - e_nu (mu != nu) has
-// h + Df[mu] + Db[nu], because at most one of the two lexicographic offsets is odd (only the
-// stride-1 direction has odd offsets) and floor((a + even + odd)/2) = floor((a + odd)/2) +
-// even/2.  So every link a thread reads is base[parity] + mu V + (a sum of at most two
-// per-thread offsets), formed once per thread instead of once per load.
-struct NbrOffsets {
-  int f[4], b[4];
-};
-__device__ __forceinline__ NbrOffsets nbr_offsets(const Geom &g, const Site &s, int cb) {
-  NbrOffsets o;
-#pragma unroll
-  for (int d = 0; d < 4; d++) {
-    o.f[d] = ((s.lex + fwd(g, s, d)) >> 1) - cb;
-    o.b[d] = ((s.lex + bwd(g, s, d)) >> 1) - cb;
-  }
-  return o;
-}
-
-// force_half_x with the links addressed through NbrOffsets: the same loads, products and
-// results (bit for bit), fewer integer instructions per load.
+// force_half_x with the pair's exchange first: each thread forms its two cross products,
+// both warps of the pair meet at the barrier at once, and the four cross-plane staples start
+// the staple sums.  The cross products, the partner's and the own links they multiply are
+// then dead before the in-half plane and the backward staples, so fewer values stay live
+// through the longest part of the body; the backward staples run with nu outermost so that
+// U_nu(x-nu) is loaded once for both links (24 link loads per thread instead of 26).  Same
+// products as force_half_x, summed in another order.
 template <class T, int HALF>
-__device__ __forceinline__ double force_half_xd(const Geom &g, const LinkT<T> *__restrict__ U,
+__device__ __forceinline__ double force_half_xe(const Geom &g, const LinkT<T> *__restrict__ U,
                                                 T *__restrict__ P, const T *__restrict__ extra,
                                                 T f, T scale_, int mode,
                                                 LinkT<T> *__restrict__ Uout, T dt_upd, int p,
-                                                int cb, bool valid, Su2<T> (*xs)[2],
+                                                int cb, bool valid, XchgT<T> xs,
                                                 int bar_id) {
   const Site s = site_from_eo(g, p, cb);
-  const int V = g.V;
-  const NbrOffsets no = nbr_offsets(g, s, cb);
-  // the links of this parity and of the other one, at this thread's half-index
-  const LinkT<T> *__restrict__ Bp = U + (size_t)p * g.Vh + cb;
-  const LinkT<T> *__restrict__ Bq = U + (size_t)(1 - p) * g.Vh + cb;
-  // link U_mu at the site displaced by o (components in {-1, 0, 1}, at most two nonzero)
+  const size_t V = (size_t)g.V, NL = 4 * V;
+  int fo[4], bo[4];
+#pragma unroll
+  for (int d = 0; d < 4; d++) {
+    fo[d] = fwd(g, s, d);
+    bo[d] = bwd(g, s, d);
+  }
   auto L = [&](int mu, int o0, int o1, int o2, int o3) -> Su2<T> {
     const int o[4] = {o0, o1, o2, o3};
-    int delta = mu * V, odd = 0;
+    int lex = s.lex, odd = 0;
 #pragma unroll
     for (int d = 0; d < 4; d++) {
-      if (o[d] > 0) delta += no.f[d];
-      if (o[d] < 0) delta += no.b[d];
+      if (o[d] > 0) lex += fo[d];
+      if (o[d] < 0) lex += bo[d];
       odd ^= (o[d] != 0);
     }
-    return ld_link((odd ? Bq : Bp) + delta);
+    return ld_link(U + (size_t)mu * V + eo_of(g, lex, p ^ odd));
   };
   auto E = [](int d, int k) { return d == k ? 1 : 0; };
   constexpr int m0 = 2 * HALF, m1 = 2 * HALF + 1;
-  Su2<T> X0, X1;
-  if (HALF == 0) {
-    X0 = mul(L(2, 1, 0, 0, 0), dag(L(0, 0, 0, 1, 0)));  // A_{0,2}
-    X1 = mul(L(3, 1, 0, 0, 0), dag(L(0, 0, 0, 0, 1)));  // A_{0,3}
-  } else {
-    X0 = mul(L(1, 0, 0, 1, 0), dag(L(2, 0, 1, 0, 0)));  // A_{2,1}
-    X1 = mul(L(1, 0, 0, 0, 1), dag(L(3, 0, 1, 0, 0)));  // A_{3,1}
-  }
   const int t = threadIdx.x;
-  xs[t][0] = X0;
-  xs[t][1] = X1;
   Su2<T> K[2];
+  {
+    Su2<T> X0, X1;
+    if (HALF == 0) {
+      X0 = mul(L(2, 1, 0, 0, 0), dag(L(0, 0, 0, 1, 0)));  // A_{0,2}
+      X1 = mul(L(3, 1, 0, 0, 0), dag(L(0, 0, 0, 0, 1)));  // A_{0,3}
+    } else {
+      X0 = mul(L(1, 0, 0, 1, 0), dag(L(2, 0, 1, 0, 0)));  // A_{2,1}
+      X1 = mul(L(1, 0, 0, 0, 1), dag(L(3, 0, 1, 0, 0)));  // A_{3,1}
+    }
+    xs[0][t] = as_link(X0);
+    xs[1][t] = as_link(X1);
+    warp_pair_sync(bar_id);
+    const Su2<T> Y0 = from_link(xs[0][t ^ 32]), Y1 = from_link(xs[1][t ^ 32]);
+    if (HALF == 0) {  // K_0 = A_{0,k} U_k^+;  K_1 = A_{1,k} U_k^+ with A_{1,k} = Y^+  (k = 2, 3)
+      const Su2<T> u2 = L(2, 0, 0, 0, 0), u3 = L(3, 0, 0, 0, 0);
+      K[0] = mul_acc(mul(X0, dag(u2)), X1, dag(u3));
+      K[1] = mul_acc(mul(dag(Y0), dag(u2)), dag(Y1), dag(u3));
+    } else {  // K_k = A_{k,0} U_0^+ + A_{k,1} U_1^+ with A_{k,0} = A_{0,k}^+ = Y^+  (k = 2, 3)
+      const Su2<T> u0 = L(0, 0, 0, 0, 0), u1 = L(1, 0, 0, 0, 0);
+      K[0] = mul_acc(mul(dag(Y0), dag(u0)), X0, dag(u1));
+      K[1] = mul_acc(mul(dag(Y1), dag(u0)), X1, dag(u1));
+    }
+  }
+  // the plane inside the half
   {
     const Su2<T> A = mul(L(m1, E(m0, 0), E(m0, 1), E(m0, 2), E(m0, 3)),
                          dag(L(m0, E(m1, 0), E(m1, 1), E(m1, 2), E(m1, 3))));
-    K[0] = mul(A, dag(L(m1, 0, 0, 0, 0)));
-    K[1] = mul(dag(A), dag(L(m0, 0, 0, 0, 0)));
+    K[0] = mul_acc(K[0], A, dag(L(m1, 0, 0, 0, 0)));
+    K[1] = mul_acc(K[1], dag(A), dag(L(m0, 0, 0, 0, 0)));
   }
+  // backward staples U_nu(x+mu-nu)^+ U_mu(x-nu)^+ U_nu(x-nu), nu outermost: U_nu(x-nu) is
+  // loaded once for both links of the half (each K[j] still sums its staples in order of nu)
 #pragma unroll
-  for (int j = 0; j < 2; j++) {
-    const int mu = m0 + j;
+  for (int nu = 0; nu < 4; nu++) {
+    const Su2<T> c = L(nu, -E(nu, 0), -E(nu, 1), -E(nu, 2), -E(nu, 3));
 #pragma unroll
-    for (int nu = 0; nu < 4; nu++) {
+    for (int j = 0; j < 2; j++) {
+      const int mu = m0 + j;
       if (nu == mu) continue;
       const Su2<T> e = L(nu, E(mu, 0) - E(nu, 0), E(mu, 1) - E(nu, 1), E(mu, 2) - E(nu, 2),
                          E(mu, 3) - E(nu, 3));
       const Su2<T> h = L(mu, -E(nu, 0), -E(nu, 1), -E(nu, 2), -E(nu, 3));
-      const Su2<T> c = L(nu, -E(nu, 0), -E(nu, 1), -E(nu, 2), -E(nu, 3));
       K[j] = mul_acc(K[j], mul(dag(e), dag(h)), c);
     }
   }
-  warp_pair_sync(bar_id);
-  const Su2<T> Y0 = xs[t ^ 32][0], Y1 = xs[t ^ 32][1];
-  if (HALF == 0) {
-    const Su2<T> u2 = L(2, 0, 0, 0, 0), u3 = L(3, 0, 0, 0, 0);
-    K[0] = mul_acc(K[0], X0, dag(u2));
-    K[0] = mul_acc(K[0], X1, dag(u3));
-    K[1] = mul_acc(K[1], dag(Y0), dag(u2));
-    K[1] = mul_acc(K[1], dag(Y1), dag(u3));
-  } else {
-    const Su2<T> u0 = L(0, 0, 0, 0, 0), u1 = L(1, 0, 0, 0, 0);
-    K[0] = mul_acc(K[0], dag(Y0), dag(u0));
-    K[0] = mul_acc(K[0], X0, dag(u1));
-    K[1] = mul_acc(K[1], dag(Y1), dag(u0));
-    K[1] = mul_acc(K[1], X1, dag(u1));
-  }
   if (!valid) return 0.;
   const size_t self = (size_t)p * g.Vh + cb;
-  const size_t NL = 4 * (size_t)V;
   double k2 = 0.;
 #pragma unroll
   for (int j = 0; j < 2; j++)
-    k2 += finish_link<T>(L(m0 + j, 0, 0, 0, 0), K[j], (m0 + j) * (size_t)V + self, NL, P, extra,
-                         f, scale_, mode, Uout, dt_upd);
+    k2 += finish_link<T>(L(m0 + j, 0, 0, 0, 0), K[j], (m0 + j) * V + self, NL, P, extra, f,
+                         scale_, mode, Uout, dt_upd);
   return k2;
 }
 

@@ -141,6 +141,8 @@ __device__ __forceinline__ void st_link(Link64 *p, const Su2<double> &u) {
                "d"(u.br), "d"(u.bi)
                : "memory");
 }
+// The FP32 load is left to the compiler (__ldg) rather than written as inline PTX: a link it
+// can no longer keep in a register it may then load again (an L1 hit) instead of spilling.
 __device__ __forceinline__ Su2<float> ld_link(const Link32 *p) {
   const float4 v = __ldg(p);
   return Su2<float>{v.x, v.y, v.z, v.w};
@@ -217,7 +219,10 @@ __device__ __forceinline__ Su2<double> restore_su(const Su2<double> &u) {
 //   cos a = sum_k (-1)^k a^2k/(2k)!,   sin(a)/a = sum_k (-1)^k a^2k/(2k+1)!.
 // FP64 keeps k <= 7 (first omitted terms below 1e-18), FP32 k <= 4 (below 3e-10).  Larger
 // arguments take the square root and sincos.  At alpha = 0 the reference divides 0/0; here
-// the limit (the identity) is returned.
+// the limit (the identity) is returned.  The large-argument branch evaluates sincospi(alpha/pi):
+// the pi-scaled reduction is exact, whereas sincos keeps a local array for its slow
+// reduction path, whose stack frame costs every thread local-memory traffic even when the
+// branch is never taken.
 namespace detail {
 // n! is exact in double for n <= 18, so (+-1)/n! below is the correctly rounded coefficient
 __host__ __device__ constexpr double fact(int n) { return n <= 1 ? 1.0 : n * fact(n - 1); }
@@ -251,7 +256,7 @@ __device__ __forceinline__ Su2<double> exp_alg(double a, double b, double c) {
   } else {
     const double alpha = sqrt(t2);
     double s;
-    sincos(alpha, &s, &co);
+    sincospi(alpha * 0.318309886183790671537767526745, &s, &co);
     f = s / alpha;
   }
   return Su2<double>{co, f * c, f * b, f * a};
@@ -264,7 +269,7 @@ __device__ __forceinline__ Su2<float> exp_alg(float a, float b, float c) {
   } else {
     const float alpha = sqrtf(t2);
     float s;
-    sincosf(alpha, &s, &co);
+    sincospif(alpha * 0.318309886183790671538f, &s, &co);
     f = s / alpha;
   }
   return Su2<float>{co, f * c, f * b, f * a};

@@ -37,7 +37,6 @@ struct su2b_ctx {
   su2b::TrajDev *traj = nullptr;
   su2b::TrajParams *tparams = nullptr, *h_tparams = nullptr;
   unsigned long long *counts = nullptr;
-  unsigned *sched = nullptr;  // SM-local tile schedule of the force kernel (zeroed at creation)
 
   // pinned host mirrors
   double *h_red = nullptr;

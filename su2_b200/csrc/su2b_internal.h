@@ -39,18 +39,14 @@ enum ForceMode : int {
 };
 // launch shapes of the SU(2) force kernel (threads per block, minimum resident blocks per
 // SM, which caps registers): one thread per site 0 (256,4) 1 (128,8) 2 (128,4) 3 (128,6)
-// 4 (256,2) 5 (256,3) 7 (64,16); two threads per site 6 split, 8 xsplit (128,8); 9 one thread
-// per link; 10 xsplit with per-thread neighbour offsets; 11 the same on persistent blocks
-// with the SM-local tile schedule (needs the sched scratch of SCHED_WORDS words, zeroed
-// once; without it variant 11 runs as 10)
-constexpr int FORCE_VARIANTS = 12;
-constexpr int SCHED_MAX_REGIONS = 1024;
-constexpr int SCHED_WORDS = 2 * SCHED_MAX_REGIONS + 32;
+// 4 (256,2) 5 (256,3) 7 (64,16); two threads per site 6 split, 8 xsplit, 10 xsplit with the
+// pair's exchange first, all (128,8); 9 one thread per link
+constexpr int FORCE_VARIANTS = 11;
 template <class T>
 cudaError_t force_update(const Geom &g, const void *U, int group, T *P, const T *extra, double f,
                          double scale, double xi, int mode, double *kin_part, int *nblocks,
                          void *Uout, double dt_upd, cudaStream_t s, int variant = 1,
-                         bool pdl = false, unsigned *sched = nullptr);
+                         bool pdl = false);
 
 // U = exp(dt P) U (update_gauge.hh:8-16); with round_dn > 0 the links are rounded first,
 // U = exp(dt P) round(U) (round_and_update_gauge, update_gauge.hh:20-26)
