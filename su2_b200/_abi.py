@@ -117,16 +117,16 @@ SIGNATURES = {
     "su2b_tune_get": (i32, [_P, i32, C.POINTER(C.c_int)]),
     "su2b_tune_set": (i32, [_P, i32, i32]),
 }
-FORCE_VARIANTS = 11
+FORCE_VARIANTS = 10
 BATCH_VARIANTS = 4
 # (threads per block, min blocks per SM) of the batched force kernel
 BATCH_SHAPES = [(64, 8), (128, 4), (128, 6), (256, 3)]
 # (threads per block, min resident blocks per SM) of the force kernel's launch shapes; the
 # "split" shapes run two threads per site (d = 4; other d use (128, 8)), "xsplit" with the
-# cross-plane products formed once per site and swapped in shared memory ("xsplit_e": with
-# that exchange at the start of the body); the anisotropic action always runs (128, 6)
+# cross-plane products formed once per site and swapped in shared memory; the anisotropic
+# action always runs (128, 6)
 FORCE_SHAPES = [(256, 4), (128, 8), (128, 4), (128, 6), (256, 2), (256, 3), ("split", 128, 8),
-                (64, 16), ("xsplit", 128, 8), ("link", 128, 6), ("xsplit_e", 128, 8)]
+                (64, 16), ("xsplit", 128, 8), ("link", 128, 6)]
 
 K_FORCE, K_UPDATE, K_PLAQUETTE, K_MOMENTA, K_RESTORE, K_METROPOLIS, K_CLOVER, K_STAGGERED, \
     K_OTHER = range(9)

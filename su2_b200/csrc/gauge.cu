@@ -689,34 +689,6 @@ __global__ void __launch_bounds__(NT, MINB)
   }
 }
 
-// xsplit with the pair's exchange at the start of the body (force_half_xe)
-template <class T, int NT, int MINB>
-__global__ void __launch_bounds__(NT, MINB)
-  k_force_su2_xsplit_e(Geom g, const LinkT<T> *__restrict__ U, T *__restrict__ P,
-                       const T *__restrict__ extra, T f, T scale_, int mode, T wt, T ws,
-                       double *kin_part, LinkT<T> *__restrict__ Uout, T dt_upd) {
-  static_assert(NT == 128, "two warp pairs per block, hardware barriers 1 and 2");
-  __shared__ double sh[NT / 32];
-  __shared__ LinkT<T> xs[2][NT];
-  pdl_trigger();
-  pdl_wait();
-  const int w = threadIdx.x >> 5;
-  const int half = w & 1, p = (w >> 1) & 1;
-  const int cb = blockIdx.x * (NT / 4) + (w >> 2) * 32 + (threadIdx.x & 31);
-  const bool valid = cb < g.Vh;
-  const int cbc = valid ? cb : g.Vh - 1;
-  const int bar_id = 1 + (w >> 1);
-  const double k2 =
-    half == 0 ? force_half_xe<T, 0>(g, U, P, extra, f, scale_, mode, Uout, dt_upd, p, cbc,
-                                    valid, xs, bar_id)
-              : force_half_xe<T, 1>(g, U, P, extra, f, scale_, mode, Uout, dt_upd, p, cbc,
-                                    valid, xs, bar_id);
-  if (mode & FM_KINETIC) {
-    const double r = block_sum<NT>(k2, sh);
-    if (threadIdx.x == 0) kin_part[blockIdx.x] = r;
-  }
-}
-
 // launch with the programmatic-stream-serialization attribute when pdl is set
 template <typename... KArgs, typename... Args>
 cudaError_t launch_force(void (*kern)(KArgs...), dim3 grid, int nt, cudaStream_t s, bool pdl,
@@ -810,18 +782,6 @@ cudaError_t force_update(const Geom &g, const void *U, int group, T *P, const T 
       launch_force(k_force_su2_xsplit<T, NTV, MB>, grid, NTV, s, pdl, SU2B_FORCE_ARGS);    \
     if (e_ != cudaSuccess) return e_;                                                      \
   } while (0)
-#define SU2B_FORCE_XSPLIT_E(NTV, MB)                                                         \
-  do {                                                                                     \
-    if (g.nd != 4) {                                                                       \
-      SU2B_FORCE_LAUNCH(128, 8, false);                                                    \
-      break;                                                                               \
-    }                                                                                      \
-    const dim3 grid(cdiv(g.Vh, NTV / 4));                                                  \
-    nb = grid.x;                                                                           \
-    const cudaError_t e_ =                                                                 \
-      launch_force(k_force_su2_xsplit_e<T, NTV, MB>, grid, NTV, s, pdl, SU2B_FORCE_ARGS);  \
-    if (e_ != cudaSuccess) return e_;                                                      \
-  } while (0)
     // the anisotropic action (rare) runs one launch shape; the tuned shapes are isotropic and
     // carry no code for the plane weights
     if (aniso) {
@@ -837,7 +797,6 @@ cudaError_t force_update(const Geom &g, const void *U, int group, T *P, const T 
         case 6: SU2B_FORCE_SPLIT(128, 8); break;
         case 8: SU2B_FORCE_XSPLIT(128, 8); break;
         case 9: SU2B_FORCE_LINK(6); break;
-        case 10: SU2B_FORCE_XSPLIT_E(128, 8); break;
         default: SU2B_FORCE_LAUNCH(64, 16, false); break;
       }
     }
@@ -845,7 +804,6 @@ cudaError_t force_update(const Geom &g, const void *U, int group, T *P, const T 
 #undef SU2B_FORCE_SPLIT
 #undef SU2B_FORCE_XSPLIT
 #undef SU2B_FORCE_LINK
-#undef SU2B_FORCE_XSPLIT_E
 #undef SU2B_FORCE_ARGS
     if (nblocks) *nblocks = nb;
   } else {

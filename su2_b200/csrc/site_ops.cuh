@@ -349,98 +349,6 @@ __device__ __forceinline__ double force_half_x(const Geom &g, const LinkT<T> *__
   return k2;
 }
 
-// force_half_x with the pair's exchange first: each thread forms its two cross products,
-// both warps of the pair meet at the barrier at once, and the four cross-plane staples start
-// the staple sums.  The cross products, the partner's and the own links they multiply are
-// then dead before the in-half plane and the backward staples, so fewer values stay live
-// through the longest part of the body; the backward staples run with nu outermost so that
-// U_nu(x-nu) is loaded once for both links (24 link loads per thread instead of 26).  Same
-// products as force_half_x, summed in another order.
-template <class T, int HALF>
-__device__ __forceinline__ double force_half_xe(const Geom &g, const LinkT<T> *__restrict__ U,
-                                                T *__restrict__ P, const T *__restrict__ extra,
-                                                T f, T scale_, int mode,
-                                                LinkT<T> *__restrict__ Uout, T dt_upd, int p,
-                                                int cb, bool valid, XchgT<T> xs,
-                                                int bar_id) {
-  const Site s = site_from_eo(g, p, cb);
-  const size_t V = (size_t)g.V, NL = 4 * V;
-  int fo[4], bo[4];
-#pragma unroll
-  for (int d = 0; d < 4; d++) {
-    fo[d] = fwd(g, s, d);
-    bo[d] = bwd(g, s, d);
-  }
-  auto L = [&](int mu, int o0, int o1, int o2, int o3) -> Su2<T> {
-    const int o[4] = {o0, o1, o2, o3};
-    int lex = s.lex, odd = 0;
-#pragma unroll
-    for (int d = 0; d < 4; d++) {
-      if (o[d] > 0) lex += fo[d];
-      if (o[d] < 0) lex += bo[d];
-      odd ^= (o[d] != 0);
-    }
-    return ld_link(U + (size_t)mu * V + eo_of(g, lex, p ^ odd));
-  };
-  auto E = [](int d, int k) { return d == k ? 1 : 0; };
-  constexpr int m0 = 2 * HALF, m1 = 2 * HALF + 1;
-  const int t = threadIdx.x;
-  Su2<T> K[2];
-  {
-    Su2<T> X0, X1;
-    if (HALF == 0) {
-      X0 = mul(L(2, 1, 0, 0, 0), dag(L(0, 0, 0, 1, 0)));  // A_{0,2}
-      X1 = mul(L(3, 1, 0, 0, 0), dag(L(0, 0, 0, 0, 1)));  // A_{0,3}
-    } else {
-      X0 = mul(L(1, 0, 0, 1, 0), dag(L(2, 0, 1, 0, 0)));  // A_{2,1}
-      X1 = mul(L(1, 0, 0, 0, 1), dag(L(3, 0, 1, 0, 0)));  // A_{3,1}
-    }
-    xs[0][t] = as_link(X0);
-    xs[1][t] = as_link(X1);
-    warp_pair_sync(bar_id);
-    const Su2<T> Y0 = from_link(xs[0][t ^ 32]), Y1 = from_link(xs[1][t ^ 32]);
-    if (HALF == 0) {  // K_0 = A_{0,k} U_k^+;  K_1 = A_{1,k} U_k^+ with A_{1,k} = Y^+  (k = 2, 3)
-      const Su2<T> u2 = L(2, 0, 0, 0, 0), u3 = L(3, 0, 0, 0, 0);
-      K[0] = mul_acc(mul(X0, dag(u2)), X1, dag(u3));
-      K[1] = mul_acc(mul(dag(Y0), dag(u2)), dag(Y1), dag(u3));
-    } else {  // K_k = A_{k,0} U_0^+ + A_{k,1} U_1^+ with A_{k,0} = A_{0,k}^+ = Y^+  (k = 2, 3)
-      const Su2<T> u0 = L(0, 0, 0, 0, 0), u1 = L(1, 0, 0, 0, 0);
-      K[0] = mul_acc(mul(dag(Y0), dag(u0)), X0, dag(u1));
-      K[1] = mul_acc(mul(dag(Y1), dag(u0)), X1, dag(u1));
-    }
-  }
-  // the plane inside the half
-  {
-    const Su2<T> A = mul(L(m1, E(m0, 0), E(m0, 1), E(m0, 2), E(m0, 3)),
-                         dag(L(m0, E(m1, 0), E(m1, 1), E(m1, 2), E(m1, 3))));
-    K[0] = mul_acc(K[0], A, dag(L(m1, 0, 0, 0, 0)));
-    K[1] = mul_acc(K[1], dag(A), dag(L(m0, 0, 0, 0, 0)));
-  }
-  // backward staples U_nu(x+mu-nu)^+ U_mu(x-nu)^+ U_nu(x-nu), nu outermost: U_nu(x-nu) is
-  // loaded once for both links of the half (each K[j] still sums its staples in order of nu)
-#pragma unroll
-  for (int nu = 0; nu < 4; nu++) {
-    const Su2<T> c = L(nu, -E(nu, 0), -E(nu, 1), -E(nu, 2), -E(nu, 3));
-#pragma unroll
-    for (int j = 0; j < 2; j++) {
-      const int mu = m0 + j;
-      if (nu == mu) continue;
-      const Su2<T> e = L(nu, E(mu, 0) - E(nu, 0), E(mu, 1) - E(nu, 1), E(mu, 2) - E(nu, 2),
-                         E(mu, 3) - E(nu, 3));
-      const Su2<T> h = L(mu, -E(nu, 0), -E(nu, 1), -E(nu, 2), -E(nu, 3));
-      K[j] = mul_acc(K[j], mul(dag(e), dag(h)), c);
-    }
-  }
-  if (!valid) return 0.;
-  const size_t self = (size_t)p * g.Vh + cb;
-  double k2 = 0.;
-#pragma unroll
-  for (int j = 0; j < 2; j++)
-    k2 += finish_link<T>(L(m0 + j, 0, 0, 0, 0), K[j], (m0 + j) * V + self, NL, P, extra, f,
-                         scale_, mode, Uout, dt_upd);
-  return k2;
-}
-
 // plaquettes of one site: sums over planes mu<nu of ReTr U_mu(x) U_nu(x+mu) U_mu(x+nu)^+
 // U_nu(x)^+ (flat-gauge_energy.hpp:31-94), FP64 products; {full, spatial (mu >= 1), xi-weighted}
 template <class T, int ND>

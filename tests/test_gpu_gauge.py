@@ -454,28 +454,6 @@ def test_every_force_launch_shape_is_exact(gpu, orc, precision, dims):
 
 
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
-@pytest.mark.parametrize("dims", [(8, 8, 8, 8), (6, 6, 6, 6), (16, 8, 8, 16)],
-                         ids=["8^4", "6^4", "16x8x8x16"])
-def test_early_exchange_shape_follows_xsplit(gpu, orc, precision, dims):
-    """The xsplit force with the warp pair's exchange first forms xsplit's products and sums
-    them in another order: a chain of graph-replayed trajectories (accepts and rejects)
-    takes the same decisions, with Delta H and the links equal up to that rounding."""
-    shapes = gpu._abi.FORCE_SHAPES
-    U = hot(orc, 0, dims, 4)
-    out = {}
-    for name in ("xsplit", "xsplit_e"):
-        with make(gpu, 0, dims, 4, beta=2.3, precision=precision) as c:
-            c.upload(U)
-            c.force_variant = shapes.index((name, 128, 8))
-            res = [c.md_update("omf2", 4, 1.0, seed=3, traj=k) for k in range(12)]
-            out[name] = ([(r.accepted, r.dH) for r in res], c.download())
-    tol = 1e-9 if precision == "fp64" else 1e-3
-    for (a, da), (b, db) in zip(out["xsplit"][0], out["xsplit_e"][0]):
-        assert a == b and da == pytest.approx(db, abs=tol)
-    assert rel(out["xsplit_e"][1], out["xsplit"][1]) < (1e-12 if precision == "fp64" else 1e-5)
-
-
-@pytest.mark.parametrize("precision", ["fp64", "mixed"])
 @pytest.mark.parametrize("dims,nd", [((6, 1, 1, 4), 2), ((4, 6, 1, 4), 3), ((6, 4, 1, 6), 3)],
                          ids=["6x4-d2", "4x6x4-d3", "6x4x6-d3"])
 def test_every_force_launch_shape_below_four_dims(gpu, orc, precision, dims, nd):
