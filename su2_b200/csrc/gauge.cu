@@ -15,30 +15,60 @@ namespace {
 inline int cdiv(long a, long b) { return (int)((a + b - 1) / b); }
 
 // ------------------------------------------------------------------------------------
-// layout conversion: thread i walks the reference order i = lex*nd + mu
+// layout conversion between the reference's host order and the even/odd device layout
+// SU(2) links go through shared memory, both sides coalesced: a block takes a tile of
+// 64 consecutive reference sites (32 half-indices h in both parities).  The device side is
+// read (or written) as 32 consecutive links per direction and parity -- the site of
+// half-index h and parity p is 2h or 2h+1, whichever has parity p -- and the host side as
+// the tile's 64 nd consecutive 32-byte records.
+constexpr int CONV_TILE = 64;  // sites per block; 64 nd <= 256 threads
+__device__ __forceinline__ int tile_lex(const Geom &g, int h, int p) {
+  const Site s = site_from_lex(g, 2 * h);
+  return 2 * h + (s.p != p);
+}
 template <class T>
-__global__ void k_links_from_host_su2(Geom g, const double *__restrict__ aos, LinkT<T> *U) {
-  const long n = (long)g.V * g.nd;
-  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n;
-       i += (long)gridDim.x * blockDim.x) {
-    const int lex = (int)(i / g.nd), mu = (int)(i - (long)lex * g.nd);
-    const Site s = site_from_lex(g, lex);
-    const double *src = aos + 4 * i;
-    Su2<double> u{src[0], src[1], src[2], src[3]};
-    st_link(U + (size_t)mu * g.V + eo_of(g, lex, s.p), from64<T>(u));
+__global__ void __launch_bounds__(256)
+  k_links_to_host_tiled(Geom g, const LinkT<T> *__restrict__ U, double *aos) {
+  __shared__ Link64 tile[CONV_TILE * 4];
+  const int lex0 = blockIdx.x * CONV_TILE, t = threadIdx.x;
+  const int nl = CONV_TILE * g.nd;
+  if (t < nl) {
+    const int mu = t / CONV_TILE, r = t % CONV_TILE, p = r / 32;
+    const int h = lex0 / 2 + (r % 32);
+    if (h < g.Vh) {
+      const int lex = tile_lex(g, h, p);
+      const Su2<double> u = to64(ld_link(U + (size_t)mu * g.V + (size_t)p * g.Vh + h));
+      tile[(lex - lex0) * g.nd + mu] = Link64{u.ar, u.ai, u.br, u.bi};
+    }
+  }
+  __syncthreads();
+  const long i = (long)lex0 * g.nd + t;
+  if (t < nl && i < (long)g.V * g.nd) {
+    const Link64 v = tile[t];
+    st_link((Link64 *)aos + i, Su2<double>{v.ar, v.ai, v.br, v.bi});
   }
 }
 template <class T>
-__global__ void k_links_to_host_su2(Geom g, const LinkT<T> *__restrict__ U, double *aos) {
-  const long n = (long)g.V * g.nd;
-  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n;
-       i += (long)gridDim.x * blockDim.x) {
-    const int lex = (int)(i / g.nd), mu = (int)(i - (long)lex * g.nd);
-    const Site s = site_from_lex(g, lex);
-    const Su2<double> u = to64(ld_link_rw(U + (size_t)mu * g.V + eo_of(g, lex, s.p)));
-    st_link((Link64 *)aos + i, u);  // one 32-byte store (aos is 32-byte aligned)
+__global__ void __launch_bounds__(256)
+  k_links_from_host_tiled(Geom g, const double *__restrict__ aos, LinkT<T> *U) {
+  __shared__ Link64 tile[CONV_TILE * 4];
+  const int lex0 = blockIdx.x * CONV_TILE, t = threadIdx.x;
+  const int nl = CONV_TILE * g.nd;
+  const long i = (long)lex0 * g.nd + t;
+  if (t < nl && i < (long)g.V * g.nd) tile[t] = ((const Link64 *)aos)[i];
+  __syncthreads();
+  if (t < nl) {
+    const int mu = t / CONV_TILE, r = t % CONV_TILE, p = r / 32;
+    const int h = lex0 / 2 + (r % 32);
+    if (h < g.Vh) {
+      const int lex = tile_lex(g, h, p);
+      const Link64 v = tile[(lex - lex0) * g.nd + mu];
+      st_link(U + (size_t)mu * g.V + (size_t)p * g.Vh + h,
+              from64<T>(Su2<double>{v.ar, v.ai, v.br, v.bi}));
+    }
   }
 }
+
 // U(1) angles and adjoint fields: na reals per link, SoA on the device
 template <class T>
 __global__ void k_adj_from_host(Geom g, const double *__restrict__ aos, T *P, int na) {
@@ -80,8 +110,13 @@ __global__ void k_spinor_to_host(Geom g, const double2 *__restrict__ psi, double
 // ------------------------------------------------------------------------------------
 // plaquettes: per site, sum over planes mu<nu of ReTr U_mu(x) U_nu(x+mu) U_mu(x+nu)^+ U_nu(x)^+
 // (flat-gauge_energy.hpp:31-94), FP64 products.  Partials {full, spatial, xi-weighted}.
+// FP64 links take twice the registers of FP32 ones: half the resident blocks, no spills
+template <class T, int NT> constexpr int plaq_min_blocks() {
+  return sizeof(T) == 8 ? 512 / NT : 1024 / NT;
+}
+
 template <class T, int ND, int NT>
-__global__ void __launch_bounds__(NT, 1024 / NT)
+__global__ void __launch_bounds__(NT, plaq_min_blocks<T, NT>())
   k_plaq_su2(Geom g, const LinkT<T> *__restrict__ U, double xi, double *part) {
   __shared__ double shk[4 * (NT / 32)];
   const int w = threadIdx.x >> 5, p = w & 1;
@@ -104,7 +139,7 @@ __global__ void __launch_bounds__(NT, 1024 / NT)
 // Without PLAQ only the momenta and |P|^2 (the start plaquettes are known from the previous
 // trajectory); the partial layout stays the same, so the kinetic sums are identical.
 template <class T, int ND, int NT, bool PLAQ = true>
-__global__ void __launch_bounds__(NT, 1024 / NT)
+__global__ void __launch_bounds__(NT, plaq_min_blocks<T, NT>())
   k_momenta_plaq_su2(Geom g, const LinkT<T> *__restrict__ U, T *__restrict__ P,
                      const TrajParams *__restrict__ tp, double xi, double *part) {
   __shared__ double shk[4 * (NT / 32)];
@@ -568,7 +603,7 @@ cudaError_t links_from_host(const Geom &g, const double *aos, void *U, int group
                             cudaStream_t s) {
   const size_t n = (size_t)g.V * g.nd;
   if (group == 0)
-    k_links_from_host_su2<T><<<flat_grid(n, 256), 256, 0, s>>>(g, aos, (LinkT<T> *)U);
+    k_links_from_host_tiled<T><<<cdiv(g.V, CONV_TILE), 256, 0, s>>>(g, aos, (LinkT<T> *)U);
   else
     k_adj_from_host<double><<<flat_grid(n, 256), 256, 0, s>>>(g, aos, (double *)U, 1);
   return cudaGetLastError();
@@ -578,7 +613,7 @@ cudaError_t links_to_host(const Geom &g, const void *U, double *aos, int group,
                           cudaStream_t s) {
   const size_t n = (size_t)g.V * g.nd;
   if (group == 0)
-    k_links_to_host_su2<T><<<flat_grid(n, 256), 256, 0, s>>>(g, (const LinkT<T> *)U, aos);
+    k_links_to_host_tiled<T><<<cdiv(g.V, CONV_TILE), 256, 0, s>>>(g, (const LinkT<T> *)U, aos);
   else
     k_adj_to_host<double><<<flat_grid(n, 256), 256, 0, s>>>(g, (const double *)U, aos, 1);
   return cudaGetLastError();

@@ -4,6 +4,7 @@
 // All three read the device links in the even/odd layout; products are accumulated in FP64
 // whatever the link storage (FP32 links of a mixed-precision context are promoted), and sums
 // go through per-block partials reduced in a fixed order.
+#include <utility>
 #include "site_ops.cuh"
 #include "su2b.h"
 #include "su2b_ctx.h"
@@ -137,8 +138,10 @@ template <class T, int NT>
 __global__ void __launch_bounds__(NT)
   k_ape(Geom g, const void *__restrict__ Uin, void *__restrict__ Uout, int group, double alpha,
         double beta, int start) {
-  const int lex = blockIdx.x * NT + threadIdx.x;
-  const int i = blockIdx.y;
+  // consecutive blocks take the directions of one band of sites, so the neighbour links a
+  // band reads for one direction are still in L2 when the next direction reads them
+  const int i = blockIdx.x % g.nd;
+  const int lex = (blockIdx.x / g.nd) * NT + threadIdx.x;
   if (lex >= g.V) return;
   const Site s = site_from_lex(g, lex);
   const size_t self = (size_t)i * g.V + (size_t)s.p * g.Vh + (lex >> 1);
@@ -268,7 +271,7 @@ extern "C" int su2b_ape_smear(su2b_ctx *ctx, double alpha, int spatial) {
     return su2b_fail(ctx, SU2B_ERR_INVALID, "APE smearing is not possible in 2 dimensions");
   SU2B_CKS(su2b_ensure_aux(ctx));
   const double beta = (1.0 - alpha) / (double)(2 * (ctx->g.nd - 1 - start));
-  const dim3 grid((ctx->g.V + NT_O - 1) / NT_O, ctx->g.nd);
+  const dim3 grid(((ctx->g.V + NT_O - 1) / NT_O) * ctx->g.nd);
   if (ctx->link64)
     k_ape<double, NT_O><<<grid, NT_O, 0, ctx->stream>>>(ctx->g, ctx->U, ctx->U_aux, ctx->group,
                                                         alpha, beta, start);
@@ -277,8 +280,8 @@ extern "C" int su2b_ape_smear(su2b_ctx *ctx, double alpha, int spatial) {
                                                        alpha, beta, start);
   SU2B_CK(cudaGetLastError());
   ctx->launches++;
-  SU2B_CK(cudaMemcpyAsync(ctx->U, ctx->U_aux, ctx->link_bytes() * ctx->NL, cudaMemcpyDeviceToDevice,
-                     ctx->stream));
+  // the smeared field becomes the context's field by exchanging the two buffers (no copy)
+  std::swap(ctx->U, ctx->U_aux);
   SU2B_CK(cudaStreamSynchronize(ctx->stream));
   ctx->phases_valid = false;
   return SU2B_OK;

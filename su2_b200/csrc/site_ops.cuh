@@ -349,25 +349,36 @@ __device__ __forceinline__ double force_half_x(const Geom &g, const LinkT<T> *__
   return k2;
 }
 
+// ReTr U_mu(x) U_nu(x+mu) (U_nu(x) U_mu(x+nu))^+ of one plaquette, in the storage precision:
+// FP64 links in FP64; FP32 links (mixed precision) with the products in FP32 (the trace of
+// one plaquette to about 1e-7 relative), returned in FP64 for the FP64 sums
+template <class T>
+__device__ __forceinline__ double plaq_trace(const Su2<T> &um, const Su2<T> &a,
+                                             const Su2<T> &un, const Su2<T> &b) {
+  return (double)retr_mul(mul(um, a), dag(mul(un, b)));
+}
+
 // plaquettes of one site: sums over planes mu<nu of ReTr U_mu(x) U_nu(x+mu) U_mu(x+nu)^+
-// U_nu(x)^+ (flat-gauge_energy.hpp:31-94), FP64 products; {full, spatial (mu >= 1), xi-weighted}
+// U_nu(x)^+ (flat-gauge_energy.hpp:31-94), each plaquette's trace in the storage precision
+// (plaq_trace) and every sum in FP64; {full, spatial (mu >= 1), xi-weighted}.  The site's own
+// links are read where each plane needs them (L1 hits after the first), so that no more than
+// one plane's four links stay live.
 template <class T, int ND>
 __device__ __forceinline__ void plaq_site(const Geom &g, const LinkT<T> *__restrict__ U, int p,
                                           int cb, double xi, double &full, double &spat,
                                           double &wsum) {
   const Site s = site_from_eo(g, p, cb);
-  Su2<double> u[ND];
-#pragma unroll
-  for (int mu = 0; mu < ND; mu++) u[mu] = to64(ld_link(U + (size_t)mu * g.V + p * g.Vh + cb));
+  const LinkT<T> *__restrict__ own = U + (size_t)p * g.Vh + cb;
 #pragma unroll
   for (int mu = 0; mu < ND - 1; mu++) {
     const int lpm = s.lex + fwd(g, s, mu);
 #pragma unroll
     for (int nu = mu + 1; nu < ND; nu++) {
       const int lpn = s.lex + fwd(g, s, nu);
-      const Su2<double> A = to64(ld_link(U + (size_t)nu * g.V + eo_of(g, lpm, 1 - p)));
-      const Su2<double> B = to64(ld_link(U + (size_t)mu * g.V + eo_of(g, lpn, 1 - p)));
-      const double tr = retr_mul(mul(u[mu], A), dag(mul(u[nu], B)));
+      const Su2<T> A = ld_link(U + (size_t)nu * g.V + eo_of(g, lpm, 1 - p));
+      const Su2<T> B = ld_link(U + (size_t)mu * g.V + eo_of(g, lpn, 1 - p));
+      const double tr = plaq_trace<T>(ld_link(own + (size_t)mu * g.V), A,
+                                      ld_link(own + (size_t)nu * g.V), B);
       full += tr;
       if (mu >= 1) spat += tr;
       wsum += (((mu == 0) ^ (nu == 0)) ? 1.0 / xi : xi) * tr;

@@ -340,10 +340,12 @@ def test_full_size_32_4(gpu, orc, precision):
     tol = 1e-12 if precision == "fp64" else 1e-5
     with make(gpu, group, dims, nd, beta=2.4, precision=precision) as c:
         c.upload(U)
-        # reductions are FP64 over the stored links (FP32-rounded in mixed precision)
+        # the sums are FP64 over the stored links (FP32-rounded in mixed precision); mixed
+        # precision forms each plaquette's products in FP32 (about 1e-7 per plaquette, a
+        # few 1e-11 of the sum over 6.3 M plaquettes)
         Us = U if precision == "fp64" else U.astype(np.float32).astype(np.float64)
         assert c.gauge_energy() == pytest.approx(orc.gauge_energy(group, dims, nd, Us),
-                                                 rel=1e-12)
+                                                 rel=1e-12 if precision == "fp64" else 1e-9)
         F = orc.gauge_derivative(group, dims, nd, 2.4, U)
         assert rel(c.derivative(), F) < tol
         r = c.md_update("omf2", 4, 0.2, seed=11, traj=1, revtest=True, accept_reject=False)
