@@ -617,14 +617,27 @@ def profile_run(args):
                 u1.md_update("omf2", 2, 0.2, seed=7, traj=k, fermion_mass=0.05, cg_tol=1e-10)
             batch.md_update("leapfrog", 10, 1.0, traj=k)
 
+    def launches():  # over every context of the loop
+        n = c.kernel_launches()
+        if u1 is not None:
+            n += u1.kernel_launches() + batch.kernel_launches()
+        return n
+
     for k in range(args.warmup):
         step(k)
     c.synchronize()
-    n0 = c.kernel_launches()
+    if u1 is not None:
+        u1.synchronize()
+        torch.cuda.synchronize()
+    n0 = launches()
     for k in range(args.steps):
+        # an NVTX range per timed step, so that a profiler can select exactly these launches
+        # (ncu --nvtx --nvtx-include "profile_step/")
+        torch.cuda.nvtx.range_push("profile_step")
         step(args.warmup + k)
+        torch.cuda.nvtx.range_pop()
     c.synchronize()
-    n1 = c.kernel_launches()
+    n1 = launches()
     print(json.dumps({"profile_run": f"SU(2) d=4 {L}^4, beta={BETA}", "op": args.profile_op,
                       "precision": args.precision,
                       "force_variant": su2_b200._abi.FORCE_SHAPES[args.force_variant],

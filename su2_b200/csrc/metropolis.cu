@@ -5,16 +5,76 @@
 // of other directions only, so all of them update independently and in any order.  A sweep
 // is 2*nd launches.  Per link: staples once (get_staples.hh:26-80), then N_hit proposals
 // U -> U R with R = random_element(delta) (random_element.hh:9-34), dS = beta/Nc (ReTr(U K) -
-// ReTr(U R K)), accept with min(1, exp(-dS)), restoreSU after each accepted hit.  All
-// arithmetic is FP64 whatever the link storage.  Random numbers: one Philox4x32-10 draw per
+// ReTr(U R K)), accept with min(1, exp(-dS)), restoreSU after each accepted hit.  FP64 links:
+// all arithmetic in FP64.  FP32 links (mixed precision): the staple sum, the proposal R and
+// the product U R in FP32; the action change dS (the traces of the FP32 values, in FP64), the
+// accept test and the reunitarisation in FP64.  Random numbers: one Philox4x32-10 draw per
 // hit, counter {reference link index, hit, sweep, TAG_METRO}: 32-bit uniforms for alpha, u,
-// theta and the accept test.
+// theta and the accept test, the same stream in both precisions.
 #include "su2b_internal.h"
 
 namespace su2b {
 namespace {
 
 template <class T> using LinkT = typename LinkOf<T>::type;
+
+// One link of a pass with FP32 storage (see the file comment); returns its accepted hits.
+template <int ND>
+__device__ __forceinline__ unsigned metro_link_fp32(const Geom &g, Link32 *__restrict__ U, int mu,
+                                                    int p, int cb, double beta_nc, double delta,
+                                                    int N_hit, uint64_t seed, uint32_t sweep,
+                                                    float wt, float ws) {
+  const Site s = site_from_eo(g, p, cb);
+  const int lpm = s.lex + fwd(g, s, mu);
+  Su2<float> K = zero_su2<float>();
+#pragma unroll
+  for (int nu = 0; nu < ND; nu++) {
+    if (nu == mu) continue;
+    const int lpn = s.lex + fwd(g, s, nu);
+    const Su2<float> A = ld_link_rw(U + (size_t)nu * g.V + eo_of(g, lpm, 1 - p));
+    const Su2<float> B = ld_link_rw(U + (size_t)mu * g.V + eo_of(g, lpn, 1 - p));
+    const Su2<float> D = ld_link_rw(U + (size_t)nu * g.V + eo_of(g, s.lex, p));
+    K = mul_acc(K, scale((nu == 0 || mu == 0) ? wt : ws, mul(A, dag(B))), dag(D));
+  }
+#pragma unroll
+  for (int nu = 0; nu < ND; nu++) {
+    if (nu == mu) continue;
+    const int b = bwd(g, s, nu);
+    const Su2<float> A = ld_link_rw(U + (size_t)nu * g.V + eo_of(g, lpm + b, p));
+    const Su2<float> B = ld_link_rw(U + (size_t)mu * g.V + eo_of(g, s.lex + b, 1 - p));
+    const Su2<float> D = ld_link_rw(U + (size_t)nu * g.V + eo_of(g, s.lex + b, 1 - p));
+    K = mul_acc(K, scale((nu == 0 || mu == 0) ? wt : ws, mul(dag(A), dag(B))), D);
+  }
+  const Su2<double> K64 = to64(K);
+  const size_t l = (size_t)mu * g.V + (size_t)p * g.Vh + cb;
+  Su2<float> u = ld_link_rw(U + l);
+  double tr_u = retr_mul(to64(u), K64);
+  const uint32_t lref = (uint32_t)s.lex * (uint32_t)g.nd + (uint32_t)mu;
+  const float d2 = (float)(2.0 * delta);
+  unsigned acc = 0;
+  for (int n = 0; n < N_hit; n++) {
+    uint32_t r[4];
+    philox(lref, (uint32_t)n, sweep, TAG_METRO, seed, r);
+    float sa, ca, st, ct;
+    sincospif(d2 * (float)u01_32(r[0]), &sa, &ca);
+    const float uu = fmaf(2.0f, (float)u01_32(r[1]), -1.0f);
+    sincospif(2.0f * (float)u01_32(r[2]), &st, &ct);
+    const float rr = sqrtf(fmaxf(0.0f, fmaf(-uu, uu, 1.0f)));
+    const Su2<float> R{ca, sa * uu, sa * rr * st, sa * rr * ct};
+    const Su2<float> uR = mul(u, R);
+    const double tr_uR = retr_mul(to64(uR), K64);
+    const double dS = beta_nc * (tr_u - tr_uR);
+    bool a = dS < 0;
+    if (!a) a = u01_32(r[3]) < exp(-dS);
+    if (a) {
+      u = from64<float>(restore_su(to64(uR)));
+      tr_u = retr_mul(to64(u), K64);
+      acc++;
+    }
+  }
+  st_link(U + l, u);
+  return acc;
+}
 
 template <class T, int ND, int NT>
 __global__ void __launch_bounds__(NT)
@@ -26,7 +86,11 @@ __global__ void __launch_bounds__(NT)
   __syncthreads();
   const int cb = blockIdx.x * NT + threadIdx.x;
   unsigned int acc = 0;
-  if (cb < g.Vh) {
+  if constexpr (sizeof(T) == 4) {
+    if (cb < g.Vh)
+      acc = metro_link_fp32<ND>(g, (Link32 *)U, mu, p, cb, beta_nc, delta, N_hit, seed, sweep,
+                                (float)wt, (float)ws);
+  } else if (cb < g.Vh) {
     const Site s = site_from_eo(g, p, cb);
     // staple sum in FP64
     const int lpm = s.lex + fwd(g, s, mu);

@@ -255,6 +255,24 @@ def test_metropolis_checkerboard(gpu, orc, group, dims, nd):
         np.testing.assert_array_equal(rates, r_want)
 
 
+@pytest.mark.parametrize("group,dims,nd", [g for g in GEOMS if g[0] == 0],
+                         ids=[i for g, i in zip(GEOMS, GEOM_IDS) if g[0] == 0])
+def test_metropolis_checkerboard_mixed_precision(gpu, orc, group, dims, nd):
+    """FP32 links: the staple sum and the proposals in FP32, dS, the accept test and the
+    reunitarisation in FP64, on the FP64 path's random stream -- the same accept decisions
+    as the oracle's FP64 replay and the links within FP32 rounding."""
+    U = hot(orc, group, dims, nd)
+    Us = U.astype(np.float32).astype(np.float64)
+    for xi in (1.0, 1.3):
+        U_want, r_want = orc.metropolis_checkerboard(group, dims, nd, 2.3, 0.3, 4, 99, 3, Us,
+                                                     xi=xi)
+        with make(gpu, group, dims, nd, beta=2.3, xi=xi, precision="mixed") as c:
+            c.upload(U)
+            rates = c.sweep(0.3, 4, 99, 3)
+            assert rel(c.download(), U_want) < 1e-5
+        np.testing.assert_array_equal(rates, r_want)
+
+
 @pytest.mark.parametrize("group,dims,nd", [GEOMS[0], GEOMS[4]], ids=[GEOM_IDS[0], GEOM_IDS[4]])
 def test_gauge_invariance(gpu, orc, group, dims, nd):
     U = hot(orc, group, dims, nd)
