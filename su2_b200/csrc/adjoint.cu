@@ -121,7 +121,7 @@ __global__ void k_exp_adjoint(size_t NL, const T *__restrict__ Z, T b, T *__rest
       s2 = 0.5 - t2 / 24.0;
     } else {
       double sn, cs;
-      sincos(th, &sn, &cs);
+      sincospi(th * M_1_PI_D, &sn, &cs);
       c1 = (1.0 - cs) / (th * th);
       c2 = (th - sn) / (th * th * th);
       s1 = sn / th;

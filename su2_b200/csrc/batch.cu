@@ -52,6 +52,9 @@ constexpr int BATCH_NT[SU2B_BATCH_VARIANTS] = {64, 128, 128, 256};
 
 template <class T> struct Bufs {
   LinkT<T> *b[3];
+  // buffer k by selection: indexing the kernel-parameter array by a variable would copy it
+  // to local memory
+  __device__ __forceinline__ LinkT<T> *at(int k) const { return k == 0 ? b[0] : k == 1 ? b[1] : b[2]; }
 };
 
 template <class T, int NT, int MINB>
@@ -66,8 +69,8 @@ __global__ void __launch_bounds__(NT, MINB)
     const ChainDev &d = ch[c];
     const int cb = (tile - d.tile0) * (NT / 2) + (w >> 1) * 32 + (threadIdx.x & 31);
     const int S = cur[c];
-    const LinkT<T> *U = bufs.b[(S + rel_in) % 3] + d.off_link;
-    LinkT<T> *Uo = rel_out >= 0 ? bufs.b[(S + rel_out) % 3] + d.off_link : nullptr;
+    const LinkT<T> *U = bufs.at((S + rel_in) % 3) + d.off_link;
+    LinkT<T> *Uo = rel_out >= 0 ? bufs.at((S + rel_out) % 3) + d.off_link : nullptr;
     T *P = Pall + d.off_adj;
     const T f = (T)(d.beta / 2.0);
     double k2 = 0.;
@@ -128,7 +131,7 @@ __global__ void __launch_bounds__(NT)
     const int c = chain_of(ch, nchains, tile);
     const ChainDev &d = ch[c];
     const int cb = (tile - d.tile0) * (NT / 2) + (w >> 1) * 32 + (threadIdx.x & 31);
-    const LinkT<T> *U = bufs.b[(cur[c] + rel) % 3] + d.off_link;
+    const LinkT<T> *U = bufs.at((cur[c] + rel) % 3) + d.off_link;
     double full = 0., spat = 0., wsum = 0.;
     if (cb < d.g.Vh) {
       if (d.g.nd == 4)
@@ -175,7 +178,7 @@ __global__ void __launch_bounds__(NT)
         P[2 * NL + l] = cc;
         v[0] += (double)a * a + (double)b * b + (double)cc * cc;
       }
-      const LinkT<T> *U = bufs.b[cur[c] % 3] + d.off_link;
+      const LinkT<T> *U = bufs.at(cur[c] % 3) + d.off_link;
       double wsum = 0.;
       if (d.g.nd == 4)
         plaq_site<T, 4>(d.g, U, p, cb, 1.0, v[1], v[2], wsum);

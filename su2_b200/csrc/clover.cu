@@ -101,14 +101,14 @@ __global__ void __launch_bounds__(NT)
         const int fm = fwd(g, s, mu), bm = bwd(g, s, mu), fn = fwd(g, s, nu),
                   bn = bwd(g, s, nu);
         const int x = s.lex, q_ = 1 - p;
-        double im = sin(((A(mu, x, p) + A(nu, x + fm, q_)) + (-A(mu, x + fn, q_))) +
+        double im = sin_pi_scaled(((A(mu, x, p) + A(nu, x + fm, q_)) + (-A(mu, x + fn, q_))) +
                         (-A(nu, x, p)));
         if (cloverdef) {
-          im += sin(((A(nu, x, p) + (-A(mu, x + bm + fn, p))) + (-A(nu, x + bm, q_))) +
+          im += sin_pi_scaled(((A(nu, x, p) + (-A(mu, x + bm + fn, p))) + (-A(nu, x + bm, q_))) +
                     A(mu, x + bm, q_));
-          im += sin((((-A(mu, x + bm, q_)) + (-A(nu, x + bm + bn, p))) + A(mu, x + bm + bn, p)) +
+          im += sin_pi_scaled((((-A(mu, x + bm, q_)) + (-A(nu, x + bm + bn, p))) + A(mu, x + bm + bn, p)) +
                     A(nu, x + bn, q_));
-          im += sin((((-A(nu, x + bn, q_)) + A(mu, x + bn, q_)) + A(nu, x + fm + bn, p)) +
+          im += sin_pi_scaled((((-A(nu, x + bn, q_)) + A(mu, x + bn, q_)) + A(nu, x + fm + bn, p)) +
                     (-A(mu, x, p)));
         }
         G[mu][nu] = im;  // G = i*im (u1.hh:201-203)

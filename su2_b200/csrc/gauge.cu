@@ -195,7 +195,7 @@ __global__ void __launch_bounds__(NT)
         const int lpn = s.lex + fwd(g, s, nu);
         const double A = U[(size_t)nu * g.V + eo_of(g, lpm, 1 - p)];
         const double B = U[(size_t)mu * g.V + eo_of(g, lpn, 1 - p)];
-        const double tr = cos(((u[mu] + A) + (-B)) + (-u[nu]));
+        const double tr = cospi((((u[mu] + A) + (-B)) + (-u[nu])) * M_1_PI_D);
         full += tr;
         if (mu >= 1) spat += tr;
         wsum += (((mu == 0) ^ (nu == 0)) ? 1.0 / xi : xi) * tr;
@@ -316,7 +316,7 @@ __global__ void __launch_bounds__(NT)
   double k2 = 0.;
   if (cb < g.Vh) {
     const Site s = site_from_eo(g, p, cb);
-    const int lpm = s.lex + fwd(g, s, mu);
+    const int lpm = s.lex + fwd_rt(g, s, mu);  // mu from the block index
     double Kr = 0., Ki = 0.;
 #pragma unroll
     for (int nu = 0; nu < ND; nu++) {
@@ -326,7 +326,7 @@ __global__ void __launch_bounds__(NT)
       const double B = U[(size_t)mu * g.V + eo_of(g, lpn, 1 - p)];
       const double D = U[(size_t)nu * g.V + eo_of(g, s.lex, p)];
       double sn, cs;
-      sincos((A + (-B)) + (-D), &sn, &cs);
+      sincospi(((A + (-B)) + (-D)) * M_1_PI_D, &sn, &cs);
       const double w = aniso ? ((nu == 0 || mu == 0) ? wt : ws) : 1.0;
       Kr += w * cs;
       Ki += w * sn;
@@ -339,14 +339,14 @@ __global__ void __launch_bounds__(NT)
       const double B = U[(size_t)mu * g.V + eo_of(g, s.lex + b, 1 - p)];
       const double D = U[(size_t)nu * g.V + eo_of(g, s.lex + b, 1 - p)];
       double sn, cs;
-      sincos(((-A) + (-B)) + D, &sn, &cs);
+      sincospi((((-A) + (-B)) + D) * M_1_PI_D, &sn, &cs);
       const double w = aniso ? ((nu == 0 || mu == 0) ? wt : ws) : 1.0;
       Kr += w * cs;
       Ki += w * sn;
     }
     const size_t l = (size_t)mu * g.V + (size_t)p * g.Vh + cb;
     double su, cu;
-    sincos(U[l], &su, &cu);
+    sincospi(U[l] * M_1_PI_D, &su, &cu);
     double d = f * (cu * Ki + su * Kr);  // Im(e^{i theta} K), adjointfield.hh:79-81
     if (mode & FM_EXTRA) d += extra[l];
     const double pn = (mode & FM_HAS_IN) ? P[l] + scale_ * d : scale_ * d;

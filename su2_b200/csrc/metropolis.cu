@@ -25,7 +25,7 @@ __device__ __forceinline__ unsigned metro_link_fp32(const Geom &g, Link32 *__res
                                                     int N_hit, uint64_t seed, uint32_t sweep,
                                                     float wt, float ws) {
   const Site s = site_from_eo(g, p, cb);
-  const int lpm = s.lex + fwd(g, s, mu);
+  const int lpm = s.lex + fwd_rt(g, s, mu);  // mu is known at run time only
   Su2<float> K = zero_su2<float>();
 #pragma unroll
   for (int nu = 0; nu < ND; nu++) {
@@ -93,7 +93,7 @@ __global__ void __launch_bounds__(NT)
   } else if (cb < g.Vh) {
     const Site s = site_from_eo(g, p, cb);
     // staple sum in FP64
-    const int lpm = s.lex + fwd(g, s, mu);
+    const int lpm = s.lex + fwd_rt(g, s, mu);  // mu is known at run time only
     Su2<double> K = zero_su2<double>();
 #pragma unroll
     for (int nu = 0; nu < ND; nu++) {
@@ -156,7 +156,7 @@ __global__ void __launch_bounds__(NT)
   unsigned int acc = 0;
   if (cb < g.Vh) {
     const Site s = site_from_eo(g, p, cb);
-    const int lpm = s.lex + fwd(g, s, mu);
+    const int lpm = s.lex + fwd_rt(g, s, mu);  // mu is known at run time only
     double Kr = 0., Ki = 0.;
 #pragma unroll
     for (int nu = 0; nu < ND; nu++) {
@@ -166,7 +166,7 @@ __global__ void __launch_bounds__(NT)
       const double B = U[(size_t)mu * g.V + eo_of(g, lpn, 1 - p)];
       const double D = U[(size_t)nu * g.V + eo_of(g, s.lex, p)];
       double sn, cs;
-      sincos((A + (-B)) + (-D), &sn, &cs);
+      sincospi(((A + (-B)) + (-D)) * M_1_PI_D, &sn, &cs);
       const double w = (nu == 0 || mu == 0) ? wt : ws;
       Kr += w * cs;
       Ki += w * sn;
@@ -179,7 +179,7 @@ __global__ void __launch_bounds__(NT)
       const double B = U[(size_t)mu * g.V + eo_of(g, s.lex + b, 1 - p)];
       const double D = U[(size_t)nu * g.V + eo_of(g, s.lex + b, 1 - p)];
       double sn, cs;
-      sincos(((-A) + (-B)) + D, &sn, &cs);
+      sincospi((((-A) + (-B)) + D) * M_1_PI_D, &sn, &cs);
       const double w = (nu == 0 || mu == 0) ? wt : ws;
       Kr += w * cs;
       Ki += w * sn;
@@ -192,8 +192,8 @@ __global__ void __launch_bounds__(NT)
       philox(lref, (uint32_t)n, sweep, TAG_METRO, seed, r);
       const double th = M_PI * delta * (2.0 * u01_32(r[0]) - 1.0);
       double s0, c0, s1, c1;
-      sincos(u, &s0, &c0);
-      sincos(u + th, &s1, &c1);
+      sincospi(u * M_1_PI_D, &s0, &c0);
+      sincospi((u + th) * M_1_PI_D, &s1, &c1);
       const double dS = beta * ((c0 * Kr - s0 * Ki) - (c1 * Kr - s1 * Ki));
       bool a = dS < 0;
       if (!a) a = u01_32(r[1]) < exp(-dS);

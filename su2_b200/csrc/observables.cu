@@ -25,15 +25,39 @@ __device__ __forceinline__ double angle_at(const Geom &g, const double *__restri
 __device__ __forceinline__ double2 cmul2(double2 x, double2 y) {
   return make_double2(x.x * y.x - x.y * y.y, x.x * y.y + x.y * y.x);
 }
+// e^{i a} through sincospi(a/pi): exact argument reduction, and no local-memory frame (the
+// slow reduction path of sincos keeps one, which every kernel using it then carries)
 __device__ __forceinline__ double2 phase(double a) {
   double s, c;
-  sincos(a, &s, &c);
+  sincospi(a * 0.318309886183790671537767526745, &s, &c);
   return make_double2(c, s);
 }
 
-__device__ __forceinline__ int lex_of(const Geom &g, const int c[4]) {
-  return ((c[0] * g.L[1] + c[1]) * g.L[2] + c[2]) * g.L[3] + c[3];
-}
+// A lattice point held as four scalar coordinates.  Steps take the direction at run time;
+// with an int[4] indexed by a variable the point (and the geometry) would live in local
+// memory, with scalars and a selection it stays in registers.
+struct Point {
+  int c0, c1, c2, c3;
+  __device__ __forceinline__ explicit Point(const Site &s)
+    : c0(s.c[0]), c1(s.c[1]), c2(s.c[2]), c3(s.c[3]) {}
+  __device__ __forceinline__ static int wrap(int v, int L) {
+    return v < 0 ? v + L : (v >= L ? v - L : v);
+  }
+  __device__ __forceinline__ void step(const Geom &g, int d, int dir) {
+    if (d == 0)
+      c0 = wrap(c0 + dir, g.L[0]);
+    else if (d == 1)
+      c1 = wrap(c1 + dir, g.L[1]);
+    else if (d == 2)
+      c2 = wrap(c2 + dir, g.L[2]);
+    else
+      c3 = wrap(c3 + dir, g.L[3]);
+  }
+  __device__ __forceinline__ int lex(const Geom &g) const {
+    return ((c0 * g.L[1] + c1) * g.L[2] + c2) * g.L[3] + c3;
+  }
+  __device__ __forceinline__ int par() const { return (c0 + c1 + c2 + c3) & 1; }
+};
 
 // polyakov_loop (polyakov_loop.hh:26-38): one thread per spatial point, the product of the
 // temporal links along t, ReTr (SU(2): 2 Re a; U(1): Re of the phase product)
@@ -75,14 +99,10 @@ __global__ void __launch_bounds__(NT)
   if (lex0 < g.V) {
     const Site s0 = site_from_lex(g, lex0);
     for (int mu = 1; mu < g.nd; mu++) {
-      int c[4] = {s0.c[0], s0.c[1], s0.c[2], s0.c[3]};
-      auto step = [&](int d, int dir) {
-        c[d] += dir;
-        if (c[d] < 0) c[d] += g.L[d];
-        if (c[d] >= g.L[d]) c[d] -= g.L[d];
-      };
-      auto here = [&]() { return lex_of(g, c); };
-      auto par = [&]() { return (c[0] + c[1] + c[2] + c[3]) & 1; };
+      Point c(s0);
+      auto step = [&](int d, int dir) { c.step(g, d, dir); };
+      auto here = [&]() { return c.lex(g); };
+      auto par = [&]() { return c.par(); };
       if (group == 0) {
         const LinkT<T> *U = (const LinkT<T> *)Uv;
         Su2<double> L{1.0, 0.0, 0.0, 0.0};
@@ -146,15 +166,11 @@ __global__ void __launch_bounds__(NT)
   const Site s = site_from_lex(g, lex);
   const size_t self = (size_t)i * g.V + (size_t)s.p * g.Vh + (lex >> 1);
   auto at = [&](int d0, int d1, int dir0, int dir1, int *lx, int *pr) {
-    int c[4] = {s.c[0], s.c[1], s.c[2], s.c[3]};
-    c[d0] += dir0;
-    c[d1] += dir1;
-    for (int k = 0; k < 4; k++) {
-      if (c[k] < 0) c[k] += g.L[k];
-      if (c[k] >= g.L[k]) c[k] -= g.L[k];
-    }
-    *lx = lex_of(g, c);
-    *pr = (c[0] + c[1] + c[2] + c[3]) & 1;
+    Point c(s);
+    c.step(g, d0, dir0);
+    c.step(g, d1, dir1);
+    *lx = c.lex(g);
+    *pr = c.par();
   };
   if (group == 0) {
     const LinkT<T> *U = (const LinkT<T> *)Uin;

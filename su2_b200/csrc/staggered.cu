@@ -79,7 +79,12 @@ __global__ void __launch_bounds__(NT)
     const Site s = site_from_eo(g, p, cb);
     R accr = 0, acci = 0;
     int esum = 0;
-    for (int mu = 0; mu < g.nd; mu++) {
+    // a compile-time bound with a guard keeps every index constant: with the runtime bound the
+    // loop indexes the site's coordinates and the geometry by a variable, which puts both in
+    // local memory
+#pragma unroll
+    for (int mu = 0; mu < 4; mu++) {
+      if (mu >= g.nd) break;
       const R eta = (esum & 1) ? R(-0.5) : R(0.5);
       esum += s.c[mu];
       const int lp = s.lex + fwd(g, s, mu), lm = s.lex + bwd(g, s, mu);
@@ -125,10 +130,11 @@ __global__ void k_fforce(Geom g, const double2 *__restrict__ ph, const double2 *
   if (cb >= g.Vh) return;
   const Site s = site_from_eo(g, p, cb);
   int esum = 0;
-  for (int nu = 0; nu < mu; nu++) esum += s.c[nu];
+#pragma unroll
+  for (int nu = 0; nu < 3; nu++) esum += nu < mu ? s.c[nu] : 0;  // constant indexes
   const double eta = (esum & 1) ? -1.0 : 1.0;
   const size_t l = (size_t)mu * g.V + (size_t)p * g.Vh + cb;
-  const int sx = p * g.Vh + cb, sp = eo_of(g, s.lex + fwd(g, s, mu), 1 - p);
+  const int sx = p * g.Vh + cb, sp = eo_of(g, s.lex + fwd_rt(g, s, mu), 1 - p);
   const double2 u = ph[l], ud = make_double2(u.x, -u.y);
   // v_xp = (1/2 eta i) U chi1(x+mu);  v_x = (-1/2 eta (-i)) U^+ chi1(x)
   const double2 v_xp = cm(cm(make_double2(0.0, 0.5 * eta), u), chi1[sp]);
@@ -267,7 +273,9 @@ __device__ __forceinline__ double2 hop_site64_f(const Geom &g, const double2 *__
   const Site s = site_from_eo(g, p, cb);
   double accr = 0, acci = 0;
   int esum = 0;
-  for (int mu = 0; mu < g.nd; mu++) {
+#pragma unroll
+  for (int mu = 0; mu < 4; mu++) {  // constant indexes (see k_hop)
+    if (mu >= g.nd) break;
     const double eta = (esum & 1) ? -0.5 : 0.5;
     esum += s.c[mu];
     const int lp = s.lex + fwd(g, s, mu), lm = s.lex + bwd(g, s, mu);
@@ -296,7 +304,9 @@ __device__ __forceinline__ float2 hop_site32(const Geom &g, const float2 *__rest
   const Site s = site_from_eo(g, p, cb);
   float accr = 0.f, acci = 0.f;
   int esum = 0;
-  for (int mu = 0; mu < g.nd; mu++) {
+#pragma unroll
+  for (int mu = 0; mu < 4; mu++) {  // constant indexes (see k_hop)
+    if (mu >= g.nd) break;
     const float eta = (esum & 1) ? -0.5f : 0.5f;
     esum += s.c[mu];
     const int lp = s.lex + fwd(g, s, mu), lm = s.lex + bwd(g, s, mu);

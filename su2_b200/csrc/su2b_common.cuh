@@ -98,6 +98,25 @@ __device__ __forceinline__ int fwd(const Geom &g, const Site &s, int mu) {
 __device__ __forceinline__ int bwd(const Geom &g, const Site &s, int mu) {
   return s.c[mu] == 0 ? (g.L[mu] - 1) * g.st[mu] : -g.st[mu];
 }
+// The same for a direction known only at run time.  Selecting among the four entries keeps
+// every array index constant; indexing the site's coordinates or the geometry by a variable
+// would place both in local memory.
+__device__ __forceinline__ int pick4(int k, int a0, int a1, int a2, int a3) {
+  return k == 0 ? a0 : k == 1 ? a1 : k == 2 ? a2 : a3;
+}
+__device__ __forceinline__ int coord_rt(const Site &s, int mu) {
+  return pick4(mu, s.c[0], s.c[1], s.c[2], s.c[3]);
+}
+__device__ __forceinline__ int fwd_rt(const Geom &g, const Site &s, int mu) {
+  const int L = pick4(mu, g.L[0], g.L[1], g.L[2], g.L[3]);
+  const int st = pick4(mu, g.st[0], g.st[1], g.st[2], g.st[3]);
+  return coord_rt(s, mu) == L - 1 ? -(L - 1) * st : st;
+}
+__device__ __forceinline__ int bwd_rt(const Geom &g, const Site &s, int mu) {
+  const int L = pick4(mu, g.L[0], g.L[1], g.L[2], g.L[3]);
+  const int st = pick4(mu, g.st[0], g.st[1], g.st[2], g.st[3]);
+  return coord_rt(s, mu) == 0 ? (L - 1) * st : -st;
+}
 // even/odd index of the site with lexicographic index lex and parity p
 __device__ __forceinline__ int eo_of(const Geom &g, int lex, int p) {
   return p * g.Vh + (lex >> 1);
@@ -274,6 +293,12 @@ __device__ __forceinline__ Su2<float> exp_alg(float a, float b, float c) {
   }
   return Su2<float>{co, f * c, f * b, f * a};
 }
+
+// FP64 trigonometry of an angle through the pi-scaled functions (sincospi(a/pi) etc.): their
+// argument reduction is exact, and unlike sin/cos/sincos they carry no local-memory frame
+// for a slow reduction path (the product a * (1/pi) rounds once, 1e-16 relative)
+constexpr double M_1_PI_D = 0.318309886183790671537767526745;
+__device__ __forceinline__ double sin_pi_scaled(double a) { return sinpi(a * M_1_PI_D); }
 
 // ------------------------------------------------------------------------------------
 // Philox4x32-10 (Salmon, Moraes, Dror, Shaw, SC'11); counter {index, draw, step, tag}
