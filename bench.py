@@ -401,6 +401,21 @@ def ours(args):
     torch.cuda.synchronize()
     metro = 5 / (ev[0].elapsed_time(ev[1]) / 1e3)
     flow = 10 / (ev[2].elapsed_time(ev[3]) / 1e3)
+    # the same two in the other precision: FP64 Metropolis, mixed-precision flow
+    fp64.upload(U_th)
+    mixed.upload(U_th)
+    ev2 = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    ev2[0].record(s2)
+    for sweep in range(5):
+        fp64.sweep(0.15, 8, seed, 5000 + sweep)
+    ev2[1].record(s2)
+    ev2[2].record(s)
+    for _ in range(10):
+        mixed.runge_kutta(0.01)
+    ev2[3].record(s)
+    torch.cuda.synchronize()
+    metro64 = 5 / (ev2[0].elapsed_time(ev2[1]) / 1e3)
+    flow32 = 10 / (ev2[2].elapsed_time(ev2[3]) / 1e3)
 
     # ---- the measurements taken between trajectories (FP64 context, thermalised field):
     #      wall time per call, each call returns its value to the host ----
@@ -458,7 +473,8 @@ def ours(args):
                                   "fp64": {str(shapes[k]): v for k, v in tune_d.items()}},
             "timed_chain_stats": {"mixed": stats(res_m, V), "fp64": stats(res_d, V),
                                   "plain_fp64": stats(res_p, V)},
-            "metropolis_sweeps_per_s": metro, "flow_rk3_steps_per_s_fp64": flow,
+            "metropolis_sweeps_per_s": {"mixed": metro, "fp64": metro64},
+            "flow_rk3_steps_per_s": {"fp64": flow, "mixed": flow32},
             "between_trajectories_fp64": obs}), flush=True)
         r3 = lambda v: float(f"{v:.4g}")  # noqa: E731
         line = {

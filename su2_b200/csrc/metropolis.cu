@@ -5,18 +5,36 @@
 // of other directions only, so all of them update independently and in any order.  A sweep
 // is 2*nd launches.  Per link: staples once (get_staples.hh:26-80), then N_hit proposals
 // U -> U R with R = random_element(delta) (random_element.hh:9-34), dS = beta/Nc (ReTr(U K) -
-// ReTr(U R K)), accept with min(1, exp(-dS)), restoreSU after each accepted hit.  FP64 links:
-// all arithmetic in FP64.  FP32 links (mixed precision): the staple sum, the proposal R and
-// the product U R in FP32; the action change dS (the traces of the FP32 values, in FP64), the
-// accept test and the reunitarisation in FP64.  Random numbers: one Philox4x32-10 draw per
-// hit, counter {reference link index, hit, sweep, TAG_METRO}: 32-bit uniforms for alpha, u,
-// theta and the accept test, the same stream in both precisions.
+// ReTr(U R K)), accept with min(1, exp(-dS)), restoreSU after each accepted hit.
+//   FP64 links: all arithmetic in FP64.
+//   FP32 links (mixed precision): the staple sum, the proposal R and the product U R in FP32;
+//   the action change dS (the traces of the FP32 values, in FP64), the accept test and the
+//   reunitarisation in FP64.
+// In both, the accept test u < exp(-dS) goes through accept_fp64, which takes the FP64
+// test's decisions (FP32 exp with a guard band, FP64 exp inside the band).  Random numbers:
+// one Philox4x32-10 draw per hit, counter {reference link index, hit, sweep, TAG_METRO}:
+// 32-bit uniforms for alpha, u, theta and the accept test, the same stream in both
+// precisions.
 #include "su2b_internal.h"
 
 namespace su2b {
 namespace {
 
 template <class T> using LinkT = typename LinkOf<T>::type;
+
+// The FP64 accept test u < exp(-dS) (dS >= 0), decided by FP32 exp where that is safe.  The
+// FP32 value differs from the FP64 one by at most the rounding of dS to float (|dS| 2^-24
+// relative to the result) plus expf's error (2 ulp); outside a guard band of twice that
+// bound the FP32 comparison gives the FP64 decision, inside it (and where expf underflows)
+// the test is taken in FP64.  The decisions are those of the FP64 test.
+__device__ __forceinline__ bool accept_fp64(double u, double dS) {
+  const float ef = expf(-(float)dS);
+  if (!(ef > 1e-30f)) return u < exp(-dS);
+  const double band = (double)ef * (2.0 * (double)dS * 0x1p-24 + 8.0 * 0x1p-24);
+  if (u < (double)ef - band) return true;
+  if (u >= (double)ef + band) return false;
+  return u < exp(-dS);
+}
 
 // One link of a pass with FP32 storage (see the file comment); returns its accepted hits.
 template <int ND>
@@ -65,7 +83,7 @@ __device__ __forceinline__ unsigned metro_link_fp32(const Geom &g, Link32 *__res
     const double tr_uR = retr_mul(to64(uR), K64);
     const double dS = beta_nc * (tr_u - tr_uR);
     bool a = dS < 0;
-    if (!a) a = u01_32(r[3]) < exp(-dS);
+    if (!a) a = accept_fp64(u01_32(r[3]), dS);
     if (a) {
       u = from64<float>(restore_su(to64(uR)));
       tr_u = retr_mul(to64(u), K64);
@@ -128,7 +146,7 @@ __global__ void __launch_bounds__(NT)
       const Su2<double> uR = mul(u, R);
       const double dS = beta_nc * (retr_mul(u, K) - retr_mul(uR, K));
       bool a = dS < 0;
-      if (!a) a = u01_32(r[3]) < exp(-dS);
+      if (!a) a = accept_fp64(u01_32(r[3]), dS);
       if (a) {
         u = restore_su(uR);
         acc++;
