@@ -254,6 +254,50 @@ SU2B_API int su2b_batch_autotune(su2b_batch *b, double *times_us);
 SU2B_API int su2b_batch_tune_get(su2b_batch *b, int *variant);
 SU2B_API int su2b_batch_tune_set(su2b_batch *b, int variant);
 
+/* ---- one lattice over time slabs ------------------------------------------------------------ */
+/* The t-slab decomposition of one SU(2) lattice: the lattice is cut into nslabs slabs of
+ * Lt / nslabs time slices (an even number).  A slab holds its slices and one ghost slice of
+ * links on each side.  A trajectory runs every force step on each slab's own sites, then
+ * refreshes the ghost slices from the neighbouring slabs; the plaquette and kinetic sums add
+ * over the slabs before the accept/reject.  The momenta are the Philox streams of the whole
+ * lattice, so a trajectory equals the one of a single-lattice context (su2b_hmc_trajectory)
+ * with the same seed and traj: the same links and accept decisions, the energies to rounding
+ * (the sums add in another order).  The reference splits the same site loops over OpenMP
+ * threads along t (flat-gaugemonomial.hh:105-131, flat-sweep.hh:83,128).
+ * A handle holds the slabs first .. first + count - 1.  With count == nslabs every slab lives
+ * on one device and the ghost slices are device copies.  With one slab per process
+ * (count == 1, one GPU each) the handles exchange ghost slices and sums through NCCL
+ * (su2b_slabs_connect; NCCL is loaded at run time from libnccl.so.2).
+ * Trajectories: leapfrog, omf2 and omf4 with Philox momenta (momenta_host, revtest and
+ * fermions return SU2B_ERR_UNSUPPORTED).  Lt % nslabs != 0 or an odd Lt / nslabs return
+ * SU2B_ERR_INVALID. */
+typedef struct su2b_slabs su2b_slabs;
+SU2B_API int su2b_slabs_create(int Lx, int Ly, int Lz, int Lt, int ndims, double beta,
+                               double xi, int precision, int nslabs, int first, int count,
+                               int device, su2b_slabs **out);
+SU2B_API int su2b_slabs_destroy(su2b_slabs *h);
+SU2B_API const char *su2b_slabs_last_error(const su2b_slabs *h);
+SU2B_API int su2b_slabs_info(const su2b_slabs *h, int *nslabs, int *first, int *count,
+                             int *slices);
+/* ncclGetUniqueId into id (128 bytes), for one process to pass to the others */
+SU2B_API int su2b_slabs_nccl_id(void *id);
+/* joins the NCCL communicator of nranks = nslabs processes; rank = the handle's slab */
+SU2B_API int su2b_slabs_connect(su2b_slabs *h, const void *id, int nranks, int rank);
+/* U_host: the whole lattice's field in the reference host layout; upload takes each slab's
+ * slices and ghost slices from it, download writes the handle's slabs' slices into it */
+SU2B_API int su2b_slabs_upload(su2b_slabs *h, const double *U_host);
+SU2B_API int su2b_slabs_download(su2b_slabs *h, double *U_host);
+SU2B_API int su2b_slabs_hmc_trajectory(su2b_slabs *h, const su2b_hmc_params *prm,
+                                       su2b_traj_result *res);
+/* gauge_energy of the whole lattice (as su2b_gauge_energy) */
+SU2B_API int su2b_slabs_gauge_energy(su2b_slabs *h, int spatial_only, double *out);
+/* su2b_autotune on the first slab; every slab takes its choice */
+SU2B_API int su2b_slabs_autotune(su2b_slabs *h, double *times_us);
+SU2B_API int su2b_slabs_tune_get(su2b_slabs *h, int *variant);
+SU2B_API int su2b_slabs_tune_set(su2b_slabs *h, int variant);
+SU2B_API int su2b_slabs_kernel_launches(su2b_slabs *h, long *count);
+SU2B_API int su2b_slabs_stream(su2b_slabs *h, void **stream);
+
 /* ---- gauge configurations on disk ------------------------------------------------------- */
 /* gaugeconfig<G>::save / load (gaugeconfig.hh:225-252): the reference's raw binary format, one
  * in-memory _su2 (40 bytes: size_t N_c = 2, then Re a, Im a, Re b, Im b) or _u1 (16 bytes:

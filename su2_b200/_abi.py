@@ -116,6 +116,23 @@ SIGNATURES = {
     "su2b_flow_adjoint": (i32, [_P, f64, i32, i32, _D, _D]),
     "su2b_tune_get": (i32, [_P, i32, C.POINTER(C.c_int)]),
     "su2b_tune_set": (i32, [_P, i32, i32]),
+    "su2b_slabs_create": (i32, [i32, i32, i32, i32, i32, f64, f64, i32, i32, i32, i32, i32,
+                                C.POINTER(_P)]),
+    "su2b_slabs_destroy": (i32, [_P]),
+    "su2b_slabs_last_error": (C.c_char_p, [_P]),
+    "su2b_slabs_info": (i32, [_P, C.POINTER(i32), C.POINTER(i32), C.POINTER(i32),
+                              C.POINTER(i32)]),
+    "su2b_slabs_nccl_id": (i32, [_P]),
+    "su2b_slabs_connect": (i32, [_P, _P, i32, i32]),
+    "su2b_slabs_upload": (i32, [_P, _D]),
+    "su2b_slabs_download": (i32, [_P, _D]),
+    "su2b_slabs_hmc_trajectory": (i32, [_P, C.POINTER(HmcParams), C.POINTER(TrajResult)]),
+    "su2b_slabs_gauge_energy": (i32, [_P, i32, _D]),
+    "su2b_slabs_autotune": (i32, [_P, _D]),
+    "su2b_slabs_tune_get": (i32, [_P, C.POINTER(i32)]),
+    "su2b_slabs_tune_set": (i32, [_P, i32]),
+    "su2b_slabs_kernel_launches": (i32, [_P, C.POINTER(C.c_long)]),
+    "su2b_slabs_stream": (i32, [_P, C.POINTER(_P)]),
 }
 FORCE_VARIANTS = 10
 BATCH_VARIANTS = 4

@@ -61,7 +61,7 @@ def build(verbose: bool = False) -> str:
     with cf.ThreadPoolExecutor(max_workers=min(8, os.cpu_count() or 1)) as ex:
         objs = list(ex.map(lambda s: _compile(s, headers, verbose), srcs))
     if _needs(LIB, objs):
-        cmd = [NVCC] + ARCH + ["-ccbin", HOST_CXX, "-shared", "-o", LIB] + objs
+        cmd = [NVCC] + ARCH + ["-ccbin", HOST_CXX, "-shared", "-o", LIB] + objs + ["-ldl"]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{r.stderr}")

@@ -98,6 +98,9 @@ int su2b_make_geom(int Lx, int Ly, int Lz, int Lt, int nd, Geom *g, std::string 
   g->V = (int)V;
   g->Vh = (int)(V / 2);
   for (int k = 0; k < 4; k++) g->dv[k] = make_fastdiv((uint32_t)L[k]);
+  g->cb0 = 0;
+  g->ncb = g->Vh;
+  g->lex0 = 0;
   return 1;
 }
 

@@ -120,9 +120,9 @@ __global__ void __launch_bounds__(NT, plaq_min_blocks<T, NT>())
   k_plaq_su2(Geom g, const LinkT<T> *__restrict__ U, double xi, double *part) {
   __shared__ double shk[4 * (NT / 32)];
   const int w = threadIdx.x >> 5, p = w & 1;
-  const int cb = blockIdx.x * (NT / 2) + (w >> 1) * 32 + (threadIdx.x & 31);
+  const int cb = g.cb0 + blockIdx.x * (NT / 2) + (w >> 1) * 32 + (threadIdx.x & 31);
   double full = 0., spat = 0., wsum = 0.;
-  if (cb < g.Vh) plaq_site<T, ND>(g, U, p, cb, xi, full, spat, wsum);
+  if (cb < g.cb0 + g.ncb) plaq_site<T, ND>(g, U, p, cb, xi, full, spat, wsum);
   const int b = blockIdx.x;
   double v[3] = {full, spat, wsum};
   block_sums<NT, 3>(v, shk);
@@ -144,16 +144,16 @@ __global__ void __launch_bounds__(NT, plaq_min_blocks<T, NT>())
                      const TrajParams *__restrict__ tp, double xi, double *part) {
   __shared__ double shk[4 * (NT / 32)];
   const int w = threadIdx.x >> 5, p = w & 1;
-  const int cb = blockIdx.x * (NT / 2) + (w >> 1) * 32 + (threadIdx.x & 31);
+  const int cb = g.cb0 + blockIdx.x * (NT / 2) + (w >> 1) * 32 + (threadIdx.x & 31);
   double k2 = 0., full = 0., spat = 0., wsum = 0.;
-  if (cb < g.Vh) {
+  if (cb < g.cb0 + g.ncb) {
     const uint64_t seed = tp->seed;
     const uint32_t traj = tp->traj;
     const Site s = site_from_eo(g, p, cb);
     const size_t NL = (size_t)g.V * ND;
 #pragma unroll
     for (int mu = 0; mu < ND; mu++) {
-      const uint32_t lref = (uint32_t)s.lex * (uint32_t)ND + (uint32_t)mu;
+      const uint32_t lref = (uint32_t)(s.lex + g.lex0) * (uint32_t)ND + (uint32_t)mu;
       const size_t l = (size_t)mu * g.V + (size_t)p * g.Vh + cb;
       T n0, n1, n2;
       momentum_normals<T>(lref, traj, seed, 3, n0, n1, n2);
@@ -259,9 +259,9 @@ __global__ void __launch_bounds__(NT, MINB)
   // +-z / +-y neighbours of a site are mostly the own links of another warp of the block
   const int w = threadIdx.x >> 5;
   const int p = w & 1;
-  const int cb = blockIdx.x * (NT / 2) + (w >> 1) * 32 + (threadIdx.x & 31);
+  const int cb = g.cb0 + blockIdx.x * (NT / 2) + (w >> 1) * 32 + (threadIdx.x & 31);
   double k2 = 0.;
-  if (cb < g.Vh)
+  if (cb < g.cb0 + g.ncb)
     k2 = force_site_impl<T, ND, ANISO>(g, U, P, extra, f, scale_, mode, wt, ws, Uout, dt_upd, p,
                                        cb);
   if (mode & FM_KINETIC) {
@@ -284,13 +284,13 @@ __global__ void __launch_bounds__(32 * ND, MINB)
   pdl_trigger();
   pdl_wait();
   const int mu = threadIdx.x >> 5, p = blockIdx.x & 1;
-  const int cb = (blockIdx.x >> 1) * 32 + (threadIdx.x & 31);
+  const int cb = g.cb0 + (blockIdx.x >> 1) * 32 + (threadIdx.x & 31);
   double k2 = 0.;
   // the direction is a compile-time constant in each warp's body (static site indexing)
 #define SU2B_LINK_BODY(M)                                                                     \
   k2 = force_link_impl<T, ND, (M < ND ? M : 0)>(g, U, P, extra, f, scale_, mode, Uout, dt_upd, \
                                                  p, cb)
-  if (cb < g.Vh) {
+  if (cb < g.cb0 + g.ncb) {
     switch (mu) {
       case 0: SU2B_LINK_BODY(0); break;
       case 1: SU2B_LINK_BODY(1); break;
@@ -643,7 +643,7 @@ template <class T>
 cudaError_t plaq_partials(const Geom &g, const void *U, int group, double xi, double *part,
                           int *nblocks, cudaStream_t s) {
   constexpr int NT = 256;
-  const dim3 grid(cdiv(g.Vh, NT / 2));
+  const dim3 grid(cdiv(group == 0 ? g.ncb : g.Vh, NT / 2));
   *nblocks = grid.x;
   if (group == 0) {
     const LinkT<T> *u = (const LinkT<T> *)U;
@@ -681,9 +681,9 @@ __global__ void __launch_bounds__(NT, MINB)
   pdl_wait();
   const int w = threadIdx.x >> 5;
   const int half = w & 1, p = (w >> 1) & 1;
-  const int cb = blockIdx.x * (NT / 4) + (w >> 2) * 32 + (threadIdx.x & 31);
+  const int cb = g.cb0 + blockIdx.x * (NT / 4) + (w >> 2) * 32 + (threadIdx.x & 31);
   double k2 = 0.;
-  if (cb < g.Vh)
+  if (cb < g.cb0 + g.ncb)
     k2 = half == 0 ? force_half_impl<T, 0, false>(g, U, P, extra, f, scale_, mode, wt, ws, Uout,
                                                   dt_upd, p, cb)
                    : force_half_impl<T, 1, false>(g, U, P, extra, f, scale_, mode, wt, ws, Uout,
@@ -709,9 +709,9 @@ __global__ void __launch_bounds__(NT, MINB)
   pdl_wait();
   const int w = threadIdx.x >> 5;
   const int half = w & 1, p = (w >> 1) & 1;
-  const int cb = blockIdx.x * (NT / 4) + (w >> 2) * 32 + (threadIdx.x & 31);
-  const bool valid = cb < g.Vh;
-  const int cbc = valid ? cb : g.Vh - 1;
+  const int cb = g.cb0 + blockIdx.x * (NT / 4) + (w >> 2) * 32 + (threadIdx.x & 31);
+  const bool valid = cb < g.cb0 + g.ncb;
+  const int cbc = valid ? cb : g.cb0 + g.ncb - 1;
   const int bar_id = 1 + (w >> 1);
   const double k2 =
     half == 0 ? force_half_x<T, 0>(g, U, P, extra, f, scale_, mode, Uout, dt_upd, p, cbc, valid,
@@ -756,7 +756,7 @@ cudaError_t force_update(const Geom &g, const void *U, int group, T *P, const T 
 #define SU2B_FORCE_ARGS g, u, P, extra, (T)f, (T)scale, mode, wt, ws, kin_part, uo, (T)dt_upd
 #define SU2B_FORCE_LAUNCH(NTV, MB, AN)                                                       \
   do {                                                                                     \
-    const dim3 grid(cdiv(g.Vh, NTV / 2));                                                  \
+    const dim3 grid(cdiv(g.ncb, NTV / 2));                                                  \
     nb = grid.x;                                                                           \
     cudaError_t e_;                                                                        \
     switch (g.nd) {                                                                        \
@@ -781,7 +781,7 @@ cudaError_t force_update(const Geom &g, const void *U, int group, T *P, const T 
       SU2B_FORCE_LAUNCH(128, 8, false);                                                    \
       break;                                                                               \
     }                                                                                      \
-    const dim3 grid(cdiv(g.Vh, NTV / 4));                                                  \
+    const dim3 grid(cdiv(g.ncb, NTV / 4));                                                  \
     nb = grid.x;                                                                           \
     const cudaError_t e_ =                                                                 \
       launch_force(k_force_su2_split<T, NTV, MB>, grid, NTV, s, pdl, SU2B_FORCE_ARGS);     \
@@ -789,7 +789,7 @@ cudaError_t force_update(const Geom &g, const void *U, int group, T *P, const T 
   } while (0)
 #define SU2B_FORCE_LINK(MB)                                                                  \
   do {                                                                                     \
-    const dim3 grid(2 * cdiv(g.Vh, 32));                                                   \
+    const dim3 grid(2 * cdiv(g.ncb, 32));                                                   \
     nb = grid.x;                                                                           \
     cudaError_t e_;                                                                        \
     switch (g.nd) {                                                                        \
@@ -811,7 +811,7 @@ cudaError_t force_update(const Geom &g, const void *U, int group, T *P, const T 
       SU2B_FORCE_LAUNCH(128, 8, false);                                                    \
       break;                                                                               \
     }                                                                                      \
-    const dim3 grid(cdiv(g.Vh, NTV / 4));                                                  \
+    const dim3 grid(cdiv(g.ncb, NTV / 4));                                                  \
     nb = grid.x;                                                                           \
     const cudaError_t e_ =                                                                 \
       launch_force(k_force_su2_xsplit<T, NTV, MB>, grid, NTV, s, pdl, SU2B_FORCE_ARGS);    \
@@ -916,7 +916,7 @@ template <class T>
 cudaError_t momenta_plaq(const Geom &g, const void *U, T *P, const TrajParams *tp, double xi,
                          double *part, int *nblocks, cudaStream_t s, bool plaq) {
   constexpr int NT = 256;
-  const dim3 grid(cdiv(g.Vh, NT / 2));
+  const dim3 grid(cdiv(g.ncb, NT / 2));
   *nblocks = grid.x;
   const LinkT<T> *u = (const LinkT<T> *)U;
 #define SU2B_MP(ND)                                                                          \

@@ -18,16 +18,10 @@
 
 using namespace su2b;
 
-namespace {
-
-struct Op {
-  int kind;  // 0 momenta: P -= c * deriv;  1 gauge: U = exp(c P) U
-  double c;
-};
-
 // integrator.hh: the step sequence of each scheme, with the reference's coefficient
 // arithmetic (dtau = tau/nsteps, omf2 lambda = 0.1938, omf4 Omelyan constants).
-std::vector<Op> schedule(int integ, int n, double tau) {
+std::vector<HmcOp> su2b_schedule(int integ, int n, double tau) {
+  using Op = HmcOp;
   std::vector<Op> o;
   const double dtau = tau / (double)n;
   auto M = [&](double c) { o.push_back({0, c}); };
@@ -99,6 +93,32 @@ std::vector<Op> schedule(int integ, int n, double tau) {
   return o;
 }
 
+// a momentum step and the gauge step after it become one fused force launch
+std::vector<HmcFusedOp> su2b_fuse(const std::vector<HmcOp> &ops) {
+  int last_m = -1;
+  for (int i = 0; i < (int)ops.size(); i++)
+    if (ops[i].kind == 0) last_m = i;
+  std::vector<HmcFusedOp> f;
+  for (int i = 0; i < (int)ops.size(); i++) {
+    if (ops[i].kind == 0 && i + 1 < (int)ops.size() && ops[i + 1].kind == 1) {
+      f.push_back({1, ops[i].c, ops[i + 1].c, i == last_m});
+      i++;
+    } else if (ops[i].kind == 0) {
+      f.push_back({0, ops[i].c, 0.0, i == last_m});
+    } else {
+      f.push_back({2, 0.0, ops[i].c, false});
+    }
+  }
+  return f;
+}
+
+namespace {
+
+using Op = HmcOp;
+using FOp = HmcFusedOp;
+std::vector<Op> schedule(int integ, int n, double tau) { return su2b_schedule(integ, n, tau); }
+std::vector<FOp> fuse(const std::vector<Op> &ops) { return su2b_fuse(ops); }
+
 int kinetic_now(su2b_ctx *ctx, int slot);
 
 bool low_precision(int integ) { return integ == SU2B_LP_LEAPFROG || integ == SU2B_LP_OMF4; }
@@ -169,29 +189,6 @@ int kinetic_now(su2b_ctx *ctx, int slot) {
 // reads links from one buffer and writes the updated links to another.  The start field S
 // is never written, so a rejected trajectory needs no copy; the two other buffers X, Y
 // alternate.  The closing restoreSU writes the final field and sums its plaquettes.
-struct FOp {
-  int kind;  // 0 momentum step, 1 momentum + gauge step, 2 gauge step alone
-  double cm, cg;
-  bool kinetic;
-};
-
-std::vector<FOp> fuse(const std::vector<Op> &ops) {
-  int last_m = -1;
-  for (int i = 0; i < (int)ops.size(); i++)
-    if (ops[i].kind == 0) last_m = i;
-  std::vector<FOp> f;
-  for (int i = 0; i < (int)ops.size(); i++) {
-    if (ops[i].kind == 0 && i + 1 < (int)ops.size() && ops[i + 1].kind == 1) {
-      f.push_back({1, ops[i].c, ops[i + 1].c, i == last_m});
-      i++;
-    } else if (ops[i].kind == 0) {
-      f.push_back({0, ops[i].c, 0.0, i == last_m});
-    } else {
-      f.push_back({2, 0.0, ops[i].c, false});
-    }
-  }
-  return f;
-}
 
 // queues the trajectory; returns the buffer that holds the final field in *fin
 // cached: the start plaquettes are those the previous trajectory left in red[] (its start

@@ -1,0 +1,716 @@
+// slabs.cu -- one lattice over time slabs: the t-slab decomposition of the HMC trajectory.
+//
+// The reference runs one lattice per process and splits the site loops over OpenMP threads
+// along t (flat-sweep.hh:83,128; flat-gaugemonomial.hh:105-131).  Here the lattice (extent Lt
+// in t, the slowest index of both the host order and the even/odd layout) is cut into
+// nslabs slabs of Tl = Lt / nslabs slices.  A slab is an ordinary context over Tl + 2
+// slices: its own slices 1 .. Tl and a ghost slice on each side (local slice 0 is the global
+// slice t0 - 1, local slice Tl + 1 the global slice t0 + Tl, periodically), with the
+// geometry's site range (cb0, ncb) set to its own slices and lex0 to the global index of its
+// local site 0.  The trajectory kernels then run on a slab unchanged:
+//   - a site's force step reads neighbours at most one slice away, so the ghost slices hold
+//     everything the slab's own sites read;
+//   - after each force launch that writes a link buffer, the ghost slices of that buffer are
+//     refreshed from the neighbouring slabs (the halo exchange);
+//   - the momenta are the Philox streams of the whole lattice (keyed by lex + lex0), and the
+//     plaquette and kinetic partials cover the slab's own sites; the sums add over the slabs
+//     before the accept/reject, which every slab then takes identically.
+// So a trajectory gives the links and accept decisions of a single-lattice context with the
+// same seed and trajectory index; the energies agree to rounding (the sums add in another
+// order).
+//
+// In a slab the sites of local slice t and parity p are the even/odd indices
+// t S/2 .. (t+1) S/2 - 1 (S sites per slice, even), so a face is 2 nd contiguous pieces of S/2
+// links, one per direction and parity.  Tl is even, so a global site has the same local
+// parity in every slab that holds it and the pieces map one to one.
+//
+// Transport.  Slabs on one device (count == nslabs) exchange faces with one copy kernel
+// over a table of pieces and add their sums with a kernel over the slabs' reduction
+// buffers, all queued on one stream, one CUDA graph per trajectory.  Slabs in separate
+// processes (one GPU each, count == 1) pack their two faces, exchange them with NCCL
+// send/recv and add the sums with an NCCL all-reduce; NCCL is loaded at run time.
+#include <dlfcn.h>
+#include <nccl.h>
+
+#include <array>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "su2b.h"
+#include "su2b_ctx.h"
+
+using namespace su2b;
+
+namespace {
+
+struct Piece {
+  const uint4 *src;
+  uint4 *dst;
+};
+
+// every piece of the table: n 16-byte words from src to dst (piece = blockIdx.y)
+__global__ void __launch_bounds__(256) k_copy_pieces(const Piece *__restrict__ pc, long n) {
+  const Piece q = pc[blockIdx.y];
+  for (long i = blockIdx.x * 256l + threadIdx.x; i < n; i += (long)gridDim.x * 256)
+    q.dst[i] = q.src[i];
+}
+
+// red[r][i] = sum over the slabs in slab order, for i < n, written back to every slab
+__global__ void k_sum_slabs(double *const *__restrict__ red, int nslab, int n) {
+  const int i = threadIdx.x;
+  if (i < n) {
+    double v = 0.;
+    for (int r = 0; r < nslab; r++) v += red[r][i];
+    for (int r = 0; r < nslab; r++) red[r][i] = v;
+  }
+}
+
+// ---- NCCL, resolved from libnccl.so.2 when the first handle connects ----
+struct NcclApi {
+  ncclResult_t (*get_unique_id)(ncclUniqueId *);
+  ncclResult_t (*comm_init_rank)(ncclComm_t *, int, ncclUniqueId, int);
+  ncclResult_t (*comm_destroy)(ncclComm_t);
+  ncclResult_t (*send)(const void *, size_t, ncclDataType_t, int, ncclComm_t, cudaStream_t);
+  ncclResult_t (*recv)(void *, size_t, ncclDataType_t, int, ncclComm_t, cudaStream_t);
+  ncclResult_t (*group_start)();
+  ncclResult_t (*group_end)();
+  ncclResult_t (*all_reduce)(const void *, void *, size_t, ncclDataType_t, ncclRedOp_t,
+                             ncclComm_t, cudaStream_t);
+  const char *(*error_string)(ncclResult_t);
+};
+
+const NcclApi *nccl_api(std::string *why) {
+  static std::mutex m;
+  static NcclApi api;
+  static int state = 0;  // 0 not tried, 1 loaded, -1 failed
+  static std::string err;
+  std::lock_guard<std::mutex> lock(m);
+  if (state == 0) {
+    void *h = dlopen("libnccl.so.2", RTLD_NOW | RTLD_GLOBAL);
+    if (!h) h = dlopen("libnccl.so", RTLD_NOW | RTLD_GLOBAL);
+    state = -1;
+    if (!h) {
+      err = std::string("libnccl.so.2 not found: ") + dlerror();
+    } else {
+      bool ok = true;
+      auto sym = [&](const char *name) {
+        void *p = dlsym(h, name);
+        if (!p) ok = false;
+        return p;
+      };
+      api.get_unique_id = (decltype(api.get_unique_id))sym("ncclGetUniqueId");
+      api.comm_init_rank = (decltype(api.comm_init_rank))sym("ncclCommInitRank");
+      api.comm_destroy = (decltype(api.comm_destroy))sym("ncclCommDestroy");
+      api.send = (decltype(api.send))sym("ncclSend");
+      api.recv = (decltype(api.recv))sym("ncclRecv");
+      api.group_start = (decltype(api.group_start))sym("ncclGroupStart");
+      api.group_end = (decltype(api.group_end))sym("ncclGroupEnd");
+      api.all_reduce = (decltype(api.all_reduce))sym("ncclAllReduce");
+      api.error_string = (decltype(api.error_string))sym("ncclGetErrorString");
+      if (ok)
+        state = 1;
+      else
+        err = "libnccl.so.2 lacks a symbol (ncclSend / ncclRecv need NCCL >= 2.7)";
+    }
+  }
+  if (state == 1) return &api;
+  *why = err;
+  return nullptr;
+}
+
+}  // namespace
+
+struct su2b_slabs {
+  int nslabs = 0, first = 0, count = 0, device = 0;
+  int Lt = 0, nd = 4, Tl = 0;
+  long S = 0;  // sites per time slice
+  bool link64 = true;
+  std::vector<su2b_ctx *> sl;
+  std::vector<cudaStream_t> own;  // the streams the slab contexts were created with
+  cudaStream_t s = nullptr;       // every slab's work is queued here
+  std::vector<std::array<void *, 3>> buf;  // each slab's three link buffers
+  int role[3] = {0, 1, 2};  // the buffers that hold the current field, and the two others
+  long piece_n = 0;         // 16-byte words per piece (S/2 links)
+  int npieces = 0;          // pieces per exchange table
+  Piece *xchg[3] = {};      // one device: the exchange of buffer k between all slabs
+  double **reds = nullptr;  // one device: the slabs' reduction buffers
+  // NCCL (one slab per process)
+  const NcclApi *nc = nullptr;
+  ncclComm_t comm = nullptr;
+  int nranks = 1, rank = 0;
+  uint4 *sendbuf = nullptr, *recvbuf = nullptr;  // [lower face | upper face]
+  Piece *pack[3] = {}, *unpack[3] = {};
+  std::vector<void *> allocs;
+  struct Graph {
+    cudaGraphExec_t exec;
+    int fin;
+    long kernels;
+  };
+  std::map<std::string, Graph> graphs;
+  long launches = 0;
+  std::string err;
+};
+
+namespace {
+
+int fail(su2b_slabs *h, int code, const std::string &msg) {
+  h->err = msg;
+  return code;
+}
+// the first slab context's error becomes the handle's, unless the handle has its own
+int from_ctx(su2b_slabs *h, int rc) {
+  if (rc != SU2B_OK && h->err.empty())
+    for (const su2b_ctx *c : h->sl)
+      if (!c->err.empty()) {
+        h->err = c->err;
+        break;
+      }
+  return rc;
+}
+#define SLAB_CUDA(call)                                                                    \
+  do {                                                                                     \
+    cudaError_t e_ = (call);                                                               \
+    if (e_ != cudaSuccess)                                                                 \
+      return fail(h, SU2B_ERR_CUDA,                                                        \
+                  std::string(#call) + ": " + cudaGetErrorString(e_));                     \
+  } while (0)
+
+// the table of pieces of local slice ts of buffer k of slab r, to dst(mu, p)
+template <class Dst>
+void face_pieces(su2b_slabs *h, int r, int k, int ts, Dst dst, std::vector<Piece> *out) {
+  const su2b_ctx *c = h->sl[r];
+  const size_t words = c->link_bytes() / 16;  // 16-byte words per link
+  for (int mu = 0; mu < h->nd; mu++)
+    for (int p = 0; p < 2; p++) {
+      const size_t l = (size_t)mu * c->g.V + (size_t)p * c->g.Vh + (size_t)ts * (h->S / 2);
+      out->push_back({(const uint4 *)h->buf[r][k] + l * words, dst(mu, p)});
+    }
+}
+size_t slice_word(const su2b_ctx *c, long S, int mu, int p, int ts) {
+  const size_t l = (size_t)mu * c->g.V + (size_t)p * c->g.Vh + (size_t)ts * (S / 2);
+  return l * (c->link_bytes() / 16);
+}
+
+int upload_table(su2b_slabs *h, const std::vector<Piece> &v, Piece **dev) {
+  void *p = nullptr;
+  SLAB_CUDA(cudaMalloc(&p, sizeof(Piece) * v.size()));
+  h->allocs.push_back(p);
+  SLAB_CUDA(cudaMemcpy(p, v.data(), sizeof(Piece) * v.size(), cudaMemcpyHostToDevice));
+  *dev = (Piece *)p;
+  return SU2B_OK;
+}
+
+// one device: for every slab r, its first slice goes to the upper ghost slice of slab r - 1
+// and its last slice to the lower ghost slice of slab r + 1 (periodically)
+int build_local_tables(su2b_slabs *h) {
+  const int R = h->count;
+  for (int k = 0; k < 3; k++) {
+    std::vector<Piece> v;
+    for (int r = 0; r < R; r++) {
+      const int dn = (r + R - 1) % R, up = (r + 1) % R;
+      const su2b_ctx *cd = h->sl[dn], *cu = h->sl[up];
+      face_pieces(h, r, k, 1, [&](int mu, int p) {
+        return (uint4 *)h->buf[dn][k] + slice_word(cd, h->S, mu, p, h->Tl + 1);
+      }, &v);
+      face_pieces(h, r, k, h->Tl, [&](int mu, int p) {
+        return (uint4 *)h->buf[up][k] + slice_word(cu, h->S, mu, p, 0);
+      }, &v);
+    }
+    h->npieces = (int)v.size();
+    SU2B_CKS(upload_table(h, v, &h->xchg[k]));
+  }
+  std::vector<double *> reds;
+  for (su2b_ctx *c : h->sl) reds.push_back(c->red);
+  void *p = nullptr;
+  SLAB_CUDA(cudaMalloc(&p, sizeof(double *) * reds.size()));
+  h->allocs.push_back(p);
+  SLAB_CUDA(cudaMemcpy(p, reds.data(), sizeof(double *) * reds.size(), cudaMemcpyHostToDevice));
+  h->reds = (double **)p;
+  return SU2B_OK;
+}
+
+// NCCL: the faces of buffer k packed as [first slice | last slice], and the received faces
+// [from the slab below | from the slab above] unpacked into [ghost 0 | ghost Tl + 1]
+int build_nccl_tables(su2b_slabs *h) {
+  const su2b_ctx *c = h->sl[0];
+  const long face = 2l * h->nd * h->piece_n;
+  for (int k = 0; k < 3; k++) {
+    std::vector<Piece> pk, up;
+    int i = 0;
+    face_pieces(h, 0, k, 1, [&](int, int) { return h->sendbuf + (i++) * h->piece_n; }, &pk);
+    face_pieces(h, 0, k, h->Tl, [&](int, int) { return h->sendbuf + (i++) * h->piece_n; },
+                &pk);
+    for (int side = 0; side < 2; side++)
+      for (int mu = 0; mu < h->nd; mu++)
+        for (int p = 0; p < 2; p++)
+          up.push_back({h->recvbuf + side * face + (2 * mu + p) * h->piece_n,
+                        (uint4 *)h->buf[0][k] +
+                          slice_word(c, h->S, mu, p, side == 0 ? 0 : h->Tl + 1)});
+    SU2B_CKS(upload_table(h, pk, &h->pack[k]));
+    SU2B_CKS(upload_table(h, up, &h->unpack[k]));
+  }
+  return SU2B_OK;
+}
+
+cudaError_t copy_pieces(const Piece *tab, int npieces, long n, cudaStream_t s) {
+  const long blocks = (n + 255) / 256;
+  k_copy_pieces<<<dim3((unsigned)(blocks < 64 ? blocks : 64), npieces), 256, 0, s>>>(tab, n);
+  return cudaGetLastError();
+}
+
+#define NCCL_CK(call)                                                                      \
+  do {                                                                                     \
+    ncclResult_t r_ = (call);                                                              \
+    if (r_ != ncclSuccess)                                                                 \
+      return fail(h, SU2B_ERR_CUDA, std::string(#call) + ": " + h->nc->error_string(r_));  \
+  } while (0)
+
+// refresh the ghost slices of buffer k of every slab
+int exchange(su2b_slabs *h, int k) {
+  if (!h->comm) {
+    SLAB_CUDA(copy_pieces(h->xchg[k], h->npieces, h->piece_n, h->s));
+    h->launches++;
+    return SU2B_OK;
+  }
+  const long face = 2l * h->nd * h->piece_n;
+  const size_t bytes = (size_t)face * 16;
+  const int up = (h->rank + 1) % h->nranks, dn = (h->rank + h->nranks - 1) % h->nranks;
+  SLAB_CUDA(copy_pieces(h->pack[k], 4 * h->nd, h->piece_n, h->s));
+  // with two slabs both neighbours are one process: sends and receives to one peer match
+  // in the order they are posted, so the order is the same on every rank
+  NCCL_CK(h->nc->group_start());
+  NCCL_CK(h->nc->send(h->sendbuf + face, bytes, ncclUint8, up, h->comm, h->s));
+  NCCL_CK(h->nc->send(h->sendbuf, bytes, ncclUint8, dn, h->comm, h->s));
+  NCCL_CK(h->nc->recv(h->recvbuf, bytes, ncclUint8, dn, h->comm, h->s));
+  NCCL_CK(h->nc->recv(h->recvbuf + face, bytes, ncclUint8, up, h->comm, h->s));
+  NCCL_CK(h->nc->group_end());
+  SLAB_CUDA(copy_pieces(h->unpack[k], 4 * h->nd, h->piece_n, h->s));
+  h->launches += 2;
+  return SU2B_OK;
+}
+
+// red[0 .. n-1] of every slab becomes the sum over all slabs
+int sum_over_slabs(su2b_slabs *h, int n) {
+  if (!h->comm) {
+    k_sum_slabs<<<1, 32, 0, h->s>>>(h->reds, h->count, n);
+    SLAB_CUDA(cudaGetLastError());
+    h->launches++;
+    return SU2B_OK;
+  }
+  NCCL_CK(h->nc->all_reduce(h->sl[0]->red, h->sl[0]->red, (size_t)n, ncclFloat64, ncclSum,
+                            h->comm, h->s));
+  return SU2B_OK;
+}
+
+bool connected(const su2b_slabs *h) { return h->count == h->nslabs || h->comm != nullptr; }
+
+void set_roles(su2b_slabs *h) {
+  for (int r = 0; r < h->count; r++) {
+    h->sl[r]->U = h->buf[r][h->role[0]];
+    h->sl[r]->U_old = h->buf[r][h->role[1]];
+    h->sl[r]->U2 = h->buf[r][h->role[2]];
+  }
+}
+
+// the fused trajectory over all slabs (the single-lattice form is enqueue_fused in hmc.cu):
+// S (buffer role[0]) is never written; X and Y alternate; *fin receives the buffer that holds
+// the final field
+template <class T>
+int enqueue(su2b_slabs *h, const std::vector<HmcFusedOp> &fops, int *fin) {
+  const int R = h->count;
+  const int iS = h->role[0], iX = h->role[1], iY = h->role[2];
+  cudaStream_t s = h->s;
+  std::vector<int> nb_start(R, 0), nb_kin(R, 0), nb_plaq(R, 0);
+  for (int r = 0; r < R; r++) {
+    su2b_ctx *ctx = h->sl[r];
+    SU2B_LAUNCH(SU2B_K_MOMENTA, momenta_plaq<T>(ctx->g, h->buf[r][iS], (T *)ctx->P,
+                                                ctx->tparams, ctx->xi, ctx->part_slot(1),
+                                                &nb_start[r], s, true));
+  }
+  const double f = h->sl[0]->beta / h->sl[0]->Nc();
+  int cur = iS, F = -1;
+  auto next = [&](int c) { return c == iX ? iY : iX; };
+  for (size_t i = 0; i < fops.size(); i++) {
+    const HmcFusedOp &o = fops[i];
+    int mode = FM_HAS_IN | (o.kinetic ? FM_KINETIC : 0);
+    int out;
+    if (o.kind == 1) {
+      mode |= FM_UPDATE;
+      out = next(cur);
+    } else {  // the last momentum step writes the reunitarised final field
+      mode |= FM_RESTORE;
+      out = F = (cur == iS) ? iX : next(cur);
+    }
+    for (int r = 0; r < R; r++) {
+      su2b_ctx *ctx = h->sl[r];
+      int nb = 0;
+      SU2B_LAUNCH(SU2B_K_FORCE,
+                  force_update<T>(ctx->g, h->buf[r][cur], 0, (T *)ctx->P, nullptr, f, -o.cm,
+                                  ctx->xi, mode, ctx->part_slot(2), &nb, h->buf[r][out], o.cg, s,
+                                  ctx->tune_force, false));
+      if (o.kinetic) nb_kin[r] = nb;
+    }
+    SU2B_CKS(exchange(h, out));
+    if (o.kind == 1) cur = out;
+  }
+  for (int r = 0; r < R; r++) {
+    su2b_ctx *ctx = h->sl[r];
+    SU2B_LAUNCH(SU2B_K_PLAQUETTE, plaq_partials<T>(ctx->g, h->buf[r][F], 0, ctx->xi,
+                                                   ctx->part_slot(0), &nb_plaq[r], s));
+    SU2B_CK(cudaMemsetAsync(ctx->red, 0, 10 * sizeof(double), s));
+    SU2B_LAUNCH(SU2B_K_OTHER, reduce_final(ctx->part_slot(1), nb_start[r], 4, ctx->red, s));
+    SU2B_LAUNCH(SU2B_K_OTHER, reduce_final(ctx->part_slot(2), nb_kin[r], 1, ctx->red + 4, s));
+    SU2B_LAUNCH(SU2B_K_OTHER, reduce_final(ctx->part_slot(0), nb_plaq[r], 3, ctx->red + 5, s));
+  }
+  SU2B_CKS(sum_over_slabs(h, 8));
+  for (int r = 0; r < R; r++) {
+    su2b_ctx *ctx = h->sl[r];
+    SU2B_LAUNCH(SU2B_K_OTHER, accept_step(ctx->red, ctx->tparams, ctx->traj, s));
+  }
+  su2b_ctx *ctx = h->sl[0];
+  SU2B_CK(cudaMemcpyAsync(ctx->h_traj, ctx->traj, sizeof(TrajDev), cudaMemcpyDeviceToHost, s));
+  SU2B_CK(cudaMemcpyAsync(ctx->h_red, ctx->red, 10 * sizeof(double), cudaMemcpyDeviceToHost, s));
+  *fin = F;
+  return SU2B_OK;
+}
+
+long ctx_launches(const su2b_slabs *h) {
+  long n = 0;
+  for (const su2b_ctx *c : h->sl) n += c->launches;
+  return n;
+}
+void reset_launches(su2b_slabs *h, const std::vector<long> &ctx_n, long own_n) {
+  for (size_t r = 0; r < h->sl.size(); r++) h->sl[r]->launches = ctx_n[r];
+  h->launches = own_n;
+}
+
+int trajectory(su2b_slabs *h, const su2b_hmc_params *prm, su2b_traj_result *res) {
+  if (!prm || !res) return fail(h, SU2B_ERR_INVALID, "params or result is NULL");
+  if (prm->n_steps < 1) return fail(h, SU2B_ERR_INVALID, "n_steps must be >= 1");
+  if (!connected(h))
+    return fail(h, SU2B_ERR_INVALID,
+                "the handle holds a part of the slabs: connect it to the others first");
+  if (prm->momenta_host || prm->revtest || prm->fermion_mass > 0.0)
+    return fail(h, SU2B_ERR_UNSUPPORTED,
+                "slabs take Philox momenta, no reversibility test and no fermions");
+  const std::vector<HmcFusedOp> fops =
+    su2b_fuse(su2b_schedule(prm->integrator, prm->n_steps, prm->tau));
+  const bool fused_form = prm->integrator == SU2B_LEAPFROG || prm->integrator == SU2B_OMF2 ||
+                          prm->integrator == SU2B_OMF4;
+  for (size_t i = 0; i < fops.size(); i++)
+    if (!fused_form || fops[i].kind != (i + 1 == fops.size() ? 0 : 1))
+      return fail(h, SU2B_ERR_UNSUPPORTED,
+                  "slabs run leapfrog, omf2 and omf4 (momentum steps with fused gauge steps)");
+  for (su2b_ctx *c : h->sl) c->begin_call();
+  cudaStream_t s = h->s;
+  for (su2b_ctx *c : h->sl) {
+    TrajParams &tp = *c->h_tparams;
+    tp.beta = c->beta;
+    tp.Nc = c->Nc();
+    tp.u_host = prm->uniform_host;
+    tp.seed = prm->seed;
+    tp.traj = prm->traj;
+    tp.accept_reject = prm->accept_reject;
+    SLAB_CUDA(cudaMemcpyAsync(c->tparams, c->h_tparams, sizeof(TrajParams),
+                              cudaMemcpyHostToDevice, s));
+  }
+  int F = -1;
+  if (h->comm) {  // NCCL: launched directly
+    const int rc = h->link64 ? enqueue<double>(h, fops, &F) : enqueue<float>(h, fops, &F);
+    if (rc != SU2B_OK) return from_ctx(h, rc);
+  } else {
+    char key[192];
+    snprintf(key, sizeof key, "%d/%d/%.17g/%d%d%d/%d", prm->integrator, prm->n_steps, prm->tau,
+             h->role[0], h->role[1], h->role[2], h->sl[0]->tune_force);
+    auto it = h->graphs.find(key);
+    if (it == h->graphs.end()) {
+      // the capture counts the graph's kernels; each replay adds them
+      std::vector<long> ctx_n;
+      for (const su2b_ctx *c : h->sl) ctx_n.push_back(c->launches);
+      const long own_n = h->launches, n0 = ctx_launches(h) + own_n;
+      cudaGraph_t graph = nullptr;
+      SLAB_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+      const int rc = h->link64 ? enqueue<double>(h, fops, &F) : enqueue<float>(h, fops, &F);
+      const cudaError_t ec = cudaStreamEndCapture(s, &graph);
+      const long kernels = ctx_launches(h) + h->launches - n0;
+      reset_launches(h, ctx_n, own_n);
+      if (rc != SU2B_OK) {
+        if (graph) cudaGraphDestroy(graph);
+        return from_ctx(h, rc);
+      }
+      SLAB_CUDA(ec);
+      su2b_slabs::Graph gr{nullptr, F, kernels};
+      const cudaError_t ei = cudaGraphInstantiate(&gr.exec, graph, 0);
+      cudaGraphDestroy(graph);
+      SLAB_CUDA(ei);
+      it = h->graphs.emplace(key, gr).first;
+    }
+    F = it->second.fin;
+    SLAB_CUDA(cudaGraphLaunch(it->second.exec, s));
+    h->launches += it->second.kernels;
+  }
+  SLAB_CUDA(cudaStreamSynchronize(s));
+  const TrajDev &t = *h->sl[0]->h_traj;
+  const double *red = h->sl[0]->h_red;
+  if (t.accepted) {  // the final field becomes current
+    const int S0 = h->role[0], X0 = h->role[1], Y0 = h->role[2];
+    h->role[0] = F;
+    h->role[1] = S0;
+    h->role[2] = (F == X0) ? Y0 : X0;
+    set_roles(h);
+  }
+  res->accepted = t.accepted;
+  res->dH = t.dH;
+  for (int k = 0; k < 3; k++) {
+    res->H_old[k] = t.H_old[k];
+    res->H_new[k] = t.H_new[k];
+  }
+  res->ddH = 0.0;
+  res->plaquette = t.accepted ? red[5] : red[1];
+  res->cg_iterations = 0;
+  return SU2B_OK;
+}
+
+}  // namespace
+
+extern "C" int su2b_slabs_create(int Lx, int Ly, int Lz, int Lt, int ndims, double beta,
+                                 double xi, int precision, int nslabs, int first, int count,
+                                 int device, su2b_slabs **out) {
+  if (!out) return SU2B_ERR_INVALID;
+  *out = nullptr;
+  if (ndims < 2 || ndims > 4 || nslabs < 1 || count < 1 || first < 0 ||
+      first + count > nslabs)
+    return SU2B_ERR_INVALID;
+  if (Lt % nslabs != 0 || (Lt / nslabs) % 2 != 0) return SU2B_ERR_INVALID;
+  su2b_slabs *h = new su2b_slabs();
+  h->nslabs = nslabs;
+  h->first = first;
+  h->count = count;
+  h->device = device;
+  h->Lt = Lt;
+  h->nd = ndims;
+  h->Tl = Lt / nslabs;
+  h->S = (long)Lx * Ly * Lz;
+  auto fin = [&](int rc) -> int {
+    if (rc != SU2B_OK) {
+      su2b_slabs_destroy(h);
+      return rc;
+    }
+    *out = h;
+    return SU2B_OK;
+  };
+  for (int r = 0; r < count; r++) {
+    su2b_ctx *c = nullptr;
+    const int rc = su2b_ctx_create(SU2B_GROUP_SU2, Lx, Ly, Lz, h->Tl + 2, ndims, beta, xi,
+                                   precision, device, &c);
+    if (rc != SU2B_OK) return fin(rc);
+    h->sl.push_back(c);
+    h->own.push_back(c->stream);
+    const int t0 = (first + r) * h->Tl;
+    c->g.cb0 = (int)(h->S / 2);
+    c->g.ncb = (int)(h->Tl * h->S / 2);
+    c->g.lex0 = (int)((long)(t0 - 1) * h->S);
+    h->buf.push_back({c->U, c->U_old, c->U2});
+  }
+  h->link64 = h->sl[0]->link64;
+  h->s = h->sl[0]->stream;
+  for (su2b_ctx *c : h->sl) c->stream = h->s;
+  h->piece_n = (h->S / 2) * (long)(h->sl[0]->link_bytes() / 16);
+  if (cudaSetDevice(device) != cudaSuccess) return fin(fail(h, SU2B_ERR_CUDA, "cudaSetDevice"));
+  if (count == nslabs) return fin(build_local_tables(h));
+  return fin(SU2B_OK);
+}
+
+extern "C" int su2b_slabs_destroy(su2b_slabs *h) {
+  if (!h) return SU2B_ERR_INVALID;
+  cudaSetDevice(h->device);
+  if (h->s) cudaStreamSynchronize(h->s);
+  for (auto &kv : h->graphs) cudaGraphExecDestroy(kv.second.exec);
+  if (h->comm && h->nc) h->nc->comm_destroy(h->comm);
+  for (void *p : h->allocs) cudaFree(p);
+  for (size_t r = 0; r < h->sl.size(); r++) {
+    h->sl[r]->stream = h->own[r];
+    su2b_ctx_destroy(h->sl[r]);
+  }
+  delete h;
+  return SU2B_OK;
+}
+
+extern "C" const char *su2b_slabs_last_error(const su2b_slabs *h) {
+  return h ? h->err.c_str() : "null handle";
+}
+
+extern "C" int su2b_slabs_info(const su2b_slabs *h, int *nslabs, int *first, int *count,
+                               int *slices) {
+  if (!h) return SU2B_ERR_INVALID;
+  if (nslabs) *nslabs = h->nslabs;
+  if (first) *first = h->first;
+  if (count) *count = h->count;
+  if (slices) *slices = h->Tl;
+  return SU2B_OK;
+}
+
+extern "C" int su2b_slabs_nccl_id(void *id) {
+  if (!id) return SU2B_ERR_INVALID;
+  std::string why;
+  const NcclApi *nc = nccl_api(&why);
+  if (!nc) return SU2B_ERR_UNSUPPORTED;
+  ncclUniqueId u;
+  if (nc->get_unique_id(&u) != ncclSuccess) return SU2B_ERR_CUDA;
+  memcpy(id, &u, sizeof u);
+  return SU2B_OK;
+}
+
+extern "C" int su2b_slabs_connect(su2b_slabs *h, const void *id, int nranks, int rank) {
+  if (!h) return SU2B_ERR_INVALID;
+  h->err.clear();
+  if (!id) return fail(h, SU2B_ERR_INVALID, "id is NULL");
+  if (h->comm) return fail(h, SU2B_ERR_INVALID, "already connected");
+  if (h->count != 1 || nranks != h->nslabs || rank != h->first)
+    return fail(h, SU2B_ERR_INVALID,
+                "connect wants one slab per process: nranks = nslabs, rank = first");
+  std::string why;
+  h->nc = nccl_api(&why);
+  if (!h->nc) return fail(h, SU2B_ERR_UNSUPPORTED, why);
+  SLAB_CUDA(cudaSetDevice(h->device));
+  ncclUniqueId u;
+  memcpy(&u, id, sizeof u);
+  ncclComm_t comm = nullptr;
+  NCCL_CK(h->nc->comm_init_rank(&comm, nranks, u, rank));
+  h->comm = comm;
+  h->nranks = nranks;
+  h->rank = rank;
+  const size_t bytes = (size_t)4 * h->nd * h->piece_n * 16;  // two faces
+  void *a = nullptr, *b = nullptr;
+  SLAB_CUDA(cudaMalloc(&a, bytes));
+  h->allocs.push_back(a);
+  SLAB_CUDA(cudaMalloc(&b, bytes));
+  h->allocs.push_back(b);
+  h->sendbuf = (uint4 *)a;
+  h->recvbuf = (uint4 *)b;
+  return build_nccl_tables(h);
+}
+
+// host field of the whole lattice (reference order, t slowest): rows of S nd links
+extern "C" int su2b_slabs_upload(su2b_slabs *h, const double *U_host) {
+  if (!h) return SU2B_ERR_INVALID;
+  h->err.clear();
+  if (!U_host) return fail(h, SU2B_ERR_INVALID, "U_host is NULL");
+  SLAB_CUDA(cudaSetDevice(h->device));
+  const size_t row = (size_t)h->S * h->nd * 4;  // doubles per time slice
+  for (int r = 0; r < h->count; r++) {
+    su2b_ctx *c = h->sl[r];
+    c->begin_call();
+    const int t0 = (h->first + r) * h->Tl;
+    const int lo = (t0 + h->Lt - 1) % h->Lt, hi = (t0 + h->Tl) % h->Lt;
+    SLAB_CUDA(cudaMemcpyAsync(c->stage, U_host + lo * row, row * 8, cudaMemcpyHostToDevice,
+                              h->s));
+    SLAB_CUDA(cudaMemcpyAsync(c->stage + row, U_host + t0 * row, h->Tl * row * 8,
+                              cudaMemcpyHostToDevice, h->s));
+    SLAB_CUDA(cudaMemcpyAsync(c->stage + (h->Tl + 1) * row, U_host + hi * row, row * 8,
+                              cudaMemcpyHostToDevice, h->s));
+    su2b_ctx *ctx = c;
+    if (h->link64)
+      SU2B_LAUNCH(SU2B_K_OTHER, links_from_host<double>(c->g, c->stage, c->U, 0, h->s));
+    else
+      SU2B_LAUNCH(SU2B_K_OTHER, links_from_host<float>(c->g, c->stage, c->U, 0, h->s));
+  }
+  SLAB_CUDA(cudaStreamSynchronize(h->s));
+  return SU2B_OK;
+}
+
+extern "C" int su2b_slabs_download(su2b_slabs *h, double *U_host) {
+  if (!h) return SU2B_ERR_INVALID;
+  h->err.clear();
+  if (!U_host) return fail(h, SU2B_ERR_INVALID, "U_host is NULL");
+  SLAB_CUDA(cudaSetDevice(h->device));
+  const size_t row = (size_t)h->S * h->nd * 4;
+  for (int r = 0; r < h->count; r++) {
+    su2b_ctx *c = h->sl[r];
+    c->begin_call();
+    const int t0 = (h->first + r) * h->Tl;
+    su2b_ctx *ctx = c;
+    if (h->link64)
+      SU2B_LAUNCH(SU2B_K_OTHER, links_to_host<double>(c->g, c->U, c->stage, 0, h->s));
+    else
+      SU2B_LAUNCH(SU2B_K_OTHER, links_to_host<float>(c->g, c->U, c->stage, 0, h->s));
+    SLAB_CUDA(cudaMemcpyAsync(U_host + t0 * row, c->stage + row, h->Tl * row * 8,
+                              cudaMemcpyDeviceToHost, h->s));
+  }
+  SLAB_CUDA(cudaStreamSynchronize(h->s));
+  return SU2B_OK;
+}
+
+extern "C" int su2b_slabs_hmc_trajectory(su2b_slabs *h, const su2b_hmc_params *prm,
+                                         su2b_traj_result *res) {
+  if (!h) return SU2B_ERR_INVALID;
+  h->err.clear();
+  SLAB_CUDA(cudaSetDevice(h->device));
+  return trajectory(h, prm, res);
+}
+
+extern "C" int su2b_slabs_gauge_energy(su2b_slabs *h, int spatial_only, double *out) {
+  if (!h) return SU2B_ERR_INVALID;
+  h->err.clear();
+  if (!out) return fail(h, SU2B_ERR_INVALID, "out is NULL");
+  if (!connected(h))
+    return fail(h, SU2B_ERR_INVALID,
+                "the handle holds a part of the slabs: connect it to the others first");
+  SLAB_CUDA(cudaSetDevice(h->device));
+  for (su2b_ctx *ctx : h->sl) {
+    ctx->begin_call();
+    int nb = 0;
+    if (h->link64)
+      SU2B_LAUNCH(SU2B_K_PLAQUETTE, plaq_partials<double>(ctx->g, ctx->U, 0, ctx->xi,
+                                                          ctx->part_slot(0), &nb, h->s));
+    else
+      SU2B_LAUNCH(SU2B_K_PLAQUETTE, plaq_partials<float>(ctx->g, ctx->U, 0, ctx->xi,
+                                                         ctx->part_slot(0), &nb, h->s));
+    SU2B_LAUNCH(SU2B_K_OTHER, reduce_final(ctx->part_slot(0), nb, 3, ctx->red, h->s));
+  }
+  SU2B_CKS(sum_over_slabs(h, 3));
+  su2b_ctx *c = h->sl[0];
+  SLAB_CUDA(cudaMemcpyAsync(c->h_red, c->red, 3 * sizeof(double), cudaMemcpyDeviceToHost, h->s));
+  SLAB_CUDA(cudaStreamSynchronize(h->s));
+  *out = c->h_red[spatial_only ? 1 : 0];
+  return SU2B_OK;
+}
+
+extern "C" int su2b_slabs_autotune(su2b_slabs *h, double *times_us) {
+  if (!h) return SU2B_ERR_INVALID;
+  h->err.clear();
+  const int rc = su2b_autotune(h->sl[0], nullptr, 1, times_us);
+  if (rc != SU2B_OK) return from_ctx(h, rc);
+  for (su2b_ctx *c : h->sl) c->tune_force = h->sl[0]->tune_force;
+  return SU2B_OK;
+}
+
+extern "C" int su2b_slabs_tune_get(su2b_slabs *h, int *variant) {
+  if (!h || !variant) return SU2B_ERR_INVALID;
+  *variant = h->sl[0]->tune_force;
+  return SU2B_OK;
+}
+
+extern "C" int su2b_slabs_tune_set(su2b_slabs *h, int variant) {
+  if (!h) return SU2B_ERR_INVALID;
+  h->err.clear();
+  if (variant < 0 || variant >= FORCE_VARIANTS)
+    return fail(h, SU2B_ERR_INVALID, "force variant out of range");
+  for (su2b_ctx *c : h->sl) c->tune_force = variant;
+  return SU2B_OK;
+}
+
+extern "C" int su2b_slabs_kernel_launches(su2b_slabs *h, long *count) {
+  if (!h || !count) return SU2B_ERR_INVALID;
+  *count = ctx_launches(h) + h->launches;
+  return SU2B_OK;
+}
+
+extern "C" int su2b_slabs_stream(su2b_slabs *h, void **stream) {
+  if (!h || !stream) return SU2B_ERR_INVALID;
+  *stream = (void *)h->s;
+  return SU2B_OK;
+}

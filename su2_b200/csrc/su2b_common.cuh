@@ -47,6 +47,13 @@ struct Geom {
   int st[4];    // lexicographic stride of each direction (st[3] = 1)
   int V, Vh;    // volume, half volume
   FastDiv dv[4];
+  // The sites the trajectory kernels (force, plaquettes, momenta) cover: even/odd indices
+  // cb0 .. cb0 + ncb - 1 of each parity.  0 and Vh for a whole lattice; for a time slab with
+  // one ghost slice on each side, the slab's own slices.
+  int cb0, ncb;
+  // index in the whole lattice of the local site with lexicographic index 0 (the slab's
+  // first ghost slice; may be negative), added to a site's index for its Philox stream
+  int lex0;
 };
 
 // a site held in registers: coordinates, lexicographic index and parity

@@ -95,6 +95,19 @@ struct su2b_ctx {
   double *part_slot(int k) { return part + (size_t)k * 3 * part_cap; }
 };
 
+// the integrator schedules (integrator.hh), shared by the single-lattice and slab drivers
+struct HmcOp {
+  int kind;  // 0 momenta: P -= c * deriv;  1 gauge: U = exp(c P) U
+  double c;
+};
+struct HmcFusedOp {
+  int kind;  // 0 momentum step, 1 momentum + gauge step, 2 gauge step alone
+  double cm, cg;
+  bool kinetic;  // the last momentum step: its launch also sums |P|^2
+};
+std::vector<HmcOp> su2b_schedule(int integ, int n, double tau);
+std::vector<HmcFusedOp> su2b_fuse(const std::vector<HmcOp> &ops);
+
 // helpers shared by the api*.cu files
 int su2b_fail(su2b_ctx *ctx, int code, const char *fmt, ...);
 int su2b_adj_upload(su2b_ctx *ctx, const double *host, void *dev);

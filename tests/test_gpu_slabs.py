@@ -1,0 +1,190 @@
+"""One lattice over time slabs (su2b_slabs_*) against the single-lattice trajectory.
+
+The slab trajectory runs the same kernels on each slab's own sites with ghost slices
+refreshed after every force launch, and takes the Philox momenta of the whole lattice, so it
+must give the single-lattice context's links bit for bit and its accept decisions, with the
+energies equal to rounding (the sums add in another order: dH within 1e-13 of the energies'
+magnitude, plaquette sums within 1e-12 relative).  Slabs here all live on one device (the exchange is a device copy); the
+NCCL transport between processes shares everything but the copy.
+"""
+import numpy as np
+import pytest
+
+from helpers import rel
+
+pytestmark = pytest.mark.gpu
+
+SEED, TRAFO = 13526463, 654321
+
+
+def hot(orc, dims, nd):
+    return orc.hotstart(0, dims, nd, SEED, 1.0, TRAFO)
+
+
+def single(gpu, dims, nd, precision, beta=2.3):
+    Lx, Ly, Lz, Lt = dims
+    return gpu.gaugeconfig(Lx, Ly, Lz, Lt, nd, beta, group="su2", precision=precision)
+
+
+def slabs(dims, nd, nslabs, precision, beta=2.3, **kw):
+    from su2_b200.slabs import slab_lattice
+    return slab_lattice(dims, nd, beta, nslabs, precision=precision, **kw)
+
+
+def chain(lat, n, integrator="omf2", n_steps=4, tau=1.0, seed=11):
+    """n trajectories: even ones are accepted without the test; odd ones take one coarse
+    step (n = 1, tau = 2: dH large and positive) and the test with the uniform 0.999999,
+    so the chain sees accepted and rejected trajectories."""
+    return [lat.md_update(integrator, n_steps, tau, seed=seed, traj=k, accept_reject=False)
+            if k % 2 == 0 else
+            lat.md_update(integrator, 1, 2.0, seed=seed, traj=k, uniform=0.999999)
+            for k in range(n)]
+
+
+def same_chain(a, b):
+    assert [r.accepted for r in a] == [r.accepted for r in b]
+    for x, y in zip(a, b):
+        # the energies are sums over the lattice added in another order
+        scale = sum(abs(h) for h in x.H_old + x.H_new)
+        assert x.dH == pytest.approx(y.dH, abs=1e-13 * scale + 1e-9)
+        assert x.plaquette == pytest.approx(y.plaquette, rel=1e-12)
+        for k in range(2):
+            assert x.H_old[k] == pytest.approx(y.H_old[k], rel=1e-12)
+            assert x.H_new[k] == pytest.approx(y.H_new[k], rel=1e-12)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+@pytest.mark.parametrize("dims,nd,nslabs", [
+    ((8, 8, 8, 8), 4, 1), ((8, 8, 8, 8), 4, 2), ((8, 8, 8, 8), 4, 4),
+    ((4, 6, 8, 12), 4, 3), ((4, 6, 8, 12), 4, 6), ((8, 6, 1, 8), 3, 2), ((6, 1, 1, 8), 2, 4)],
+    ids=["8^4/1", "8^4/2", "8^4/4", "4x6x8x12/3", "4x6x8x12/6", "8x6x8-d3/2", "6x8-d2/4"])
+def test_slabs_equal_the_single_lattice(gpu, orc, precision, dims, nd, nslabs):
+    U = hot(orc, dims, nd)
+    with single(gpu, dims, nd, precision) as c, slabs(dims, nd, nslabs, precision) as s:
+        c.upload(U)
+        s.upload(U)
+        assert s.gauge_energy() == pytest.approx(c.gauge_energy(), rel=1e-13)
+        assert s.gauge_energy(True) == pytest.approx(c.gauge_energy(True), rel=1e-13, abs=1e-12)
+        a, b = chain(c, 8), chain(s, 8)
+        same_chain(a, b)
+        acc = [r.accepted for r in a]
+        assert any(acc) and not all(acc)
+        assert np.array_equal(c.download(), s.download())
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+@pytest.mark.parametrize("integrator,n_steps", [("leapfrog", 5), ("omf4", 2), ("omf2", 1)])
+def test_slab_integrators(gpu, orc, precision, integrator, n_steps):
+    dims, nd = (6, 6, 6, 8), 4
+    U = hot(orc, dims, nd)
+    with single(gpu, dims, nd, precision) as c, slabs(dims, nd, 2, precision) as s:
+        c.upload(U)
+        s.upload(U)
+        same_chain(chain(c, 4, integrator, n_steps, 0.5), chain(s, 4, integrator, n_steps, 0.5))
+        assert np.array_equal(c.download(), s.download())
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_every_force_shape_on_slabs(gpu, orc, precision):
+    """Each launch shape of the force kernel, the two-threads-per-site ones and the
+    one-thread-per-link one included, covers exactly a slab's own sites: the same links
+    as the single lattice with that shape."""
+    dims, nd = (6, 6, 6, 8), 4
+    U = hot(orc, dims, nd)
+    for v in range(gpu._abi.FORCE_VARIANTS):
+        with single(gpu, dims, nd, precision) as c, slabs(dims, nd, 2, precision) as s:
+            c.force_variant = v
+            s.tune_set(v)
+            assert s.tune_get() == v
+            c.upload(U)
+            s.upload(U)
+            same_chain(chain(c, 2), chain(s, 2))
+            assert np.array_equal(c.download(), s.download()), v
+
+
+def test_slabs_at_the_workload_size(gpu):
+    """32^4, beta 2.4, omf2 tau 1 n 16 in mixed precision over 2 and 4 slabs, with the
+    launch shape the tuner picks: the single lattice's links after three trajectories."""
+    dims, nd = (32, 32, 32, 32), 4
+    rng = np.random.default_rng(7)
+    q = rng.standard_normal((32 ** 4 * 4, 4))
+    U = (q / np.linalg.norm(q, axis=1, keepdims=True)).ravel()
+    with single(gpu, dims, nd, "mixed", beta=2.4) as c:
+        c.upload(U)
+        c.autotune()
+        v = c.force_variant
+        ref = chain(c, 3, "omf2", 16, 1.0, seed=3)
+        Uc = c.download()
+    for n in (2, 4):
+        with slabs(dims, nd, n, "mixed", beta=2.4) as s:
+            s.upload(U)
+            s.tune_set(v)
+            same_chain(ref, chain(s, 3, "omf2", 16, 1.0, seed=3))
+            assert np.array_equal(Uc, s.download())
+
+
+def test_part_of_the_slabs(gpu, orc):
+    """A handle of one slab of two uploads its slices and ghosts from the whole field and
+    downloads only its own slices; without a communicator it refuses trajectories and
+    sums."""
+    dims, nd = (4, 4, 4, 8), 4
+    U = hot(orc, dims, nd)
+    with slabs(dims, nd, 2, "fp64", first=1, count=1) as s:
+        assert s.slices() == (4, 8)
+        s.upload(U)
+        out = np.zeros_like(U)
+        s.download(out)
+        row = 4 * 4 * 4 * nd * 4
+        assert np.array_equal(out[4 * row:], U[4 * row:])
+        assert not out[:4 * row].any()
+        with pytest.raises(gpu.Su2bError) as e:
+            s.md_update("omf2", 2, 1.0)
+        assert e.value.code == gpu._abi.ERR_INVALID
+        with pytest.raises(gpu.Su2bError):
+            s.gauge_energy()
+
+
+def test_slab_errors(gpu, orc):
+    from su2_b200.slabs import slab_lattice
+    # Lt = 8: not a multiple of 3; one (odd) slice per slab; more slabs than slices
+    for nslabs in (3, 8, 16):
+        with pytest.raises(gpu.Su2bError) as e:
+            slab_lattice((4, 4, 4, 8), 4, 2.3, nslabs)
+        assert e.value.code == gpu._abi.ERR_INVALID
+    with pytest.raises(gpu.Su2bError):
+        slab_lattice((4, 4, 4, 8), 4, 2.3, 2, first=1, count=2)
+    dims, nd = (4, 4, 4, 8), 4
+    U = hot(orc, dims, nd)
+    with slabs(dims, nd, 2, "fp64") as s:
+        s.upload(U)
+        for integ in ("euler", "ruth", "lp_leapfrog"):
+            with pytest.raises(gpu.Su2bError) as e:
+                s.md_update(integ, 2, 1.0)
+            assert e.value.code == gpu._abi.ERR_UNSUPPORTED
+        with pytest.raises(gpu.Su2bError) as e:
+            s.md_update("omf2", 2, 1.0, momenta=orc.initnormal(0, dims, nd, 5)[0])
+        assert e.value.code == gpu._abi.ERR_UNSUPPORTED
+        with pytest.raises(gpu.Su2bError) as e:
+            s.tune_set(gpu._abi.FORCE_VARIANTS)
+        assert e.value.code == gpu._abi.ERR_INVALID
+        # the handle still works after the refusals
+        assert np.isfinite(s.md_update("omf2", 2, 1.0).dH)
+
+
+def test_slab_graph_replay(gpu, orc):
+    """A trajectory is one graph: every replay queues the same kernels, and the kernel
+    count is the per-slab force launches plus the exchanges and reductions."""
+    dims, nd, n = (6, 6, 6, 8), 4, 2
+    U = hot(orc, dims, nd)
+    with slabs(dims, nd, n, "mixed") as s:
+        s.upload(U)
+        counts = []
+        for k in range(4):
+            n0 = s.kernel_launches()
+            s.md_update("omf2", 3, 1.0, seed=1, traj=k, uniform=1e-300)
+            counts.append(s.kernel_launches() - n0)
+        nf = 2 * 3 + 1  # omf2 force launches
+        # per slab: momenta, nf forces, plaquettes, three reductions, accept; per launch
+        # step one exchange; one cross-slab sum
+        assert counts == [n * (nf + 6) + nf + 1] * 4
+        assert rel(s.download(), U) > 0
