@@ -201,6 +201,25 @@ def blocked(x, nblocks=20):
     return float(x.mean()), float(b.std(ddof=1) / np.sqrt(nblocks))
 
 
+def ks_effective(a, b):
+    """Two-sample Kolmogorov-Smirnov test of two Markov chains' samples.  The statistic D is
+    the samples' own; its p-value takes each chain's effective size n / (2 tau), with
+    2 tau = (20-block error / naive error)^2 of the chain's mean (at least 1), in the
+    asymptotic Kolmogorov distribution.  Correlated samples (a rejected trajectory leaves the
+    field, and the next Delta H is drawn on it) make the plain p-value far too small."""
+    from scipy import stats as st
+    D = float(st.ks_2samp(a, b).statistic)
+
+    def neff(x):
+        x = np.asarray(x, dtype=np.float64)
+        naive = np.std(x, ddof=1) / np.sqrt(len(x))
+        r = max(1.0, (blocked(x)[1] / naive) ** 2)
+        return len(x) / r, r
+
+    (na, ra), (nb, rb) = neff(a), neff(b)
+    return D, float(st.kstwobign.sf(D * np.sqrt(na * nb / (na + nb)))), ra, rb
+
+
 def chain_statistics(c, U_start, n, seed, V):
     """n untimed trajectories of one precision from U_start (a Markov chain with Philox
     momenta and accept uniforms keyed by seed): Delta H, acceptance, exp(-Delta H) and the
@@ -248,6 +267,7 @@ def equal_dH_plaq(mixed, fp64, U_start, n, pairs, seed, V):
         diff.append(r[0].dH - r[1].dH)
         same += r[0].accepted == r[1].accepted
     diff = np.array(diff)
+    ks = ks_effective(dm, dd)
     rnd = lambda v: [float(f"{v[0]:.6g}"), float(f"{v[1]:.2g}")]  # noqa: E731
     return {"trajectories_per_arm": n, "errors": "20-block (exp_mdH: lognormal bound)",
             "mixed": {k: rnd(v) for k, v in sm.items()},
@@ -255,7 +275,10 @@ def equal_dH_plaq(mixed, fp64, U_start, n, pairs, seed, V):
             "z_mixed_minus_fp64": {k: round(v, 2) for k, v in z.items()},
             "creutz_z": {k: round(v, 2) for k, v in creutz.items()},
             "dH_mean_minus_half_var": half_var,
-            "ks_p_dH": float(f"{st.ks_2samp(dm, dd).pvalue:.3g}"),
+            "ks_p_dH": float(f"{ks[1]:.3g}"),
+            "ks_dH": {"D": round(ks[0], 4), "p_iid": float(f"{st.ks_2samp(dm, dd).pvalue:.3g}"),
+                      "two_tau": {"mixed": round(ks[2], 2), "fp64": round(ks[3], 2)},
+                      "p": "asymptotic, effective sizes n / (2 tau)"},
             "paired": {"pairs": pairs, "same_momenta": True,
                        "dH_diff_mean": float(f"{diff.mean():.3g}"),
                        "dH_diff_rms": float(f"{np.sqrt(np.mean(diff ** 2)):.3g}"),
@@ -417,6 +440,26 @@ def ours(args):
     metro64 = 5 / (ev2[0].elapsed_time(ev2[1]) / 1e3)
     flow32 = 10 / (ev2[2].elapsed_time(ev2[3]) / 1e3)
 
+    # ---- one lattice over time slabs on this GPU: what the decomposition adds (per-slab
+    #      launches, a ghost-slice exchange after each force launch, the cross-slab sums),
+    #      mixed precision with the tuned force shape, device time of K trajectories ----
+    from su2_b200.slabs import slab_lattice
+    slab_rate = {}
+    for nsl in (2, 4):
+        with slab_lattice((L, L, L, L), 4, BETA, nsl, precision="mixed", device=local) as sl:
+            sl.upload(U_th)
+            sl.tune_set(mixed.force_variant)
+            for k in range(10):  # graph capture of the buffer assignments met
+                sl.md_update("omf2", NSTEPS, TAU, seed=seed, traj=600000 + k)
+            ss = torch.cuda.ExternalStream(sl.stream())
+            ea, eb = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            ea.record(ss)
+            for k in range(K):
+                sl.md_update("omf2", NSTEPS, TAU, seed=seed, traj=600010 + k)
+            eb.record(ss)
+            eb.synchronize()
+            slab_rate[str(nsl)] = K / (ea.elapsed_time(eb) / 1e3)
+
     # ---- the measurements taken between trajectories (FP64 context, thermalised field):
     #      wall time per call, each call returns its value to the host ----
     def per_call(fn, n=5):
@@ -475,6 +518,8 @@ def ours(args):
                                   "plain_fp64": stats(res_p, V)},
             "metropolis_sweeps_per_s": {"mixed": metro, "fp64": metro64},
             "flow_rk3_steps_per_s": {"fp64": flow, "mixed": flow32},
+            "time_slabs_one_gpu_mixed_traj_per_s": {"1 (the lattice)": K / t_mixed,
+                                                   **slab_rate},
             "between_trajectories_fp64": obs}), flush=True)
         r3 = lambda v: float(f"{v:.4g}")  # noqa: E731
         line = {
@@ -533,6 +578,106 @@ def cpu_baseline(U_th):
     return {"value": 1.0 / dt, "unit": "traj/s", "cores": threads, "kind": "reference",
             "sample": "1 omf2 trajectory of the 32^4 workload, reference md_update code, "
                       "OpenMP"}
+
+
+def slabs_run(args):
+    """--slabs N: one 32^4 lattice cut into N time slabs (strong scaling).  Under torchrun
+    each rank holds one slab (N = world size) and the ranks exchange ghost slices and sums
+    over NCCL; as one process, all N slabs share its GPU.  Rank 0 thermalises the field and
+    broadcasts it; value = trajectories of the lattice per second over the slowest rank's
+    device time; e2e uploads each rank's slices (with ghosts) and downloads them per step."""
+    import torch
+
+    import su2_b200
+    from su2_b200.slabs import connect_process_group, slab_lattice
+    ws, rank, local, dist = dist_setup()
+    torch.cuda.set_device(local)
+    K, W, N = args.steps, args.warmup, args.slabs
+    if ws > 1 and N != ws:
+        raise SystemExit(f"--slabs {N} under {ws} ranks: one slab per rank (N = world size)")
+    NL = L ** 4 * 4
+    seed = 20240
+    therm = su2_b200.gaugeconfig(L, L, L, L, 4, BETA, precision="mixed", device=local)
+    if rank == 0:
+        therm.upload(haar_links(NL, seed))
+        for sweep in range(args.therm_sweeps):
+            therm.sweep(0.15, 8, seed, sweep)
+        for k in range(THERM_TRAJ):
+            therm.md_update("omf2", NSTEPS, TAU, seed=seed, traj=100000 + k)
+        U_th = therm.download()
+        Uq = U_th.reshape(-1, 4)
+        Uq /= np.sqrt(np.einsum("ij,ij->i", Uq, Uq))[:, None]
+        therm.upload(U_th)
+        therm.autotune()
+        variant = therm.force_variant
+    else:
+        U_th, variant = np.empty(NL * 4), 0
+    therm.close()
+    if dist is not None:
+        t = torch.from_numpy(U_th).cuda()
+        v = torch.tensor([variant], device="cuda")
+        dist.broadcast(t, 0)
+        dist.broadcast(v, 0)
+        U_th, variant = t.cpu().numpy(), int(v.item())
+    if ws > 1:
+        lat = slab_lattice((L, L, L, L), 4, BETA, N, precision="mixed", first=rank, count=1,
+                           device=local)
+        connect_process_group(lat, dist)
+    else:
+        lat = slab_lattice((L, L, L, L), 4, BETA, N, precision="mixed", device=local)
+    lat.upload(U_th)
+    lat.tune_set(variant)
+    for k in range(max(W, 3) + 6):
+        lat.md_update("omf2", NSTEPS, TAU, seed=seed, traj=300000 + k)
+    lat.upload(U_th)
+    s = torch.cuda.ExternalStream(lat.stream())
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    clocks = Clocks(local)
+    barrier(dist)
+    n0 = lat.kernel_launches()
+    clocks.start()
+    e0.record(s)
+    res = [lat.md_update("omf2", NSTEPS, TAU, seed=seed, traj=k) for k in range(K)]
+    e1.record(s)
+    e1.synchronize()
+    clk = clocks.stop()
+    launches = lat.kernel_launches() - n0
+    t = allmax(dist, e0.elapsed_time(e1) / 1e3)
+    Uh = torch.empty(NL * 4, dtype=torch.float64, pin_memory=True).numpy()
+    Uh[:] = U_th
+    t0, t1 = lat.slices()
+    row = L ** 3 * 4 * 4
+    barrier(dist)
+    w0 = time.perf_counter()
+    for k in range(K):
+        lat.upload(Uh)
+        lat.md_update("omf2", NSTEPS, TAU, seed=seed, traj=400000 + k)
+        lat.download(Uh)
+    t_e2e = allmax(dist, time.perf_counter() - w0)
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": K / t, "unit": "traj/s", "n_gpus": ws, "steps": K,
+            "warmup": W, "ms_per_step": 1e3 * t / K, "higher_is_better": True,
+            "scaling": "strong", "vs_baseline": None,
+            "dtype": "fp32 links/forces + fp64 reductions/accept",
+            "data": "synthetic: seeded Haar-random start, Metropolis-thermalised on device",
+            "config": {"workload": WORKLOAD + " (mixed precision), one lattice over time slabs",
+                       "lattice": [L] * 4, "slabs": N, "slices_per_slab": L // N,
+                       "parallelism": f"t-slabs x{N}" + (" on one GPU" if ws == 1 else ""),
+                       "l2": "working set > 126 MB L2; no flush"},
+            "acceptance": sum(r.accepted for r in res) / K,
+            "e2e": {"value": K / t_e2e, "unit": "traj/s",
+                    "h2d_bytes_per_step": int(lat.count * (L // N + 2) * row * 8),
+                    "d2h_bytes_per_step": int((t1 - t0) * row * 8),
+                    "note": "per rank: its slices and ghost slices up, trajectory, its slices "
+                            "down; wall clock"},
+            "gpu_launches": int(launches),
+            "clocks": clk,
+        }
+        print(json.dumps(line), flush=True)
+    lat.close()
+    if dist is not None:
+        dist.destroy_process_group()
 
 
 def reference(args):
@@ -1050,9 +1195,14 @@ def main():
     ap.add_argument("--force-variant", type=int, default=3)
     ap.add_argument("--config", type=int, default=2, choices=[1, 2, 3, 4, 5],
                     help="2: the headline 32^4 HMC; 1, 3, 4, 5: the other workloads")
+    ap.add_argument("--slabs", type=int, default=0,
+                    help="one 32^4 lattice over N time slabs: one per rank under torchrun "
+                         "(NCCL), all on the GPU as one process (strong scaling)")
     args = ap.parse_args()
     if args.profile_run:
         profile_run(args)
+    elif args.impl == "ours" and args.slabs:
+        slabs_run(args)
     elif args.impl == "ours" and args.config != 2:
         {1: config1, 3: config3, 4: config4, 5: config5}[args.config](args)
     elif args.impl == "reference":
