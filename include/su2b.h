@@ -289,6 +289,10 @@ SU2B_API int su2b_slabs_upload(su2b_slabs *h, const double *U_host);
 SU2B_API int su2b_slabs_download(su2b_slabs *h, double *U_host);
 SU2B_API int su2b_slabs_hmc_trajectory(su2b_slabs *h, const su2b_hmc_params *prm,
                                        su2b_traj_result *res);
+/* flat_spacetime::sweep over the slabs (as su2b_metropolis_sweep: the same links, the same
+ * acceptance rates of the whole lattice) */
+SU2B_API int su2b_slabs_metropolis_sweep(su2b_slabs *h, double delta, int N_hit, uint64_t seed,
+                                         uint32_t sweep, double *rates);
 /* gauge_energy of the whole lattice (as su2b_gauge_energy) */
 SU2B_API int su2b_slabs_gauge_energy(su2b_slabs *h, int spatial_only, double *out);
 /* su2b_autotune on the first slab; every slab takes its choice */

@@ -128,6 +128,7 @@ SIGNATURES = {
     "su2b_slabs_download": (i32, [_P, _D]),
     "su2b_slabs_hmc_trajectory": (i32, [_P, C.POINTER(HmcParams), C.POINTER(TrajResult)]),
     "su2b_slabs_gauge_energy": (i32, [_P, i32, _D]),
+    "su2b_slabs_metropolis_sweep": (i32, [_P, f64, i32, u64, u32, _D]),
     "su2b_slabs_autotune": (i32, [_P, _D]),
     "su2b_slabs_tune_get": (i32, [_P, C.POINTER(i32)]),
     "su2b_slabs_tune_set": (i32, [_P, i32]),

@@ -67,7 +67,7 @@ __device__ __forceinline__ unsigned metro_link_fp32(const Geom &g, Link32 *__res
   const size_t l = (size_t)mu * g.V + (size_t)p * g.Vh + cb;
   Su2<float> u = ld_link_rw(U + l);
   double tr_u = retr_mul(to64(u), K64);
-  const uint32_t lref = (uint32_t)s.lex * (uint32_t)g.nd + (uint32_t)mu;
+  const uint32_t lref = (uint32_t)(s.lex + g.lex0) * (uint32_t)g.nd + (uint32_t)mu;
   const float d2 = (float)(2.0 * delta);
   unsigned acc = 0;
   for (int n = 0; n < N_hit; n++) {
@@ -102,13 +102,14 @@ __global__ void __launch_bounds__(NT)
   __shared__ unsigned int sh_acc;
   if (threadIdx.x == 0) sh_acc = 0;
   __syncthreads();
-  const int cb = blockIdx.x * NT + threadIdx.x;
+  // the sites cb0 .. cb0 + ncb - 1 of parity p (all of them but in a time slab)
+  const int cb = g.cb0 + blockIdx.x * NT + threadIdx.x;
   unsigned int acc = 0;
   if constexpr (sizeof(T) == 4) {
-    if (cb < g.Vh)
+    if (cb < g.cb0 + g.ncb)
       acc = metro_link_fp32<ND>(g, (Link32 *)U, mu, p, cb, beta_nc, delta, N_hit, seed, sweep,
                                 (float)wt, (float)ws);
-  } else if (cb < g.Vh) {
+  } else if (cb < g.cb0 + g.ncb) {
     const Site s = site_from_eo(g, p, cb);
     // staple sum in FP64
     const int lpm = s.lex + fwd_rt(g, s, mu);  // mu is known at run time only
@@ -133,7 +134,7 @@ __global__ void __launch_bounds__(NT)
     }
     const size_t l = (size_t)mu * g.V + (size_t)p * g.Vh + cb;
     Su2<double> u = to64(ld_link_rw(U + l));
-    const uint32_t lref = (uint32_t)s.lex * (uint32_t)g.nd + (uint32_t)mu;
+    const uint32_t lref = (uint32_t)(s.lex + g.lex0) * (uint32_t)g.nd + (uint32_t)mu;
     for (int n = 0; n < N_hit; n++) {
       uint32_t r[4];
       philox(lref, (uint32_t)n, sweep, TAG_METRO, seed, r);
@@ -240,7 +241,7 @@ cudaError_t metropolis_pass(const Geom &g, void *U, int group, int mu, int parit
   // anisotropic weights of get_staples (get_staples.hh:58-79): 1/xi for planes with
   // direction 0, xi otherwise; both 1 (exactly) for the isotropic action
   const double wt = xi == 1.0 ? 1.0 : 1.0 / xi, ws = xi;
-  const int grid = (g.Vh + NT - 1) / NT;
+  const int grid = ((group == 0 ? g.ncb : g.Vh) + NT - 1) / NT;
   if (group == 0) {
     LinkT<T> *u = (LinkT<T> *)U;
     const double bn = beta / 2.0;

@@ -178,20 +178,13 @@ int from_ctx(su2b_slabs *h, int rc) {
                   std::string(#call) + ": " + cudaGetErrorString(e_));                     \
   } while (0)
 
-// the table of pieces of local slice ts of buffer k of slab r, to dst(mu, p)
-template <class Dst>
-void face_pieces(su2b_slabs *h, int r, int k, int ts, Dst dst, std::vector<Piece> *out) {
-  const su2b_ctx *c = h->sl[r];
-  const size_t words = c->link_bytes() / 16;  // 16-byte words per link
-  for (int mu = 0; mu < h->nd; mu++)
-    for (int p = 0; p < 2; p++) {
-      const size_t l = (size_t)mu * c->g.V + (size_t)p * c->g.Vh + (size_t)ts * (h->S / 2);
-      out->push_back({(const uint4 *)h->buf[r][k] + l * words, dst(mu, p)});
-    }
-}
+// the 16-byte word offset of piece (mu, p) of local slice ts in a link buffer of c
 size_t slice_word(const su2b_ctx *c, long S, int mu, int p, int ts) {
   const size_t l = (size_t)mu * c->g.V + (size_t)p * c->g.Vh + (size_t)ts * (S / 2);
   return l * (c->link_bytes() / 16);
+}
+uint4 *piece_at(su2b_slabs *h, int r, int k, int mu, int p, int ts) {
+  return (uint4 *)h->buf[r][k] + slice_word(h->sl[r], h->S, mu, p, ts);
 }
 
 int upload_table(su2b_slabs *h, const std::vector<Piece> &v, Piece **dev) {
@@ -203,22 +196,21 @@ int upload_table(su2b_slabs *h, const std::vector<Piece> &v, Piece **dev) {
   return SU2B_OK;
 }
 
-// one device: for every slab r, its first slice goes to the upper ghost slice of slab r - 1
-// and its last slice to the lower ghost slice of slab r + 1 (periodically)
+// Exchange tables are ordered by piece (mu, p) first, so the entries of one piece -- all a
+// checkerboard pass changes -- are one contiguous run: entries (2 mu + p) * per_piece ..
+// One device: per piece, for every slab r, its first slice goes to the upper ghost slice of
+// slab r - 1 and its last slice to the lower ghost slice of slab r + 1 (periodically).
 int build_local_tables(su2b_slabs *h) {
   const int R = h->count;
   for (int k = 0; k < 3; k++) {
     std::vector<Piece> v;
-    for (int r = 0; r < R; r++) {
-      const int dn = (r + R - 1) % R, up = (r + 1) % R;
-      const su2b_ctx *cd = h->sl[dn], *cu = h->sl[up];
-      face_pieces(h, r, k, 1, [&](int mu, int p) {
-        return (uint4 *)h->buf[dn][k] + slice_word(cd, h->S, mu, p, h->Tl + 1);
-      }, &v);
-      face_pieces(h, r, k, h->Tl, [&](int mu, int p) {
-        return (uint4 *)h->buf[up][k] + slice_word(cu, h->S, mu, p, 0);
-      }, &v);
-    }
+    for (int mu = 0; mu < h->nd; mu++)
+      for (int p = 0; p < 2; p++)
+        for (int r = 0; r < R; r++) {
+          const int dn = (r + R - 1) % R, up = (r + 1) % R;
+          v.push_back({piece_at(h, r, k, mu, p, 1), piece_at(h, dn, k, mu, p, h->Tl + 1)});
+          v.push_back({piece_at(h, r, k, mu, p, h->Tl), piece_at(h, up, k, mu, p, 0)});
+        }
     h->npieces = (int)v.size();
     SU2B_CKS(upload_table(h, v, &h->xchg[k]));
   }
@@ -232,23 +224,21 @@ int build_local_tables(su2b_slabs *h) {
   return SU2B_OK;
 }
 
-// NCCL: the faces of buffer k packed as [first slice | last slice], and the received faces
-// [from the slab below | from the slab above] unpacked into [ghost 0 | ghost Tl + 1]
+// NCCL: the send buffer holds [first slice | last slice], each as its 2 nd pieces in (mu, p)
+// order; the receive buffer [from the slab below | from the slab above] goes to
+// [ghost 0 | ghost Tl + 1].  The pack and unpack tables list per piece its two faces.
 int build_nccl_tables(su2b_slabs *h) {
-  const su2b_ctx *c = h->sl[0];
   const long face = 2l * h->nd * h->piece_n;
   for (int k = 0; k < 3; k++) {
     std::vector<Piece> pk, up;
-    int i = 0;
-    face_pieces(h, 0, k, 1, [&](int, int) { return h->sendbuf + (i++) * h->piece_n; }, &pk);
-    face_pieces(h, 0, k, h->Tl, [&](int, int) { return h->sendbuf + (i++) * h->piece_n; },
-                &pk);
-    for (int side = 0; side < 2; side++)
-      for (int mu = 0; mu < h->nd; mu++)
-        for (int p = 0; p < 2; p++)
-          up.push_back({h->recvbuf + side * face + (2 * mu + p) * h->piece_n,
-                        (uint4 *)h->buf[0][k] +
-                          slice_word(c, h->S, mu, p, side == 0 ? 0 : h->Tl + 1)});
+    for (int mu = 0; mu < h->nd; mu++)
+      for (int p = 0; p < 2; p++) {
+        const long at = (2 * mu + p) * h->piece_n;
+        pk.push_back({piece_at(h, 0, k, mu, p, 1), h->sendbuf + at});
+        pk.push_back({piece_at(h, 0, k, mu, p, h->Tl), h->sendbuf + face + at});
+        up.push_back({h->recvbuf + at, piece_at(h, 0, k, mu, p, 0)});
+        up.push_back({h->recvbuf + face + at, piece_at(h, 0, k, mu, p, h->Tl + 1)});
+      }
     SU2B_CKS(upload_table(h, pk, &h->pack[k]));
     SU2B_CKS(upload_table(h, up, &h->unpack[k]));
   }
@@ -268,26 +258,41 @@ cudaError_t copy_pieces(const Piece *tab, int npieces, long n, cudaStream_t s) {
       return fail(h, SU2B_ERR_CUDA, std::string(#call) + ": " + h->nc->error_string(r_));  \
   } while (0)
 
-// refresh the ghost slices of buffer k of every slab
-int exchange(su2b_slabs *h, int k) {
+// a kernel launch through a slab context, its failure reported as the handle's error
+#define SLAB_LAUNCH(ctx_, kclass, call)                                                    \
+  do {                                                                                     \
+    su2b_ctx *ctx = (ctx_);                                                                \
+    const int rc_ = [&]() -> int {                                                         \
+      SU2B_LAUNCH(kclass, call);                                                           \
+      return SU2B_OK;                                                                      \
+    }();                                                                                   \
+    if (rc_ != SU2B_OK) return from_ctx(h, rc_);                                           \
+  } while (0)
+
+// refresh the ghost slices of buffer k of every slab: every piece (piece < 0) or only
+// piece 2 mu + p
+int exchange(su2b_slabs *h, int k, int piece = -1) {
+  const int n_of = piece < 0 ? 2 * h->nd : 1, first = piece < 0 ? 0 : piece;
   if (!h->comm) {
-    SLAB_CUDA(copy_pieces(h->xchg[k], h->npieces, h->piece_n, h->s));
+    const int per = 2 * h->count;  // table entries per piece
+    SLAB_CUDA(copy_pieces(h->xchg[k] + first * per, n_of * per, h->piece_n, h->s));
     h->launches++;
     return SU2B_OK;
   }
   const long face = 2l * h->nd * h->piece_n;
-  const size_t bytes = (size_t)face * 16;
+  const long at = first * h->piece_n;  // the pieces' place in each face of the buffers
+  const size_t bytes = (size_t)n_of * h->piece_n * 16;
   const int up = (h->rank + 1) % h->nranks, dn = (h->rank + h->nranks - 1) % h->nranks;
-  SLAB_CUDA(copy_pieces(h->pack[k], 4 * h->nd, h->piece_n, h->s));
+  SLAB_CUDA(copy_pieces(h->pack[k] + 2 * first, 2 * n_of, h->piece_n, h->s));
   // with two slabs both neighbours are one process: sends and receives to one peer match
   // in the order they are posted, so the order is the same on every rank
   NCCL_CK(h->nc->group_start());
-  NCCL_CK(h->nc->send(h->sendbuf + face, bytes, ncclUint8, up, h->comm, h->s));
-  NCCL_CK(h->nc->send(h->sendbuf, bytes, ncclUint8, dn, h->comm, h->s));
-  NCCL_CK(h->nc->recv(h->recvbuf, bytes, ncclUint8, dn, h->comm, h->s));
-  NCCL_CK(h->nc->recv(h->recvbuf + face, bytes, ncclUint8, up, h->comm, h->s));
+  NCCL_CK(h->nc->send(h->sendbuf + face + at, bytes, ncclUint8, up, h->comm, h->s));
+  NCCL_CK(h->nc->send(h->sendbuf + at, bytes, ncclUint8, dn, h->comm, h->s));
+  NCCL_CK(h->nc->recv(h->recvbuf + at, bytes, ncclUint8, dn, h->comm, h->s));
+  NCCL_CK(h->nc->recv(h->recvbuf + face + at, bytes, ncclUint8, up, h->comm, h->s));
   NCCL_CK(h->nc->group_end());
-  SLAB_CUDA(copy_pieces(h->unpack[k], 4 * h->nd, h->piece_n, h->s));
+  SLAB_CUDA(copy_pieces(h->unpack[k] + 2 * first, 2 * n_of, h->piece_n, h->s));
   h->launches += 2;
   return SU2B_OK;
 }
@@ -612,11 +617,10 @@ extern "C" int su2b_slabs_upload(su2b_slabs *h, const double *U_host) {
                               cudaMemcpyHostToDevice, h->s));
     SLAB_CUDA(cudaMemcpyAsync(c->stage + (h->Tl + 1) * row, U_host + hi * row, row * 8,
                               cudaMemcpyHostToDevice, h->s));
-    su2b_ctx *ctx = c;
     if (h->link64)
-      SU2B_LAUNCH(SU2B_K_OTHER, links_from_host<double>(c->g, c->stage, c->U, 0, h->s));
+      SLAB_LAUNCH(c, SU2B_K_OTHER, links_from_host<double>(c->g, c->stage, c->U, 0, h->s));
     else
-      SU2B_LAUNCH(SU2B_K_OTHER, links_from_host<float>(c->g, c->stage, c->U, 0, h->s));
+      SLAB_LAUNCH(c, SU2B_K_OTHER, links_from_host<float>(c->g, c->stage, c->U, 0, h->s));
   }
   SLAB_CUDA(cudaStreamSynchronize(h->s));
   return SU2B_OK;
@@ -632,11 +636,10 @@ extern "C" int su2b_slabs_download(su2b_slabs *h, double *U_host) {
     su2b_ctx *c = h->sl[r];
     c->begin_call();
     const int t0 = (h->first + r) * h->Tl;
-    su2b_ctx *ctx = c;
     if (h->link64)
-      SU2B_LAUNCH(SU2B_K_OTHER, links_to_host<double>(c->g, c->U, c->stage, 0, h->s));
+      SLAB_LAUNCH(c, SU2B_K_OTHER, links_to_host<double>(c->g, c->U, c->stage, 0, h->s));
     else
-      SU2B_LAUNCH(SU2B_K_OTHER, links_to_host<float>(c->g, c->U, c->stage, 0, h->s));
+      SLAB_LAUNCH(c, SU2B_K_OTHER, links_to_host<float>(c->g, c->U, c->stage, 0, h->s));
     SLAB_CUDA(cudaMemcpyAsync(U_host + t0 * row, c->stage + row, h->Tl * row * 8,
                               cudaMemcpyDeviceToHost, h->s));
   }
@@ -660,22 +663,77 @@ extern "C" int su2b_slabs_gauge_energy(su2b_slabs *h, int spatial_only, double *
     return fail(h, SU2B_ERR_INVALID,
                 "the handle holds a part of the slabs: connect it to the others first");
   SLAB_CUDA(cudaSetDevice(h->device));
-  for (su2b_ctx *ctx : h->sl) {
-    ctx->begin_call();
+  for (su2b_ctx *c : h->sl) {
+    c->begin_call();
     int nb = 0;
     if (h->link64)
-      SU2B_LAUNCH(SU2B_K_PLAQUETTE, plaq_partials<double>(ctx->g, ctx->U, 0, ctx->xi,
-                                                          ctx->part_slot(0), &nb, h->s));
+      SLAB_LAUNCH(c, SU2B_K_PLAQUETTE, plaq_partials<double>(c->g, c->U, 0, c->xi,
+                                                             c->part_slot(0), &nb, h->s));
     else
-      SU2B_LAUNCH(SU2B_K_PLAQUETTE, plaq_partials<float>(ctx->g, ctx->U, 0, ctx->xi,
-                                                         ctx->part_slot(0), &nb, h->s));
-    SU2B_LAUNCH(SU2B_K_OTHER, reduce_final(ctx->part_slot(0), nb, 3, ctx->red, h->s));
+      SLAB_LAUNCH(c, SU2B_K_PLAQUETTE, plaq_partials<float>(c->g, c->U, 0, c->xi,
+                                                            c->part_slot(0), &nb, h->s));
+    SLAB_LAUNCH(c, SU2B_K_OTHER, reduce_final(c->part_slot(0), nb, 3, c->red, h->s));
   }
   SU2B_CKS(sum_over_slabs(h, 3));
   su2b_ctx *c = h->sl[0];
   SLAB_CUDA(cudaMemcpyAsync(c->h_red, c->red, 3 * sizeof(double), cudaMemcpyDeviceToHost, h->s));
   SLAB_CUDA(cudaStreamSynchronize(h->s));
   *out = c->h_red[spatial_only ? 1 : 0];
+  return SU2B_OK;
+}
+
+// flat_spacetime::sweep (flat-sweep.hh:64-164) over the slabs, in the single lattice's
+// order of passes: direction mu, then parity p of the whole lattice.  A slab's own slices
+// start at local slice 1 and at an even global slice, so its local parity of a site is the
+// global one flipped: the slabs run local parity p ^ 1.  A pass changes the links of one
+// direction and parity only, so after it only that piece of the faces is exchanged.  The
+// links' Philox streams are keyed by their global index: the sweep is the single lattice's.
+extern "C" int su2b_slabs_metropolis_sweep(su2b_slabs *h, double delta, int N_hit,
+                                           uint64_t seed, uint32_t sweep, double *rates) {
+  if (!h) return SU2B_ERR_INVALID;
+  h->err.clear();
+  if (!rates) return fail(h, SU2B_ERR_INVALID, "rates is NULL");
+  if (N_hit < 0) return fail(h, SU2B_ERR_INVALID, "N_hit < 0");
+  if (!connected(h))
+    return fail(h, SU2B_ERR_INVALID,
+                "the handle holds a part of the slabs: connect it to the others first");
+  SLAB_CUDA(cudaSetDevice(h->device));
+  for (su2b_ctx *c : h->sl) {
+    c->begin_call();
+    SLAB_CUDA(cudaMemsetAsync(c->counts, 0, 2 * sizeof(unsigned long long), h->s));
+  }
+  for (int mu = 0; mu < h->nd; mu++)
+    for (int p = 0; p < 2; p++) {
+      const int pl = p ^ 1;
+      for (su2b_ctx *c : h->sl) {
+        if (h->link64)
+          SLAB_LAUNCH(c, SU2B_K_METROPOLIS,
+                      metropolis_pass<double>(c->g, c->U, 0, mu, pl, c->beta, c->xi, delta,
+                                              N_hit, seed, sweep, c->counts, h->s));
+        else
+          SLAB_LAUNCH(c, SU2B_K_METROPOLIS,
+                      metropolis_pass<float>(c->g, c->U, 0, mu, pl, c->beta, c->xi, delta,
+                                             N_hit, seed, sweep, c->counts, h->s));
+      }
+      SU2B_CKS(exchange(h, h->role[0], 2 * mu + pl));
+    }
+  if (h->comm)
+    NCCL_CK(h->nc->all_reduce(h->sl[0]->counts, h->sl[0]->counts, 2, ncclUint64, ncclSum,
+                              h->comm, h->s));
+  for (su2b_ctx *c : h->sl)
+    SLAB_CUDA(cudaMemcpyAsync(c->h_counts, c->counts, 2 * sizeof(unsigned long long),
+                              cudaMemcpyDeviceToHost, h->s));
+  SLAB_CUDA(cudaStreamSynchronize(h->s));
+  // every slab's counts (one device), or the all-reduced counts of the first
+  unsigned long long n0 = 0, n1 = 0;
+  for (size_t r = 0; r < (h->comm ? 1 : h->sl.size()); r++) {
+    n0 += h->sl[r]->h_counts[0];
+    n1 += h->sl[r]->h_counts[1];
+  }
+  const double nh = (double)(N_hit > 0 ? N_hit : 1);
+  const double V = (double)h->S * h->Lt;
+  rates[0] = (double)n0 / nh / (V * h->nd);
+  rates[1] = (double)n1 / nh / V;
   return SU2B_OK;
 }
 

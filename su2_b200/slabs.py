@@ -143,6 +143,14 @@ class slab_lattice:
         return TrajectoryResult(bool(r.accepted), r.dH, r.ddH, tuple(r.H_old), tuple(r.H_new),
                                 r.plaquette, r.cg_iterations)
 
+    def sweep(self, delta, N_hit, seed, sweep_index):
+        """N_hit Metropolis updates of every link (flat_spacetime::sweep) over the slabs;
+        returns the acceptance rates {overall, temporal} of the whole lattice."""
+        rates = np.zeros(2)
+        self._c(self.lib.su2b_slabs_metropolis_sweep(self.h, delta, N_hit, seed, sweep_index,
+                                                     _dp(rates)))
+        return rates
+
     def gauge_energy(self, spatial_only=False) -> float:
         out = C.c_double()
         self._c(self.lib.su2b_slabs_gauge_energy(self.h, int(spatial_only), C.byref(out)))

@@ -21,9 +21,9 @@ def hot(orc, dims, nd):
     return orc.hotstart(0, dims, nd, SEED, 1.0, TRAFO)
 
 
-def single(gpu, dims, nd, precision, beta=2.3):
+def single(gpu, dims, nd, precision, beta=2.3, xi=1.0):
     Lx, Ly, Lz, Lt = dims
-    return gpu.gaugeconfig(Lx, Ly, Lz, Lt, nd, beta, group="su2", precision=precision)
+    return gpu.gaugeconfig(Lx, Ly, Lz, Lt, nd, beta, group="su2", precision=precision, xi=xi)
 
 
 def slabs(dims, nd, nslabs, precision, beta=2.3, **kw):
@@ -70,6 +70,56 @@ def test_slabs_equal_the_single_lattice(gpu, orc, precision, dims, nd, nslabs):
         acc = [r.accepted for r in a]
         assert any(acc) and not all(acc)
         assert np.array_equal(c.download(), s.download())
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_anisotropic_slabs(gpu, orc, precision):
+    """xi != 1 (the anisotropic force and sweep weights) over 2 slabs."""
+    dims, nd, xi = (6, 6, 6, 8), 4, 0.8
+    U = hot(orc, dims, nd)
+    with single(gpu, dims, nd, precision, xi=xi) as c, \
+            slabs(dims, nd, 2, precision, xi=xi) as s:
+        c.upload(U)
+        s.upload(U)
+        same_chain(chain(c, 4), chain(s, 4))
+        for k in range(2):
+            assert np.array_equal(c.sweep(0.3, 4, 9, k), s.sweep(0.3, 4, 9, k))
+        assert np.array_equal(c.download(), s.download())
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+@pytest.mark.parametrize("dims,nd,nslabs", [
+    ((8, 8, 8, 8), 4, 2), ((8, 8, 8, 8), 4, 4), ((4, 6, 8, 12), 4, 3), ((8, 6, 1, 8), 3, 2),
+    ((6, 1, 1, 8), 2, 4)], ids=["8^4/2", "8^4/4", "4x6x8x12/3", "8x6x8-d3/2", "6x8-d2/4"])
+def test_slab_metropolis_sweeps(gpu, orc, precision, dims, nd, nslabs):
+    """The checkerboard sweep over slabs (local parity flipped, one piece of the faces
+    exchanged after each pass) gives the single lattice's links and acceptance rates."""
+    U = hot(orc, dims, nd)
+    with single(gpu, dims, nd, precision) as c, slabs(dims, nd, nslabs, precision) as s:
+        c.upload(U)
+        s.upload(U)
+        for k in range(3):
+            rc, rs = c.sweep(0.25, 6, 21, k), s.sweep(0.25, 6, 21, k)
+            assert np.array_equal(rc, rs), k
+            assert 0.01 < rc[0] < 0.99
+        assert np.array_equal(c.download(), s.download())
+        assert s.gauge_energy() == pytest.approx(c.gauge_energy(), rel=1e-13)
+
+
+def test_slabs_alternate_sweeps_and_trajectories(gpu, orc):
+    """The workload's alternation (Metropolis sweeps between HMC trajectories) over 4 slabs
+    in mixed precision: after each step the single lattice's field."""
+    dims, nd = (8, 8, 8, 16), 4
+    U = hot(orc, dims, nd)
+    with single(gpu, dims, nd, "mixed", beta=2.4) as c, \
+            slabs(dims, nd, 4, "mixed", beta=2.4) as s:
+        c.upload(U)
+        s.upload(U)
+        for k in range(3):
+            assert np.array_equal(c.sweep(0.15, 8, 5, k), s.sweep(0.15, 8, 5, k))
+            same_chain([c.md_update("omf2", 6, 1.0, seed=5, traj=k)],
+                       [s.md_update("omf2", 6, 1.0, seed=5, traj=k)])
+            assert np.array_equal(c.download(), s.download()), k
 
 
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
