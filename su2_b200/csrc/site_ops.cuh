@@ -147,7 +147,8 @@ __device__ __forceinline__ double force_half_impl(const Geom &g, const LinkT<T> 
       if (o[d] < 0) lex += bo[d];
       odd ^= (o[d] != 0);
     }
-    return ld_link(U + (size_t)mu * V + eo_of(g, lex, p ^ odd));
+    // a 32-bit link offset: 4 V < 2^31 for every volume a context accepts (V <= 2^29)
+    return ld_link(U + ((uint32_t)mu * (uint32_t)g.V + (uint32_t)eo_of(g, lex, p ^ odd)));
   };
   auto E = [](int d, int k) { return d == k ? 1 : 0; };
   constexpr int m0 = 2 * HALF, m1 = 2 * HALF + 1;
@@ -285,7 +286,8 @@ __device__ __forceinline__ double force_half_x(const Geom &g, const LinkT<T> *__
       if (o[d] < 0) lex += bo[d];
       odd ^= (o[d] != 0);
     }
-    return ld_link(U + (size_t)mu * V + eo_of(g, lex, p ^ odd));
+    // a 32-bit link offset: 4 V < 2^31 for every volume a context accepts (V <= 2^29)
+    return ld_link(U + ((uint32_t)mu * (uint32_t)g.V + (uint32_t)eo_of(g, lex, p ^ odd)));
   };
   auto E = [](int d, int k) { return d == k ? 1 : 0; };
   constexpr int m0 = 2 * HALF, m1 = 2 * HALF + 1;

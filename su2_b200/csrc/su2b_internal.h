@@ -39,9 +39,9 @@ enum ForceMode : int {
 };
 // launch shapes of the SU(2) force kernel (threads per block, minimum resident blocks per
 // SM, which caps registers): one thread per site 0 (256,4) 1 (128,8) 2 (128,4) 3 (128,6)
-// 4 (256,2) 5 (256,3) 7 (64,16); two threads per site 6 split, 8 xsplit, both (128,8); 9 one
-// thread per link
-constexpr int FORCE_VARIANTS = 10;
+// 4 (256,2) 5 (256,3) 7 (64,16); two threads per site 6 split, 8 xsplit, both (128,8), and
+// 10 split (128,5) (96 registers: FP64 links); 9 one thread per link
+constexpr int FORCE_VARIANTS = 11;
 template <class T>
 cudaError_t force_update(const Geom &g, const void *U, int group, T *P, const T *extra, double f,
                          double scale, double xi, int mode, double *kin_part, int *nblocks,
