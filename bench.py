@@ -445,10 +445,11 @@ def ours(args):
     #      mixed precision with the tuned force shape, device time of K trajectories ----
     from su2_b200.slabs import slab_lattice
     slab_rate = {}
-    for nsl in (2, 4):
+    for nsl, ov in ((2, False), (4, False), (2, True), (4, True)):
         with slab_lattice((L, L, L, L), 4, BETA, nsl, precision="mixed", device=local) as sl:
             sl.upload(U_th)
             sl.tune_set(mixed.force_variant)
+            sl.overlap = ov
             for k in range(10):  # graph capture of the buffer assignments met
                 sl.md_update("omf2", NSTEPS, TAU, seed=seed, traj=600000 + k)
             ss = torch.cuda.ExternalStream(sl.stream())
@@ -458,7 +459,7 @@ def ours(args):
                 sl.md_update("omf2", NSTEPS, TAU, seed=seed, traj=600010 + k)
             eb.record(ss)
             eb.synchronize()
-            slab_rate[str(nsl)] = K / (ea.elapsed_time(eb) / 1e3)
+            slab_rate[f"{nsl}{' overlapped' if ov else ''}"] = K / (ea.elapsed_time(eb) / 1e3)
 
     # ---- the measurements taken between trajectories (FP64 context, thermalised field):
     #      wall time per call, each call returns its value to the host ----

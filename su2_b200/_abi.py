@@ -132,6 +132,8 @@ SIGNATURES = {
     "su2b_slabs_autotune": (i32, [_P, _D]),
     "su2b_slabs_tune_get": (i32, [_P, C.POINTER(i32)]),
     "su2b_slabs_tune_set": (i32, [_P, i32]),
+    "su2b_slabs_set_overlap": (i32, [_P, i32]),
+    "su2b_slabs_get_overlap": (i32, [_P, C.POINTER(i32)]),
     "su2b_slabs_kernel_launches": (i32, [_P, C.POINTER(C.c_long)]),
     "su2b_slabs_stream": (i32, [_P, C.POINTER(_P)]),
 }

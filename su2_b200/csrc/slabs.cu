@@ -131,6 +131,11 @@ struct su2b_slabs {
   std::vector<su2b_ctx *> sl;
   std::vector<cudaStream_t> own;  // the streams the slab contexts were created with
   cudaStream_t s = nullptr;       // every slab's work is queued here
+  // overlap: each force step updates the boundary slices first and exchanges them on
+  // stream xs while the interior slices are updated on s
+  bool overlap = false;
+  cudaStream_t xs = nullptr;
+  cudaEvent_t ev_b = nullptr, ev_x = nullptr;
   std::vector<std::array<void *, 3>> buf;  // each slab's three link buffers
   int role[3] = {0, 1, 2};  // the buffers that hold the current field, and the two others
   long piece_n = 0;         // 16-byte words per piece (S/2 links)
@@ -271,11 +276,12 @@ cudaError_t copy_pieces(const Piece *tab, int npieces, long n, cudaStream_t s) {
 
 // refresh the ghost slices of buffer k of every slab: every piece (piece < 0) or only
 // piece 2 mu + p
-int exchange(su2b_slabs *h, int k, int piece = -1) {
+int exchange(su2b_slabs *h, int k, int piece = -1, cudaStream_t st = nullptr) {
+  if (!st) st = h->s;
   const int n_of = piece < 0 ? 2 * h->nd : 1, first = piece < 0 ? 0 : piece;
   if (!h->comm) {
     const int per = 2 * h->count;  // table entries per piece
-    SLAB_CUDA(copy_pieces(h->xchg[k] + first * per, n_of * per, h->piece_n, h->s));
+    SLAB_CUDA(copy_pieces(h->xchg[k] + first * per, n_of * per, h->piece_n, st));
     h->launches++;
     return SU2B_OK;
   }
@@ -283,16 +289,16 @@ int exchange(su2b_slabs *h, int k, int piece = -1) {
   const long at = first * h->piece_n;  // the pieces' place in each face of the buffers
   const size_t bytes = (size_t)n_of * h->piece_n * 16;
   const int up = (h->rank + 1) % h->nranks, dn = (h->rank + h->nranks - 1) % h->nranks;
-  SLAB_CUDA(copy_pieces(h->pack[k] + 2 * first, 2 * n_of, h->piece_n, h->s));
+  SLAB_CUDA(copy_pieces(h->pack[k] + 2 * first, 2 * n_of, h->piece_n, st));
   // with two slabs both neighbours are one process: sends and receives to one peer match
   // in the order they are posted, so the order is the same on every rank
   NCCL_CK(h->nc->group_start());
-  NCCL_CK(h->nc->send(h->sendbuf + face + at, bytes, ncclUint8, up, h->comm, h->s));
-  NCCL_CK(h->nc->send(h->sendbuf + at, bytes, ncclUint8, dn, h->comm, h->s));
-  NCCL_CK(h->nc->recv(h->recvbuf + at, bytes, ncclUint8, dn, h->comm, h->s));
-  NCCL_CK(h->nc->recv(h->recvbuf + face + at, bytes, ncclUint8, up, h->comm, h->s));
+  NCCL_CK(h->nc->send(h->sendbuf + face + at, bytes, ncclUint8, up, h->comm, st));
+  NCCL_CK(h->nc->send(h->sendbuf + at, bytes, ncclUint8, dn, h->comm, st));
+  NCCL_CK(h->nc->recv(h->recvbuf + at, bytes, ncclUint8, dn, h->comm, st));
+  NCCL_CK(h->nc->recv(h->recvbuf + face + at, bytes, ncclUint8, up, h->comm, st));
   NCCL_CK(h->nc->group_end());
-  SLAB_CUDA(copy_pieces(h->unpack[k] + 2 * first, 2 * n_of, h->piece_n, h->s));
+  SLAB_CUDA(copy_pieces(h->unpack[k] + 2 * first, 2 * n_of, h->piece_n, st));
   h->launches += 2;
   return SU2B_OK;
 }
@@ -349,16 +355,53 @@ int enqueue(su2b_slabs *h, const std::vector<HmcFusedOp> &fops, int *fin) {
       mode |= FM_RESTORE;
       out = F = (cur == iS) ? iX : next(cur);
     }
-    for (int r = 0; r < R; r++) {
+    // the force step on sites cb0 .. cb0 + ncb - 1 of slab r, its kinetic partials at kin
+    auto launch = [&](int r, int cb0, int ncb, double *kin, int *nb) -> int {
       su2b_ctx *ctx = h->sl[r];
-      int nb = 0;
+      Geom gr = ctx->g;
+      gr.cb0 = cb0;
+      gr.ncb = ncb;
       SU2B_LAUNCH(SU2B_K_FORCE,
-                  force_update<T>(ctx->g, h->buf[r][cur], 0, (T *)ctx->P, nullptr, f, -o.cm,
-                                  ctx->xi, mode, ctx->part_slot(2), &nb, h->buf[r][out], o.cg, s,
+                  force_update<T>(gr, h->buf[r][cur], 0, (T *)ctx->P, nullptr, f, -o.cm,
+                                  ctx->xi, mode, kin, nb, h->buf[r][out], o.cg, s,
                                   ctx->tune_force, false));
-      if (o.kinetic) nb_kin[r] = nb;
+      return SU2B_OK;
+    };
+    const int half = (int)(h->S / 2);  // sites of one parity in one slice
+    if (h->overlap && h->Tl > 2) {
+      // the two boundary slices first; their faces travel on the exchange stream while
+      // the interior slices are updated; the next step waits for the ghost slices
+      std::vector<int> nb0(R, 0), nb1(R, 0);
+      for (int r = 0; r < R; r++) {
+        double *kin = h->sl[r]->part_slot(2);
+        SU2B_CKS(launch(r, half, half, kin, &nb0[r]));
+        SU2B_CKS(launch(r, h->Tl * half, half, kin + nb0[r], &nb1[r]));
+      }
+      {
+        su2b_ctx *ctx = h->sl[0];
+        SU2B_CK(cudaEventRecord(h->ev_b, s));
+        SU2B_CK(cudaStreamWaitEvent(h->xs, h->ev_b, 0));
+      }
+      SU2B_CKS(exchange(h, out, -1, h->xs));
+      for (int r = 0; r < R; r++) {
+        int nb2 = 0;
+        SU2B_CKS(launch(r, 2 * half, (h->Tl - 2) * half,
+                        h->sl[r]->part_slot(2) + nb0[r] + nb1[r], &nb2));
+        if (o.kinetic) nb_kin[r] = nb0[r] + nb1[r] + nb2;
+      }
+      {
+        su2b_ctx *ctx = h->sl[0];
+        SU2B_CK(cudaEventRecord(h->ev_x, h->xs));
+        SU2B_CK(cudaStreamWaitEvent(s, h->ev_x, 0));
+      }
+    } else {
+      for (int r = 0; r < R; r++) {
+        int nb = 0;
+        SU2B_CKS(launch(r, h->sl[r]->g.cb0, h->sl[r]->g.ncb, h->sl[r]->part_slot(2), &nb));
+        if (o.kinetic) nb_kin[r] = nb;
+      }
+      SU2B_CKS(exchange(h, out));
     }
-    SU2B_CKS(exchange(h, out));
     if (o.kind == 1) cur = out;
   }
   for (int r = 0; r < R; r++) {
@@ -428,8 +471,9 @@ int trajectory(su2b_slabs *h, const su2b_hmc_params *prm, su2b_traj_result *res)
     if (rc != SU2B_OK) return from_ctx(h, rc);
   } else {
     char key[192];
-    snprintf(key, sizeof key, "%d/%d/%.17g/%d%d%d/%d", prm->integrator, prm->n_steps, prm->tau,
-             h->role[0], h->role[1], h->role[2], h->sl[0]->tune_force);
+    snprintf(key, sizeof key, "%d/%d/%.17g/%d%d%d/%d/%d", prm->integrator, prm->n_steps,
+             prm->tau, h->role[0], h->role[1], h->role[2], h->sl[0]->tune_force,
+             (int)h->overlap);
     auto it = h->graphs.find(key);
     if (it == h->graphs.end()) {
       // the capture counts the graph's kernels; each replay adds them
@@ -525,6 +569,10 @@ extern "C" int su2b_slabs_create(int Lx, int Ly, int Lz, int Lt, int ndims, doub
   for (su2b_ctx *c : h->sl) c->stream = h->s;
   h->piece_n = (h->S / 2) * (long)(h->sl[0]->link_bytes() / 16);
   if (cudaSetDevice(device) != cudaSuccess) return fin(fail(h, SU2B_ERR_CUDA, "cudaSetDevice"));
+  if (cudaStreamCreateWithFlags(&h->xs, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&h->ev_b, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&h->ev_x, cudaEventDisableTiming) != cudaSuccess)
+    return fin(fail(h, SU2B_ERR_CUDA, "exchange stream or events"));
   if (count == nslabs) return fin(build_local_tables(h));
   return fin(SU2B_OK);
 }
@@ -533,7 +581,11 @@ extern "C" int su2b_slabs_destroy(su2b_slabs *h) {
   if (!h) return SU2B_ERR_INVALID;
   cudaSetDevice(h->device);
   if (h->s) cudaStreamSynchronize(h->s);
+  if (h->xs) cudaStreamSynchronize(h->xs);
   for (auto &kv : h->graphs) cudaGraphExecDestroy(kv.second.exec);
+  if (h->ev_b) cudaEventDestroy(h->ev_b);
+  if (h->ev_x) cudaEventDestroy(h->ev_x);
+  if (h->xs) cudaStreamDestroy(h->xs);
   if (h->comm && h->nc) h->nc->comm_destroy(h->comm);
   for (void *p : h->allocs) cudaFree(p);
   for (size_t r = 0; r < h->sl.size(); r++) {
@@ -588,6 +640,7 @@ extern "C" int su2b_slabs_connect(su2b_slabs *h, const void *id, int nranks, int
   h->comm = comm;
   h->nranks = nranks;
   h->rank = rank;
+  h->overlap = true;  // the faces cross NVLink while the interior slices are updated
   const size_t bytes = (size_t)4 * h->nd * h->piece_n * 16;  // two faces
   void *a = nullptr, *b = nullptr;
   SLAB_CUDA(cudaMalloc(&a, bytes));
@@ -758,6 +811,18 @@ extern "C" int su2b_slabs_tune_set(su2b_slabs *h, int variant) {
   if (variant < 0 || variant >= FORCE_VARIANTS)
     return fail(h, SU2B_ERR_INVALID, "force variant out of range");
   for (su2b_ctx *c : h->sl) c->tune_force = variant;
+  return SU2B_OK;
+}
+
+extern "C" int su2b_slabs_set_overlap(su2b_slabs *h, int on) {
+  if (!h) return SU2B_ERR_INVALID;
+  h->overlap = on != 0;
+  return SU2B_OK;
+}
+
+extern "C" int su2b_slabs_get_overlap(const su2b_slabs *h, int *on) {
+  if (!h || !on) return SU2B_ERR_INVALID;
+  *on = h->overlap ? 1 : 0;
   return SU2B_OK;
 }
 

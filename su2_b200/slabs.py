@@ -170,6 +170,17 @@ class slab_lattice:
         """The force kernel's launch shape (an index of _abi.FORCE_SHAPES) on every slab."""
         self._c(self.lib.su2b_slabs_tune_set(self.h, int(variant)))
 
+    @property
+    def overlap(self) -> bool:
+        """Boundary slices first, their exchange overlapping the interior (su2b_slabs_set_overlap)."""
+        v = C.c_int()
+        self._c(self.lib.su2b_slabs_get_overlap(self.h, C.byref(v)))
+        return bool(v.value)
+
+    @overlap.setter
+    def overlap(self, on: bool):
+        self._c(self.lib.su2b_slabs_set_overlap(self.h, int(bool(on))))
+
     def kernel_launches(self) -> int:
         n = C.c_long()
         self._c(self.lib.su2b_slabs_kernel_launches(self.h, C.byref(n)))

@@ -238,3 +238,45 @@ def test_slab_graph_replay(gpu, orc):
         # step one exchange; one cross-slab sum
         assert counts == [n * (nf + 6) + nf + 1] * 4
         assert rel(s.download(), U) > 0
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+@pytest.mark.parametrize("dims,nslabs", [((6, 6, 6, 16), 2), ((8, 8, 8, 16), 4),
+                                         ((4, 6, 8, 12), 3), ((8, 8, 8, 8), 4)],
+                         ids=["6^3x16/2", "8^3x16/4", "4x6x8x12/3", "8^4/4-no-interior"])
+def test_overlapped_exchange_equals_the_single_lattice(gpu, orc, precision, dims, nslabs):
+    """Boundary slices first, the exchange on a second stream while the interior slices are
+    updated (the form slabs on separate GPUs run): the same links and accept decisions.
+    With two slices per slab there is no interior and the step runs as without overlap."""
+    nd = 4
+    U = hot(orc, dims, nd)
+    with single(gpu, dims, nd, precision) as c, slabs(dims, nd, nslabs, precision) as s:
+        assert not s.overlap
+        s.overlap = True
+        assert s.overlap
+        c.upload(U)
+        s.upload(U)
+        same_chain(chain(c, 6), chain(s, 6))
+        assert np.array_equal(c.download(), s.download())
+        for v in (0, 8, 9):  # a site shape, xsplit, one thread per link
+            c.force_variant = v
+            s.tune_set(v)
+            same_chain(chain(c, 2, seed=3), chain(s, 2, seed=3))
+            assert np.array_equal(c.download(), s.download()), v
+
+
+def test_overlapped_exchange_launches(gpu, orc):
+    """With overlap each force step is three launches per slab (two boundary slices, the
+    interior) and one exchange."""
+    dims, nd, n = (6, 6, 6, 16), 4, 2
+    U = hot(orc, dims, nd)
+    with slabs(dims, nd, n, "mixed") as s:
+        s.overlap = True
+        s.upload(U)
+        counts = []
+        for k in range(3):
+            n0 = s.kernel_launches()
+            s.md_update("omf2", 3, 1.0, seed=1, traj=k, uniform=1e-300)
+            counts.append(s.kernel_launches() - n0)
+        nf = 2 * 3 + 1
+        assert counts == [n * (3 * nf + 6) + nf + 1] * 3
