@@ -293,6 +293,14 @@ SU2B_API int su2b_slabs_hmc_trajectory(su2b_slabs *h, const su2b_hmc_params *prm
  * acceptance rates of the whole lattice) */
 SU2B_API int su2b_slabs_metropolis_sweep(su2b_slabs *h, double delta, int N_hit, uint64_t seed,
                                          uint32_t sweep, double *rates);
+/* the Wilson flow over the slabs: runge_kutta on the current field (as su2b_flow_step),
+ * energy_density and gradient_flow of the whole lattice (as su2b_energy_density and
+ * su2b_gradient_flow, the same rows); each RK3 stage exchanges the ghost slices it wrote */
+SU2B_API int su2b_slabs_flow_step(su2b_slabs *h, double eps);
+SU2B_API int su2b_slabs_energy_density(su2b_slabs *h, int cloverdef, int ss, double *E,
+                                       double *Q);
+SU2B_API int su2b_slabs_gradient_flow(su2b_slabs *h, double tmax, double eps, double tstart,
+                                      double *rows, int max_rows, int *n_rows);
 /* gauge_energy of the whole lattice (as su2b_gauge_energy) */
 SU2B_API int su2b_slabs_gauge_energy(su2b_slabs *h, int spatial_only, double *out);
 /* su2b_autotune on the first slab; every slab takes its choice */

@@ -129,6 +129,9 @@ SIGNATURES = {
     "su2b_slabs_hmc_trajectory": (i32, [_P, C.POINTER(HmcParams), C.POINTER(TrajResult)]),
     "su2b_slabs_gauge_energy": (i32, [_P, i32, _D]),
     "su2b_slabs_metropolis_sweep": (i32, [_P, f64, i32, u64, u32, _D]),
+    "su2b_slabs_flow_step": (i32, [_P, f64]),
+    "su2b_slabs_energy_density": (i32, [_P, i32, i32, _D, _D]),
+    "su2b_slabs_gradient_flow": (i32, [_P, f64, f64, f64, _D, i32, C.POINTER(C.c_int)]),
     "su2b_slabs_autotune": (i32, [_P, _D]),
     "su2b_slabs_tune_get": (i32, [_P, C.POINTER(i32)]),
     "su2b_slabs_tune_set": (i32, [_P, i32]),

@@ -384,8 +384,8 @@ extern "C" int su2b_gauge_action(su2b_ctx *ctx, double *out) {
 }
 
 // E, Q from clover partial sums (flat-energy_density.hh:152-163)
-static void finish_clover(const double *r, double V, int cloverdef, int ss, double *E,
-                          double *Q) {
+void su2b_finish_clover(const double *r, double V, int cloverdef, int ss, double *E,
+                        double *Q) {
   double e = -(ss ? r[1] : r[0]) / V;
   if (cloverdef) e /= 16.;
   double q = ss ? 0.0 : r[2];
@@ -401,7 +401,7 @@ extern "C" int su2b_energy_density(su2b_ctx *ctx, int cloverdef, int ss, double 
   NEED(E && Q, "E or Q is NULL");
   CKS(su2b_q_clover(ctx, ctx->U, cloverdef, 0));
   CKS(su2b_fetch_red(ctx, 3));
-  finish_clover(ctx->h_red, (double)ctx->V, cloverdef, ss, E, Q);
+  su2b_finish_clover(ctx->h_red, (double)ctx->V, cloverdef, ss, E, Q);
   return SU2B_OK;
 }
 
@@ -589,8 +589,8 @@ extern "C" int su2b_gradient_flow(su2b_ctx *ctx, double tmax, double eps, double
     const double *r = ctx->h_red;
     const double P1 = r[0] / den, Pss1 = r[1] / den;
     double E1, Q1, Ess1, Qss1;
-    finish_clover(r + 3, (double)ctx->V, 1, 0, &E1, &Q1);
-    finish_clover(r + 3, (double)ctx->V, 1, 1, &Ess1, &Qss1);
+    su2b_finish_clover(r + 3, (double)ctx->V, 1, 0, &E1, &Q1);
+    su2b_finish_clover(r + 3, (double)ctx->V, 1, 1, &Ess1, &Qss1);
     const double Ep = ndims_fact - P1;
     const double Ep_ss = ndims_fact_ss - Pss1;
     const double Ep_ts = Ep - Ep_ss;

@@ -29,9 +29,10 @@ __global__ void __launch_bounds__(NT)
   k_clover_su2(Geom g, const LinkT<T> *__restrict__ U, int cloverdef, double *part) {
   __shared__ double shk[4 * (NT / 32)];
   const int p = blockIdx.x & 1;
-  const int cb = (blockIdx.x >> 1) * NT + threadIdx.x;
+  // the sites cb0 .. cb0 + ncb - 1 of each parity (all of them but in a time slab)
+  const int cb = g.cb0 + (blockIdx.x >> 1) * NT + threadIdx.x;
   double e_all = 0., e_ss = 0., q = 0.;
-  if (cb < g.Vh) {
+  if (cb < g.cb0 + g.ncb) {
     const Site s = site_from_eo(g, p, cb);
     Su2<double> G[ND][ND];
 #pragma unroll
@@ -142,7 +143,7 @@ template <class T>
 cudaError_t clover_partials(const Geom &g, const void *U, int group, int cloverdef,
                             double *part, int *nblocks, cudaStream_t s) {
   constexpr int NT = 128;
-  const dim3 grid(2 * ((g.Vh + NT - 1) / NT));
+  const dim3 grid(2 * (((group == 0 ? g.ncb : g.Vh) + NT - 1) / NT));
   *nblocks = grid.x;
   if (group == 0) {
     const LinkT<T> *u = (const LinkT<T> *)U;

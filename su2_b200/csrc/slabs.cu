@@ -33,6 +33,8 @@
 #include <nccl.h>
 
 #include <array>
+#include <cmath>
+#include <utility>
 #include <cstring>
 #include <map>
 #include <mutex>
@@ -787,6 +789,147 @@ extern "C" int su2b_slabs_metropolis_sweep(su2b_slabs *h, double delta, int N_hi
   const double V = (double)h->S * h->Lt;
   rates[0] = (double)n0 / nh / (V * h->nd);
   rates[1] = (double)n1 / nh / V;
+  return SU2B_OK;
+}
+
+// ---- the Wilson flow over the slabs (flat-gradient_flow.hh:17-197) ----
+namespace {
+
+// one RK3 step (runge_kutta, flat-gradient_flow.hh:17-50) of every slab from link buffer a
+// into buffer b (a != b; a is left holding the middle stage): each stage is the force launch
+// with its link update fused (a -> b -> a -> b), followed by the exchange of the buffer it
+// wrote; with FP32 links the result is reunitarised in FP64, ghost links included (the same
+// elementwise operation as on the neighbour's own links, so the ghosts stay exact copies)
+int flow_step(su2b_slabs *h, int a, int b, double eps) {
+  const double zfac[3] = {(-17.0) / (36.0), (8.0) / (9.0), (-3.0) / (4.0)};
+  const double expfac[3] = {-36.0 / 4. / 17.0, 1., -1.};
+  int w = a;
+  for (int f = 0; f < 3; f++) {
+    const int nxt = w == a ? b : a;
+    for (int r = 0; r < h->count; r++) {
+      su2b_ctx *c = h->sl[r];
+      const double Nc = c->Nc();
+      const double ff = 2. * Nc * zfac[f] / c->beta * c->beta / Nc;
+      const int mode = (f == 0 ? 0 : FM_HAS_IN) | FM_UPDATE;
+      const int rc = su2b_q_force(c, h->buf[r][w], c->Z, nullptr, ff, 1.0, mode, nullptr, nullptr,
+                                  h->buf[r][nxt], -eps * expfac[f]);
+      if (rc != SU2B_OK) return from_ctx(h, rc);
+    }
+    SU2B_CKS(exchange(h, nxt));
+    w = nxt;
+  }
+  if (!h->link64)
+    for (int r = 0; r < h->count; r++) {
+      const int rc = su2b_q_restore(h->sl[r], h->buf[r][w]);
+      if (rc != SU2B_OK) return from_ctx(h, rc);
+    }
+  return SU2B_OK;
+}
+
+// plaquette sums into red[slot .. slot+2] and clover sums (cloverdef) into red[slot+3 ..
+// slot+5] of buffer k on every slab
+int measure(su2b_slabs *h, int k, int cloverdef, int slot) {
+  for (int r = 0; r < h->count; r++) {
+    su2b_ctx *c = h->sl[r];
+    int rc = su2b_q_plaq(c, h->buf[r][k], slot);
+    if (rc == SU2B_OK) rc = su2b_q_clover(c, h->buf[r][k], cloverdef, slot + 3);
+    if (rc != SU2B_OK) return from_ctx(h, rc);
+  }
+  return SU2B_OK;
+}
+
+int begin(su2b_slabs *h) {
+  h->err.clear();
+  if (!connected(h))
+    return fail(h, SU2B_ERR_INVALID,
+                "the handle holds a part of the slabs: connect it to the others first");
+  SLAB_CUDA(cudaSetDevice(h->device));
+  for (su2b_ctx *c : h->sl) c->begin_call();
+  return SU2B_OK;
+}
+
+}  // namespace
+
+// runge_kutta on the current field (as su2b_flow_step: the flowed field becomes current)
+extern "C" int su2b_slabs_flow_step(su2b_slabs *h, double eps) {
+  if (!h) return SU2B_ERR_INVALID;
+  SU2B_CKS(begin(h));
+  SU2B_CKS(flow_step(h, h->role[0], h->role[2], eps));
+  std::swap(h->role[0], h->role[2]);
+  set_roles(h);
+  SLAB_CUDA(cudaStreamSynchronize(h->s));
+  return SU2B_OK;
+}
+
+// energy_density (flat-energy_density.hh:57-164) of the whole lattice
+extern "C" int su2b_slabs_energy_density(su2b_slabs *h, int cloverdef, int ss, double *E,
+                                         double *Q) {
+  if (!h) return SU2B_ERR_INVALID;
+  if (!E || !Q) return fail(h, SU2B_ERR_INVALID, "E or Q is NULL");
+  SU2B_CKS(begin(h));
+  SU2B_CKS(measure(h, h->role[0], cloverdef, 0));
+  SU2B_CKS(sum_over_slabs(h, 6));
+  su2b_ctx *c = h->sl[0];
+  SLAB_CUDA(cudaMemcpyAsync(c->h_red, c->red, 6 * sizeof(double), cudaMemcpyDeviceToHost, h->s));
+  SLAB_CUDA(cudaStreamSynchronize(h->s));
+  su2b_finish_clover(c->h_red + 3, (double)h->S * h->Lt, cloverdef, ss, E, Q);
+  return SU2B_OK;
+}
+
+// gradient_flow (flat-gradient_flow.hh:70-197) of the current field, which stays unchanged:
+// the rows of su2b_gradient_flow, the flow running on a copy in the second link buffer
+extern "C" int su2b_slabs_gradient_flow(su2b_slabs *h, double tmax, double eps, double tstart,
+                                        double *rows, int max_rows, int *n_rows) {
+  if (!h) return SU2B_ERR_INVALID;
+  if (!n_rows) return fail(h, SU2B_ERR_INVALID, "n_rows is NULL");
+  if (!(eps > 0)) return fail(h, SU2B_ERR_INVALID, "eps must be positive");
+  if (max_rows < 0 || (!rows && max_rows > 0)) return fail(h, SU2B_ERR_INVALID, "rows buffer");
+  SU2B_CKS(begin(h));
+  const int S0 = h->role[0], Vt = h->role[1], W2 = h->role[2];
+  for (int r = 0; r < h->count; r++)
+    SLAB_CUDA(cudaMemcpyAsync(h->buf[r][Vt], h->buf[r][S0],
+                              h->sl[r]->link_bytes() * h->sl[r]->NL, cudaMemcpyDeviceToDevice,
+                              h->s));
+  const double d = (double)h->nd, V = (double)h->S * h->Lt;
+  const double ndims_fact = d * (d - 1) / 2.0, ndims_fact_ss = (d - 1) * (d - 2) / 2.0;
+  const double den = V * h->sl[0]->Nc();
+  su2b_ctx *c = h->sl[0];
+  double t[3] = {tstart, tstart, tstart};
+  int nr = 0;
+  while (t[1] < tmax - eps) {
+    t[0] = t[2];
+    t[1] = t[0] + eps;
+    // two steps per record; the reference prints the observables of the middle step
+    SU2B_CKS(flow_step(h, Vt, W2, eps));
+    SU2B_CKS(measure(h, W2, 1, 0));
+    t[2] = t[1] + eps;
+    SU2B_CKS(flow_step(h, W2, Vt, eps));
+    SU2B_CKS(sum_over_slabs(h, 6));
+    SLAB_CUDA(cudaMemcpyAsync(c->h_red, c->red, 6 * sizeof(double), cudaMemcpyDeviceToHost,
+                              h->s));
+    SLAB_CUDA(cudaStreamSynchronize(h->s));
+    const double *rd = c->h_red;
+    const double P1 = rd[0] / den, Pss1 = rd[1] / den;
+    double E1, Q1, Ess1, Qss1;
+    su2b_finish_clover(rd + 3, V, 1, 0, &E1, &Q1);
+    su2b_finish_clover(rd + 3, V, 1, 1, &Ess1, &Qss1);
+    const double Ep = ndims_fact - P1, Ep_ss = ndims_fact_ss - Pss1;
+    const double Ep_ts_bar = (Ep - Ep_ss) / (d - 1), Ep_ss_bar = Ep_ss / ndims_fact_ss;
+    if (nr < max_rows) {
+      double *o = rows + 9 * (size_t)nr;
+      o[0] = t[1];
+      o[1] = sqrt(Ep_ts_bar / Ep_ss_bar);
+      o[2] = P1;
+      o[3] = Pss1;
+      o[4] = Ep;
+      o[5] = Ep_ss;
+      o[6] = E1;
+      o[7] = Ess1;
+      o[8] = Q1;
+    }
+    nr++;
+  }
+  *n_rows = nr;
   return SU2B_OK;
 }
 

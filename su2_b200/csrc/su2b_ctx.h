@@ -115,6 +115,10 @@ int su2b_adj_download(su2b_ctx *ctx, const void *dev, double *host);
 int su2b_q_plaq(su2b_ctx *ctx, const void *U, int red_slot);
 int su2b_q_clover(su2b_ctx *ctx, const void *U, int cloverdef, int red_slot);
 int su2b_fetch_red(su2b_ctx *ctx, int n);
+// E and Q of energy_density (flat-energy_density.hh:57-164) from the clover sums r[0..2] of V sites
+void su2b_finish_clover(const double *r, double V, int cloverdef, int ss, double *E, double *Q);
+// E and Q of energy_density (flat-energy_density.hh:57-164) from the clover sums r[0..2] of V sites
+void su2b_finish_clover(const double *r, double V, int cloverdef, int ss, double *E, double *Q);
 // mode FM_UPDATE / FM_RESTORE: the force kernel also writes the next link buffer Uout
 int su2b_q_force(su2b_ctx *ctx, const void *U, void *P, const void *extra, double f,
                  double scale, int mode, double *kin_part, int *nb, void *Uout = nullptr,

@@ -151,6 +151,27 @@ class slab_lattice:
                                                      _dp(rates)))
         return rates
 
+    def runge_kutta(self, eps):
+        """One RK3 flow step of the current field (runge_kutta, flat-gradient_flow.hh:17-50)."""
+        self._c(self.lib.su2b_slabs_flow_step(self.h, eps))
+
+    def energy_density(self, cloverdef=True, ss=False):
+        """(E, Q) of the whole lattice (flat-energy_density.hh:57-164)."""
+        E, Q = C.c_double(), C.c_double()
+        self._c(self.lib.su2b_slabs_energy_density(self.h, int(cloverdef), int(ss), C.byref(E),
+                                                   C.byref(Q)))
+        return E.value, Q.value
+
+    def gradient_flow(self, tmax, eps, tstart=0.0) -> np.ndarray:
+        """Records {t, xi_R, P, P_ss, Ep, Ep_ss, Ec, Ec_ss, Q} of the whole lattice
+        (flat-gradient_flow.hh:70-197); the current field stays unchanged."""
+        max_rows = int((tmax - tstart) / (2 * eps)) + 4
+        rows = np.zeros((max_rows, 9))
+        n = C.c_int()
+        self._c(self.lib.su2b_slabs_gradient_flow(self.h, tmax, eps, tstart, _dp(rows), max_rows,
+                                                  C.byref(n)))
+        return rows[:min(n.value, max_rows)].copy()
+
     def gauge_energy(self, spatial_only=False) -> float:
         out = C.c_double()
         self._c(self.lib.su2b_slabs_gauge_energy(self.h, int(spatial_only), C.byref(out)))

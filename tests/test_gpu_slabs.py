@@ -280,3 +280,31 @@ def test_overlapped_exchange_launches(gpu, orc):
             counts.append(s.kernel_launches() - n0)
         nf = 2 * 3 + 1
         assert counts == [n * (3 * nf + 6) + nf + 1] * 3
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+@pytest.mark.parametrize("dims,nd,nslabs", [((8, 8, 8, 8), 4, 2), ((4, 6, 8, 12), 4, 3),
+                                            ((8, 6, 1, 8), 3, 4)],
+                         ids=["8^4/2", "4x6x8x12/3", "8x6x8-d3/4"])
+def test_slab_flow(gpu, orc, precision, dims, nd, nslabs):
+    """The Wilson flow over slabs: RK3 steps give the single lattice's links; energy_density
+    and the gradient_flow records (from a thermalised-like field, the current field left
+    unchanged) agree to the rounding of the sums' order."""
+    U = orc.hotstart(0, dims, nd, SEED, 0.2, TRAFO)
+    with single(gpu, dims, nd, precision) as c, slabs(dims, nd, nslabs, precision) as s:
+        c.upload(U)
+        s.upload(U)
+        for ref, got in ((c.energy_density(), s.energy_density()),
+                         (c.energy_density(False, True), s.energy_density(False, True))):
+            assert got[0] == pytest.approx(ref[0], rel=1e-12)
+            assert got[1] == pytest.approx(ref[1], rel=1e-9, abs=1e-12)
+        for _ in range(3):
+            c.runge_kutta(0.02)
+            s.runge_kutta(0.02)
+        assert np.array_equal(c.download(), s.download())
+        rc, rs = c.gradient_flow(0.3, 0.02), s.gradient_flow(0.3, 0.02)
+        assert rc.shape == rs.shape and len(rc) >= 6
+        assert np.array_equal(rc[:, 0], rs[:, 0])
+        np.testing.assert_allclose(rs[:, 1:8], rc[:, 1:8], rtol=1e-11, atol=1e-13)
+        np.testing.assert_allclose(rs[:, 8], rc[:, 8], rtol=1e-8, atol=1e-11)
+        assert np.array_equal(c.download(), s.download())  # the field is unchanged
