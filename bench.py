@@ -644,6 +644,20 @@ def slabs_run(args):
     clk = clocks.stop()
     launches = lat.kernel_launches() - n0
     t = allmax(dist, e0.elapsed_time(e1) / 1e3)
+    # the workload's other steps over the same slabs: Metropolis sweeps and RK3 flow steps
+    side = {}
+    for name, fn, n in (("metropolis_sweeps_per_s", lambda k: lat.sweep(0.15, 8, seed, 7000 + k), 5),
+                        ("flow_rk3_steps_per_s", lambda k: lat.runge_kutta(0.01), 10)):
+        lat.upload(U_th)
+        fn(0)
+        barrier(dist)
+        e0.record(s)
+        for k in range(n):
+            fn(k + 1)
+        e1.record(s)
+        e1.synchronize()
+        side[name] = n / allmax(dist, e0.elapsed_time(e1) / 1e3)
+    lat.upload(U_th)
     Uh = torch.empty(NL * 4, dtype=torch.float64, pin_memory=True).numpy()
     Uh[:] = U_th
     t0, t1 = lat.slices()
@@ -667,6 +681,7 @@ def slabs_run(args):
                        "parallelism": f"t-slabs x{N}" + (" on one GPU" if ws == 1 else ""),
                        "l2": "working set > 126 MB L2; no flush"},
             "acceptance": sum(r.accepted for r in res) / K,
+            "side": side,
             "e2e": {"value": K / t_e2e, "unit": "traj/s",
                     "h2d_bytes_per_step": int(lat.count * (L // N + 2) * row * 8),
                     "d2h_bytes_per_step": int((t1 - t0) * row * 8),
