@@ -24,8 +24,13 @@ __device__ __forceinline__ Su2<double> L(const Geom &g, const LinkT<T> *U, int m
   return to64(ld_link(U + (size_t)mu * g.V + eo_of(g, lex, p)));
 }
 
+// FP64 links: six resident blocks per SM (80 registers, 80 bytes of spills) beat the
+// compiler's free choice of 104 registers and four blocks (155 against 169 us per call at
+// 32^4); with FP32 links four blocks (128 registers, no spills) are as fast as any cap
+template <class T, int NT> constexpr int clover_min_blocks() { return sizeof(T) == 8 ? 6 : 4; }
+
 template <class T, int ND, int NT>
-__global__ void __launch_bounds__(NT)
+__global__ void __launch_bounds__(NT, clover_min_blocks<T, NT>())
   k_clover_su2(Geom g, const LinkT<T> *__restrict__ U, int cloverdef, double *part) {
   __shared__ double shk[4 * (NT / 32)];
   const int p = blockIdx.x & 1;

@@ -110,9 +110,10 @@ __global__ void k_spinor_to_host(Geom g, const double2 *__restrict__ psi, double
 // ------------------------------------------------------------------------------------
 // plaquettes: per site, sum over planes mu<nu of ReTr U_mu(x) U_nu(x+mu) U_mu(x+nu)^+ U_nu(x)^+
 // (flat-gauge_energy.hpp:31-94), FP64 products.  Partials {full, spatial, xi-weighted}.
-// FP64 links take twice the registers of FP32 ones: half the resident blocks, no spills
+// Resident blocks of 256 threads: four with FP32 links (64 registers), three with FP64 links
+// (80 registers, no spills; the plaquette call 67 against 71 us at 32^4 with two)
 template <class T, int NT> constexpr int plaq_min_blocks() {
-  return sizeof(T) == 8 ? 512 / NT : 1024 / NT;
+  return sizeof(T) == 8 ? 768 / NT : 1024 / NT;
 }
 
 template <class T, int ND, int NT>
