@@ -692,18 +692,18 @@ extern "C" int su2b_batch_autotune(su2b_batch *b, double *times_us) {
   if (!b) return SU2B_ERR_INVALID;
   b->err.clear();
   BCK(cudaSetDevice(b->device));
-  double best = 0.;
-  int bv = b->variant;
+  double t[SU2B_BATCH_VARIANTS], fastest = 0.;
   for (int v = 0; v < SU2B_BATCH_VARIANTS; v++) {
     double us = 0.;
     const int rc = b->link64 ? time_force<double>(b, v, &us) : time_force<float>(b, v, &us);
     if (rc != SU2B_OK) return rc;
     if (times_us) times_us[v] = us;
-    if (v == 0 || us < best) {
-      best = us;
-      bv = v;
-    }
+    t[v] = us;
+    fastest = (v == 0 || us < fastest) ? us : fastest;
   }
+  // as su2b_autotune: the first shape within 1 % of the fastest, so ties resolve alike
+  int bv = 0;
+  while (t[bv] > 1.01 * fastest) bv++;
   b->variant = bv;
   return SU2B_OK;
 }

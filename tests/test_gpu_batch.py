@@ -69,7 +69,8 @@ def test_batch_autotune_leaves_fields_and_every_shape_agrees(gpu, orc):
             if v == 0:
                 t = b.autotune()
                 assert all(x > 0 for x in t.values())
-                assert b.variant == min(t, key=t.get)
+                fastest = min(t.values())  # the first shape within 1 % of the fastest
+                assert b.variant == min(v for v in t if t[v] <= 1.01 * fastest)
                 for i, U in enumerate(starts):
                     assert np.array_equal(b.download(i), U.astype(np.float32).astype(np.float64))
             b.variant = v

@@ -508,7 +508,9 @@ def test_autotune_cache(gpu, orc, tmp_path):
         c.upload(U)
         t = c.autotune(path)
         assert all(v > 0 for v in t.values())
-        best = min(t, key=t.get)
+        # the first shape within 1 % of the fastest
+        fastest = min(t.values())
+        best = min(v for v in t if t[v] <= 1.01 * fastest)
         assert c.force_variant == best
     line = open(path).read().split()
     assert int(line[1]) == best and "/force/fp32/16x16x16x16/d4" in line[0]
