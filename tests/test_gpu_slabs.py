@@ -308,3 +308,22 @@ def test_slab_flow(gpu, orc, precision, dims, nd, nslabs):
         np.testing.assert_allclose(rs[:, 1:8], rc[:, 1:8], rtol=1e-11, atol=1e-13)
         np.testing.assert_allclose(rs[:, 8], rc[:, 8], rtol=1e-8, atol=1e-11)
         assert np.array_equal(c.download(), s.download())  # the field is unchanged
+
+
+def test_slab_connect_refusals(gpu):
+    """su2b_slabs_connect wants one slab per process (count 1, nranks = nslabs, rank =
+    first); the NCCL id comes from the run-time NCCL and is 128 bytes.  No communicator is
+    made here: one GPU holds no second rank."""
+    from su2_b200.slabs import nccl_unique_id, slab_lattice
+    uid = nccl_unique_id()
+    assert len(uid) == 128 and any(uid)
+    dims, nd = (4, 4, 4, 8), 4
+    with slab_lattice(dims, nd, 2.3, 2, precision="fp64") as s:  # both slabs: no communicator
+        with pytest.raises(gpu.Su2bError) as e:
+            s.connect(uid, 2, 0)
+        assert e.value.code == gpu._abi.ERR_INVALID
+    with slab_lattice(dims, nd, 2.3, 2, precision="fp64", first=1, count=1) as s:
+        for nranks, rank in ((2, 0), (3, 1), (1, 0)):  # wrong rank, wrong size
+            with pytest.raises(gpu.Su2bError) as e:
+                s.connect(uid, nranks, rank)
+            assert e.value.code == gpu._abi.ERR_INVALID
