@@ -380,7 +380,7 @@ SU2B_API int su2b_flow_adjoint(su2b_ctx *ctx, double eps, int n_steps, int check
  * with cache_path it first looks the choice up in that text file (unless retune) and writes
  * new measurements to it.  times_us (optional, SU2B_FORCE_VARIANTS entries) receives the
  * average launch time of each shape (-1 when not measured). */
-#define SU2B_FORCE_VARIANTS 11
+#define SU2B_FORCE_VARIANTS 12
 /* SU2B_TUNE_TRAJECTORY selects how su2b_hmc_trajectory runs an SU(2) trajectory without
  * fermions, reversibility test or rounding:
  *   SU2B_TRAJ_FUSED_GRAPH (default): each momentum step fused with the gauge step after it,

@@ -140,7 +140,7 @@ SIGNATURES = {
     "su2b_slabs_kernel_launches": (i32, [_P, C.POINTER(C.c_long)]),
     "su2b_slabs_stream": (i32, [_P, C.POINTER(_P)]),
 }
-FORCE_VARIANTS = 11
+FORCE_VARIANTS = 12
 BATCH_VARIANTS = 4
 # (threads per block, min blocks per SM) of the batched force kernel
 BATCH_SHAPES = [(64, 8), (128, 4), (128, 6), (256, 3)]
@@ -149,7 +149,7 @@ BATCH_SHAPES = [(64, 8), (128, 4), (128, 6), (256, 3)]
 # cross-plane products formed once per site and swapped in shared memory; the anisotropic
 # action always runs (128, 6)
 FORCE_SHAPES = [(256, 4), (128, 8), (128, 4), (128, 6), (256, 2), (256, 3), ("split", 128, 8),
-                (64, 16), ("xsplit", 128, 8), ("link", 128, 6), ("split", 128, 5)]
+                (64, 16), ("xsplit", 128, 8), ("link", 128, 6), ("split", 128, 5), ("pair", 128, 8)]
 
 K_FORCE, K_UPDATE, K_PLAQUETTE, K_MOMENTA, K_RESTORE, K_METROPOLIS, K_CLOVER, K_STAGGERED, \
     K_OTHER = range(9)

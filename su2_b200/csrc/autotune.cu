@@ -90,8 +90,18 @@ extern "C" int su2b_autotune(su2b_ctx *ctx, const char *cache_path, int retune,
   const int mode = FM_HAS_IN | FM_UPDATE;
   double t[FORCE_VARIANTS];
   int rc = SU2B_OK;
+  // site pairs run on a paired copy of the field (in U_old, a scratch buffer between
+  // trajectories), as the fused trajectory runs them
+  const bool pairs = !ctx->link64 && ctx->xi == 1.0 && pairs_apply(ctx->g);
+  if (pairs) {
+    const cudaError_t e = to_pairs(ctx->g, ctx->U, ctx->U_old, s);
+    if (e != cudaSuccess) rc = su2b_fail(ctx, SU2B_ERR_CUDA, "autotune: %s", cudaGetErrorString(e));
+  }
   for (int var = 0; var < FORCE_VARIANTS && rc == SU2B_OK; var++) {
     auto launch = [&]() -> cudaError_t {
+      if (var == FORCE_PAIR && pairs)
+        return force_pair(ctx->g, ctx->U_old, (float *)ctx->Z, f, -1e-3, mode, nullptr, nullptr,
+                          ctx->U2, 0.0, s, false);
       if (ctx->link64)
         return force_update<double>(ctx->g, ctx->U, 0, (double *)ctx->Z, nullptr, f, -1e-3,
                                     ctx->xi, mode, nullptr, nullptr, ctx->U2, 0.0, s, var);

@@ -834,6 +834,7 @@ cudaError_t force_update(const Geom &g, const void *U, int group, T *P, const T 
         case 8: SU2B_FORCE_XSPLIT(128, 8); break;
         case 9: SU2B_FORCE_LINK(6); break;
         case 10: SU2B_FORCE_SPLIT(128, 5); break;
+        case 11: SU2B_FORCE_LINK(6); break;  // site pairs: the standard-layout stand-in
         default: SU2B_FORCE_LAUNCH(64, 16, false); break;
       }
     }

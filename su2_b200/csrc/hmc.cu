@@ -218,6 +218,17 @@ int enqueue_fused(su2b_ctx *ctx, const std::vector<FOp> &fops, bool host_momenta
   void *cur = S;
   auto next = [&](void *c) { return c == X ? Y : X; };
   void *F = nullptr;
+  // site pairs (FP32 links, isotropic, d = 4, T % 4 == 0, a schedule of fused steps closed by
+  // a momentum step): the start field copied into the paired layout in X, the force launches
+  // on paired buffers, the final field written back in the standard layout
+  bool paired = !ctx->link64 && ctx->tune_force == FORCE_PAIR && ctx->xi == 1.0 &&
+                pairs_apply(ctx->g) && !fops.empty();
+  for (size_t i = 0; paired && i < fops.size(); i++)
+    if (fops[i].kind != (i + 1 == fops.size() ? 0 : 1)) paired = false;
+  if (paired) {
+    SU2B_LAUNCH(SU2B_K_OTHER, to_pairs(ctx->g, S, X, s));
+    cur = X;
+  }
   for (size_t i = 0; i < fops.size(); i++) {
     const FOp &o = fops[i];
     const bool last = i + 1 == fops.size();
@@ -242,7 +253,10 @@ int enqueue_fused(su2b_ctx *ctx, const std::vector<FOp> &fops, bool host_momenta
     // chained force launches overlap the next one's launch with the previous one's tail
     // (programmatic dependent launch; every access waits for the previous launch)
     const bool pdl = !ctx->prof;
-    if (ctx->link64)
+    if (paired)
+      SU2B_LAUNCH(SU2B_K_FORCE, force_pair(ctx->g, cur, (float *)ctx->P, f, -o.cm, mode,
+                                           ctx->part_slot(2), &nb, out, o.cg, s, pdl));
+    else if (ctx->link64)
       SU2B_LAUNCH(SU2B_K_FORCE,
                   force_update<double>(ctx->g, cur, 0, (double *)ctx->P, nullptr, f, -o.cm,
                                        ctx->xi, mode, ctx->part_slot(2), &nb, out, o.cg, s,

@@ -40,8 +40,21 @@ enum ForceMode : int {
 // launch shapes of the SU(2) force kernel (threads per block, minimum resident blocks per
 // SM, which caps registers): one thread per site 0 (256,4) 1 (128,8) 2 (128,4) 3 (128,6)
 // 4 (256,2) 5 (256,3) 7 (64,16); two threads per site 6 split, 8 xsplit, both (128,8), and
-// 10 split (128,5) (96 registers: FP64 links); 9 one thread per link
-constexpr int FORCE_VARIANTS = 11;
+// 10 split (128,5) (96 registers: FP64 links); 9 one thread per link; 11 site pairs in packed
+// FP32 (FP32 links, d = 4, T a multiple of 4: the fused trajectory runs force_pair on a paired
+// copy of the field; every other caller, and FP64 links, run the one-thread-per-link kernel,
+// whose arithmetic force_pair reproduces lane for lane)
+constexpr int FORCE_VARIANTS = 12;
+constexpr int FORCE_PAIR = 11;
+constexpr int PAIR_MINB = 8;  // resident blocks of 128 threads per SM of force_pair
+// site pairs (pairs.cu): whether a geometry takes them (d = 4, T % 4 == 0, the whole
+// lattice); the standard layout of U copied into the paired layout Upl; the fused force step
+// of FP32 links on paired buffers (Uout paired for FM_UPDATE, standard for FM_RESTORE)
+bool pairs_apply(const Geom &g);
+cudaError_t to_pairs(const Geom &g, const void *U, void *Upl, cudaStream_t s);
+cudaError_t force_pair(const Geom &g, const void *Upl, float *P, double f, double scale, int mode,
+                       double *kin_part, int *nblocks, void *Uout, double dt_upd, cudaStream_t s,
+                       bool pdl);
 template <class T>
 cudaError_t force_update(const Geom &g, const void *U, int group, T *P, const T *extra, double f,
                          double scale, double xi, int mode, double *kin_part, int *nblocks,

@@ -518,3 +518,30 @@ def test_autotune_cache(gpu, orc, tmp_path):
         c.force_variant = (best + 1) % gpu._abi.FORCE_VARIANTS
         t2 = c.autotune(path)  # cached: no measurement
         assert all(v < 0 for v in t2.values()) and c.force_variant == best
+
+
+@pytest.mark.parametrize("dims", [(8, 8, 8, 8), (4, 6, 8, 12), (6, 6, 6, 4), (4, 4, 6, 6)],
+                         ids=["8^4", "4x6x8x12", "6^3x4", "4x4x6x6-no-pairs"])
+def test_site_pairs_equal_the_link_kernel(gpu, orc, dims):
+    """The trajectory on site pairs (force shape 11: the field copied into the paired layout,
+    packed FP32 FFMA2 on both sites of a pair, the final field written back) gives the
+    one-thread-per-link kernel's links bit for bit, and its accept decisions; the energies
+    agree to the rounding of the kinetic sum's order.  With T not a multiple of 4 shape 11
+    runs the one-thread-per-link kernel itself."""
+    group, nd = 0, 4
+    U = hot(orc, group, dims, nd)
+    with make(gpu, group, dims, nd, beta=2.3, precision="mixed") as a, \
+            make(gpu, group, dims, nd, beta=2.3, precision="mixed") as b:
+        a.force_variant = 9
+        b.force_variant = 11
+        a.upload(U)
+        b.upload(U)
+        for k in range(6):
+            kw = dict(seed=4, traj=k, accept_reject=k % 2 == 1, uniform=0.999999)
+            n, tau = (3, 1.0) if k % 2 == 0 else (1, 2.0)
+            ra = a.md_update("omf2", n, tau, **kw)
+            rb = b.md_update("omf2", n, tau, **kw)
+            assert ra.accepted == rb.accepted, k
+            scale = sum(abs(h) for h in ra.H_old + ra.H_new)
+            assert ra.dH == pytest.approx(rb.dH, abs=1e-13 * scale + 1e-9), k
+            assert np.array_equal(a.download(), b.download()), k
