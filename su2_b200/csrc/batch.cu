@@ -151,8 +151,9 @@ __global__ void __launch_bounds__(NT)
 
 // the start of a batched trajectory in one pass, as in the single-lattice path: each
 // site's Philox momenta with their |P|^2 and its start plaquettes; per tile the partials
-// {sum |P|^2, plaquettes, spatial plaquettes}
-template <class T, int NT>
+// {sum |P|^2, plaquettes, spatial plaquettes}.  Without PLAQ the momenta only (the start
+// plaquettes are carried over from the previous trajectory; the plaquette partials are 0)
+template <class T, int NT, bool PLAQ>
 __global__ void __launch_bounds__(NT)
   k_batch_momenta_plaq(const ChainDev *__restrict__ ch, int nchains, int ntiles, Bufs<T> bufs,
                        const int *__restrict__ cur, T *__restrict__ Pall,
@@ -178,12 +179,14 @@ __global__ void __launch_bounds__(NT)
         P[2 * NL + l] = cc;
         v[0] += (double)a * a + (double)b * b + (double)cc * cc;
       }
-      const LinkT<T> *U = bufs.at(cur[c] % 3) + d.off_link;
-      double wsum = 0.;
-      if (d.g.nd == 4)
-        plaq_site<T, 4>(d.g, U, p, cb, 1.0, v[1], v[2], wsum);
-      else
-        plaq_site<T, 3>(d.g, U, p, cb, 1.0, v[1], v[2], wsum);
+      if (PLAQ) {
+        const LinkT<T> *U = bufs.at(cur[c] % 3) + d.off_link;
+        double wsum = 0.;
+        if (d.g.nd == 4)
+          plaq_site<T, 4>(d.g, U, p, cb, 1.0, v[1], v[2], wsum);
+        else
+          plaq_site<T, 3>(d.g, U, p, cb, 1.0, v[1], v[2], wsum);
+      }
     }
     block_sums<NT, 3>(v, shk);
     if (threadIdx.x == 0) {
@@ -197,7 +200,12 @@ __global__ void __launch_bounds__(NT)
 // the closing reductions and the accept/reject of every chain in one launch, one block per
 // chain: the start partials (3 per tile) into red[0..2], the final kinetic partials into
 // red[4], the end plaquette partials (3 per tile, the third unused) into red[5..7], each in
-// a fixed order; then the chain's accept step (accept_chain) on thread 0
+// a fixed order; then the chain's accept step (accept_chain) on thread 0.
+// cached: the start pass summed no plaquettes; the chain's start field is the previous
+// trajectory's result, whose plaquette sums are still in red -- red[5..6] if that
+// trajectory was accepted (out[c].accepted, not yet overwritten), else red[1..2].  The end
+// pass and the start pass add the same per-tile partials in the same order, so the carried
+// sums equal recomputed ones bit for bit.
 __device__ __forceinline__ void accept_chain(const ChainDev &d, const double *r,
                                              const uint32_t *__restrict__ traj, int rel_final,
                                              int *cur_c, TrajDev *out) {
@@ -228,7 +236,7 @@ __global__ void __launch_bounds__(256)
   k_batch_reduce_accept(const ChainDev *__restrict__ ch, const double *__restrict__ ps,
                         const double *__restrict__ pk, const double *__restrict__ pe,
                         double *red, const uint32_t *__restrict__ traj, int rel_final, int *cur,
-                        TrajDev *out) {
+                        TrajDev *out, int cached) {
   __shared__ double shk[7 * 8];
   const int c = blockIdx.x;
   const ChainDev &d = ch[c];
@@ -244,6 +252,11 @@ __global__ void __launch_bounds__(256)
   block_sums<256, 7>(v, shk);
   if (threadIdx.x == 0) {
     double *r = red + c * RS;
+    if (cached) {
+      const bool acc = out[c].accepted;
+      v[1] = acc ? r[5] : r[1];
+      v[2] = acc ? r[6] : r[2];
+    }
     r[0] = v[0];
     r[1] = v[1];
     r[2] = v[2];
@@ -286,6 +299,9 @@ struct su2b_batch {
   std::vector<void *> allocs;
   std::string err;
   long launches = 0;
+  // set by a batched trajectory: red holds every chain's start and end plaquette sums, so
+  // the next trajectory takes its start plaquettes from there; an upload or a retune clears it
+  bool carry = false;
 };
 
 static int bfail(su2b_batch *b, int code, const char *fmt, ...) {
@@ -456,7 +472,9 @@ static int chain_transfer(su2b_batch *b, int chain, double *host, bool up) {
 }
 
 extern "C" int su2b_batch_upload(su2b_batch *b, int chain, const double *U_host) {
-  return b ? chain_transfer(b, chain, const_cast<double *>(U_host), true) : SU2B_ERR_INVALID;
+  if (!b) return SU2B_ERR_INVALID;
+  b->carry = false;  // a new field: its plaquettes are summed afresh
+  return chain_transfer(b, chain, const_cast<double *>(U_host), true);
 }
 extern "C" int su2b_batch_download(su2b_batch *b, int chain, double *U_host) {
   return b ? chain_transfer(b, chain, U_host, false) : SU2B_ERR_INVALID;
@@ -522,8 +540,10 @@ template <int NT> int grid_for(const void *kernel, int ntiles) {
   return std::max(1, std::min(ntiles, std::max(1, per_sm) * sms));
 }
 
+// queues one batched trajectory; *nl receives the number of kernels queued
 template <class T, int NT, int MINB>
-int enqueue_batch_v(su2b_batch *b, const std::vector<BOp> &ops, int *rel_final) {
+int enqueue_batch_v(su2b_batch *b, const std::vector<BOp> &ops, int *rel_final, bool cached,
+                    long *nl_out) {
   cudaStream_t s = b->stream;
   const int v = b->variant;
   const ChainDev *ch = b->ch[v];
@@ -531,14 +551,19 @@ int enqueue_batch_v(su2b_batch *b, const std::vector<BOp> &ops, int *rel_final) 
   Bufs<T> bufs{{(LinkT<T> *)b->buf[0], (LinkT<T> *)b->buf[1], (LinkT<T> *)b->buf[2]}};
   T *P = (T *)b->P;
   const int gF = grid_for<NT>((const void *)k_batch_force<T, NT, MINB>, ntiles);
-  const int gM = grid_for<NT>((const void *)k_batch_momenta_plaq<T, NT>, ntiles);
+  const int gM = grid_for<NT>((const void *)k_batch_momenta_plaq<T, NT, true>, ntiles);
   const int gP = grid_for<NT>((const void *)k_batch_plaq<T, NT>, ntiles);
   // partial sums: the start pass, the final kinetic energy and the end plaquettes in three
   // regions, all reduced by the closing accept launch
   double *ps = b->part, *pk = b->part + 3 * (size_t)b->maxtiles,
          *pe = b->part + 4 * (size_t)b->maxtiles;
   long nl = 0;
-  k_batch_momenta_plaq<T, NT><<<gM, NT, 0, s>>>(ch, b->n, ntiles, bufs, b->cur, P, b->traj, ps);
+  if (cached)
+    k_batch_momenta_plaq<T, NT, false><<<gM, NT, 0, s>>>(ch, b->n, ntiles, bufs, b->cur, P,
+                                                         b->traj, ps);
+  else
+    k_batch_momenta_plaq<T, NT, true><<<gM, NT, 0, s>>>(ch, b->n, ntiles, bufs, b->cur, P,
+                                                        b->traj, ps);
   nl += 1;
   int cur = 0;
   auto next = [](int c) { return c == 1 ? 2 : 1; };
@@ -562,22 +587,24 @@ int enqueue_batch_v(su2b_batch *b, const std::vector<BOp> &ops, int *rel_final) 
   if (fin < 0) return bfail(b, SU2B_ERR_UNSUPPORTED, "schedule must end with a momentum step");
   k_batch_plaq<T, NT><<<gP, NT, 0, s>>>(ch, b->n, ntiles, bufs, b->cur, fin, pe);
   k_batch_reduce_accept<<<b->n, 256, 0, s>>>(ch, ps, pk, pe, b->red, b->traj, fin, b->cur,
-                                             b->res);
+                                             b->res, (int)cached);
   nl += 2;
   BCK(cudaGetLastError());
   BCK(cudaMemcpyAsync(b->h_res, b->res, sizeof(TrajDev) * b->n, cudaMemcpyDeviceToHost, s));
   BCK(cudaMemcpyAsync(b->h_red, b->red, sizeof(double) * RS * b->n, cudaMemcpyDeviceToHost, s));
   *rel_final = fin;
-  return (int)nl;
+  *nl_out = nl;
+  return SU2B_OK;
 }
 
 template <class T>
-int enqueue_batch(su2b_batch *b, const std::vector<BOp> &ops, int *rel_final) {
+int enqueue_batch(su2b_batch *b, const std::vector<BOp> &ops, int *rel_final, bool cached,
+                  long *nl) {
   switch (b->variant) {
-    case 0: return enqueue_batch_v<T, 64, 8>(b, ops, rel_final);
-    case 1: return enqueue_batch_v<T, 128, 4>(b, ops, rel_final);
-    case 2: return enqueue_batch_v<T, 128, 6>(b, ops, rel_final);
-    default: return enqueue_batch_v<T, 256, 3>(b, ops, rel_final);
+    case 0: return enqueue_batch_v<T, 64, 8>(b, ops, rel_final, cached, nl);
+    case 1: return enqueue_batch_v<T, 128, 4>(b, ops, rel_final, cached, nl);
+    case 2: return enqueue_batch_v<T, 128, 6>(b, ops, rel_final, cached, nl);
+    default: return enqueue_batch_v<T, 256, 3>(b, ops, rel_final, cached, nl);
   }
 }
 
@@ -642,8 +669,11 @@ extern "C" int su2b_batch_hmc(su2b_batch *b, int integrator, int n_steps, double
     return bfail(b, SU2B_ERR_UNSUPPORTED, "batched trajectories support leapfrog and omf2");
   *b->h_traj = traj;
   BCK(cudaMemcpyAsync(b->traj, b->h_traj, sizeof(uint32_t), cudaMemcpyHostToDevice, b->stream));
+  const bool cached = b->carry;
+  b->carry = false;  // set again only by a trajectory that completes
   char key[128];
-  snprintf(key, sizeof key, "%d/%d/%.17g/v%d", integrator, n_steps, tau, b->variant);
+  snprintf(key, sizeof key, "%d/%d/%.17g/v%d/%d", integrator, n_steps, tau, b->variant,
+           (int)cached);
   cudaGraphExec_t exec = nullptr;
   long kernels = 0;
   for (auto &g : b->graphs)
@@ -655,12 +685,13 @@ extern "C" int su2b_batch_hmc(su2b_batch *b, int integrator, int n_steps, double
     cudaGraph_t graph = nullptr;
     BCK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
     int rel = 0;
-    const int nl =
-      b->link64 ? enqueue_batch<double>(b, ops, &rel) : enqueue_batch<float>(b, ops, &rel);
+    long nl = 0;
+    const int rc = b->link64 ? enqueue_batch<double>(b, ops, &rel, cached, &nl)
+                             : enqueue_batch<float>(b, ops, &rel, cached, &nl);
     const cudaError_t ec = cudaStreamEndCapture(b->stream, &graph);
-    if (nl < 0) {
+    if (rc != SU2B_OK) {
       if (graph) cudaGraphDestroy(graph);
-      return nl;
+      return rc;
     }
     BCK(ec);
     const cudaError_t ei = cudaGraphInstantiate(&exec, graph, 0);
@@ -672,6 +703,7 @@ extern "C" int su2b_batch_hmc(su2b_batch *b, int integrator, int n_steps, double
   BCK(cudaGraphLaunch(exec, b->stream));
   BCK(cudaStreamSynchronize(b->stream));
   b->launches += kernels;
+  b->carry = true;
   for (int c = 0; c < b->n; c++) {
     const TrajDev &t = b->h_res[c];
     su2b_traj_result &r = results[c];
@@ -691,6 +723,8 @@ extern "C" int su2b_batch_hmc(su2b_batch *b, int integrator, int n_steps, double
 extern "C" int su2b_batch_autotune(su2b_batch *b, double *times_us) {
   if (!b) return SU2B_ERR_INVALID;
   b->err.clear();
+  b->carry = false;  // the tile tables change with the launch shape, and with them the order
+                     // in which the carried plaquette sums were added
   BCK(cudaSetDevice(b->device));
   double t[SU2B_BATCH_VARIANTS], fastest = 0.;
   for (int v = 0; v < SU2B_BATCH_VARIANTS; v++) {
@@ -718,6 +752,7 @@ extern "C" int su2b_batch_tune_set(su2b_batch *b, int variant) {
   if (!b) return SU2B_ERR_INVALID;
   if (variant < 0 || variant >= SU2B_BATCH_VARIANTS)
     return bfail(b, SU2B_ERR_INVALID, "batch launch shape %d out of range", variant);
+  if (variant != b->variant) b->carry = false;
   b->variant = variant;
   return SU2B_OK;
 }

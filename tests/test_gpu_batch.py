@@ -84,3 +84,37 @@ def test_batch_autotune_leaves_fields_and_every_shape_agrees(gpu, orc):
                 assert a.dH == pytest.approx(b_.dH, abs=1e-8)
         for a, b_ in zip(ref_U, Us):
             assert np.array_equal(a, b_)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_batch_carries_start_plaquettes(gpu, orc, precision):
+    """Consecutive batched trajectories take each chain's start plaquettes from the previous
+    trajectory's sums (its end field if accepted, else its start field) instead of summing
+    them again.  A batch that re-uploads its own fields before every trajectory (which drops
+    the carry-over) evolves the same: the same accept decisions, Delta H and plaquettes bit
+    for bit, the same links."""
+    from su2_b200.batch import chain_batch
+    starts = [orc.hotstart(0, c["dims"], c["ndims"], 200 + i, 1.0, 654321)
+              for i, c in enumerate(CHAINS)]
+    runs = []
+    for reupload in (False, True):
+        with chain_batch(CHAINS, precision=precision) as b:
+            for i, U in enumerate(starts):
+                b.upload(i, U)
+            res = []
+            for t in range(8):
+                if reupload:
+                    for i in range(len(CHAINS)):
+                        b.upload(i, b.download(i))
+                # fine and coarse trajectories: accepted and rejected ones
+                n, tau = (10, 1.0) if t % 2 == 0 else (2, 2.0)
+                res.append(b.md_update("leapfrog", n, tau, traj=t))
+            runs.append((res, [b.download(i) for i in range(len(CHAINS))]))
+    (a, Ua), (b_, Ub) = runs
+    acc = [r.accepted for rs in a for r in rs]
+    assert any(acc) and not all(acc)
+    for ra, rb in zip(a, b_):
+        for x, y in zip(ra, rb):
+            assert x.accepted == y.accepted and x.dH == y.dH and x.plaquette == y.plaquette
+    for u, v in zip(Ua, Ub):
+        assert np.array_equal(u, v)
