@@ -303,7 +303,10 @@ SU2B_API int su2b_slabs_gradient_flow(su2b_slabs *h, double tmax, double eps, do
                                       double *rows, int max_rows, int *n_rows);
 /* gauge_energy of the whole lattice (as su2b_gauge_energy) */
 SU2B_API int su2b_slabs_gauge_energy(su2b_slabs *h, int spatial_only, double *out);
-/* su2b_autotune on the first slab; every slab takes its choice */
+/* su2b_autotune on the first slab of the handle; every slab takes its choice.  Slabs in
+ * separate processes (a collective call: every rank calls it) reduce each shape's time to its
+ * maximum over the ranks and choose from those, so every rank runs the same shape; times_us
+ * (SU2B_FORCE_VARIANTS entries, may be NULL) receives the times the choice was made from. */
 SU2B_API int su2b_slabs_autotune(su2b_slabs *h, double *times_us);
 SU2B_API int su2b_slabs_tune_get(su2b_slabs *h, int *variant);
 SU2B_API int su2b_slabs_tune_set(su2b_slabs *h, int variant);

@@ -149,6 +149,7 @@ struct su2b_slabs {
   ncclComm_t comm = nullptr;
   int nranks = 1, rank = 0;
   uint4 *sendbuf = nullptr, *recvbuf = nullptr;  // [lower face | upper face]
+  double *tune_dev = nullptr;  // the tuner's times per force shape, reduced over the ranks
   Piece *pack[3] = {}, *unpack[3] = {};
   std::vector<void *> allocs;
   struct Graph {
@@ -651,6 +652,10 @@ extern "C" int su2b_slabs_connect(su2b_slabs *h, const void *id, int nranks, int
   h->allocs.push_back(b);
   h->sendbuf = (uint4 *)a;
   h->recvbuf = (uint4 *)b;
+  void *t = nullptr;
+  SLAB_CUDA(cudaMalloc(&t, sizeof(double) * FORCE_VARIANTS));
+  h->allocs.push_back(t);
+  h->tune_dev = (double *)t;
   return build_nccl_tables(h);
 }
 
@@ -933,12 +938,33 @@ extern "C" int su2b_slabs_gradient_flow(su2b_slabs *h, double tmax, double eps, 
   return SU2B_OK;
 }
 
+// The first slab of the handle times the shapes.  Slabs in separate processes take the
+// maximum of each shape's time over the ranks (a step waits for the slowest slab) and apply
+// the tuner's rule to it, so every rank runs the same shape.
 extern "C" int su2b_slabs_autotune(su2b_slabs *h, double *times_us) {
   if (!h) return SU2B_ERR_INVALID;
   h->err.clear();
-  const int rc = su2b_autotune(h->sl[0], nullptr, 1, times_us);
+  if (!connected(h))
+    return fail(h, SU2B_ERR_INVALID,
+                "the handle holds a part of the slabs: connect it to the others first");
+  double t[FORCE_VARIANTS] = {};
+  const int rc = su2b_autotune(h->sl[0], nullptr, 1, t);
   if (rc != SU2B_OK) return from_ctx(h, rc);
+  if (h->comm) {
+    SLAB_CUDA(cudaMemcpyAsync(h->tune_dev, t, sizeof t, cudaMemcpyHostToDevice, h->s));
+    NCCL_CK(h->nc->all_reduce(h->tune_dev, h->tune_dev, FORCE_VARIANTS, ncclFloat64, ncclMax,
+                              h->comm, h->s));
+    SLAB_CUDA(cudaMemcpyAsync(t, h->tune_dev, sizeof t, cudaMemcpyDeviceToHost, h->s));
+    SLAB_CUDA(cudaStreamSynchronize(h->s));
+    double fastest = t[0];
+    for (int v = 1; v < FORCE_VARIANTS; v++) fastest = t[v] < fastest ? t[v] : fastest;
+    int best = 0;
+    while (t[best] > 1.01 * fastest) best++;
+    h->sl[0]->tune_force = best;
+  }
   for (su2b_ctx *c : h->sl) c->tune_force = h->sl[0]->tune_force;
+  if (times_us)
+    for (int v = 0; v < FORCE_VARIANTS; v++) times_us[v] = t[v];
   return SU2B_OK;
 }
 

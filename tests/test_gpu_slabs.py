@@ -192,6 +192,32 @@ def test_part_of_the_slabs(gpu, orc):
         assert e.value.code == gpu._abi.ERR_INVALID
         with pytest.raises(gpu.Su2bError):
             s.gauge_energy()
+        with pytest.raises(gpu.Su2bError) as e:
+            s.autotune()
+        assert e.value.code == gpu._abi.ERR_INVALID
+
+
+def test_slab_autotune_picks_one_shape_for_every_slab(gpu, orc):
+    """The slab tuner times every force shape on the first slab, applies the single-lattice
+    rule (the first shape within 1 % of the fastest) and sets it on every slab; the chain in
+    that shape is the single lattice's in the same shape."""
+    dims, nd = (8, 8, 8, 8), 4
+    U = hot(orc, dims, nd)
+    with slabs(dims, nd, 2, "mixed") as s:
+        s.upload(U)
+        t = s.autotune()
+        assert np.all(t > 0)
+        fastest = t.min()
+        v = s.tune_get()
+        assert v == min(k for k in range(len(t)) if t[k] <= 1.01 * fastest)
+        assert np.array_equal(s.download(), U.astype(np.float32).astype(np.float64))
+        got = chain(s, 2, "omf2", 4, 1.0, seed=9)
+        Us = s.download()
+    with single(gpu, dims, nd, "mixed") as c:
+        c.upload(U)
+        c.force_variant = v
+        same_chain(chain(c, 2, "omf2", 4, 1.0, seed=9), got)
+        assert np.array_equal(c.download(), Us)
 
 
 def test_slab_errors(gpu, orc):
