@@ -536,7 +536,8 @@ extern "C" int su2b_slabs_create(int Lx, int Ly, int Lz, int Lt, int ndims, doub
   if (ndims < 2 || ndims > 4 || nslabs < 1 || count < 1 || first < 0 ||
       first + count > nslabs)
     return SU2B_ERR_INVALID;
-  if (Lt % nslabs != 0 || (Lt / nslabs) % 2 != 0) return SU2B_ERR_INVALID;
+  // slabs of an even, positive number of slices (Lt = 0 would leave no slice to wrap to)
+  if (Lt < 2 || Lt % nslabs != 0 || (Lt / nslabs) % 2 != 0) return SU2B_ERR_INVALID;
   su2b_slabs *h = new su2b_slabs();
   h->nslabs = nslabs;
   h->first = first;

@@ -27,10 +27,10 @@ NCCL_ID_BYTES = 128
 
 def slab_bounds(Lt: int, nslabs: int, slab: int) -> tuple[int, int]:
     """The time slices [t0, t1) of one slab; raises where su2b_slabs_create returns
-    SU2B_ERR_INVALID (Lt not a multiple of nslabs, or an odd slab thickness)."""
+    SU2B_ERR_INVALID (Lt below 2 or not a multiple of nslabs, or an odd slab thickness)."""
     if nslabs < 1 or not 0 <= slab < nslabs:
         raise ValueError(f"bad slab {slab} of {nslabs}")
-    if Lt % nslabs or (Lt // nslabs) % 2:
+    if Lt < 2 or Lt % nslabs or (Lt // nslabs) % 2:
         raise ValueError(f"Lt = {Lt} does not split into {nslabs} slabs of an even thickness")
     tl = Lt // nslabs
     return slab * tl, (slab + 1) * tl

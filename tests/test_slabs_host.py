@@ -17,10 +17,25 @@ def test_slab_bounds_cover_the_lattice_once(Lt, n):
     assert all((t1 - t0) % 2 == 0 and t1 > t0 for t0, t1 in b)
 
 
-@pytest.mark.parametrize("Lt,n,r", [(8, 3, 0), (8, 8, 0), (8, 16, 0), (8, 2, 2), (8, 0, 0)])
+@pytest.mark.parametrize("Lt,n,r", [(8, 3, 0), (8, 8, 0), (8, 16, 0), (8, 2, 2), (8, 0, 0),
+                                    (0, 1, 0), (-4, 2, 0)])
 def test_slab_bounds_reject_what_the_library_rejects(Lt, n, r):
     with pytest.raises(ValueError):
         slabs.slab_bounds(Lt, n, r)
+
+
+@pytest.mark.parametrize("Lt,n,first,count", [(8, 3, 0, 3), (8, 8, 0, 8), (0, 1, 0, 1),
+                                              (-4, 2, 0, 2), (8, 2, 1, 2), (8, 0, 0, 1)])
+def test_slabs_create_refuses_before_touching_a_device(Lt, n, first, count):
+    """su2b_slabs_create checks the decomposition before any CUDA call, so these run on a
+    machine without a GPU."""
+    import ctypes as C
+    from su2_b200 import _abi
+    lib = _abi.load()
+    h = C.c_void_p()
+    rc = lib.su2b_slabs_create(4, 4, 4, Lt, 4, 2.3, 1.0, _abi.PREC_FP64, n, first, count, 0,
+                               C.byref(h))
+    assert rc == _abi.ERR_INVALID and not h.value
 
 
 class _Handle:
