@@ -107,3 +107,24 @@ def test_noalloc_rejects_bad_sizes_before_touching_a_device():
     assert f(2, 8, 8, 8, 8, 4, p, p, None) == _abi.ERR_INVALID
     assert f(0, 8, 8, 8, 8, 5, p, p, None) == _abi.ERR_INVALID
     assert f(0, 8, 8, 2, 8, 3, p, p, None) == _abi.ERR_INVALID             # inactive Lz != 1
+
+
+def test_every_handle_entry_point_refuses_a_null_handle():
+    """Each entry point whose first argument is a context, batch or slab handle returns
+    SU2B_ERR_INVALID for a NULL handle (zero or NULL for the other arguments) before it
+    touches a device; the last_error accessors name the missing handle."""
+    from su2_b200 import _abi
+    lib = _abi.load()
+    checked = 0
+    for name, (res, args) in _abi.SIGNATURES.items():
+        if not args or args[0] is not _abi._P:
+            continue
+        vals = [0 if a in (ctypes.c_int, ctypes.c_uint32, ctypes.c_uint64, ctypes.c_long)
+                else 0.0 if a is ctypes.c_double else None for a in args]
+        r = getattr(lib, name)(*vals)
+        if name.endswith("last_error"):
+            assert r.startswith(b"null"), name
+        else:
+            assert r == _abi.ERR_INVALID, name
+        checked += 1
+    assert checked > 60
