@@ -1197,7 +1197,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--therm-sweeps", type=int, default=300)
-    ap.add_argument("--stat-traj", type=int, default=1000,
+    ap.add_argument("--stat-traj", type=int, default=5000,
                     help="untimed trajectories per precision for the Delta H / plaquette "
                          "comparison")
     ap.add_argument("--pairs", type=int, default=32,
