@@ -353,3 +353,37 @@ def test_slab_connect_refusals(gpu):
             with pytest.raises(gpu.Su2bError) as e:
                 s.connect(uid, nranks, rank)
             assert e.value.code == gpu._abi.ERR_INVALID
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_nccl_transport_with_one_rank(gpu, orc, precision):
+    """One slab holding the whole lattice, connected through NCCL to itself: each face goes
+    out through the pack table, ncclSend / ncclRecv (the slabs above and below are the rank
+    itself) and the unpack table, the sums through ncclAllReduce, and the boundary slices'
+    exchange overlaps the interior update on its own stream.  Trajectories, sweeps, flow
+    steps, the energy density and the flow records are the single lattice's."""
+    from su2_b200.slabs import nccl_unique_id
+    dims, nd = (8, 8, 8, 8), 4
+    U = hot(orc, dims, nd)
+    with single(gpu, dims, nd, precision) as c, \
+            slabs(dims, nd, 1, precision, first=0, count=1) as s:
+        s.connect(nccl_unique_id(), 1, 0)
+        assert s.overlap
+        c.upload(U)
+        s.upload(U)
+        same_chain(chain(c, 4), chain(s, 4))
+        assert np.array_equal(c.download(), s.download())
+        for k in range(2):
+            assert np.array_equal(c.sweep(0.3, 4, 9, k), s.sweep(0.3, 4, 9, k))
+        assert np.array_equal(c.download(), s.download())
+        for _ in range(2):
+            c.runge_kutta(0.02)
+            s.runge_kutta(0.02)
+        assert np.array_equal(c.download(), s.download())
+        assert s.gauge_energy() == pytest.approx(c.gauge_energy(), rel=1e-12)
+        ref, got = c.energy_density(), s.energy_density()
+        assert got[0] == pytest.approx(ref[0], rel=1e-12)
+        rc, rs = c.gradient_flow(0.1, 0.02), s.gradient_flow(0.1, 0.02)
+        assert rc.shape == rs.shape
+        np.testing.assert_allclose(rs[:, 1:8], rc[:, 1:8], rtol=1e-11, atol=1e-13)
+        assert np.array_equal(c.download(), s.download())
