@@ -148,7 +148,9 @@ def dist_setup():
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     dist = None
-    if ws > 1:
+    # a process group whenever torchrun launched the run, one rank included, so that the
+    # collective code of an N-GPU run is the code a one-GPU torchrun executes
+    if ws > 1 or "TORCHELASTIC_RUN_ID" in os.environ:
         import datetime
 
         import torch
@@ -594,7 +596,7 @@ def slabs_run(args):
     ws, rank, local, dist = dist_setup()
     torch.cuda.set_device(local)
     K, W, N = args.steps, args.warmup, args.slabs
-    if ws > 1 and N != ws:
+    if dist is not None and N != ws:
         raise SystemExit(f"--slabs {N} under {ws} ranks: one slab per rank (N = world size)")
     NL = L ** 4 * 4
     seed = 20240
@@ -620,7 +622,7 @@ def slabs_run(args):
         dist.broadcast(t, 0)
         dist.broadcast(v, 0)
         U_th, variant = t.cpu().numpy(), int(v.item())
-    if ws > 1:
+    if dist is not None:
         lat = slab_lattice((L, L, L, L), 4, BETA, N, precision="mixed", first=rank, count=1,
                            device=local)
         connect_process_group(lat, dist)
@@ -1221,6 +1223,9 @@ def main():
         slabs_run(args)
     elif args.impl == "ours" and args.config != 2:
         {1: config1, 3: config3, 4: config4, 5: config5}[args.config](args)
+        import torch.distributed as dist
+        if dist.is_available() and dist.is_initialized():
+            dist.destroy_process_group()
     elif args.impl == "reference":
         reference(args)
     else:
