@@ -644,7 +644,6 @@ extern "C" int su2b_slabs_connect(su2b_slabs *h, const void *id, int nranks, int
   h->comm = comm;
   h->nranks = nranks;
   h->rank = rank;
-  h->overlap = true;  // the faces cross NVLink while the interior slices are updated
   const size_t bytes = (size_t)4 * h->nd * h->piece_n * 16;  // two faces
   void *a = nullptr, *b = nullptr;
   SLAB_CUDA(cudaMalloc(&a, bytes));

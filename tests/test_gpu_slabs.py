@@ -355,20 +355,22 @@ def test_slab_connect_refusals(gpu):
             assert e.value.code == gpu._abi.ERR_INVALID
 
 
+@pytest.mark.parametrize("overlap", [False, True], ids=["plain", "overlapped"])
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
-def test_nccl_transport_with_one_rank(gpu, orc, precision):
+def test_nccl_transport_with_one_rank(gpu, orc, precision, overlap):
     """One slab holding the whole lattice, connected through NCCL to itself: each face goes
     out through the pack table, ncclSend / ncclRecv (the slabs above and below are the rank
-    itself) and the unpack table, the sums through ncclAllReduce, and the boundary slices'
-    exchange overlaps the interior update on its own stream.  Trajectories, sweeps, flow
-    steps, the energy density and the flow records are the single lattice's."""
+    itself) and the unpack table, the sums through ncclAllReduce; overlapped, the boundary
+    slices' exchange runs on its own stream while the interior is updated.  Trajectories,
+    sweeps, flow steps, the energy density and the flow records are the single lattice's."""
     from su2_b200.slabs import nccl_unique_id
     dims, nd = (8, 8, 8, 8), 4
     U = hot(orc, dims, nd)
     with single(gpu, dims, nd, precision) as c, \
             slabs(dims, nd, 1, precision, first=0, count=1) as s:
         s.connect(nccl_unique_id(), 1, 0)
-        assert s.overlap
+        assert not s.overlap  # the plain exchange unless asked for
+        s.overlap = overlap
         c.upload(U)
         s.upload(U)
         same_chain(chain(c, 4), chain(s, 4))
