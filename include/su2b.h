@@ -310,11 +310,12 @@ SU2B_API int su2b_slabs_gauge_energy(su2b_slabs *h, int spatial_only, double *ou
 SU2B_API int su2b_slabs_autotune(su2b_slabs *h, double *times_us);
 SU2B_API int su2b_slabs_tune_get(su2b_slabs *h, int *variant);
 SU2B_API int su2b_slabs_tune_set(su2b_slabs *h, int variant);
-/* Overlap (off by default): each force step updates the two boundary slices of every slab
- * first, exchanges their faces on a second stream while the interior slices are updated, and
- * the next step waits for the exchange.  Slabs of fewer than four slices run without it.  The
- * results are the same either way; on one B200 the split launches cost more than the exchange
- * they hide, with device copies and with NCCL alike. */
+/* Overlap (on by default after su2b_slabs_connect, off for slabs on one device): each force
+ * step updates the two boundary slices of every slab first, exchanges their faces on a second
+ * stream of the highest priority while the interior slices are updated, and the next step
+ * waits for the exchange.  Slabs of fewer than four slices run without it.  The results are
+ * the same either way; the split launches pay off against NCCL's latency, not against a
+ * device copy. */
 SU2B_API int su2b_slabs_set_overlap(su2b_slabs *h, int on);
 SU2B_API int su2b_slabs_get_overlap(const su2b_slabs *h, int *on);
 SU2B_API int su2b_slabs_kernel_launches(su2b_slabs *h, long *count);

