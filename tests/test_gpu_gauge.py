@@ -545,3 +545,39 @@ def test_site_pairs_equal_the_link_kernel(gpu, orc, dims):
             scale = sum(abs(h) for h in ra.H_old + ra.H_new)
             assert ra.dH == pytest.approx(rb.dH, abs=1e-13 * scale + 1e-9), k
             assert np.array_equal(a.download(), b.download()), k
+
+
+def test_large_lattice_64_4(gpu):
+    """At 64^4 (16.8 M sites, 2.1 GB of FP64 links per buffer), through properties that hold
+    at any size: the force of a field shifted by one site in t and in z is the force of the
+    field shifted the same way, bit for bit (every site's arithmetic moves to a thread of
+    the other parity and another block, across every periodic boundary); the plaquette sum
+    is unchanged; an omf2 trajectory is reversible to rounding; and mixed precision follows
+    FP64 on the same Philox momenta."""
+    L, nd = 64, 4
+    rng = np.random.default_rng(2024)
+    q = rng.standard_normal((L ** 4 * nd, 4))
+    q /= np.linalg.norm(q, axis=1, keepdims=True)
+    U = q.reshape(-1)
+    del q
+    shape = (L, L, L, L, nd)  # host order: t, x, y, z, direction
+
+    def shift(a, comps):
+        return np.roll(np.roll(a.reshape(shape + (comps,)), 1, axis=0), 1, axis=3).reshape(-1)
+
+    Ush = shift(U, 4)
+    dH = {}
+    for precision in ("fp64", "mixed"):
+        with make(gpu, 0, (L, L, L, L), nd, beta=2.4, precision=precision) as c:
+            c.upload(U)
+            d1, e1 = c.derivative(), c.gauge_energy()
+            c.upload(Ush)
+            d2, e2 = c.derivative(), c.gauge_energy()
+            assert np.array_equal(shift(d1, 3), d2)
+            assert e2 == pytest.approx(e1, rel=1e-12)
+            c.upload(U)
+            r = c.md_update("omf2", 4, 0.2, seed=11, traj=1, revtest=True, accept_reject=False)
+            assert abs(r.ddH) < (1e-6 if precision == "fp64" else 5e-2)
+            dH[precision] = r.dH
+    # a hot start far from equilibrium: dH of about -1.9e4, FP32 arithmetic within 1e-5 of it
+    assert dH["mixed"] == pytest.approx(dH["fp64"], rel=1e-5)
