@@ -549,11 +549,12 @@ def test_site_pairs_equal_the_link_kernel(gpu, orc, dims):
 
 def test_large_lattice_64_4(gpu):
     """At 64^4 (16.8 M sites, 2.1 GB of FP64 links per buffer), through properties that hold
-    at any size: the force of a field shifted by one site in t and in z is the force of the
-    field shifted the same way, bit for bit (every site's arithmetic moves to a thread of
-    the other parity and another block, across every periodic boundary); the plaquette sum
-    is unchanged; an omf2 trajectory is reversible to rounding; and mixed precision follows
-    FP64 on the same Philox momenta."""
+    at any size: the force and one Wilson-flow step of a field shifted by one site in t and
+    in z are those of the field shifted the same way, bit for bit (every site's arithmetic
+    moves to a thread of the other parity and another block, across every periodic
+    boundary); the plaquette sum and the clover energy density are unchanged; an omf2
+    trajectory is reversible to rounding; and mixed precision follows FP64 on the same
+    Philox momenta."""
     L, nd = 64, 4
     rng = np.random.default_rng(2024)
     q = rng.standard_normal((L ** 4 * nd, 4))
@@ -570,11 +571,17 @@ def test_large_lattice_64_4(gpu):
     for precision in ("fp64", "mixed"):
         with make(gpu, 0, (L, L, L, L), nd, beta=2.4, precision=precision) as c:
             c.upload(U)
-            d1, e1 = c.derivative(), c.gauge_energy()
+            d1, e1, q1 = c.derivative(), c.gauge_energy(), c.energy_density()
+            c.runge_kutta(0.01)
+            f1 = c.download()
             c.upload(Ush)
-            d2, e2 = c.derivative(), c.gauge_energy()
+            d2, e2, q2 = c.derivative(), c.gauge_energy(), c.energy_density()
+            c.runge_kutta(0.01)
+            f2 = c.download()
             assert np.array_equal(shift(d1, 3), d2)
+            assert np.array_equal(shift(f1, 4), f2)  # one Wilson-flow step
             assert e2 == pytest.approx(e1, rel=1e-12)
+            assert q2[0] == pytest.approx(q1[0], rel=1e-12)  # clover energy density
             c.upload(U)
             r = c.md_update("omf2", 4, 0.2, seed=11, traj=1, revtest=True, accept_reject=False)
             assert abs(r.ddH) < (1e-6 if precision == "fp64" else 5e-2)
