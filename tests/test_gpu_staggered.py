@@ -169,3 +169,29 @@ def test_pion_correlator_rejects_su2(gpu):
         with pytest.raises(su2_b200.Su2bError) as e:
             c.C_pion(0.1)
         assert e.value.code == 4
+
+
+def test_operator_and_solve_at_1024_squared(gpu):
+    """U(1) d = 2 at 1024^2 (1 M sites, 16 times the workload's volume), through properties
+    that hold at any size: a shift by two sites in t and x keeps every staggered phase and
+    parity, so D, D^+ and D D^+ of the shifted field and vector are the shifted results bit
+    for bit, and the CG solution of the shifted system is the shifted solution (to the
+    solver's tolerance: its sums add in another order)."""
+    L = 1024
+    rng = np.random.default_rng(77)
+    U = rng.uniform(-np.pi, np.pi, size=L * L * 2)
+    psi = rng.normal(size=2 * L * L)
+
+    def shift(a, comps):
+        return np.roll(a.reshape(L, L, comps), (2, 2), axis=(0, 1)).reshape(-1)
+
+    with u1(gpu, (L, 1, 1, L), 2) as c:
+        out = {}
+        for key, (Ui, pi) in (("plain", (U, psi)), ("shifted", (shift(U, 2), shift(psi, 2)))):
+            c.upload(Ui)
+            r = c.solve(pi, 0.05, tol=1e-10, tol_mode="rel")
+            assert r.converged
+            out[key] = [c.apply_D(0.05, pi), c.apply_Ddag(0.05, pi), c.DDdag(0.05, pi), r.x]
+        for k in range(3):
+            assert np.array_equal(shift(out["plain"][k], 2), out["shifted"][k])
+        assert rel(out["shifted"][3], shift(out["plain"][3], 2)) < 1e-8
