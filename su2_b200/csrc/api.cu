@@ -196,7 +196,8 @@ extern "C" const char *su2b_last_error(const su2b_ctx *ctx) {
   return ctx ? ctx->err.c_str() : "null context";
 }
 extern "C" int su2b_ctx_stream(su2b_ctx *ctx, void **stream) {
-  if (!ctx || !stream) return SU2B_ERR_INVALID;
+  if (!ctx) return SU2B_ERR_INVALID;
+  if (!stream) return su2b_fail(ctx, SU2B_ERR_INVALID, "stream is NULL");
   *stream = (void *)ctx->stream;
   return SU2B_OK;
 }
@@ -263,7 +264,8 @@ extern "C" int su2b_profile_read(su2b_ctx *ctx, int kclass, long *launches, doub
   return SU2B_OK;
 }
 extern "C" int su2b_kernel_launches(su2b_ctx *ctx, long *count) {
-  if (!ctx || !count) return SU2B_ERR_INVALID;
+  if (!ctx) return SU2B_ERR_INVALID;
+  if (!count) return su2b_fail(ctx, SU2B_ERR_INVALID, "count is NULL");
   *count = ctx->launches;
   return SU2B_OK;
 }

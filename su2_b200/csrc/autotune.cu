@@ -144,7 +144,8 @@ extern "C" int su2b_autotune(su2b_ctx *ctx, const char *cache_path, int retune,
 }
 
 extern "C" int su2b_tune_get(su2b_ctx *ctx, int kernel, int *variant) {
-  if (!ctx || !variant) return SU2B_ERR_INVALID;
+  if (!ctx) return SU2B_ERR_INVALID;
+  if (!variant) return su2b_fail(ctx, SU2B_ERR_INVALID, "variant is NULL");
   if (kernel == SU2B_TUNE_FORCE)
     *variant = ctx->tune_force;
   else if (kernel == SU2B_TUNE_TRAJECTORY)

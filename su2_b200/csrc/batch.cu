@@ -433,12 +433,14 @@ extern "C" const char *su2b_batch_last_error(const su2b_batch *b) {
   return b ? b->err.c_str() : "null batch";
 }
 extern "C" int su2b_batch_stream(su2b_batch *b, void **stream) {
-  if (!b || !stream) return SU2B_ERR_INVALID;
+  if (!b) return SU2B_ERR_INVALID;
+  if (!stream) return bfail(b, SU2B_ERR_INVALID, "stream is NULL");
   *stream = (void *)b->stream;
   return SU2B_OK;
 }
 extern "C" int su2b_batch_kernel_launches(su2b_batch *b, long *count) {
-  if (!b || !count) return SU2B_ERR_INVALID;
+  if (!b) return SU2B_ERR_INVALID;
+  if (!count) return bfail(b, SU2B_ERR_INVALID, "count is NULL");
   *count = b->launches;
   return SU2B_OK;
 }
@@ -743,7 +745,8 @@ extern "C" int su2b_batch_autotune(su2b_batch *b, double *times_us) {
 }
 
 extern "C" int su2b_batch_tune_get(su2b_batch *b, int *variant) {
-  if (!b || !variant) return SU2B_ERR_INVALID;
+  if (!b) return SU2B_ERR_INVALID;
+  if (!variant) return bfail(b, SU2B_ERR_INVALID, "variant is NULL");
   *variant = b->variant;
   return SU2B_OK;
 }

@@ -977,7 +977,8 @@ extern "C" int su2b_slabs_autotune(su2b_slabs *h, double *times_us) {
 }
 
 extern "C" int su2b_slabs_tune_get(su2b_slabs *h, int *variant) {
-  if (!h || !variant) return SU2B_ERR_INVALID;
+  if (!h) return SU2B_ERR_INVALID;
+  if (!variant) return fail(h, SU2B_ERR_INVALID, "variant is NULL");
   *variant = h->sl[0]->tune_force;
   return SU2B_OK;
 }
@@ -998,19 +999,21 @@ extern "C" int su2b_slabs_set_overlap(su2b_slabs *h, int on) {
 }
 
 extern "C" int su2b_slabs_get_overlap(const su2b_slabs *h, int *on) {
-  if (!h || !on) return SU2B_ERR_INVALID;
+  if (!h || !on) return SU2B_ERR_INVALID;  // a const handle keeps no message
   *on = h->overlap ? 1 : 0;
   return SU2B_OK;
 }
 
 extern "C" int su2b_slabs_kernel_launches(su2b_slabs *h, long *count) {
-  if (!h || !count) return SU2B_ERR_INVALID;
+  if (!h) return SU2B_ERR_INVALID;
+  if (!count) return fail(h, SU2B_ERR_INVALID, "count is NULL");
   *count = ctx_launches(h) + h->launches;
   return SU2B_OK;
 }
 
 extern "C" int su2b_slabs_stream(su2b_slabs *h, void **stream) {
-  if (!h || !stream) return SU2B_ERR_INVALID;
+  if (!h) return SU2B_ERR_INVALID;
+  if (!stream) return fail(h, SU2B_ERR_INVALID, "stream is NULL");
   *stream = (void *)h->s;
   return SU2B_OK;
 }
