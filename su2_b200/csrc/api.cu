@@ -86,10 +86,13 @@ int su2b_make_geom(int Lx, int Ly, int Lz, int Lt, int nd, Geom *g, std::string 
       return 0;
     }
   }
-  const long V = (long)Lx * Ly * Lz * Lt;
-  if (V > (1l << 29)) {
-    *why = "volume above 2^29 sites";
-    return 0;
+  // the volume formed one extent at a time against the limit, so no product can wrap
+  long V = 1;
+  for (int k = 0; k < 4; k++) {
+    if (L[k] > (1l << 29) || (V *= L[k]) > (1l << 29)) {
+      *why = "volume above 2^29 sites";
+      return 0;
+    }
   }
   g->nd = nd;
   for (int k = 0; k < 4; k++) g->L[k] = L[k];

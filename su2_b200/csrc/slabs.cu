@@ -538,6 +538,11 @@ extern "C" int su2b_slabs_create(int Lx, int Ly, int Lz, int Lt, int ndims, doub
     return SU2B_ERR_INVALID;
   // slabs of an even, positive number of slices (Lt = 0 would leave no slice to wrap to)
   if (Lt < 2 || Lt % nslabs != 0 || (Lt / nslabs) % 2 != 0) return SU2B_ERR_INVALID;
+  // the whole lattice within the single lattice's 2^29 sites: the Philox keys and lex0 are
+  // global site indices (the volume formed one extent at a time, so no product can wrap)
+  long Vg = 1;
+  for (const int Lk : {Lx, Ly, Lz, Lt})
+    if (Lk < 1 || Lk > (1l << 29) || (Vg *= Lk) > (1l << 29)) return SU2B_ERR_INVALID;
   su2b_slabs *h = new su2b_slabs();
   h->nslabs = nslabs;
   h->first = first;

@@ -42,6 +42,12 @@ def test_invalid_geometry_rejected_without_device():
     assert lib.su2b_ctx_create(0, 4, 4, 4, 4, 4, 2.0, 1.0, 9, 0, ctypes.byref(ctx)) == _abi.ERR_INVALID
     assert lib.su2b_ctx_create(0, 4, 4, 4, 4, 4, 2.0, 1.0, 0, 0, None) == _abi.ERR_INVALID
     assert lib.su2b_ctx_destroy(None) == _abi.ERR_INVALID
+    # volumes above 2^29 sites, including extents whose product wraps 64 bits (65536^4 = 2^64)
+    for dims in ((1024, 1024, 1024, 2), (65536, 65536, 65536, 65536), (2 ** 30, 2, 2, 2)):
+        assert lib.su2b_ctx_create(0, *dims, 4, 2.0, 1.0, 0, 0, ctypes.byref(ctx)) == \
+            _abi.ERR_INVALID, dims
+    assert lib.su2b_ctx_create(1, 2 ** 30, 1, 1, 4, 2, 2.0, 1.0, 0, 0, ctypes.byref(ctx)) == \
+        _abi.ERR_INVALID
 
 
 def test_null_context_is_an_error():

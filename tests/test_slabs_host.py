@@ -24,16 +24,18 @@ def test_slab_bounds_reject_what_the_library_rejects(Lt, n, r):
         slabs.slab_bounds(Lt, n, r)
 
 
-@pytest.mark.parametrize("Lt,n,first,count", [(8, 3, 0, 3), (8, 8, 0, 8), (0, 1, 0, 1),
-                                              (-4, 2, 0, 2), (8, 2, 1, 2), (8, 0, 0, 1)])
-def test_slabs_create_refuses_before_touching_a_device(Lt, n, first, count):
-    """su2b_slabs_create checks the decomposition before any CUDA call, so these run on a
-    machine without a GPU."""
+@pytest.mark.parametrize("L,Lt,n,first,count", [
+    (4, 8, 3, 0, 3), (4, 8, 8, 0, 8), (4, 0, 1, 0, 1), (4, -4, 2, 0, 2), (4, 8, 2, 1, 2),
+    (4, 8, 0, 0, 1), (1024, 1024, 512, 0, 1), (65536, 65536, 2, 0, 1)])
+def test_slabs_create_refuses_before_touching_a_device(L, Lt, n, first, count):
+    """su2b_slabs_create checks the decomposition and the whole lattice's volume (at most
+    2^29 sites, also for extents whose product wraps 64 bits) before any CUDA call, so these
+    run on a machine without a GPU."""
     import ctypes as C
     from su2_b200 import _abi
     lib = _abi.load()
     h = C.c_void_p()
-    rc = lib.su2b_slabs_create(4, 4, 4, Lt, 4, 2.3, 1.0, _abi.PREC_FP64, n, first, count, 0,
+    rc = lib.su2b_slabs_create(L, L, L, Lt, 4, 2.3, 1.0, _abi.PREC_FP64, n, first, count, 0,
                                C.byref(h))
     assert rc == _abi.ERR_INVALID and not h.value
 
