@@ -378,8 +378,9 @@ SU2B_API int su2b_flow_adjoint(su2b_ctx *ctx, double eps, int n_steps, int check
 
 /* ---- launch-shape autotuning ------------------------------------------------------------ */
 /* The SU(2) force kernel has SU2B_FORCE_VARIANTS launch shapes (threads per block x register
- * cap).  su2b_autotune times them all on the context's field (CUDA events, the same memory
- * traffic as a trajectory step, into scratch buffers) and keeps the fastest for this context
+ * cap).  su2b_autotune times them all on the context's field (CUDA events over launches
+ * chained by programmatic dependent launch as in a trajectory, the same memory traffic as a
+ * trajectory step, into scratch buffers) and keeps the fastest for this context
  * (the first shape in index order within 1 % of the fastest: shapes that tie round
  * differently, and this keeps the choice, and so the chain, the same from run to run);
  * with cache_path it first looks the choice up in that text file (unless retune) and writes

@@ -98,15 +98,18 @@ extern "C" int su2b_autotune(su2b_ctx *ctx, const char *cache_path, int retune,
     if (e != cudaSuccess) rc = su2b_fail(ctx, SU2B_ERR_CUDA, "autotune: %s", cudaGetErrorString(e));
   }
   for (int var = 0; var < FORCE_VARIANTS && rc == SU2B_OK; var++) {
+    // chained with programmatic dependent launch, as the trajectory's force launches run:
+    // the shapes differ in how well the next launch's early blocks share the SMs with the
+    // tail of the running one, so timing them unchained can rank them differently
     auto launch = [&]() -> cudaError_t {
       if (var == FORCE_PAIR && pairs)
         return force_pair(ctx->g, ctx->U_old, (float *)ctx->Z, f, -1e-3, mode, nullptr, nullptr,
-                          ctx->U2, 0.0, s, false);
+                          ctx->U2, 0.0, s, true);
       if (ctx->link64)
         return force_update<double>(ctx->g, ctx->U, 0, (double *)ctx->Z, nullptr, f, -1e-3,
-                                    ctx->xi, mode, nullptr, nullptr, ctx->U2, 0.0, s, var);
+                                    ctx->xi, mode, nullptr, nullptr, ctx->U2, 0.0, s, var, true);
       return force_update<float>(ctx->g, ctx->U, 0, (float *)ctx->Z, nullptr, f, -1e-3, ctx->xi,
-                                 mode, nullptr, nullptr, ctx->U2, 0.0, s, var);
+                                 mode, nullptr, nullptr, ctx->U2, 0.0, s, var, true);
     };
     cudaError_t e = cudaSuccess;
     for (int k = 0; k < 2 && e == cudaSuccess; k++) e = launch();
