@@ -962,13 +962,21 @@ extern "C" int su2b_slabs_autotune(su2b_slabs *h, double *times_us) {
                 "the handle holds a part of the slabs: connect it to the others first");
   double t[FORCE_VARIANTS] = {};
   const int rc = su2b_autotune(h->sl[0], nullptr, 1, t);
-  if (rc != SU2B_OK) return from_ctx(h, rc);
+  if (rc != SU2B_OK && !h->comm) return from_ctx(h, rc);
   if (h->comm) {
+    // a rank whose timing failed still joins the all-reduce, with a time that marks the
+    // failure on every rank, so that no rank is left waiting in the collective
+    constexpr double FAILED = 1e300;
+    if (rc != SU2B_OK)
+      for (double &x : t) x = FAILED;
     SLAB_CUDA(cudaMemcpyAsync(h->tune_dev, t, sizeof t, cudaMemcpyHostToDevice, h->s));
     NCCL_CK(h->nc->all_reduce(h->tune_dev, h->tune_dev, FORCE_VARIANTS, ncclFloat64, ncclMax,
                               h->comm, h->s));
     SLAB_CUDA(cudaMemcpyAsync(t, h->tune_dev, sizeof t, cudaMemcpyDeviceToHost, h->s));
     SLAB_CUDA(cudaStreamSynchronize(h->s));
+    if (rc != SU2B_OK) return from_ctx(h, rc);
+    if (t[0] >= FAILED)
+      return fail(h, SU2B_ERR_CUDA, "the launch-shape timing failed on another rank");
     double fastest = t[0];
     for (int v = 1; v < FORCE_VARIANTS; v++) fastest = t[v] < fastest ? t[v] : fastest;
     int best = 0;
