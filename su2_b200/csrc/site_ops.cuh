@@ -122,6 +122,10 @@ __device__ __forceinline__ double force_site_impl(const Geom &g, const LinkT<T> 
 // threads share a site, so each holds two staple sums instead of four and needs about half
 // the registers; the forward product A of the plane inside the half serves both of its links,
 // the four planes that cross the halves compute A in both threads (64 FMAs more per site).
+// The backward staples come first, and both loops run over the direction nu outside the two
+// links, so U_nu(x-nu) and U_nu(x) are each loaded once for both: in FP32 this order runs
+// about 3 % faster than the links outside with the forward staples first (the loads the
+// diagonal backward staples wait on longest are issued earliest).
 template <class T, int HALF, bool ANISO>
 __device__ __forceinline__ double force_half_impl(const Geom &g, const LinkT<T> *__restrict__ U,
                                                   T *__restrict__ P,
@@ -154,10 +158,26 @@ __device__ __forceinline__ double force_half_impl(const Geom &g, const LinkT<T> 
   constexpr int m0 = 2 * HALF, m1 = 2 * HALF + 1;
   Su2<T> K[2] = {zero_su2<T>(), zero_su2<T>()};
 #pragma unroll
-  for (int j = 0; j < 2; j++) {
-    const int mu = m0 + j;
+  for (int nu = 0; nu < 4; nu++) {
+    const Su2<T> c = L(nu, -E(nu, 0), -E(nu, 1), -E(nu, 2), -E(nu, 3));  // U_nu(x-nu)
 #pragma unroll
-    for (int nu = 0; nu < 4; nu++) {
+    for (int j = 0; j < 2; j++) {
+      const int mu = m0 + j;
+      if (nu == mu) continue;
+      const Su2<T> e = L(nu, E(mu, 0) - E(nu, 0), E(mu, 1) - E(nu, 1), E(mu, 2) - E(nu, 2),
+                         E(mu, 3) - E(nu, 3));                           // U_nu(x+mu-nu)
+      const Su2<T> h = L(mu, -E(nu, 0), -E(nu, 1), -E(nu, 2), -E(nu, 3));  // U_mu(x-nu)
+      Su2<T> eh = mul(dag(e), dag(h));
+      if (ANISO) eh = scale((mu == 0 || nu == 0) ? wt : ws, eh);
+      K[j] = mul_acc(K[j], eh, c);
+    }
+  }
+#pragma unroll
+  for (int nu = 0; nu < 4; nu++) {
+    const Su2<T> cn = L(nu, 0, 0, 0, 0);  // U_nu(x)
+#pragma unroll
+    for (int j = 0; j < 2; j++) {
+      const int mu = m0 + j;
       if (nu == mu) continue;
       const bool both = (nu == m0 || nu == m1);
       if (both && nu < mu) continue;
@@ -165,23 +185,8 @@ __device__ __forceinline__ double force_half_impl(const Geom &g, const LinkT<T> 
       const Su2<T> b = L(mu, E(nu, 0), E(nu, 1), E(nu, 2), E(nu, 3));  // U_mu(x+nu)
       Su2<T> A = mul(a, dag(b));
       if (ANISO) A = scale((mu == 0 || nu == 0) ? wt : ws, A);
-      K[j] = mul_acc(K[j], A, dag(L(nu, 0, 0, 0, 0)));
+      K[j] = mul_acc(K[j], A, dag(cn));
       if (both) K[nu - m0] = mul_acc(K[nu - m0], dag(A), dag(L(mu, 0, 0, 0, 0)));
-    }
-  }
-#pragma unroll
-  for (int j = 0; j < 2; j++) {
-    const int mu = m0 + j;
-#pragma unroll
-    for (int nu = 0; nu < 4; nu++) {
-      if (nu == mu) continue;
-      const Su2<T> e = L(nu, E(mu, 0) - E(nu, 0), E(mu, 1) - E(nu, 1), E(mu, 2) - E(nu, 2),
-                         E(mu, 3) - E(nu, 3));                           // U_nu(x+mu-nu)
-      const Su2<T> h = L(mu, -E(nu, 0), -E(nu, 1), -E(nu, 2), -E(nu, 3));  // U_mu(x-nu)
-      const Su2<T> c = L(nu, -E(nu, 0), -E(nu, 1), -E(nu, 2), -E(nu, 3));  // U_nu(x-nu)
-      Su2<T> eh = mul(dag(e), dag(h));
-      if (ANISO) eh = scale((mu == 0 || nu == 0) ? wt : ws, eh);
-      K[j] = mul_acc(K[j], eh, c);
     }
   }
   const size_t self = (size_t)p * g.Vh + cb;
