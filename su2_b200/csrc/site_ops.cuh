@@ -8,6 +8,15 @@ namespace su2b {
 
 template <class T> using LinkT = typename LinkOf<T>::type;
 
+// Prefetch into L1 of the momentum components of link l (SoA, NL apart): the force step
+// reads them only at its end, where every thread then waits on them; requested at the start
+// the lines arrive while the staples are summed (about 4 % of the launch at 32^4)
+template <class T>
+__device__ __forceinline__ void prefetch_momenta(const T *P, size_t l, size_t NL) {
+#pragma unroll
+  for (int k = 0; k < 3; k++) asm volatile("prefetch.global.L1 [%0];" ::"l"(P + k * NL + l));
+}
+
 // Fused gauge force + momentum update for all ND links of a site
 // (flat-gaugemonomial.hh:105-131 + update_momenta.hh:10-33):
 //   K_mu = sum_{nu != mu} U_nu(x+mu) U_mu(x+nu)^+ U_nu(x)^+ + U_nu(x+mu-nu)^+ U_mu(x-nu)^+ U_nu(x-nu)
@@ -78,6 +87,10 @@ __device__ __forceinline__ double force_site_impl(const Geom &g, const LinkT<T> 
     lb[mu] = bwd(g, s, mu);
   }
   Su2<T> ux[ND], K[ND];
+  if (mode & FM_HAS_IN) {
+#pragma unroll
+    for (int mu = 0; mu < ND; mu++) prefetch_momenta(P, mu * V + self, NL);
+  }
 #pragma unroll
   for (int mu = 0; mu < ND; mu++) {
     ux[mu] = ld_link(U + mu * V + self);
@@ -160,6 +173,11 @@ __device__ __forceinline__ double force_half_impl(const Geom &g, const LinkT<T> 
   };
   auto E = [](int d, int k) { return d == k ? 1 : 0; };
   constexpr int m0 = 2 * HALF, m1 = 2 * HALF + 1;
+  const size_t self = (size_t)p * g.Vh + cb;
+  if (mode & FM_HAS_IN) {
+    prefetch_momenta(P, m0 * V + self, NL);
+    prefetch_momenta(P, m1 * V + self, NL);
+  }
   Su2<T> K[2] = {zero_su2<T>(), zero_su2<T>()};
 #pragma unroll
   for (int nu = 0; nu < 4; nu++) {
@@ -193,7 +211,6 @@ __device__ __forceinline__ double force_half_impl(const Geom &g, const LinkT<T> 
       if (both) K[nu - m0] = mul_acc(K[nu - m0], dag(A), dag(L(mu, 0, 0, 0, 0)));
     }
   }
-  const size_t self = (size_t)p * g.Vh + cb;
   double k2 = 0.;
 #pragma unroll
   for (int j = 0; j < 2; j++)
