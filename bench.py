@@ -526,6 +526,7 @@ def ours(args):
             "between_trajectories_fp64": obs,
             # the long forms of the headline line's entries
             "headline_notes": {
+                "data": "synthetic: seeded Haar-random start, Metropolis-thermalised on device",
                 "config": {"workload": WORKLOAD + " (mixed precision)", "lattice": [L] * 4,
                            "replicas": ws,
                            "l2": "working set (three link buffers, P) > 126 MB L2; no flush"},
@@ -552,7 +553,7 @@ def ours(args):
             "warmup": W, "ms_per_step": r3(1e3 * t_mixed / K), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None,
             "dtype": "fp32 links + fp64 sums/accept",
-            "data": "synthetic, seeded, thermalised on device",
+            "data": "synthetic, seeded",
             "config": {"workload": "SU(2) 32^4 beta 2.4 omf2 tau 1 n 16, mixed",
                        "parallelism": f"replicas x{ws}", "l2": "working set > L2, no flush"},
             "fp64": r3(ws * K / t_fp64), "plain_fp64": r3(ws * K / t_plain),
